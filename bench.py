@@ -1,0 +1,459 @@
+#!/usr/bin/env python
+"""Benchmark of the all-vs-all scoring path on B200 (one JSON line on rank 0).
+
+Default workload (the one the headline metric is quoted on): gap-block ``score_matrix``,
+1,000 query x 10,000 reference CDR3-like junctions ('CASS' + uniform middle + 'F', length
+uniform 10-20; numpy PCG64 seed 1 for queries, seed 0 for refs), BLOSUM62 penalties,
+gap_open 8, gap_extend 1, central_prior(21); int32 output bit-identical to seqtree's C++.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload gapblock|hamming|
+                    levenshtein|nw|sw] [--impl ours|reference]
+
+* ``value``: pairs/s with inputs resident in HBM (device sets) and the result written to HBM,
+  device-timed with CUDA events on the launching stream; the L2 is flushed (a 256 MiB write)
+  between timed steps.  N > 1 (torchrun): every rank scores its own query block (weak scaling,
+  no data-path collective); value = all ranks' pairs / max over ranks of the device time.
+* ``e2e``: the same metric through the public API (``seqtree_b200.gapblock.score_matrix`` on
+  Python lists): packing, host->device copy, kernels and the device->host copy of the result.
+* ``cpu_baseline``: the reference's own C++ (``oracle/_ref``) on the host cores, rank 0, N=1.
+* ``--impl reference``: times that CPU implementation alone, on this workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+AA20 = "ACDEFGHIKLMNPQRSTVWY"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ----------------------------------------------------------------------------- workloads ----
+def cdr3(seed: int, n: int, lo: int = 10, hi: int = 20) -> list[str]:
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(lo, hi + 1, size=n)
+    mid = rng.integers(0, 20, size=int((lens - 5).sum()))
+    letters = np.array(list(AA20))[mid]
+    out, p = [], 0
+    for L in lens:
+        k = int(L) - 5
+        out.append("CASS" + "".join(letters[p:p + k]) + "F")
+        p += k
+    return out
+
+
+def uniform_strings(seed: int, n: int, lo: int, hi: int, alphabet: str) -> list[str]:
+    rng = np.random.default_rng(seed)
+    lens = rng.integers(lo, hi + 1, size=n)
+    codes = rng.integers(0, len(alphabet), size=int(lens.sum()))
+    letters = np.array(list(alphabet))[codes]
+    out, p = [], 0
+    for L in lens:
+        out.append("".join(letters[p:p + int(L)]))
+        p += int(L)
+    return out
+
+
+# Background amino-acid frequencies (Robinson & Robinson 1991), order ACDEFGHIKLMNPQRSTVWY.
+BG_FREQ = np.array([7.805, 1.925, 5.364, 6.295, 3.856, 7.377, 2.199, 5.142, 5.744, 9.019, 2.243,
+                    4.487, 5.203, 4.264, 5.129, 7.120, 5.841, 6.441, 1.330, 3.216])
+
+
+def proteins(seed: int, n: int) -> list[str]:
+    """Residues i.i.d. from background frequencies; length log-normal, median 180, sigma 0.5,
+    clipped to 50-500."""
+    rng = np.random.default_rng(seed)
+    lens = np.clip(np.round(rng.lognormal(np.log(180), 0.5, size=n)), 50, 500).astype(int)
+    p = BG_FREQ / BG_FREQ.sum()
+    codes = rng.choice(20, size=int(lens.sum()), p=p)
+    letters = np.array(list(AA20))[codes]
+    out, o = [], 0
+    for L in lens:
+        out.append("".join(letters[o:o + int(L)]))
+        o += int(L)
+    return out
+
+
+def make_workload(name: str, rank: int):
+    """Returns dict(queries, refs, kind, params, metric, cells_fn)."""
+    qseed = 1 + 1000 * rank  # rank 0 scores exactly the named workload
+    if name == "gapblock":
+        return dict(kind="gapblock", queries=cdr3(qseed, 1000), refs=cdr3(0, 10000),
+                    config={"workload": "gapblock score_matrix 1000x10000 CDR3 junctions (len 10-20), "
+                                        "BLOSUM62, gap_open 8, gap_extend 1, central_prior(21)",
+                            "queries": 1000, "refs": 10000, "matrix": "BLOSUM62",
+                            "gap_open": 8, "gap_extend": 1, "prior": "central_prior(21)"},
+                    metric="gapblock score_matrix pairs/s")
+    if name == "hamming":
+        return dict(kind="hamming", queries=uniform_strings(qseed, 20000, 12, 12, "ACGT"),
+                    refs=uniform_strings(0, 20000, 12, 12, "ACGT"),
+                    config={"workload": "hamming_matrix 20000x20000 ACGT L=12", "queries": 20000,
+                            "refs": 20000}, metric="hamming_matrix pairs/s")
+    if name == "levenshtein":
+        return dict(kind="levenshtein", queries=uniform_strings(qseed, 20000, 30, 60, "ACGT"),
+                    refs=uniform_strings(0, 20000, 30, 60, "ACGT"),
+                    config={"workload": "levenshtein_matrix 20000x20000 ACGT len 30-60",
+                            "queries": 20000, "refs": 20000}, metric="levenshtein_matrix pairs/s")
+    if name in ("nw", "sw"):
+        mode = "global" if name == "nw" else "local"
+        return dict(kind="align", mode=mode, queries=proteins(qseed, 4096), refs=proteins(0, 4096),
+                    config={"workload": f"align_dist_matrix {mode} 4096x4096 proteins (log-normal "
+                                        "median 180, 50-500), BLOSUM62, gap 11/1",
+                            "queries": 4096, "refs": 4096, "mode": mode},
+                    metric=f"align_dist_matrix ({mode}) pairs/s")
+    raise SystemExit(f"unknown workload {name}")
+
+
+def cells_of(w) -> float:
+    """Algorithmic cells: gap block 2*min(m,n) (min(m,n) at d == 0); DP m*n; Hamming L."""
+    lq = np.array([len(s) for s in w["queries"]], dtype=np.float64)
+    lr = np.array([len(s) for s in w["refs"]], dtype=np.float64)
+    if w["kind"] == "gapblock":
+        vq, cq = np.unique(lq, return_counts=True)
+        vr, cr = np.unique(lr, return_counts=True)
+        L = np.minimum(vq[:, None], vr[None, :])
+        mult = np.where(vq[:, None] == vr[None, :], 1.0, 2.0)
+        return float((cq[:, None] * cr[None, :] * L * mult).sum())
+    if w["kind"] == "hamming":
+        return float(lq.sum() * len(lr)) if len(lr) else 0.0
+    return float(lq.sum() * lr.sum())
+
+
+# ----------------------------------------------------------------------------- helpers ------
+def peaks() -> tuple[float, str]:
+    try:
+        return float(json.loads(PEAKS_FILE.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ----------------------------------------------------------------------------- reference ----
+def cpu_reference_call(w, threads: int):
+    import oracle
+    if w["kind"] == "gapblock":
+        from seqtree_b200.gapblock import central_prior, prior_cube
+        width = max(map(len, w["queries"] + w["refs"]))
+        cube = w.setdefault("_cube", prior_cube(central_prior(21), width))
+        if oracle.ref_available():
+            return lambda q: oracle.ref_gapblock_matrix(q, w["refs"], matrix="blosum62",
+                                                        gap_open=8, gap_extend=1, prior=cube,
+                                                        prior_width=width, threads=threads), \
+                "reference"
+        from seqtree_b200.matrix import SubstitutionMatrix
+        pen = SubstitutionMatrix.blosum62().penalty_grid
+        return lambda q: oracle.gapblock_matrix(q, w["refs"], pen, gap_open=8, prior=cube,
+                                                prior_width=width, threads=threads or os.cpu_count()), \
+            "port"
+    if w["kind"] in ("hamming", "levenshtein"):
+        lev = w["kind"] == "levenshtein"
+        if oracle.ref_available():
+            return lambda q: oracle.ref_distance_matrix(q, w["refs"], lev, threads=threads), "reference"
+        fn = oracle.levenshtein_matrix if lev else oracle.hamming_matrix
+        return lambda q: fn(q, w["refs"], threads=threads or os.cpu_count()), "port"
+    if oracle.ref_available():
+        return lambda q: oracle.ref_align_matrix(q, w["refs"], "blosum62", mode=w["mode"],
+                                                 dist=True, threads=threads), "reference"
+    from seqtree_b200.matrix import SubstitutionMatrix
+    sim = SubstitutionMatrix.blosum62().similarity_grid
+    return lambda q: oracle.align_matrix(q, w["refs"], sim, mode=w["mode"], dist=True,
+                                         threads=threads or os.cpu_count()), "port"
+
+
+def cpu_sample_rows(w, budget_s: float, threads: int) -> int:
+    """Query rows such that one timed CPU call takes about budget_s seconds."""
+    call, _ = cpu_reference_call(w, threads)
+    n = min(len(w["queries"]), 8)
+    t = time.perf_counter()
+    call(w["queries"][:n])
+    dt = max(time.perf_counter() - t, 1e-4)
+    rows = int(n * budget_s / dt)
+    return max(1, min(len(w["queries"]), rows))
+
+
+def run_cpu_baseline(w, budget_s=10.0, threads=0, reps=1):
+    call, kind = cpu_reference_call(w, threads)
+    rows = cpu_sample_rows(w, budget_s / max(reps, 1), threads)
+    q = w["queries"][:rows]
+    times = []
+    for _ in range(reps):
+        t = time.perf_counter()
+        call(q)
+        times.append(time.perf_counter() - t)
+    pairs = rows * len(w["refs"])
+    cores = threads if threads > 0 else (os.cpu_count() or 1)
+    return {"value": pairs / statistics.median(times), "unit": "pairs/s", "cores": cores,
+            "kind": kind,
+            "sample": f"{rows} of {len(w['queries'])} query rows x {len(w['refs'])} refs "
+                      f"(rows are independent), median of {reps}"}
+
+
+def main_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    w = make_workload(args.workload, 0)
+    call, kind = cpu_reference_call(w, 0)
+    # Each step is a bounded sample of the workload sized so the whole run stays in minutes.
+    budget = float(os.environ.get("SEQTREE_B200_REF_STEP_S", "5"))
+    rows = cpu_sample_rows(w, budget, 0)
+    q = w["queries"][:rows]
+    for _ in range(args.warmup):
+        call(q)
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        call(q)
+        times.append(time.perf_counter() - t)
+    pairs = rows * len(w["refs"])
+    v = pairs * len(times) / sum(times)
+    cores = os.cpu_count() or 1
+    line = {"impl": "reference", "metric": w["metric"], "value": v, "unit": "pairs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": dict(w["config"], sample_rows=rows),
+            "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cores, "kind": kind,
+                             "sample": f"{rows} of {len(w['queries'])} query rows per step"},
+            "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- ours ---------
+def main_ours(args):
+    import torch
+
+    world, rank, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    import seqtree_b200 as stb
+    from seqtree_b200 import _lib, device
+    from seqtree_b200.gapblock import central_prior, prior_cube
+
+    w = make_workload(args.workload, rank)
+    q, r = w["queries"], w["refs"]
+    N, K = len(q), len(r)
+    stream = torch.cuda.current_stream()
+    out = torch.empty((N, K), dtype=torch.int32, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
+    B62 = stb.SubstitutionMatrix.blosum62()
+
+    if w["kind"] == "gapblock":
+        width = max(map(len, q + r))
+        cube = prior_cube(central_prior(21), width)
+        qs, rs = device.SeqSet(q, "aa"), device.SeqSet(r, "aa")
+
+        def step():
+            device.gapblock_into(qs, rs, out.data_ptr(), stream.cuda_stream, matrix=B62,
+                                 gap_open=8, gap_extend=1, prior=cube, prior_width=width)
+
+        def e2e_call():
+            return stb.gapblock.score_matrix(q, r, B62, gap_open=8, gap_extend=1,
+                                             gap_prior=central_prior(21))
+    elif w["kind"] in ("hamming", "levenshtein"):
+        qs, rs = device.SeqSet(q, None), device.SeqSet(r, None)
+        into = device.hamming_into if w["kind"] == "hamming" else device.levenshtein_into
+        api = stb.distance.hamming_matrix if w["kind"] == "hamming" else stb.distance.levenshtein_matrix
+
+        def step():
+            into(qs, rs, out.data_ptr(), stream.cuda_stream)
+
+        def e2e_call():
+            return api(q, r)
+    else:
+        qs, rs = device.SeqSet(q, "aa"), device.SeqSet(r, "aa")
+
+        def step():
+            device.align_into(qs, rs, out.data_ptr(), stream.cuda_stream, matrix=B62,
+                              mode=w["mode"], gap_open=11, gap_extend=1, dist=True)
+
+        def e2e_call():
+            return stb.pairwise.dist_matrix(q, r, B62, mode=w["mode"])
+
+    # warm-up (plans, workspace, module load)
+    for _ in range(max(args.warmup, 3) if args.warmup >= 3 else args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches = _lib.last_launch_count()
+    kernel_name = _lib.last_kernel_name()
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    sampler = ClockSampler(local)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    with sampler:
+        for i in range(args.steps):
+            flush.zero_()  # evict the previous step's output from L2 (outside the events)
+            ev[i][0].record(stream)
+            step()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = [a.elapsed_time(b) for a, b in ev]
+        # end-to-end through the public API on host lists (pinned result buffer)
+        e2e_times, h2d = [], 0
+        for _ in range(args.e2e_steps):
+            t = time.perf_counter()
+            res = e2e_call()
+            e2e_times.append(time.perf_counter() - t)
+            del res
+    total_ms = sum(ms)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    pairs_rank = N * K
+    value = pairs_rank * world * args.steps / (total_ms / 1e3)
+    e2e_s = statistics.median(e2e_times) if e2e_times else float("nan")
+    in_bytes = sum(len(s) for s in q + r) + 8 * (N + K + 2)
+    e2e = {"value": pairs_rank / e2e_s, "unit": "pairs/s", "h2d_bytes_per_step": in_bytes,
+           "d2h_bytes_per_step": 4 * pairs_rank, "seconds_per_step": e2e_s}
+
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return 0
+
+    hbm, src = peaks()
+    per_launch_s = (total_ms / args.steps) / 1e3
+    out_bytes = 4.0 * pairs_rank
+    in_dev_bytes = float(sum(len(s) for s in q + r))
+    achieved = (out_bytes + in_dev_bytes) / per_launch_s / 1e9
+    cells = cells_of(w)
+    line = {
+        "metric": w["metric"], "value": value, "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded, shapes and distributions of the named workload)",
+        "config": dict(w["config"], l2="flushed between timed steps (256 MiB write)",
+                       parallelism=f"{world} independent query blocks" if world > 1 else "single GPU"),
+        "gcups": cells * world * args.steps / (total_ms / 1e3) / 1e9,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "note": f"algorithmic bytes = 4 B/pair output + input residues; peak {src}; "
+                             "the gap-block kernel is integer-issue bound, see profiles/"},
+        "e2e": e2e,
+        "gpu_launches": launches * args.steps,
+        "kernel": kernel_name,
+        "clocks": sampler.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = run_cpu_baseline(w, budget_s=args.cpu_seconds, threads=0)
+        except Exception as e:  # the checker is absent: report, do not fail the run
+            line["cpu_baseline"] = {"value": None, "error": str(e)}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="gapblock",
+                    choices=["gapblock", "hamming", "levenshtein", "nw", "sw"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        return main_reference(args)
+    return main_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,167 @@
+/*
+ * seqtree_b200 -- C ABI of the B200 (sm_100a) all-vs-all scoring library.
+ *
+ * Drop-in boundary for the dense matrix calls of seqtree 0.6.0.  Every entry point below names
+ * the reference interface it replaces (file:line inside the seqtree project).  Plain pointers
+ * and sizes only: no C++ or torch types cross this boundary, so it binds from ctypes, cffi,
+ * pybind11 or any FFI.
+ *
+ * Conventions shared by every call
+ *   - Sequences cross as one st_strings: all sequences concatenated in `bytes`, with
+ *     `offsets` holding count+1 non-decreasing byte offsets (offsets[0] == 0).
+ *   - Results are dense row-major int32 matrices, row i = queries[i] against every ref,
+ *     exactly the reference's std::vector<int32_t> / ScoreMatrix layout.
+ *   - Each call returns ST_OK (0) or an error code, and fills `err` (may be NULL) with the
+ *     code and the message the reference would raise: ST_EINVAL <-> std::invalid_argument
+ *     (Python ValueError), ST_EOVERFLOW <-> std::overflow_error (Python OverflowError).
+ *   - `threads` is accepted for signature parity with the reference and ignored: the work
+ *     runs on the current CUDA device.
+ *   - There is no CPU fallback.  Without a usable CUDA device the calls return ST_ENODEV.
+ *   - Calls are thread-safe; calls on the same device are serialised internally.
+ */
+#ifndef SEQTREE_B200_H
+#define SEQTREE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    ST_OK = 0,
+    ST_EINVAL = 1,    /* bad argument (reference: std::invalid_argument)              */
+    ST_EOVERFLOW = 2, /* a result does not fit int32 (reference: std::overflow_error) */
+    ST_ECUDA = 3,     /* CUDA runtime error                                          */
+    ST_ETIMEOUT = 4,  /* a bounded device-side wait gave up                          */
+    ST_ENOMEM = 5,    /* device or pinned host allocation failed                     */
+    ST_ENODEV = 6     /* no usable CUDA device                                        */
+};
+
+/* Alphabet codes: the reference's enum class Alphabet (include/seqtree/types.hpp:9). */
+enum { ST_ALPHABET_AA = 0, ST_ALPHABET_NT = 1, ST_ALPHABET_IUPAC = 2 };
+
+/* Alignment modes: the reference's enum class AlignMode (include/seqtree/seqtree.hpp:182). */
+enum { ST_MODE_GLOBAL = 0, ST_MODE_LOCAL = 1 };
+
+typedef struct st_strings {
+    const char *bytes;      /* concatenated sequences (may be NULL when offsets[count]==0) */
+    const int64_t *offsets; /* count + 1 entries                                          */
+    int64_t count;
+} st_strings;
+
+typedef struct st_error {
+    int32_t code;
+    char message[256];
+} st_error;
+
+/* Library version, encoded as major*10000 + minor*100 + patch. */
+int32_t st_version(void);
+
+/* Number of visible CUDA devices (0 when none). */
+int32_t st_device_count(void);
+
+/*
+ * Dense single-gap-block penalty matrix.
+ * Replaces seqtree::gapblock_matrix (include/seqtree/seqtree.hpp:218-222,
+ * src/gapblock.cpp:66-133) and its binding _core.gapblock_matrix (src/_bindings.cpp:218-233,
+ * 570-576).
+ *   penalty      A*A row-major penalty grid (SubstitutionMatrix::penalty, seqtree.hpp:60), or
+ *                NULL for unit cost (the reference's null matrix).
+ *   matrix_size  A of `penalty` (checked against the alphabet like the reference); ignored
+ *                when `penalty` is NULL.
+ *   prior        the [m][d][i] gap-prior cube of (prior_width+1)^3 entries, or NULL /
+ *                prior_len == 0 for no prior.
+ *   out          N*K int32, host memory (pinned or pageable).
+ */
+int32_t st_gapblock_matrix(const st_strings *queries, const st_strings *refs, int32_t alphabet,
+                           const int32_t *penalty, int32_t matrix_size, int32_t gap_open,
+                           int32_t gap_extend, const int32_t *prior, int64_t prior_len,
+                           uint32_t prior_width, int32_t threads, int32_t *out, st_error *err);
+
+/*
+ * Dense Gotoh Needleman-Wunsch / Smith-Waterman similarity matrix.
+ * Replaces seqtree::align_score_matrix (include/seqtree/seqtree.hpp:198-201,
+ * src/pairwise.cpp:338-344) and _core.align_score_matrix (src/_bindings.cpp:527-546).
+ *   similarity   A*A row-major similarity grid (SubstitutionMatrix::similarity, seqtree.hpp:61).
+ *   mode         ST_MODE_GLOBAL or ST_MODE_LOCAL.
+ */
+int32_t st_align_score_matrix(const st_strings *queries, const st_strings *refs,
+                              const int32_t *similarity, int32_t matrix_size, int32_t alphabet,
+                              int32_t mode, int32_t gap_open, int32_t gap_extend,
+                              int32_t threads, int32_t *out, st_error *err);
+
+/*
+ * Dense sequence-level Gram distance d = s(a,a) + s(b,b) - 2 s(a,b) over Gotoh scores.
+ * Replaces seqtree::align_dist_matrix (include/seqtree/seqtree.hpp:206-209,
+ * src/pairwise.cpp:346-352) and _core.align_dist_matrix (src/_bindings.cpp:548-568).
+ */
+int32_t st_align_dist_matrix(const st_strings *queries, const st_strings *refs,
+                             const int32_t *similarity, int32_t matrix_size, int32_t alphabet,
+                             int32_t mode, int32_t gap_open, int32_t gap_extend,
+                             int32_t threads, int32_t *out, st_error *err);
+
+/*
+ * Dense Hamming matrix over raw bytes, case-sensitive.
+ * Replaces seqtree::hamming_matrix (include/seqtree/seqtree.hpp:237-238,
+ * src/distance.cpp:97-102) and _core.hamming_matrix (src/_bindings.cpp:586-600).
+ * Fails with ST_EINVAL when any (a[i], b[k]) pair differs in length.
+ */
+int32_t st_hamming_matrix(const st_strings *a, const st_strings *b, int32_t threads,
+                          int32_t *out, st_error *err);
+
+/*
+ * Dense Levenshtein (unit-cost edit distance) matrix over raw bytes, case-sensitive.
+ * Replaces seqtree::levenshtein_matrix (include/seqtree/seqtree.hpp:239-240,
+ * src/distance.cpp:104-109) and _core.levenshtein_matrix (src/_bindings.cpp:602-615).
+ */
+int32_t st_levenshtein_matrix(const st_strings *a, const st_strings *b, int32_t threads,
+                              int32_t *out, st_error *err);
+
+/* ------------------------------------------------------------------------------------------
+ * Device-resident form.  For callers whose sequences stay on the GPU across many calls (and
+ * for measuring the kernels alone): a sequence set is uploaded and encoded once, and the
+ * *_sets calls write into DEVICE memory on the given stream without any host round trip.
+ * These have no single reference counterpart; they are the same computations as the calls
+ * above, split at the host/device boundary.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct st_seqset_s *st_seqset;
+
+/* Upload and encode a set.  alphabet = ST_ALPHABET_* for gap-block / alignment use, or -1 to
+ * keep raw bytes (Hamming / Levenshtein).  Invalid symbols fail with the reference message. */
+int32_t st_seqset_create(const st_strings *seqs, int32_t alphabet, st_seqset *out,
+                         st_error *err);
+void st_seqset_destroy(st_seqset set);
+int64_t st_seqset_count(st_seqset set);
+
+int32_t st_gapblock_matrix_sets(st_seqset queries, st_seqset refs, const int32_t *penalty,
+                                int32_t matrix_size, int32_t gap_open, int32_t gap_extend,
+                                const int32_t *prior, int64_t prior_len, uint32_t prior_width,
+                                int32_t *out_device, void *cuda_stream, st_error *err);
+
+int32_t st_align_matrix_sets(st_seqset queries, st_seqset refs, const int32_t *similarity,
+                             int32_t matrix_size, int32_t mode, int32_t gap_open,
+                             int32_t gap_extend, int32_t dist, int32_t *out_device,
+                             void *cuda_stream, st_error *err);
+
+int32_t st_hamming_matrix_sets(st_seqset a, st_seqset b, int32_t *out_device, void *cuda_stream,
+                               st_error *err);
+
+int32_t st_levenshtein_matrix_sets(st_seqset a, st_seqset b, int32_t *out_device,
+                                   void *cuda_stream, st_error *err);
+
+/* Launch statistics of the last *_sets / host call on this thread: how many kernels of this
+ * library it launched and the name of the main kernel variant it chose. */
+int32_t st_last_launch_count(void);
+const char *st_last_kernel_name(void);
+
+/* Pinned host buffers from a per-device cache.  A result written into one of these travels
+ * device->host at full PCIe rate.  st_host_free returns the block to the cache. */
+void *st_host_alloc(uint64_t bytes);
+void st_host_free(void *ptr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SEQTREE_B200_H */

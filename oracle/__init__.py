@@ -1,0 +1,302 @@
+"""CPU checkers for the all-vs-all scoring path -- TEST INFRASTRUCTURE ONLY.
+
+Two checkers live here, both loaded with ctypes:
+
+* ``port``: ``oracle/oracle.c``, a plain-C restatement of the reference arithmetic
+  (seqtree 0.6.0 ``src/gapblock.cpp:39-62``, ``src/pairwise.cpp:76-125``,
+  ``src/distance.cpp:68-95``), built into ``oracle/liboracle.so``.
+* ``ref``: the reference's own hot-path C++ sources compiled here by ``oracle/Makefile`` into
+  ``oracle/_ref/libseqtree_ref.so`` (present wherever the build ran; the file travels with
+  the repository snapshot).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may import this
+package, and only as the checker or the timed CPU baseline -- never on the product path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+PORT_SO = HERE / "liboracle.so"
+REF_SO = HERE / "_ref" / "libseqtree_ref.so"
+
+ALPHABETS = {"aa": 0, "nt": 1, "iupac": 2}
+MATRIX_IDS = {"blosum62": 0, "blosum45": 1, "blosum80": 2, "pam250": 3, "pam100": 4,
+              "structural": 5, "unit": 6, "custom": 7}
+
+_i64p = ctypes.POINTER(ctypes.c_int64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+
+
+def build() -> None:
+    """Compile both checkers (the reference one only where its source tree exists)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def pack(strings) -> tuple[np.ndarray, np.ndarray]:
+    """list[str] -> (uint8 bytes, int64 offsets of len+1)."""
+    bs = [s.encode("latin-1") if isinstance(s, str) else bytes(s) for s in strings]
+    lens = np.fromiter((len(b) for b in bs), dtype=np.int64, count=len(bs))
+    off = np.zeros(len(bs) + 1, dtype=np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = np.frombuffer(b"".join(bs), dtype=np.uint8) if bs else np.zeros(0, np.uint8)
+    if data.size == 0:
+        data = np.zeros(1, np.uint8)
+    return np.ascontiguousarray(data), off
+
+
+def _p(a, t):
+    return a.ctypes.data_as(t)
+
+
+class OracleError(Exception):
+    def __init__(self, code: int, msg: str):
+        super().__init__(msg)
+        self.code = code
+
+
+# ----------------------------------------------------------------------------- port ---------
+_port = None
+
+
+def port():
+    global _port
+    if _port is None:
+        if not PORT_SO.exists():
+            build()
+        lib = ctypes.CDLL(str(PORT_SO))
+        lib.or_alphabet_size.restype = ctypes.c_int
+        lib.or_encode.restype = ctypes.c_int64
+        lib.or_encode.argtypes = [ctypes.c_int, _u8p, ctypes.c_int64, _u8p]
+        lib.or_penalty_from_similarity.argtypes = [ctypes.c_int, _i32p, _i32p]
+        lib.or_gapblock_matrix.argtypes = [_u8p, _i64p, ctypes.c_int64, _u8p, _i64p,
+                                           ctypes.c_int64, _i32p, ctypes.c_int, ctypes.c_int32,
+                                           ctypes.c_int32, _i32p, ctypes.c_uint32, _i32p,
+                                           ctypes.c_int]
+        lib.or_align_matrix.argtypes = [_u8p, _i64p, ctypes.c_int64, _u8p, _i64p, ctypes.c_int64,
+                                        _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_int, _i32p, ctypes.c_int]
+        for f in (lib.or_hamming_matrix, lib.or_levenshtein_matrix):
+            f.argtypes = [_u8p, _i64p, ctypes.c_int64, _u8p, _i64p, ctypes.c_int64, _i32p,
+                          ctypes.c_int]
+        _port = lib
+    return _port
+
+
+def encode(strings, alphabet: str = "aa"):
+    """Encode with the reference codec; raises ValueError naming the first bad symbol."""
+    data, off = pack(strings)
+    codes = np.zeros_like(data)
+    n = int(off[-1])
+    bad = port().or_encode(ALPHABETS[alphabet], _p(data, _u8p), n, _p(codes, _u8p))
+    if bad >= 0:
+        raise ValueError(f"symbol '{chr(data[bad])}' is not in the alphabet")
+    return codes, off
+
+
+def penalty_from_similarity(sim: np.ndarray | None, size: int) -> np.ndarray:
+    pen = np.zeros(size * size, np.int32)
+    s = None if sim is None else np.ascontiguousarray(sim, np.int32).ravel()
+    port().or_penalty_from_similarity(size, None if s is None else _p(s, _i32p), _p(pen, _i32p))
+    return pen.reshape(size, size)
+
+
+def gapblock_matrix(queries, refs, pen, alphabet="aa", gap_open=1, gap_extend=1, prior=None,
+                    prior_width=0, threads=os.cpu_count() or 1) -> np.ndarray:
+    """Port of gapblock_matrix; `pen` is an A*A penalty grid."""
+    qc, qo = encode(queries, alphabet)
+    rc, ro = encode(refs, alphabet)
+    N, K = len(queries), len(refs)
+    out = np.zeros((N, K), np.int32)
+    pen = np.ascontiguousarray(pen, np.int32).ravel()
+    A = int(round(pen.size ** 0.5))
+    pr = None if prior is None or len(prior) == 0 else np.ascontiguousarray(prior, np.int32)
+    port().or_gapblock_matrix(_p(qc, _u8p), _p(qo, _i64p), N, _p(rc, _u8p), _p(ro, _i64p), K,
+                              _p(pen, _i32p), A, gap_open, gap_extend,
+                              None if pr is None else _p(pr, _i32p), prior_width,
+                              _p(out, _i32p), threads)
+    return out
+
+
+def align_matrix(queries, refs, sim, alphabet="aa", mode="global", gap_open=11, gap_extend=1,
+                 dist=False, threads=os.cpu_count() or 1) -> np.ndarray:
+    """Port of align_score_matrix / align_dist_matrix; `sim` is an A*A similarity grid."""
+    qc, qo = encode(queries, alphabet)
+    rc, ro = encode(refs, alphabet)
+    N, K = len(queries), len(refs)
+    out = np.zeros((N, K), np.int32)
+    sim = np.ascontiguousarray(sim, np.int32).ravel()
+    A = int(round(sim.size ** 0.5))
+    st = port().or_align_matrix(_p(qc, _u8p), _p(qo, _i64p), N, _p(rc, _u8p), _p(ro, _i64p), K,
+                                _p(sim, _i32p), A, int(mode == "local"), gap_open, gap_extend,
+                                int(dist), _p(out, _i32p), threads)
+    if st == 2:
+        raise OverflowError("the alignment %s does not fit in 32 bits" %
+                            ("distance" if dist else "score"))
+    return out
+
+
+def hamming_matrix(a, b, threads=os.cpu_count() or 1) -> np.ndarray:
+    ad, ao = pack(a)
+    bd, bo = pack(b)
+    la, lb = np.diff(ao), np.diff(bo)
+    if len(a) and len(b) and (np.any(la != la[0]) or np.any(lb != la[0])):
+        raise ValueError("hamming distance is only defined for equal-length sequences")
+    out = np.zeros((len(a), len(b)), np.int32)
+    port().or_hamming_matrix(_p(ad, _u8p), _p(ao, _i64p), len(a), _p(bd, _u8p), _p(bo, _i64p),
+                             len(b), _p(out, _i32p), threads)
+    return out
+
+
+def levenshtein_matrix(a, b, threads=os.cpu_count() or 1) -> np.ndarray:
+    ad, ao = pack(a)
+    bd, bo = pack(b)
+    out = np.zeros((len(a), len(b)), np.int32)
+    port().or_levenshtein_matrix(_p(ad, _u8p), _p(ao, _i64p), len(a), _p(bd, _u8p),
+                                 _p(bo, _i64p), len(b), _p(out, _i32p), threads)
+    return out
+
+
+# ----------------------------------------------------------------------------- ref ----------
+_ref = None
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def ref():
+    """The reference's own C++ (oracle/_ref). Raises FileNotFoundError when it was not built."""
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            raise FileNotFoundError(str(REF_SO))
+        lib = ctypes.CDLL(str(REF_SO))
+        lib.ref_matrix_tables.argtypes = [ctypes.c_int, _i32p, ctypes.c_int, _i32p, _i32p,
+                                          ctypes.POINTER(ctypes.c_int), _i32p]
+        lib.ref_gapblock_matrix.argtypes = [
+            ctypes.c_char_p, _i64p, ctypes.c_int64, ctypes.c_char_p, _i64p, ctypes.c_int64,
+            ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
+            _i32p, ctypes.c_int64, ctypes.c_uint32, ctypes.c_int, _i32p, ctypes.c_char_p,
+            ctypes.c_int]
+        lib.ref_align_matrix.argtypes = [
+            ctypes.c_char_p, _i64p, ctypes.c_int64, ctypes.c_char_p, _i64p, ctypes.c_int64,
+            ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int32,
+            ctypes.c_int32, ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_char_p, ctypes.c_int]
+        lib.ref_align_score.argtypes = [
+            ctypes.c_char_p, ctypes.c_int64, ctypes.c_char_p, ctypes.c_int64, ctypes.c_int,
+            ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
+            _i32p, ctypes.c_char_p, ctypes.c_int]
+        lib.ref_distance_matrix.argtypes = [
+            ctypes.c_char_p, _i64p, ctypes.c_int64, ctypes.c_char_p, _i64p, ctypes.c_int64,
+            ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_char_p, ctypes.c_int]
+        _ref = lib
+    return _ref
+
+
+def _raise(code: int, err) -> None:
+    msg = err.value.decode(errors="replace")
+    if code == 1:
+        raise ValueError(msg)
+    if code == 2:
+        raise OverflowError(msg)
+    raise RuntimeError(msg)
+
+
+def _matrix_args(matrix, size=0):
+    """matrix: a name from MATRIX_IDS, ('unit', size), ('custom', sim grid) or None."""
+    if matrix is None:
+        return -1, None, 0, None
+    if isinstance(matrix, str):
+        return MATRIX_IDS[matrix.lower()], None, size, None
+    kind, payload = matrix
+    if kind == "unit":
+        return MATRIX_IDS["unit"], None, int(payload), None
+    sim = np.ascontiguousarray(payload, np.int32)
+    return MATRIX_IDS["custom"], _p(sim, _i32p), sim.shape[0], sim
+
+
+def ref_tables(matrix) -> tuple[np.ndarray, np.ndarray, int]:
+    """(similarity, penalty, scale) of a reference matrix."""
+    mid, simp, size, _keep = _matrix_args(matrix)
+    sim = np.zeros(32 * 32, np.int32)
+    pen = np.zeros(32 * 32, np.int32)
+    A = ctypes.c_int(0)
+    scale = ctypes.c_int32(0)
+    st = ref().ref_matrix_tables(mid, simp, size, _p(sim, _i32p), _p(pen, _i32p),
+                                 ctypes.byref(A), ctypes.byref(scale))
+    if st:
+        raise ValueError("bad matrix")
+    a = A.value
+    return sim[: a * a].reshape(a, a).copy(), pen[: a * a].reshape(a, a).copy(), scale.value
+
+
+def ref_gapblock_matrix(queries, refs, alphabet="aa", matrix=None, gap_open=1, gap_extend=1,
+                        prior=(), prior_width=0, threads=0) -> np.ndarray:
+    qd, qo = pack(queries)
+    rd, ro = pack(refs)
+    mid, simp, size, _keep = _matrix_args(matrix)
+    pr = np.ascontiguousarray(np.asarray(prior, dtype=np.int64).astype(np.int32))
+    if pr.size == 0:
+        pr = np.zeros(1, np.int32)
+        plen = 0
+    else:
+        plen = int(np.asarray(prior).size)
+    out = np.zeros((len(queries), len(refs)), np.int32)
+    err = ctypes.create_string_buffer(512)
+    st = ref().ref_gapblock_matrix(qd.tobytes(), _p(qo, _i64p), len(queries), rd.tobytes(),
+                                   _p(ro, _i64p), len(refs), ALPHABETS[alphabet], mid, simp, size,
+                                   gap_open, gap_extend, _p(pr, _i32p), plen, prior_width,
+                                   threads, _p(out, _i32p), err, 512)
+    if st:
+        _raise(st, err)
+    return out
+
+
+def ref_align_matrix(queries, refs, matrix="blosum62", mode="global", gap_open=11,
+                     gap_extend=1, alphabet="aa", dist=False, threads=0) -> np.ndarray:
+    qd, qo = pack(queries)
+    rd, ro = pack(refs)
+    mid, simp, size, _keep = _matrix_args(matrix)
+    out = np.zeros((len(queries), len(refs)), np.int32)
+    err = ctypes.create_string_buffer(512)
+    st = ref().ref_align_matrix(qd.tobytes(), _p(qo, _i64p), len(queries), rd.tobytes(),
+                                _p(ro, _i64p), len(refs), ALPHABETS[alphabet], mid, simp, size,
+                                int(mode == "local"), gap_open, gap_extend, int(dist), threads,
+                                _p(out, _i32p), err, 512)
+    if st:
+        _raise(st, err)
+    return out
+
+
+def ref_align_score(q, r, matrix="blosum62", mode="global", gap_open=11, gap_extend=1,
+                    alphabet="aa") -> int:
+    mid, simp, size, _keep = _matrix_args(matrix)
+    out = ctypes.c_int32(0)
+    err = ctypes.create_string_buffer(512)
+    qb, rb = q.encode("latin-1"), r.encode("latin-1")
+    st = ref().ref_align_score(qb, len(qb), rb, len(rb), ALPHABETS[alphabet], mid, simp, size,
+                               int(mode == "local"), gap_open, gap_extend, ctypes.byref(out),
+                               err, 512)
+    if st:
+        _raise(st, err)
+    return out.value
+
+
+def ref_distance_matrix(a, b, levenshtein: bool, threads=0) -> np.ndarray:
+    ad, ao = pack(a)
+    bd, bo = pack(b)
+    out = np.zeros((len(a), len(b)), np.int32)
+    err = ctypes.create_string_buffer(512)
+    st = ref().ref_distance_matrix(ad.tobytes(), _p(ao, _i64p), len(a), bd.tobytes(),
+                                   _p(bo, _i64p), len(b), int(levenshtein), threads,
+                                   _p(out, _i32p), err, 512)
+    if st:
+        _raise(st, err)
+    return out

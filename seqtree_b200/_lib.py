@@ -1,0 +1,179 @@
+"""ctypes binding of ``libseqtree_b200.so`` (the C ABI in ``include/seqtree_b200.h``).
+
+The library is the only compute path: importing this module fails loudly when the shared
+library is missing, and every call runs on the current CUDA device (there is no CPU fallback).
+ctypes releases the GIL for the duration of each foreign call, as the reference's binding does
+(seqtree ``src/_bindings.cpp:227,537,558,592,608``).
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libseqtree_b200.so"
+
+ST_OK, ST_EINVAL, ST_EOVERFLOW, ST_ECUDA, ST_ETIMEOUT, ST_ENOMEM, ST_ENODEV = range(7)
+ALPHABET_AA, ALPHABET_NT, ALPHABET_IUPAC = 0, 1, 2
+MODE_GLOBAL, MODE_LOCAL = 0, 1
+
+
+class st_strings(ctypes.Structure):
+    _fields_ = [("bytes", ctypes.c_void_p), ("offsets", ctypes.c_void_p),
+                ("count", ctypes.c_int64)]
+
+
+class st_error(ctypes.Structure):
+    _fields_ = [("code", ctypes.c_int32), ("message", ctypes.c_char * 256)]
+
+
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_sp = ctypes.POINTER(st_strings)
+_ep = ctypes.POINTER(st_error)
+
+# (name, restype, argtypes) of every symbol declared in include/seqtree_b200.h
+SIGNATURES = [
+    ("st_version", ctypes.c_int32, []),
+    ("st_device_count", ctypes.c_int32, []),
+    ("st_gapblock_matrix", ctypes.c_int32,
+     [_sp, _sp, ctypes.c_int32, _i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p,
+      ctypes.c_int64, ctypes.c_uint32, ctypes.c_int32, ctypes.c_void_p, _ep]),
+    ("st_align_score_matrix", ctypes.c_int32,
+     [_sp, _sp, _i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, _ep]),
+    ("st_align_dist_matrix", ctypes.c_int32,
+     [_sp, _sp, _i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, _ep]),
+    ("st_hamming_matrix", ctypes.c_int32, [_sp, _sp, ctypes.c_int32, ctypes.c_void_p, _ep]),
+    ("st_levenshtein_matrix", ctypes.c_int32, [_sp, _sp, ctypes.c_int32, ctypes.c_void_p, _ep]),
+    ("st_seqset_create", ctypes.c_int32,
+     [_sp, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p), _ep]),
+    ("st_seqset_destroy", None, [ctypes.c_void_p]),
+    ("st_seqset_count", ctypes.c_int64, [ctypes.c_void_p]),
+    ("st_gapblock_matrix_sets", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, _i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+      _i32p, ctypes.c_int64, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_align_matrix_sets", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, _i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_hamming_matrix_sets", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_levenshtein_matrix_sets", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_last_launch_count", ctypes.c_int32, []),
+    ("st_last_kernel_name", ctypes.c_char_p, []),
+    ("st_host_alloc", ctypes.c_void_p, [ctypes.c_uint64]),
+    ("st_host_free", None, [ctypes.c_void_p]),
+]
+
+
+def _load() -> ctypes.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"seqtree_b200: the CUDA library {LIB_PATH} is not built; run "
+            "`python -m seqtree_b200.build` (there is no CPU fallback)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    for name, res, args in SIGNATURES:
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def check(code: int, err: st_error) -> None:
+    """Raise the Python exception the reference's binding raises for the same failure."""
+    if code == ST_OK:
+        return
+    msg = err.message.decode("utf-8", "replace")
+    if code == ST_EINVAL:
+        raise ValueError(msg)
+    if code == ST_EOVERFLOW:
+        raise OverflowError(msg)
+    if code == ST_ENOMEM:
+        raise MemoryError(msg)
+    raise RuntimeError(msg)
+
+
+class Packed:
+    """A list of sequences as one byte buffer plus int64 offsets (keeps both alive)."""
+
+    __slots__ = ("data", "offsets", "struct")
+
+    def __init__(self, seqs):
+        seqs = list(seqs)
+        for s in seqs:
+            if not isinstance(s, (str, bytes)):
+                raise TypeError("sequences must be str")
+        joined = "".join(s if isinstance(s, str) else s.decode("latin-1") for s in seqs)
+        data = joined.encode("utf-8")
+        lens = np.fromiter((len(s) for s in seqs), dtype=np.int64, count=len(seqs))
+        if len(data) != int(lens.sum()):  # non-ASCII text: byte lengths differ from len()
+            enc = [s.encode("utf-8") if isinstance(s, str) else s for s in seqs]
+            data = b"".join(enc)
+            lens = np.fromiter((len(b) for b in enc), dtype=np.int64, count=len(enc))
+        off = np.zeros(len(seqs) + 1, dtype=np.int64)
+        np.cumsum(lens, out=off[1:])
+        self.data = np.frombuffer(data + b"\0", dtype=np.uint8)
+        self.offsets = off
+        self.struct = st_strings(self.data.ctypes.data, self.offsets.ctypes.data, len(seqs))
+
+    @property
+    def count(self) -> int:
+        return int(self.struct.count)
+
+    def ref(self):
+        return ctypes.byref(self.struct)
+
+
+class _PinnedOwner:
+    """Returns a pinned block to the library's cache when the last view is gone."""
+
+    __slots__ = ("ptr",)
+
+    def __init__(self, ptr: int):
+        self.ptr = ptr
+
+    def __del__(self):
+        if self.ptr:
+            lib.st_host_free(ctypes.c_void_p(self.ptr))
+            self.ptr = 0
+
+
+def pinned_int32(rows: int, cols: int) -> np.ndarray:
+    """An int32 (rows, cols) array in page-locked host memory from the library's cache.
+
+    Device results copy into it at full PCIe rate.  Falls back to ordinary memory when no
+    pinned block can be had (the copy is then slower, the result identical).
+    """
+    n = rows * cols
+    if n == 0:
+        return np.zeros((rows, cols), np.int32)
+    ptr = lib.st_host_alloc(n * 4)
+    if not ptr:
+        return np.empty((rows, cols), np.int32)
+    buf = (ctypes.c_int32 * n).from_address(ptr)
+    buf._owner = _PinnedOwner(ptr)  # the ctypes array is the numpy base; it owns the block
+    return np.frombuffer(buf, dtype=np.int32, count=n).reshape(rows, cols)
+
+
+def i32_ptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_i32p)
+
+
+def last_launch_count() -> int:
+    return int(lib.st_last_launch_count())
+
+
+def last_kernel_name() -> str:
+    return (lib.st_last_kernel_name() or b"").decode()
+
+
+def device_count() -> int:
+    return int(lib.st_device_count())
+

@@ -1,0 +1,320 @@
+// extern "C" entry points of libseqtree_b200 (declared in include/seqtree_b200.h).
+//
+// Host-buffer calls follow the reference's validation order exactly, so the same bad input
+// fails with the same message: gap costs, alphabet, matrix size, empty shapes (no further
+// checks, as in the reference), symbol encoding (queries before refs), then per-family checks.
+#include <algorithm>
+#include <memory>
+
+#include "common.cuh"
+
+namespace stb {
+void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int32_t matrix_size,
+                   int32_t go, int32_t ge, const int32_t* prior, int64_t prior_len,
+                   uint32_t prior_width, int32_t* out_d, cudaStream_t stream);
+void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int32_t matrix_size,
+                int32_t mode, int32_t go, int32_t ge, int32_t dist, int32_t* out_d,
+                cudaStream_t stream);
+void hamming_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream_t stream);
+void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream_t stream);
+int last_launches();
+const char* last_kernel();
+void* host_alloc(uint64_t bytes);
+void host_free(void* p);
+}  // namespace stb
+
+using namespace stb;
+
+namespace {
+
+template <class F>
+int32_t guard(st_error* err, F&& f) {
+    try {
+        f();
+        if (err) {
+            err->code = ST_OK;
+            err->message[0] = 0;
+        }
+        return ST_OK;
+    } catch (const StError& e) {
+        if (err) {
+            err->code = e.code;
+            std::snprintf(err->message, sizeof err->message, "%s", e.what());
+        }
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        if (err) {
+            err->code = ST_ENOMEM;
+            std::snprintf(err->message, sizeof err->message, "seqtree_b200: out of host memory");
+        }
+        return ST_ENOMEM;
+    } catch (const std::exception& e) {
+        if (err) {
+            err->code = ST_ECUDA;
+            std::snprintf(err->message, sizeof err->message, "%s", e.what());
+        }
+        return ST_ECUDA;
+    }
+}
+
+int64_t count_of(const st_strings* s) { return s ? s->count : 0; }
+
+void check_strings(const st_strings* s) {
+    if (!s) fail(ST_EINVAL, "seqtree_b200: null st_strings");
+    if (s->count < 0) fail(ST_EINVAL, "seqtree_b200: negative sequence count");
+    if (s->count > 0 && !s->offsets) fail(ST_EINVAL, "seqtree_b200: null offsets");
+}
+
+// Transient device sets for one host call: storage borrowed from the context.
+struct Transient {
+    std::unique_ptr<st_seqset_s> q, r;
+};
+
+// Device -> host copy of the N*K result, then the error words written by the kernels.
+void finish(Context& ctx, int32_t* out, int64_t N, int64_t K, int32_t* out_d) {
+    const size_t bytes = size_t(N) * size_t(K) * sizeof(int32_t);
+    STB_CUDA(cudaMemcpyAsync(out, out_d, bytes, cudaMemcpyDeviceToHost, ctx.stream));
+    STB_CUDA(cudaMemcpyAsync(ctx.flags_h + 8, ctx.flags_d + 8, 8 * sizeof(int64_t),
+                             cudaMemcpyDeviceToHost, ctx.stream));
+    STB_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+void check_timeout(Context& ctx) {
+    if (ctx.flags_h[8] != 0)
+        fail(ST_ETIMEOUT, "seqtree_b200: a bounded device-side wait gave up (shared-memory staging)");
+}
+
+void clear_flags(Context& ctx) {
+    STB_CUDA(cudaMemsetAsync(ctx.flags_d + 8, 0, 8 * sizeof(int64_t), ctx.stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t st_version(void) { return 100; }
+
+int32_t st_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int32_t st_last_launch_count(void) { return last_launches(); }
+const char* st_last_kernel_name(void) { return last_kernel(); }
+
+void* st_host_alloc(uint64_t bytes) { return host_alloc(bytes); }
+void st_host_free(void* ptr) { host_free(ptr); }
+
+int32_t st_gapblock_matrix(const st_strings* queries, const st_strings* refs, int32_t alphabet,
+                           const int32_t* penalty, int32_t matrix_size, int32_t gap_open,
+                           int32_t gap_extend, const int32_t* prior, int64_t prior_len,
+                           uint32_t prior_width, int32_t threads, int32_t* out, st_error* err) {
+    (void)threads;
+    return guard(err, [&] {
+        reset_launches();
+        check_strings(queries);
+        check_strings(refs);
+        // src/gapblock.cpp:71-81
+        if (gap_open < 0 || gap_extend < 0) fail(ST_EINVAL, "gap_open and gap_extend must be >= 0");
+        const int A = alphabet_size(alphabet);
+        if (A == 0) fail(ST_EINVAL, "unknown alphabet code " + std::to_string(alphabet));
+        if (penalty && matrix_size != A) fail(ST_EINVAL, "matrix size does not match the alphabet");
+        const int64_t N = count_of(queries), K = count_of(refs);
+        if (N == 0 || K == 0) return;
+        if (!out) fail(ST_EINVAL, "seqtree_b200: null output buffer");
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        clear_flags(ctx);
+        // src/gapblock.cpp:85-94: queries are encoded before refs.
+        Transient t;
+        t.q.reset(make_seqset(queries, alphabet, ctx.stream, nullptr, nullptr, ctx.tq));
+        t.r.reset(make_seqset(refs, alphabet, ctx.stream, nullptr, nullptr, ctx.tr));
+        int32_t* out_d = ctx.out_buf.as<int32_t>(size_t(N) * size_t(K));
+        gapblock_sets(*t.q, *t.r, penalty, matrix_size, gap_open, gap_extend, prior, prior_len,
+                      prior_width, out_d, ctx.stream);
+        finish(ctx, out, N, K, out_d);
+        check_timeout(ctx);
+    });
+}
+
+static int32_t align_common(const st_strings* queries, const st_strings* refs,
+                            const int32_t* similarity, int32_t matrix_size, int32_t alphabet,
+                            int32_t mode, int32_t gap_open, int32_t gap_extend, int32_t dist,
+                            int32_t* out, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_strings(queries);
+        check_strings(refs);
+        // src/pairwise.cpp:62-68 (check), then the empty shortcut (:281-282), then encoding.
+        if (gap_open < 0 || gap_extend < 0)
+            fail(ST_EINVAL, "seqtree: gap_open and gap_extend must be >= 0 (they are magnitudes, "
+                            "and are subtracted)");
+        const int A = alphabet_size(alphabet);
+        if (A == 0) fail(ST_EINVAL, "unknown alphabet code " + std::to_string(alphabet));
+        if (!similarity || matrix_size != A) fail(ST_EINVAL, "matrix size does not match the alphabet");
+        if (mode != ST_MODE_GLOBAL && mode != ST_MODE_LOCAL)
+            fail(ST_EINVAL, "unknown mode (use 'global' or 'local')");
+        const int64_t N = count_of(queries), K = count_of(refs);
+        if (N == 0 || K == 0) return;
+        if (!out) fail(ST_EINVAL, "seqtree_b200: null output buffer");
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        clear_flags(ctx);
+        Transient t;
+        int64_t bad = -1;
+        char bc = 0;
+        t.q.reset(make_seqset(queries, alphabet, ctx.stream, &bad, &bc, ctx.tq));
+        if (bad >= 0) fail(ST_EINVAL, std::string("invalid symbol '") + bc + "' in sequence");
+        t.r.reset(make_seqset(refs, alphabet, ctx.stream, &bad, &bc, ctx.tr));
+        if (bad >= 0) fail(ST_EINVAL, std::string("invalid symbol '") + bc + "' in sequence");
+        int32_t* out_d = ctx.out_buf.as<int32_t>(size_t(N) * size_t(K));
+        align_sets(*t.q, *t.r, similarity, matrix_size, mode, gap_open, gap_extend, dist, out_d,
+                   ctx.stream);
+        finish(ctx, out, N, K, out_d);
+        check_timeout(ctx);
+        if (ctx.flags_h[9] != 0)
+            fail(ST_EOVERFLOW, std::string("seqtree: the alignment ") + (dist ? "distance" : "score") +
+                                   " does not fit in 32 bits -- the gap costs are absurdly large "
+                                   "for these sequences");
+    });
+}
+
+int32_t st_align_score_matrix(const st_strings* queries, const st_strings* refs,
+                              const int32_t* similarity, int32_t matrix_size, int32_t alphabet,
+                              int32_t mode, int32_t gap_open, int32_t gap_extend,
+                              int32_t threads, int32_t* out, st_error* err) {
+    (void)threads;
+    return align_common(queries, refs, similarity, matrix_size, alphabet, mode, gap_open,
+                        gap_extend, 0, out, err);
+}
+
+int32_t st_align_dist_matrix(const st_strings* queries, const st_strings* refs,
+                             const int32_t* similarity, int32_t matrix_size, int32_t alphabet,
+                             int32_t mode, int32_t gap_open, int32_t gap_extend,
+                             int32_t threads, int32_t* out, st_error* err) {
+    (void)threads;
+    return align_common(queries, refs, similarity, matrix_size, alphabet, mode, gap_open,
+                        gap_extend, 1, out, err);
+}
+
+static int32_t distance_common(const st_strings* a, const st_strings* b, bool lev, int32_t* out,
+                               st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_strings(a);
+        check_strings(b);
+        const int64_t N = count_of(a), K = count_of(b);
+        if (N == 0 || K == 0) return;  // src/distance.cpp:34
+        if (!out) fail(ST_EINVAL, "seqtree_b200: null output buffer");
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        clear_flags(ctx);
+        Transient t;
+        t.q.reset(make_seqset(a, -1, ctx.stream, nullptr, nullptr, ctx.tq));
+        t.r.reset(make_seqset(b, -1, ctx.stream, nullptr, nullptr, ctx.tr));
+        int32_t* out_d = ctx.out_buf.as<int32_t>(size_t(N) * size_t(K));
+        if (lev)
+            levenshtein_sets(*t.q, *t.r, out_d, ctx.stream);
+        else
+            hamming_sets(*t.q, *t.r, out_d, ctx.stream);
+        finish(ctx, out, N, K, out_d);
+    });
+}
+
+int32_t st_hamming_matrix(const st_strings* a, const st_strings* b, int32_t threads, int32_t* out,
+                          st_error* err) {
+    (void)threads;
+    return distance_common(a, b, false, out, err);
+}
+
+int32_t st_levenshtein_matrix(const st_strings* a, const st_strings* b, int32_t threads,
+                              int32_t* out, st_error* err) {
+    (void)threads;
+    return distance_common(a, b, true, out, err);
+}
+
+// ------------------------------------------------------------------------- device sets ------
+int32_t st_seqset_create(const st_strings* seqs, int32_t alphabet, st_seqset* out, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_strings(seqs);
+        if (!out) fail(ST_EINVAL, "seqtree_b200: null output handle");
+        *out = nullptr;
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        *out = make_seqset(seqs, alphabet, ctx.stream, nullptr, nullptr, nullptr);
+        STB_CUDA(cudaStreamSynchronize(ctx.stream));
+    });
+}
+
+void st_seqset_destroy(st_seqset set) { delete set; }
+
+int64_t st_seqset_count(st_seqset set) { return set ? set->count : -1; }
+
+static void check_set(st_seqset s) {
+    if (!s) fail(ST_EINVAL, "seqtree_b200: null sequence set");
+    int dev = -1;
+    STB_CUDA(cudaGetDevice(&dev));
+    if (dev != s->device) fail(ST_EINVAL, "seqtree_b200: sequence set lives on another device");
+}
+
+int32_t st_gapblock_matrix_sets(st_seqset queries, st_seqset refs, const int32_t* penalty,
+                                int32_t matrix_size, int32_t gap_open, int32_t gap_extend,
+                                const int32_t* prior, int64_t prior_len, uint32_t prior_width,
+                                int32_t* out_device, void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_set(queries);
+        check_set(refs);
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        auto stream = static_cast<cudaStream_t>(cuda_stream);
+        gapblock_sets(*queries, *refs, penalty, matrix_size, gap_open, gap_extend, prior, prior_len,
+                      prior_width, out_device, stream);
+    });
+}
+
+int32_t st_align_matrix_sets(st_seqset queries, st_seqset refs, const int32_t* similarity,
+                             int32_t matrix_size, int32_t mode, int32_t gap_open,
+                             int32_t gap_extend, int32_t dist, int32_t* out_device,
+                             void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_set(queries);
+        check_set(refs);
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        align_sets(*queries, *refs, similarity, matrix_size, mode, gap_open, gap_extend, dist,
+                   out_device, static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int32_t st_hamming_matrix_sets(st_seqset a, st_seqset b, int32_t* out_device, void* cuda_stream,
+                               st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_set(a);
+        check_set(b);
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        hamming_sets(*a, *b, out_device, static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int32_t st_levenshtein_matrix_sets(st_seqset a, st_seqset b, int32_t* out_device,
+                                   void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_set(a);
+        check_set(b);
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        levenshtein_sets(*a, *b, out_device, static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+}  // extern "C"

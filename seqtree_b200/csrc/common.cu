@@ -1,0 +1,303 @@
+// Per-device context, workspace, pinned host cache and sequence-set upload/encoding.
+#include "common.cuh"
+
+#include <algorithm>
+#include <atomic>
+#include <map>
+
+namespace stb {
+
+// ----------------------------------------------------------------------------- launches -----
+namespace {
+thread_local int t_launches = 0;
+thread_local const char* t_kernel = "";
+}  // namespace
+
+void note_launch(const char* kernel_name, int count) {
+    t_launches += count;
+    if (kernel_name && *kernel_name) t_kernel = kernel_name;
+}
+void reset_launches() {
+    t_launches = 0;
+    t_kernel = "";
+}
+int last_launches() { return t_launches; }
+const char* last_kernel() { return t_kernel; }
+
+// ----------------------------------------------------------------------------- buffers ------
+void* DevBuf::get(size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (bytes > cap) {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+        size_t want = std::max<size_t>(bytes + bytes / 8, 4096);
+        want = (want + 255) & ~size_t(255);
+        STB_CUDA(cudaMalloc(&ptr, want));
+        cap = want;
+    }
+    return ptr;
+}
+
+DevBuf::~DevBuf() {
+    // Contexts live until process exit; the driver reclaims device memory then.
+}
+
+bool same_as_last(std::vector<uint8_t>& slot, const void* data, size_t bytes) {
+    if (slot.size() == bytes && (bytes == 0 || std::memcmp(slot.data(), data, bytes) == 0))
+        return true;
+    slot.assign(static_cast<const uint8_t*>(data), static_cast<const uint8_t*>(data) + bytes);
+    return false;
+}
+
+// ----------------------------------------------------------------------------- context ------
+namespace {
+std::mutex g_ctx_mu;
+std::map<int, std::unique_ptr<Context>> g_ctx;
+}  // namespace
+
+Context& context() {
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    int n = 0;
+    if (e == cudaSuccess) e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n <= 0 || dev < 0) {
+        cudaGetLastError();
+        fail(ST_ENODEV, std::string("seqtree_b200: no usable CUDA device (") +
+                            cudaGetErrorString(e == cudaSuccess ? cudaErrorNoDevice : e) + ")");
+    }
+    std::lock_guard<std::mutex> lk(g_ctx_mu);
+    auto it = g_ctx.find(dev);
+    if (it != g_ctx.end()) return *it->second;
+    auto c = std::make_unique<Context>();
+    c->device = dev;
+    STB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    STB_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, dev));
+    STB_CUDA(cudaDeviceGetAttribute(&c->max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin,
+                                    dev));
+    STB_CUDA(cudaMalloc(&c->flags_d, 64 * sizeof(int64_t)));
+    STB_CUDA(cudaHostAlloc(&c->flags_h, 64 * sizeof(int64_t), cudaHostAllocDefault));
+    Context& ref = *c;
+    g_ctx.emplace(dev, std::move(c));
+    return ref;
+}
+
+int32_t alphabet_size(int32_t alphabet) {
+    switch (alphabet) {
+        case ST_ALPHABET_AA: return 24;   // "ARNDCQEGHILKMFPSTWYVBZX*"  (src/codec.cpp:9)
+        case ST_ALPHABET_NT: return 4;    // "ACGT"                      (src/codec.cpp:10)
+        case ST_ALPHABET_IUPAC: return 15;// "ACGTRYSWKMBDHVN"           (src/codec.cpp:11)
+        default: return 0;
+    }
+}
+
+// ----------------------------------------------------------------------------- encoding -----
+namespace {
+
+const char* symbols(int32_t alphabet) {
+    switch (alphabet) {
+        case ST_ALPHABET_AA: return "ARNDCQEGHILKMFPSTWYVBZX*";
+        case ST_ALPHABET_NT: return "ACGT";
+        default: return "ACGTRYSWKMBDHVN";
+    }
+}
+
+struct Lut {
+    uint8_t v[256];
+};
+
+// Case-insensitive symbol -> code table; 0xFF marks symbols outside the alphabet
+// (the reference Codec, src/codec.cpp:23-35).
+Lut make_lut(int32_t alphabet) {
+    Lut l;
+    std::memset(l.v, 0xFF, sizeof l.v);
+    const char* s = symbols(alphabet);
+    for (int i = 0; s[i]; ++i) {
+        unsigned char up = static_cast<unsigned char>(s[i]);
+        unsigned char lo = (up >= 'A' && up <= 'Z') ? static_cast<unsigned char>(up - 'A' + 'a') : up;
+        l.v[up] = static_cast<uint8_t>(i);
+        l.v[lo] = static_cast<uint8_t>(i);
+    }
+    return l;
+}
+
+// One pass over the bytes: code = lut[byte]; the smallest index of an invalid byte is
+// recorded with atomicMin so the error names the same symbol the reference's sequential
+// encoder stops at.
+__global__ void encode_kernel(const uint8_t* __restrict__ in, uint8_t* __restrict__ out,
+                              int64_t n, Lut lut, unsigned long long* first_bad) {
+    __shared__ uint8_t s_lut[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) s_lut[i] = lut.v[i];
+    __syncthreads();
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x * 4;
+    for (int64_t base = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) * 4; base < n;
+         base += stride) {
+        if (base + 4 <= n) {
+            uint32_t w = *reinterpret_cast<const uint32_t*>(in + base);  // buffers are padded
+            uint32_t o = 0;
+            bool bad = false;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                uint8_t c = s_lut[(w >> (8 * b)) & 0xFF];
+                if (c == 0xFF && !bad) {
+                    atomicMin(first_bad, (unsigned long long)(base + b));
+                    bad = true;
+                }
+                o |= uint32_t(c) << (8 * b);
+            }
+            *reinterpret_cast<uint32_t*>(out + base) = o;
+        } else {
+            for (int64_t i = base; i < n; ++i) {
+                uint8_t c = s_lut[in[i]];
+                if (c == 0xFF) atomicMin(first_bad, (unsigned long long)i);
+                out[i] = c;
+            }
+        }
+    }
+}
+
+__global__ void lengths_kernel(const int64_t* __restrict__ off, int32_t* __restrict__ len,
+                               int64_t count) {
+    int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < count) len[i] = int32_t(off[i + 1] - off[i]);
+}
+
+}  // namespace
+
+st_seqset_s* make_seqset(const st_strings* s, int32_t alphabet, cudaStream_t stream,
+                         int64_t* bad_index, char* bad_char, DevBuf* storage) {
+    static std::atomic<uint64_t> next_uid{1};
+    if (!s || (s->count > 0 && !s->offsets)) fail(ST_EINVAL, "seqtree_b200: null sequence set");
+    if (alphabet != -1 && alphabet_size(alphabet) == 0)
+        fail(ST_EINVAL, "unknown alphabet code " + std::to_string(alphabet));
+    Context& ctx = context();
+    auto set = std::make_unique<st_seqset_s>();
+    set->device = ctx.device;
+    set->uid = next_uid.fetch_add(1);
+    set->alphabet = alphabet;
+    set->count = s->count;
+    set->h_off.assign(s->offsets, s->offsets + (s->count + 1));
+    if (set->h_off.empty()) set->h_off.push_back(0);
+    const int64_t base = set->h_off[0];
+    for (auto& o : set->h_off) o -= base;
+    set->total = set->h_off.back();
+    set->h_len.resize(size_t(s->count));
+    int32_t mx = 0;
+    for (int64_t i = 0; i < s->count; ++i) {
+        int64_t l = set->h_off[i + 1] - set->h_off[i];
+        if (l < 0 || l > INT32_MAX) fail(ST_EINVAL, "seqtree_b200: offsets must be non-decreasing");
+        set->h_len[size_t(i)] = int32_t(l);
+        mx = std::max<int32_t>(mx, int32_t(l));
+    }
+    set->max_len = mx;
+    const size_t padded = size_t(set->total) + 64;
+    if (storage) {
+        set->owns = false;
+        set->d_bytes = storage[0].as<uint8_t>(padded);
+        set->d_off = storage[1].as<int64_t>(size_t(s->count + 1));
+        set->d_len = storage[2].as<int32_t>(size_t(std::max<int64_t>(s->count, 1)));
+    } else {
+        STB_CUDA(cudaMalloc(&set->d_bytes, padded));
+        STB_CUDA(cudaMalloc(&set->d_off, sizeof(int64_t) * size_t(s->count + 1)));
+        STB_CUDA(cudaMalloc(&set->d_len, sizeof(int32_t) * size_t(std::max<int64_t>(s->count, 1))));
+    }
+    STB_CUDA(cudaMemsetAsync(set->d_bytes, 0, padded, stream));
+    STB_CUDA(cudaMemcpyAsync(set->d_off, set->h_off.data(), sizeof(int64_t) * size_t(s->count + 1),
+                             cudaMemcpyHostToDevice, stream));
+    if (s->count > 0) {
+        lengths_kernel<<<unsigned(ceil_div(s->count, 256)), 256, 0, stream>>>(set->d_off, set->d_len,
+                                                                              s->count);
+        STB_CUDA(cudaGetLastError());
+        note_launch(nullptr);
+    }
+    if (set->total > 0) {
+        const uint8_t* src = reinterpret_cast<const uint8_t*>(s->bytes) + base;
+        if (alphabet < 0) {
+            STB_CUDA(cudaMemcpyAsync(set->d_bytes, src, size_t(set->total), cudaMemcpyHostToDevice,
+                                     stream));
+        } else {
+            DevBuf& raw = ctx.work_c;
+            uint8_t* d_raw = raw.as<uint8_t>(padded);
+            STB_CUDA(cudaMemsetAsync(d_raw + set->total, 0, 64, stream));
+            STB_CUDA(cudaMemcpyAsync(d_raw, src, size_t(set->total), cudaMemcpyHostToDevice, stream));
+            auto* flag = reinterpret_cast<unsigned long long*>(ctx.flags_d);
+            const unsigned long long none = ~0ull;
+            STB_CUDA(cudaMemcpyAsync(flag, &none, sizeof none, cudaMemcpyHostToDevice, stream));
+            const Lut lut = make_lut(alphabet);
+            const int64_t words = ceil_div(set->total, 4);
+            const unsigned grid = unsigned(std::min<int64_t>(ceil_div(words, 256), ctx.num_sms * 8));
+            encode_kernel<<<grid, 256, 0, stream>>>(d_raw, set->d_bytes, set->total, lut, flag);
+            STB_CUDA(cudaGetLastError());
+            note_launch(nullptr);
+            STB_CUDA(cudaMemcpyAsync(ctx.flags_h, flag, sizeof none, cudaMemcpyDeviceToHost, stream));
+            STB_CUDA(cudaStreamSynchronize(stream));
+            const unsigned long long bad = static_cast<unsigned long long>(ctx.flags_h[0]);
+            if (bad != none) {
+                if (bad_index) {
+                    *bad_index = int64_t(bad);
+                    if (bad_char) *bad_char = char(src[bad]);
+                } else {
+                    fail(ST_EINVAL, std::string("symbol '") + char(src[bad]) +
+                                        "' is not in the alphabet");
+                }
+            } else if (bad_index) {
+                *bad_index = -1;
+            }
+        }
+    } else if (bad_index) {
+        *bad_index = -1;
+    }
+    return set.release();
+}
+
+}  // namespace stb
+
+st_seqset_s::~st_seqset_s() {
+    if (!owns) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != device) cudaSetDevice(device);
+    if (d_bytes) cudaFree(d_bytes);
+    if (d_off) cudaFree(d_off);
+    if (d_len) cudaFree(d_len);
+    if (prev >= 0 && prev != device) cudaSetDevice(prev);
+}
+
+// ----------------------------------------------------------------------------- pinned -------
+namespace stb {
+namespace {
+std::mutex g_pin_mu;
+std::multimap<size_t, void*> g_pin_free;  // size -> block
+std::map<void*, size_t> g_pin_size;
+}  // namespace
+
+void* host_alloc(uint64_t bytes) {
+    size_t want = size_t(bytes == 0 ? 1 : bytes);
+    want = (want + 4095) & ~size_t(4095);
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        auto it = g_pin_free.lower_bound(want);
+        if (it != g_pin_free.end() && it->first <= want + want / 4) {
+            void* p = it->second;
+            g_pin_free.erase(it);
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, want, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_size[p] = want;
+    return p;
+}
+
+void host_free(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    auto it = g_pin_size.find(p);
+    if (it == g_pin_size.end()) return;
+    g_pin_free.emplace(it->second, p);
+}
+}  // namespace stb

@@ -1,0 +1,119 @@
+// Shared host/device infrastructure of libseqtree_b200: error plumbing, the per-device
+// context (stream, grow-only device workspace, pinned staging), and the device-resident
+// sequence set.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/seqtree_b200.h"
+
+namespace stb {
+
+// ----------------------------------------------------------------------------- errors -------
+// Every failure inside the library is a StError carrying the C-ABI code and the exact message
+// the reference raises for the same condition; the extern "C" wrappers turn it into st_error.
+struct StError : std::runtime_error {
+    int32_t code;
+    StError(int32_t c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+[[noreturn]] inline void fail(int32_t code, const std::string& msg) { throw StError(code, msg); }
+
+#define STB_CUDA(expr)                                                                        \
+    do {                                                                                      \
+        cudaError_t e_ = (expr);                                                              \
+        if (e_ != cudaSuccess)                                                                \
+            ::stb::fail(e_ == cudaErrorMemoryAllocation ? ST_ENOMEM : ST_ECUDA,               \
+                        std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " +       \
+                            __FILE__ + ":" + std::to_string(__LINE__));                      \
+    } while (0)
+
+// Launch bookkeeping: the number of kernels the last call launched and the main variant.
+void note_launch(const char* kernel_name, int count = 1);
+void reset_launches();
+
+// ----------------------------------------------------------------------------- context ------
+// A device buffer that only grows; reused across calls so steady-state calls allocate nothing.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t cap = 0;
+    void* get(size_t bytes);
+    template <class T>
+    T* as(size_t count) { return static_cast<T*>(get(count * sizeof(T))); }
+    ~DevBuf();
+};
+
+struct Context {
+    int device = 0;
+    std::mutex mu;              // serialises calls on this device
+    cudaStream_t stream = nullptr;
+    int num_sms = 148;
+    int max_smem_optin = 0;
+    // Small device word area for error reporting, with a pinned host mirror.  Word 0: first
+    // invalid symbol of an encode; word 8: a bounded wait gave up; word 9: an int32 overflow;
+    // words 16-19: byte-presence bitmap.  Words 8-15 are cleared before and read after each
+    // host call.
+    int64_t* flags_d = nullptr;
+    int64_t* flags_h = nullptr;
+    // named scratch, grow-only
+    DevBuf out_buf, q_codes, r_codes, table_buf, prior_buf, ftab_buf, work_a, work_b, work_c;
+    // storage of the transient sets made by the host-buffer entry points
+    DevBuf tq[3], tr[3];  // bytes, offsets, lengths
+    // plans reused by transient sets (rebuilt in place for every call)
+    std::shared_ptr<void> tmp_query_plan, tmp_ref_plan;
+};
+
+// Context of the current CUDA device (created on first use).  Fails with ST_ENODEV when no
+// device is usable.
+Context& context();
+
+// Byte-exact content cache: returns true when `bytes` equals what was uploaded last time
+// under `slot`, so re-uploads of unchanged tables are skipped.
+bool same_as_last(std::vector<uint8_t>& slot, const void* data, size_t bytes);
+
+// ----------------------------------------------------------------------------- sets ---------
+// A sequence set resident on one device: the concatenated (encoded or raw) bytes, offsets and
+// lengths, plus host-side length metadata used to plan launches.
+}  // namespace stb
+
+struct st_seqset_s {
+    int device = 0;
+    int32_t alphabet = -1;      // ST_ALPHABET_* or -1 for raw bytes
+    int64_t count = 0;
+    int64_t total = 0;          // bytes
+    int32_t max_len = 0;
+    std::vector<int64_t> h_off; // count + 1
+    std::vector<int32_t> h_len; // count
+    uint8_t* d_bytes = nullptr; // encoded codes (alphabet >= 0) or raw bytes, +64 B padding
+    int64_t* d_off = nullptr;
+    int32_t* d_len = nullptr;
+    bool owns = true;           // false: storage borrowed from the context (transient set)
+    uint64_t uid = 0;           // unique per set; plans record the uid they were built for
+    // plan caches (opaque; transient sets share the context's)
+    std::shared_ptr<void> gb_query_plan, gb_ref_plan;
+    ~st_seqset_s();
+};
+
+namespace stb {
+
+// Uploads and encodes `s` onto the current device.  When `bad_index` is non-null the first
+// invalid symbol's byte index is returned there (or -1) instead of failing, so a caller can
+// order errors across two sets exactly as the reference does.
+// `storage` (three buffers: bytes, offsets, lengths) makes a transient set that borrows
+// context memory instead of allocating.
+st_seqset_s* make_seqset(const st_strings* s, int32_t alphabet, cudaStream_t stream,
+                         int64_t* bad_index, char* bad_char, DevBuf* storage = nullptr);
+
+int32_t alphabet_size(int32_t alphabet);
+
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace stb

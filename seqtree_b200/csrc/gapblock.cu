@@ -1,0 +1,621 @@
+// Dense single-gap-block penalty matrix on sm_100a.
+//
+// Reference arithmetic (seqtree src/gapblock.cpp:39-62): for a pair (q, r) with L = min(m,n),
+// d = |m-n|, the layout whose block opens at column i of the shorter sequence costs
+//     pre[i] + suf[i] + prior[i]     (prefix on diagonal 0, suffix on diagonal d)
+// and the score is the minimum over i in [0, L] plus gap_open + (d-1)*gap_extend; at d == 0
+// it is the plain substitution sum.  With P0[j] = pen on diagonal 0 and Pd[j] = pen on
+// diagonal d, pre[i] + suf[i] = S + C[i] where S = sum_j Pd[j] and C[i] = sum_{j<i}(P0 - Pd),
+// so one forward sweep visits every block position -- that is the form computed here.  The
+// result is the same integer as the reference's (integer sums, no reassociation hazard while
+// the reference itself does not overflow int32).
+//
+// Fast path (every length <= 64, L*max_pen <= 8191): two queries of equal length share a
+// warp-uniform row of a (q1, q2, r) pair table in shared memory, so one 32-bit LDS returns the
+// two penalties as int16x2 and one DPX __viaddmin_s16x2 keeps both running minima.  Refs of a
+// 1024-column chunk are processed in groups of equal length (d, L and the prior row are then
+// warp-uniform and the table row read is bank-conflict free); results go through a shared
+// tile so that global stores stay coalesced in the original column order.
+// General path: one thread per pair in int32 for any lengths and penalty magnitudes.
+#include <algorithm>
+#include <map>
+#include <numeric>
+
+#include "common.cuh"
+
+namespace stb {
+
+namespace {
+
+constexpr int kRC = 1024;    // refs per chunk (columns of one CTA tile)
+constexpr int kGP = 8;       // query pairs per CTA (rows of one CTA tile = 16)
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+// ---------------------------------------------------------------------------- plans ---------
+// Launch plans depend only on the lengths of a set, so a device-resident set builds them once;
+// transient sets (host-buffer calls) rebuild them in place inside the context's plan objects,
+// whose device buffers only grow.
+struct QueryPlan {
+    uint64_t uid = 0;                    // set the plan was built for
+    int64_t P = 0;                       // query pairs
+    std::vector<int2> pairs;             // original indices (second may be -1)
+    std::vector<int32_t> plen;           // m of each pair
+    DevBuf d_pairs, d_plen;
+};
+
+struct RefPlan {
+    uint64_t uid = 0;
+    int64_t nchunks = 0;
+    int64_t ntasks = 0;
+    std::vector<int32_t> sorted;
+    std::vector<int4> tasks;
+    std::vector<int32_t> task_off;
+    DevBuf d_sorted;                     // global ref index, sorted by length inside each chunk
+    DevBuf d_tasks;                      // int4 (n, start in sorted, count <= 32, chunk)
+    DevBuf d_task_off;                   // nchunks + 1
+};
+
+// Queries sorted by length (stable) and paired within each length; an odd one out is paired
+// with a dummy (-1).  Each length's pairs are padded with dummy pairs (-1, -1) to a multiple
+// of 4, so that every slice of 4 consecutive pairs has one length.  Dummy results are never
+// stored.
+void build_query_plan(QueryPlan& plan, const st_seqset_s& q, cudaStream_t stream) {
+    const int64_t N = q.count;
+    std::vector<int32_t> order(static_cast<size_t>(N));
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t a, int32_t b) { return q.h_len[size_t(a)] < q.h_len[size_t(b)]; });
+    plan.pairs.clear();
+    plan.plen.clear();
+    for (int64_t i = 0; i < N;) {
+        const int32_t m = q.h_len[size_t(order[size_t(i)])];
+        int64_t e = i;
+        while (e < N && q.h_len[size_t(order[size_t(e)])] == m) ++e;
+        const size_t first = plan.pairs.size();
+        for (int64_t t = i; t < e; t += 2)
+            plan.pairs.push_back(make_int2(order[size_t(t)], t + 1 < e ? order[size_t(t + 1)] : -1));
+        while ((plan.pairs.size() - first) % 4) plan.pairs.push_back(make_int2(-1, -1));
+        plan.plen.resize(plan.pairs.size(), m);
+        i = e;
+    }
+    plan.P = int64_t(plan.pairs.size());
+    STB_CUDA(cudaMemcpyAsync(plan.d_pairs.as<int2>(size_t(plan.P)), plan.pairs.data(),
+                             sizeof(int2) * size_t(plan.P), cudaMemcpyHostToDevice, stream));
+    STB_CUDA(cudaMemcpyAsync(plan.d_plen.as<int32_t>(size_t(plan.P)), plan.plen.data(),
+                             sizeof(int32_t) * size_t(plan.P), cudaMemcpyHostToDevice, stream));
+    plan.uid = q.uid;
+}
+
+// Refs in chunks of kRC columns (original order); inside a chunk a counting sort by length
+// yields warp tasks of <= 32 refs of one length.
+void build_ref_plan(RefPlan& plan, const st_seqset_s& r, cudaStream_t stream) {
+    const int64_t K = r.count;
+    plan.nchunks = ceil_div(K, kRC);
+    plan.sorted.resize(size_t(K));
+    plan.tasks.clear();
+    plan.task_off.assign(size_t(plan.nchunks + 1), 0);
+    std::vector<int32_t> cnt(size_t(r.max_len) + 2);
+    std::vector<int32_t> start(cnt.size());
+    for (int64_t c = 0; c < plan.nchunks; ++c) {
+        const int64_t k0 = c * kRC, k1 = std::min<int64_t>(K, k0 + kRC);
+        std::fill(cnt.begin(), cnt.end(), 0);
+        for (int64_t k = k0; k < k1; ++k) cnt[size_t(r.h_len[size_t(k)]) + 1]++;
+        for (size_t l = 1; l < cnt.size(); ++l) cnt[l] += cnt[l - 1];
+        std::copy(cnt.begin(), cnt.end(), start.begin());
+        for (int64_t k = k0; k < k1; ++k)
+            plan.sorted[size_t(k0 + start[size_t(r.h_len[size_t(k)])]++)] = int32_t(k);
+        for (int32_t l = 0; l <= r.max_len; ++l) {
+            const int32_t b = cnt[size_t(l)], e = cnt[size_t(l) + 1];
+            for (int32_t s = b; s < e; s += 32)
+                plan.tasks.push_back(make_int4(l, int32_t(k0) + s, std::min(32, e - s), int32_t(c)));
+        }
+        plan.task_off[size_t(c + 1)] = int32_t(plan.tasks.size());
+    }
+    plan.ntasks = int64_t(plan.tasks.size());
+    STB_CUDA(cudaMemcpyAsync(plan.d_sorted.as<int32_t>(size_t(K)), plan.sorted.data(),
+                             sizeof(int32_t) * size_t(K), cudaMemcpyHostToDevice, stream));
+    STB_CUDA(cudaMemcpyAsync(plan.d_tasks.as<int4>(plan.tasks.size()), plan.tasks.data(),
+                             sizeof(int4) * plan.tasks.size(), cudaMemcpyHostToDevice, stream));
+    STB_CUDA(cudaMemcpyAsync(plan.d_task_off.as<int32_t>(plan.task_off.size()),
+                             plan.task_off.data(), sizeof(int32_t) * plan.task_off.size(),
+                             cudaMemcpyHostToDevice, stream));
+    plan.uid = r.uid;
+}
+
+template <class Plan>
+Plan& plan_slot(std::shared_ptr<void>& own, std::shared_ptr<void>& shared, bool owns) {
+    std::shared_ptr<void>& slot = owns ? own : shared;
+    if (!slot) slot = std::make_shared<Plan>();
+    return *static_cast<Plan*>(slot.get());
+}
+
+// ---------------------------------------------------------------------------- fast kernel ---
+// Shared-memory query profile: for the CTA's query pair p and position j, the 32-word row
+// QP[p][j][b] = pen(q1[j], b) | pen(q2[j], b) << 16 (b < A, zero padded) -- one pass over the
+// 32 banks.  A warp unit is (32 refs of one length) x (a slice of 4 pairs of one length); the
+// four pairs are swept together, so every lookup address is a per-lane register (the ref
+// residue's byte offset, with the slice base folded in) plus a compile-time immediate
+// ((pair * LQ + j) * 128).  Query-longer and ref-longer pairs then share one inner loop: the
+// diagonal-d offset is either shifted by d rows (query longer) or taken from the ref residue
+// d positions further on (ref longer).
+constexpr int kRow = 32;        // words per profile row
+constexpr int kPairsPerSlice = 4;
+
+struct FastArgs {
+    const int32_t* pen;      // A*A penalty grid (padded to a multiple of 4 words)
+    int pen_words;
+    int A;
+    const uint8_t* qcodes;
+    const int64_t* qoff;
+    const uint8_t* rcodes;
+    const int64_t* roff;
+    const int32_t* rlen;
+    int64_t K;
+    const int2* pairs;       // (q1, q2); -1 marks a dummy slot
+    const int32_t* plen;
+    int64_t P;               // a multiple of 4; every slice of 4 pairs has one length
+    const int32_t* ref_sorted;
+    const int4* tasks;
+    const int32_t* task_off;
+    const uint32_t* prior2;  // [(M*W1 + d)*W1 + i], normalised, clamped, both halves; or null
+    const int32_t* ftab;     // [m*W1 + n]: per-(m,n) additive term (prior minimum + gap cost)
+    int W1;
+    uint32_t bias2;          // BIAS in both halves
+    int32_t* out;
+    unsigned long long* err; // set when the bounded wait for the staging copy gives up
+};
+
+// One non-blocking probe of an mbarrier phase (callers bound the number of probes).
+__device__ __forceinline__ uint32_t mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok;
+}
+
+template <int LQ, int LMAX, bool PRIOR>
+__global__ void __launch_bounds__(kThreads, 2) gapblock_fast_kernel(const FastArgs a) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    constexpr int kRowB = kRow * 4;
+    constexpr int kPairB = LQ * kRowB;
+    uint32_t* s_qp = reinterpret_cast<uint32_t*>(smem);                      // kGP*LQ rows
+    uint32_t* s_tile = reinterpret_cast<uint32_t*>(smem + kGP * kPairB);      // [kGP][kRC]
+    int32_t* s_ftab = reinterpret_cast<int32_t*>(s_tile + kGP * kRC);
+    int32_t* s_pen = s_ftab + ((a.W1 * a.W1 + 3) & ~3);
+    uint8_t* s_len = reinterpret_cast<uint8_t*>(s_pen + a.pen_words);
+    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_len + kRC);
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int chunk = blockIdx.x;
+    const int64_t k0 = int64_t(chunk) * kRC;
+    const int kcount = int(a.K - k0 < kRC ? a.K - k0 : kRC);
+    const int p0 = blockIdx.y * kGP;
+    const int np = int(a.P - p0 < kGP ? a.P - p0 : kGP);
+
+    const uint32_t bar = uint32_t(__cvta_generic_to_shared(s_bar));
+    const uint32_t bytes = uint32_t(a.pen_words) * 4u;
+    // Stage the penalty grid with one bulk (TMA) copy that completes on an mbarrier, while the
+    // other threads load the per-chunk lengths and the (m, n) term table.
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+                "r"(uint32_t(__cvta_generic_to_shared(s_pen))),
+            "l"(a.pen), "r"(bytes), "r"(bar)
+            : "memory");
+    }
+    for (int i = tid; i < a.W1 * a.W1; i += kThreads) s_ftab[i] = a.ftab[i];
+    for (int c = tid; c < kcount; c += kThreads) s_len[c] = uint8_t(a.rlen[k0 + c]);
+    __syncthreads();
+    {
+        // Bounded wait on phase 0 by every thread.  If any thread runs out, the CTA records
+        // the failure, waits once more (bounded) for its copy in flight, and leaves as a
+        // whole -- the host then reports ST_ETIMEOUT and no tile is stored.
+        uint32_t done = 0;
+        for (int it = 0; it < (1 << 20) && !done; ++it) done = mbar_try_wait(bar, 0);
+        if (__syncthreads_or(!done)) {
+            if (tid == 0) atomicExch(a.err, 1ull);
+            for (int it = 0; it < (1 << 20) && !done; ++it) done = mbar_try_wait(bar, 0);
+            __syncthreads();
+            return;
+        }
+    }
+    // Query profile of the CTA's pairs (rows past a pair's length and dummy pairs are zero).
+    {
+        const int A = a.A;
+        for (int idx = tid; idx < np * LQ * kRow; idx += kThreads) {
+            const int pl = idx / (LQ * kRow);
+            const int j = (idx / kRow) % LQ;
+            const int b = idx % kRow;
+            const int2 pr = a.pairs[p0 + pl];
+            const int m = a.plen[p0 + pl];
+            uint32_t v = 0;
+            if (b < A && j < m && pr.x >= 0) {
+                const int c1 = a.qcodes[a.qoff[pr.x] + j];
+                const int c2 = a.qcodes[a.qoff[pr.y >= 0 ? pr.y : pr.x] + j];
+                v = uint32_t(s_pen[c1 * A + b]) | (uint32_t(s_pen[c2 * A + b]) << 16);
+            }
+            s_qp[idx] = v;
+        }
+    }
+    __syncthreads();
+
+    const int t0 = a.task_off[chunk], t1 = a.task_off[chunk + 1];
+    const int nslices = np / kPairsPerSlice;
+    const int units = (t1 - t0) * nslices;
+    for (int u = warp; u < units; u += kWarps) {
+        const int4 task = a.tasks[t0 + u / nslices];
+        const int slice = u - (u / nslices) * nslices;
+        const int n = task.x;
+        const int m = a.plen[p0 + slice * kPairsPerSlice];
+        const bool valid = lane < task.z;
+        const int k = a.ref_sorted[task.y + (valid ? lane : 0)];
+        const int col = int(k - k0);
+        const uint8_t* rb = a.rcodes + a.roff[k];
+        const int L = min(m, n);
+        const int d = abs(m - n);
+        const uint32_t sbase = uint32_t(slice * kPairsPerSlice * kPairB);
+        uint32_t r0[LMAX], rd[LMAX];
+#pragma unroll
+        for (int j = 0; j < LMAX; ++j) {
+            if (j < L) {
+                r0[j] = sbase + uint32_t(rb[j]) * 4u;
+                rd[j] = m > n ? r0[j] + uint32_t(d * kRowB) : sbase + uint32_t(rb[j + d]) * 4u;
+            }
+        }
+        uint32_t res[kPairsPerSlice];
+        if (d == 0) {
+            uint32_t S[kPairsPerSlice] = {0u, 0u, 0u, 0u};
+#pragma unroll
+            for (int j = 0; j < LMAX; ++j) {
+                if (j < L) {
+#pragma unroll
+                    for (int q = 0; q < kPairsPerSlice; ++q)
+                        S[q] += *reinterpret_cast<const uint32_t*>(smem + r0[j] + (q * LQ + j) * kRowB);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kPairsPerSlice; ++q) res[q] = S[q];
+        } else {
+            uint32_t pr[PRIOR ? LMAX + 1 : 1];
+            if constexpr (PRIOR) {
+                const uint32_t* row = a.prior2 + (size_t(max(m, n)) * a.W1 + d) * a.W1;
+#pragma unroll
+                for (int j = 0; j <= LMAX; ++j)
+                    if (j <= L) pr[j] = row[j];
+            }
+            uint32_t S[kPairsPerSlice], Cb[kPairsPerSlice], best[kPairsPerSlice];
+#pragma unroll
+            for (int q = 0; q < kPairsPerSlice; ++q) {
+                S[q] = 0u;
+                Cb[q] = a.bias2;
+                if constexpr (PRIOR) best[q] = a.bias2 + pr[0];
+                else best[q] = a.bias2;
+            }
+#pragma unroll
+            for (int j = 0; j < LMAX; ++j) {
+                if (j < L) {
+#pragma unroll
+                    for (int q = 0; q < kPairsPerSlice; ++q) {
+                        const uint32_t p0v =
+                            *reinterpret_cast<const uint32_t*>(smem + r0[j] + (q * LQ + j) * kRowB);
+                        const uint32_t pdv =
+                            *reinterpret_cast<const uint32_t*>(smem + rd[j] + (q * LQ + j) * kRowB);
+                        S[q] += pdv;
+                        Cb[q] = Cb[q] + p0v - pdv;  // per-half exact: halves stay in [0, 2^15)
+                        if constexpr (PRIOR)
+                            best[q] = __viaddmin_s16x2(Cb[q], pr[j + 1], best[q]);
+                        else
+                            best[q] = __viaddmin_s16x2(Cb[q], 0u, best[q]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kPairsPerSlice; ++q) res[q] = S[q] + best[q] - a.bias2;
+        }
+        if (valid) {
+#pragma unroll
+            for (int q = 0; q < kPairsPerSlice; ++q)
+                s_tile[(slice * kPairsPerSlice + q) * kRC + col] = res[q];
+        }
+    }
+    __syncthreads();
+
+    // Coalesced write-out of the (2*np) x kcount tile, adding the per-(m,n) term.
+    const bool vec = (a.K & 3) == 0;
+    const int cols4 = (kcount + 3) / 4;
+    for (int idx = tid; idx < 2 * np * cols4; idx += kThreads) {
+        const int s = idx / cols4;
+        const int c = (idx - s * cols4) * 4;
+        const int2 pr = a.pairs[p0 + s / 2];
+        const int orig = (s & 1) ? pr.y : pr.x;
+        if (orig < 0) continue;
+        const int m = a.plen[p0 + s / 2];
+        const int32_t* frow = s_ftab + m * a.W1;
+        const int sh = (s & 1) * 16;
+        int32_t* dst = a.out + int64_t(orig) * a.K + k0 + c;
+        const uint32_t* src = s_tile + (s / 2) * kRC + c;
+        if (vec && c + 4 <= kcount) {
+            int4 v;
+            v.x = int32_t(((src[0] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + 0]]));
+            v.y = int32_t(((src[1] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + 1]]));
+            v.z = int32_t(((src[2] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + 2]]));
+            v.w = int32_t(((src[3] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + 3]]));
+            *reinterpret_cast<int4*>(dst) = v;
+        } else {
+            for (int t = 0; t < 4 && c + t < kcount; ++t)
+                dst[t] = int32_t(((src[t] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + t]]));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------- general -------
+struct GeneralArgs {
+    const uint8_t* qcodes;
+    const int64_t* qoff;
+    const uint8_t* rcodes;
+    const int64_t* roff;
+    int64_t N, K;
+    const int32_t* pen;   // A*A
+    int A;
+    int32_t go, ge;
+    const int32_t* prior; // (pw+1)^3 or null
+    int64_t pw1;
+    int32_t* out;
+};
+
+// One thread per (i, k) in row-major order, int32 arithmetic with the reference's wrap.
+__global__ void __launch_bounds__(256) gapblock_general_kernel(const GeneralArgs a) {
+    extern __shared__ int32_t s_pen[];
+    for (int i = threadIdx.x; i < a.A * a.A; i += blockDim.x) s_pen[i] = a.pen[i];
+    __syncthreads();
+    const int64_t total = a.N * a.K;
+    for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
+         idx += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = idx / a.K, k = idx - i * a.K;
+        const uint8_t* q = a.qcodes + a.qoff[i];
+        const uint8_t* r = a.rcodes + a.roff[k];
+        const int m = int(a.qoff[i + 1] - a.qoff[i]);
+        const int n = int(a.roff[k + 1] - a.roff[k]);
+        const int L = min(m, n), d = abs(m - n);
+        int32_t v;
+        if (d == 0) {
+            uint32_t s = 0;
+            for (int j = 0; j < L; ++j) s += uint32_t(s_pen[q[j] * a.A + r[j]]);
+            v = int32_t(s);
+        } else {
+            const bool ql = m > n;
+            const int32_t* prow =
+                a.prior ? a.prior + (int64_t(max(m, n)) * a.pw1 + d) * a.pw1 : nullptr;
+            int32_t S = 0, C = 0;
+            int32_t best = prow ? prow[0] : 0;
+            for (int j = 0; j < L; ++j) {
+                const int32_t p0v = s_pen[q[j] * a.A + r[j]];
+                const int32_t pdv = ql ? s_pen[q[j + d] * a.A + r[j]] : s_pen[q[j] * a.A + r[j + d]];
+                S += pdv;
+                C += p0v - pdv;
+                const int32_t cand = C + (prow ? prow[j + 1] : 0);
+                best = cand < best ? cand : best;
+            }
+            v = int32_t(uint32_t(S) + uint32_t(best) + uint32_t(a.go) +
+                        uint32_t(d - 1) * uint32_t(a.ge));
+        }
+        a.out[idx] = v;
+    }
+}
+
+template <int LQ, int LMAX, bool PRIOR>
+const char* launch_fast(const FastArgs& args, dim3 grid, size_t smem, cudaStream_t stream) {
+    auto kern = gapblock_fast_kernel<LQ, LMAX, PRIOR>;
+    STB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    kern<<<grid, kThreads, smem, stream>>>(args);
+    STB_CUDA(cudaGetLastError());
+    return "gapblock_fast_kernel";
+}
+
+template <int LQ, bool PRIOR>
+const char* dispatch_lmax(int lmax, const FastArgs& args, dim3 grid, size_t smem,
+                          cudaStream_t stream) {
+    if (lmax <= 8) return launch_fast<LQ, 8, PRIOR>(args, grid, smem, stream);
+    if (lmax <= 16) return launch_fast<LQ, 16, PRIOR>(args, grid, smem, stream);
+    if (lmax <= 24) return launch_fast<LQ, 24, PRIOR>(args, grid, smem, stream);
+    return launch_fast<LQ, 32, PRIOR>(args, grid, smem, stream);
+}
+
+// Profile height LQ >= longest query (32 or 64), LMAX >= longest min(m, n).
+int profile_height(int longest_query) { return longest_query <= 32 ? 32 : 64; }
+
+const char* dispatch_fast(int lq, int lmax, bool prior, const FastArgs& args, dim3 grid,
+                          size_t smem, cudaStream_t stream) {
+    if (lq == 32)
+        return prior ? dispatch_lmax<32, true>(lmax, args, grid, smem, stream)
+                     : dispatch_lmax<32, false>(lmax, args, grid, smem, stream);
+    return prior ? dispatch_lmax<64, true>(lmax, args, grid, smem, stream)
+                 : dispatch_lmax<64, false>(lmax, args, grid, smem, stream);
+}
+
+// Device-side tables of the fast path and the arguments they were built from.
+struct GbTables {
+    std::vector<uint8_t> key;
+    DevBuf pen, ftab, prior2;
+};
+
+GbTables& gb_tables(int device) {
+    static std::mutex mu;
+    static std::map<int, std::unique_ptr<GbTables>> all;
+    std::lock_guard<std::mutex> lk(mu);
+    auto& p = all[device];
+    if (!p) p = std::make_unique<GbTables>();
+    return *p;
+}
+
+// Penalty grid (padded to 16 bytes for the bulk copy); per-(M,d) prior rows shifted by their
+// minimum (added back through ftab) and clamped at CAP = 2*BIAS + 1 -- a clamped position can
+// never win, because the position holding the row's minimum scores at most BIAS while a
+// clamped one scores above it; ftab[m][n] = prior minimum + gap_open + (d-1)*gap_extend
+// (int32 wrap, as the reference's int32 arithmetic).
+void build_tables(GbTables& tb, const std::vector<int32_t>& pen, int A, int32_t go, int32_t ge,
+                  int W, int32_t bias, const int32_t* prior, int64_t W1p, cudaStream_t stream) {
+    const int pen_words = int((size_t(A) * A + 3) & ~size_t(3));
+    std::vector<int32_t> pen_padded(size_t(pen_words), 0);
+    std::copy(pen.begin(), pen.end(), pen_padded.begin());
+    const int W1 = W + 1;
+    const int32_t cap = 2 * bias + 1;
+    std::vector<int32_t> ftab(size_t(W1) * W1, 0);
+    std::vector<uint32_t> prior2;
+    if (prior) prior2.assign(size_t(W1) * W1 * W1, 0);
+    for (int m = 0; m <= W; ++m)
+        for (int n = 0; n <= W; ++n) {
+            const int M = std::max(m, n), d = std::abs(m - n), L = std::min(m, n);
+            if (d == 0) continue;
+            int32_t pmin = 0;
+            if (prior) {
+                const int32_t* row = prior + (int64_t(M) * W1p + d) * W1p;
+                pmin = row[0];
+                for (int i = 1; i <= L; ++i) pmin = std::min(pmin, row[i]);
+                if (m >= n) {  // fill each (M, d) row once
+                    uint32_t* dst = prior2.data() + (size_t(M) * W1 + d) * W1;
+                    for (int i = 0; i <= L; ++i)
+                        dst[i] = uint32_t(std::min<int64_t>(int64_t(row[i]) - pmin, cap)) * 0x10001u;
+                }
+            }
+            ftab[size_t(m) * W1 + n] = int32_t(uint32_t(pmin) + uint32_t(go) +
+                                               uint32_t(d - 1) * uint32_t(ge));
+        }
+    STB_CUDA(cudaMemcpyAsync(tb.pen.as<int32_t>(pen_padded.size()), pen_padded.data(),
+                             pen_padded.size() * 4, cudaMemcpyHostToDevice, stream));
+    STB_CUDA(cudaMemcpyAsync(tb.ftab.as<int32_t>(ftab.size()), ftab.data(), ftab.size() * 4,
+                             cudaMemcpyHostToDevice, stream));
+    if (prior)
+        STB_CUDA(cudaMemcpyAsync(tb.prior2.as<uint32_t>(prior2.size()), prior2.data(),
+                                 prior2.size() * 4, cudaMemcpyHostToDevice, stream));
+}
+
+}  // namespace
+
+// Validated inputs -> device matrix.  `out_d` is device memory of N*K int32.
+void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int32_t matrix_size,
+                   int32_t go, int32_t ge, const int32_t* prior, int64_t prior_len,
+                   uint32_t prior_width, int32_t* out_d, cudaStream_t stream) {
+    if (go < 0 || ge < 0) fail(ST_EINVAL, "gap_open and gap_extend must be >= 0");
+    if (qs.alphabet < 0 || qs.alphabet != rs.alphabet)
+        fail(ST_EINVAL, "seqtree_b200: gap-block sets must be encoded with one alphabet");
+    const int A = alphabet_size(qs.alphabet);
+    if (penalty && matrix_size != A) fail(ST_EINVAL, "matrix size does not match the alphabet");
+    const int64_t N = qs.count, K = rs.count;
+    if (N == 0 || K == 0) return;
+    const int32_t longest = std::max(qs.max_len, rs.max_len);
+    const int64_t W1p = int64_t(prior_width) + 1;
+    const bool has_prior = prior && prior_len > 0;
+    if (has_prior) {
+        if (prior_len != W1p * W1p * W1p)
+            fail(ST_EINVAL, "prior table must have (prior_width + 1)^3 entries");
+        if (uint32_t(longest) > prior_width)
+            fail(ST_EINVAL, "a sequence is longer than the prior table's width");
+    }
+    Context& ctx = context();
+
+    // Penalty grid (unit cost when null): src/gapblock.cpp:25-31.
+    std::vector<int32_t> pen(size_t(A) * A);
+    for (int x = 0; x < A; ++x)
+        for (int y = 0; y < A; ++y) pen[size_t(x) * A + y] = penalty ? penalty[x * A + y] : int32_t(x != y);
+    int64_t maxpen = 0;
+    bool nonneg = true;
+    for (int32_t v : pen) {
+        maxpen = std::max<int64_t>(maxpen, v);
+        nonneg &= v >= 0;
+    }
+    const int32_t Lmax = std::min(qs.max_len, rs.max_len);
+    const int64_t lmaxpen = int64_t(Lmax) * maxpen;
+    const bool fast = nonneg && longest <= 64 && Lmax <= 32 && lmaxpen <= 8191;
+
+    if (!fast) {
+        int32_t* d_pen = ctx.table_buf.as<int32_t>(pen.size());
+        STB_CUDA(cudaMemcpyAsync(d_pen, pen.data(), pen.size() * 4, cudaMemcpyHostToDevice, stream));
+        int32_t* d_prior = nullptr;
+        if (has_prior) {
+            d_prior = ctx.prior_buf.as<int32_t>(size_t(prior_len));
+            STB_CUDA(cudaMemcpyAsync(d_prior, prior, size_t(prior_len) * 4, cudaMemcpyHostToDevice,
+                                     stream));
+        }
+        GeneralArgs g{qs.d_bytes, qs.d_off, rs.d_bytes, rs.d_off, N, K, d_pen, A, go, ge,
+                      d_prior, W1p, out_d};
+        const int64_t blocks = std::min<int64_t>(ceil_div(N * K, 256), int64_t(ctx.num_sms) * 16);
+        gapblock_general_kernel<<<unsigned(blocks), 256, size_t(A) * A * 4, stream>>>(g);
+        STB_CUDA(cudaGetLastError());
+        note_launch("gapblock_general_kernel");
+        return;
+    }
+
+    // ---- fast path planning ----
+    QueryPlan& qp = plan_slot<QueryPlan>(qs.gb_query_plan, ctx.tmp_query_plan, qs.owns);
+    RefPlan& rp = plan_slot<RefPlan>(rs.gb_ref_plan, ctx.tmp_ref_plan, rs.owns);
+    if (qp.uid != qs.uid) build_query_plan(qp, qs, stream);
+    if (rp.uid != rs.uid) build_ref_plan(rp, rs, stream);
+    // Device tables for this (matrix, gaps, prior, lengths): rebuilt only when they change, so
+    // repeated calls with the same arguments enqueue nothing but the kernel.
+    GbTables& tb = gb_tables(ctx.device);
+    const int W = longest, W1 = W + 1;
+    const int32_t bias = int32_t(std::max<int64_t>(lmaxpen, 1));
+    const int pen_words = int((size_t(A) * A + 3) & ~size_t(3));
+    {
+        std::vector<uint8_t> key;
+        auto put = [&key](const void* p, size_t n) {
+            const auto* b = static_cast<const uint8_t*>(p);
+            key.insert(key.end(), b, b + n);
+        };
+        const int64_t hdr[8] = {A, go, ge, W, bias, int64_t(prior_width), has_prior, 0};
+        put(hdr, sizeof hdr);
+        put(pen.data(), pen.size() * 4);
+        if (has_prior) put(prior, size_t(prior_len) * 4);
+        if (!same_as_last(tb.key, key.data(), key.size())) build_tables(tb, pen, A, go, ge, W, bias,
+                                                                      has_prior ? prior : nullptr,
+                                                                      W1p, stream);
+    }
+    int32_t* d_pen = static_cast<int32_t*>(tb.pen.ptr);
+    int32_t* d_ftab = static_cast<int32_t*>(tb.ftab.ptr);
+    uint32_t* d_prior2 = has_prior ? static_cast<uint32_t*>(tb.prior2.ptr) : nullptr;
+    auto* err = reinterpret_cast<unsigned long long*>(ctx.flags_d + 8);
+    STB_CUDA(cudaMemsetAsync(err, 0, 8, stream));
+
+    FastArgs fa{};
+    fa.pen = d_pen;
+    fa.pen_words = pen_words;
+    fa.A = A;
+    fa.qcodes = qs.d_bytes;
+    fa.qoff = qs.d_off;
+    fa.rcodes = rs.d_bytes;
+    fa.roff = rs.d_off;
+    fa.rlen = rs.d_len;
+    fa.K = K;
+    fa.pairs = static_cast<int2*>(qp.d_pairs.ptr);
+    fa.plen = static_cast<int32_t*>(qp.d_plen.ptr);
+    fa.P = qp.P;
+    fa.ref_sorted = static_cast<int32_t*>(rp.d_sorted.ptr);
+    fa.tasks = static_cast<int4*>(rp.d_tasks.ptr);
+    fa.task_off = static_cast<int32_t*>(rp.d_task_off.ptr);
+    fa.prior2 = d_prior2;
+    fa.ftab = d_ftab;
+    fa.W1 = W1;
+    fa.bias2 = uint32_t(bias) * 0x10001u;
+    fa.out = out_d;
+    fa.err = err;
+
+    const int lq = profile_height(qs.max_len);
+    const size_t smem = size_t(kGP) * lq * kRow * 4 + size_t(kGP) * kRC * 4 +
+                        size_t((W1 * W1 + 3) & ~3) * 4 + size_t(pen_words) * 4 + kRC + 16;
+    const dim3 grid(unsigned(rp.nchunks), unsigned(ceil_div(qp.P, kGP)));
+    if (grid.y > 65535) fail(ST_EINVAL, "seqtree_b200: too many query pairs for one launch");
+    const char* name = dispatch_fast(lq, Lmax, has_prior, fa, grid, smem, stream);
+    note_launch(name);
+    // The timeout flag is read by the caller after its synchronisation point.
+}
+
+}  // namespace stb

@@ -1,0 +1,137 @@
+"""Single-gap-block scoring for anchored loops (CDR3 / junction) -- the dense matrix path.
+
+Mirrors the matrix-facing part of seqtree's ``python/seqtree/gapblock.py``: ``score_matrix``
+(``:512-564``), the gap-prior builders ``central_prior`` (``:79-94``), ``profile_prior``
+(``:97-125``), ``frame_prior`` (``:128-146``), ``positions_prior`` (``:149-185``), ``gap_cost``
+(``:60-76``) and the ``[m][d][i]`` prior cube (``_prior_cube``, ``:492-509``).  The matrix itself
+is computed by the CUDA library.
+
+The score of a pair is a non-negative penalty: the block of length ``d = |len(q) - len(r)|`` is
+placed at whichever of the ``min(len) + 1`` positions minimises substitution cost plus prior,
+plus ``gap_open + (d-1) * gap_extend``; equal lengths score the plain substitution sum.
+"""
+from __future__ import annotations
+
+from collections.abc import Callable, Iterable, Sequence
+
+from ._core import gapblock_matrix as _gapblock_matrix
+from .matrix import ScoreMatrix, SubstitutionMatrix
+
+__all__ = ["score_matrix", "central_prior", "profile_prior", "frame_prior", "positions_prior",
+           "gap_cost", "ScoreMatrix", "UNREACHABLE"]
+
+#: A prior large enough that no layout carrying it wins, small enough not to overflow int32
+#: once a substitution cost is added (python/seqtree/gapblock.py:48-50).
+UNREACHABLE = 1 << 20
+
+#: ``prior(block_start, block_length, longer_length) -> int``; must be >= 0 and 0 at d == 0.
+GapPrior = Callable[[int, int, int], int]
+
+
+def gap_cost(d: int, gap_open: int, gap_extend: int) -> int:
+    """Affine cost of one gap block of length ``d``; ``d == 0`` costs nothing."""
+    if d < 0:
+        raise ValueError("gap length must be >= 0")
+    return 0 if d == 0 else gap_open + (d - 1) * gap_extend
+
+
+def central_prior(lam: int) -> GapPrior:
+    """``lam * |block midpoint - m/2|`` as ``int(lam * |2i + d - m| // 2)``; 0 at d == 0."""
+    if lam < 0:
+        raise ValueError("lam must be >= 0")
+
+    def prior(i: int, d: int, m: int) -> int:
+        return 0 if d == 0 else int(lam * abs(2 * i + d - m) // 2)
+
+    return prior
+
+
+def profile_prior(lam: int, w: Callable[[int, int], float] | Sequence[float]) -> GapPrior:
+    """``int(lam * sum(w(j, m) for j in block))``: lam per unit of positional weight deleted."""
+    if lam < 0:
+        raise ValueError("lam must be >= 0")
+    wfn = w if callable(w) else (lambda j, m: w[j])
+
+    def prior(i: int, d: int, m: int) -> int:
+        return int(lam * sum(wfn(j, m) for j in range(i, i + d)))
+
+    return prior
+
+
+def frame_prior(lam: int, c: int) -> GapPrior:
+    """Pin the block to frame column ``c``: ``lam * |i - c|`` (0 at d == 0)."""
+    if lam < 0:
+        raise ValueError("lam must be >= 0")
+    if c < 0:
+        raise ValueError("c must be >= 0")
+
+    def prior(i: int, d: int, m: int) -> int:
+        return 0 if d == 0 else lam * abs(i - c)
+
+    return prior
+
+
+def positions_prior(starts: Iterable[int]) -> GapPrior:
+    """Allow the block only at ``starts`` (negative = from the end of the shorter sequence,
+    clamped into range); 0 at a permitted start, :data:`UNREACHABLE` elsewhere."""
+    ss = tuple(starts)
+    if not ss:
+        raise ValueError("need at least one start position")
+
+    def prior(i: int, d: int, m: int) -> int:
+        if d == 0:
+            return 0
+        shorter = m - d
+        for p in ss:
+            allowed = min(p, shorter) if p >= 0 else max(0, shorter + p)
+            if i == allowed:
+                return 0
+        return UNREACHABLE
+
+    return prior
+
+
+def _default_gap_open(matrix: SubstitutionMatrix | None) -> int:
+    return 2 * matrix.scale() if matrix is not None else 1
+
+
+def prior_cube(prior: GapPrior, width: int) -> list[int]:
+    """Flatten ``prior`` to ``[m][d][i]`` with stride ``width + 1``.
+
+    Only reachable cells are filled -- ``d >= 1`` and ``i <= m - d`` -- the rest stay zero and
+    are never read.  A negative prior value raises ValueError naming the cell.
+    """
+    w1 = width + 1
+    cube = [0] * (w1 * w1 * w1)
+    for m in range(w1):
+        for d in range(1, m + 1):
+            base = (m * w1 + d) * w1
+            for i in range(m - d + 1):
+                v = int(prior(i, d, m))
+                if v < 0:
+                    raise ValueError(f"gap_prior({i}, {d}, {m}) = {v} is negative")
+                cube[base + i] = v
+    return cube
+
+
+_prior_cube = prior_cube
+
+
+def score_matrix(queries: Sequence[str], refs: Sequence[str],
+                 matrix: SubstitutionMatrix | None = None, gap_open: int | None = None,
+                 gap_extend: int = 1, gap_prior: GapPrior | None = None, alphabet: str = "aa",
+                 threads: int = 0) -> ScoreMatrix:
+    """Gap-block penalty of every query against every reference, on the GPU.
+
+    ``gap_open`` defaults to ``2 * matrix.scale()`` (1 for unit cost).  ``gap_prior`` is
+    materialised once into a lookup cube.  Returns a (len(queries), len(refs)) int32
+    :class:`ScoreMatrix`; ``numpy.asarray`` wraps it without copying.
+    """
+    q, r = list(queries), list(refs)
+    if gap_open is None:
+        gap_open = _default_gap_open(matrix)
+    if gap_open < 0 or gap_extend < 0:
+        raise ValueError("gap_open and gap_extend must be >= 0")
+    width = max((len(s) for s in q + r), default=0)
+    cube = prior_cube(gap_prior, width) if gap_prior is not None else []
+    return _gapblock_matrix(q, r, alphabet, matrix, gap_open, gap_extend, cube, width, threads)

@@ -1,0 +1,166 @@
+"""Gap-block score_matrix on the GPU, bit-exact against the reference's C++ (golden vectors) and
+the CPU oracle, mirroring python/seqtree tests/test_gapblock.py:479-557."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import as_np, cdr3, prior_by_name, rand_seqs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def st(cuda_ready):
+    import seqtree_b200
+    return seqtree_b200
+
+
+def _mat(st, name):
+    return None if name is None else getattr(st.SubstitutionMatrix, name)()
+
+
+def _oracle_gapblock(st, q, r, matrix, go, ge, prior, alphabet="aa"):
+    width = max(map(len, q + r), default=0)
+    cube = st.gapblock.prior_cube(prior, width) if prior else None
+    A = {"aa": 24, "nt": 4, "iupac": 15}[alphabet]
+    pen = matrix.penalty_grid if matrix is not None else oracle.penalty_from_similarity(None, A)
+    return oracle.gapblock_matrix(q, r, pen, alphabet=alphabet, gap_open=go, gap_extend=ge,
+                                  prior=cube, prior_width=width, threads=os.cpu_count() or 1)
+
+
+def test_golden_vectors(st, golden_gapblock):
+    for case in golden_gapblock:
+        sm = st.score_matrix(case["queries"], case["refs"], _mat(st, case["matrix"]),
+                             gap_open=case["gap_open"], gap_extend=case["gap_extend"],
+                             gap_prior=prior_by_name(case["prior"]), alphabet=case["alphabet"])
+        assert as_np(sm).tolist() == case["expected"], case["name"]
+
+
+@pytest.mark.parametrize("prior", ["none", "central21", "frame21_5", "positions", "profile21"])
+def test_is_a_valid_ball(st, prior):
+    rng = np.random.default_rng(11)
+    seqs = rand_seqs(rng, 30, 4, 20)
+    D = as_np(st.score_matrix(seqs, seqs, st.SubstitutionMatrix.blosum62(), gap_open=28,
+                              gap_prior=prior_by_name(prior)))
+    assert (np.diagonal(D) == 0).all() and (D >= 0).all() and (D == D.T).all()
+
+
+@pytest.mark.parametrize("matrix", ["blosum62", "structural", "pam250"])
+@pytest.mark.parametrize("prior", ["none", "central21", "positions"])
+def test_junction_shapes_against_the_oracle(st, matrix, prior):
+    """Uneven CDR3-like sets (odd counts, K not a multiple of 4, many length groups)."""
+    rng = np.random.default_rng(hash((matrix, prior)) & 0xFFFF)
+    q = cdr3(rng, 131, 8, 25)
+    r = cdr3(rng, 1029, 8, 25)
+    m = _mat(st, matrix)
+    got = as_np(st.score_matrix(q, r, m, gap_open=8, gap_prior=prior_by_name(prior)))
+    exp = _oracle_gapblock(st, q, r, m, 8, 1, prior_by_name(prior))
+    assert np.array_equal(got, exp)
+
+
+def test_general_path_long_sequences_and_big_penalties(st):
+    rng = np.random.default_rng(3)
+    q = rand_seqs(rng, 17, 1, 150)
+    r = rand_seqs(rng, 23, 1, 150)
+    m = st.SubstitutionMatrix.blosum62()
+    for prior in (None, prior_by_name("central21")):
+        got = as_np(st.score_matrix(q, r, m, gap_open=28, gap_prior=prior))
+        assert np.array_equal(got, _oracle_gapblock(st, q, r, m, 28, 1, prior))
+    big = st.SubstitutionMatrix.from_similarity((np.eye(24, dtype=np.int64) * 5000).tolist())
+    q = cdr3(rng, 9)
+    r = cdr3(rng, 11)
+    got = as_np(st.score_matrix(q, r, big, gap_open=3))
+    assert np.array_equal(got, _oracle_gapblock(st, q, r, big, 3, 1, None))
+
+
+def test_unit_cost_and_alphabets(st):
+    rng = np.random.default_rng(5)
+    q = rand_seqs(rng, 33, 0, 30, "ACGTacgt")
+    r = rand_seqs(rng, 41, 0, 30, "ACGT")
+    got = as_np(st.score_matrix(q, r, None, gap_open=1, alphabet="nt"))
+    assert np.array_equal(got, _oracle_gapblock(st, q, r, None, 1, 1, None, "nt"))
+    sm = st.score_matrix(["ACGT", "ACTT"], ["ACGT"], None, gap_open=1)
+    assert sm[0, 0] == 0 and sm[1, 0] == 1
+
+
+def test_full_size_workload_against_the_oracle(st):
+    """1,000 x 10,000 CDR3 junctions, BLOSUM62, gap_open 8, central prior -- every cell."""
+    q = cdr3(np.random.default_rng(1), 1000)
+    r = cdr3(np.random.default_rng(0), 10000)
+    m = st.SubstitutionMatrix.blosum62()
+    prior = prior_by_name("central21")
+    got = as_np(st.score_matrix(q, r, m, gap_open=8, gap_prior=prior))
+    if oracle.ref_available():
+        width = max(map(len, q + r))
+        exp = oracle.ref_gapblock_matrix(q, r, matrix="blosum62", gap_open=8,
+                                         prior=st.gapblock.prior_cube(prior, width),
+                                         prior_width=width)
+    else:
+        exp = _oracle_gapblock(st, q, r, m, 8, 1, prior)
+    assert np.array_equal(got, exp)
+
+
+def test_threads_argument_is_ignored(st):
+    rng = np.random.default_rng(13)
+    q, r = rand_seqs(rng, 64, 6, 18), rand_seqs(rng, 40, 6, 18)
+    m = st.SubstitutionMatrix.blosum62()
+    ref = as_np(st.score_matrix(q, r, m, 28, 1, prior_by_name("central21"), threads=1))
+    for t in (2, 4, 0):
+        assert np.array_equal(as_np(st.score_matrix(q, r, m, 28, 1, prior_by_name("central21"),
+                                                    threads=t)), ref)
+
+
+def test_buffer_and_indexing(st):
+    m = st.SubstitutionMatrix.blosum62()
+    sm = st.score_matrix(["CASSL", "CASL"], ["CASSL"], m, 28)
+    mv = memoryview(sm)
+    assert mv.format == "i" and mv.shape == (2, 1) and mv.c_contiguous
+    assert mv[0, 0] == 0 and mv[1, 0] == sm[1, 0] > 0
+    sm = st.score_matrix(["CASSL", "CASL", "CAS"], ["CASSL", "CASSY"], m, 28)
+    for i in range(3):
+        assert sm.row(i) == [sm[i, 0], sm[i, 1]]
+    with pytest.raises(IndexError):
+        sm.row(3)
+    assert st.score_matrix([], ["ACGT"]).shape == (0, 1)
+    assert st.score_matrix(["ACGT"], []).shape == (1, 0)
+
+
+def test_bad_input_raises(st):
+    m = st.SubstitutionMatrix.blosum62()
+    with pytest.raises(ValueError):
+        st.score_matrix(["CAS"], ["CAS"], m, gap_open=-1)
+    with pytest.raises(ValueError, match="negative"):
+        st.score_matrix(["CAS"], ["CA"], m, 28, gap_prior=lambda i, d, m_: -1)
+    with pytest.raises(ValueError, match="alphabet"):
+        st.score_matrix(["CAS#"], ["CASS"], m, 28)
+    with pytest.raises(ValueError, match="symbol 'J'"):
+        st.score_matrix(["CASS"], ["CAJS", "CAS#"], m, 28)
+    from seqtree_b200 import _core
+    with pytest.raises(ValueError, match=r"\(prior_width \+ 1\)\^3"):
+        _core.gapblock_matrix(["CAS"], ["CA"], "aa", m, 8, 1, [0] * 7, 3)
+    with pytest.raises(ValueError, match="longer than the prior"):
+        _core.gapblock_matrix(["CASSS"], ["CA"], "aa", m, 8, 1, [0] * 64, 3)
+
+
+def test_device_sets_match_host_calls(st):
+    import torch
+    from seqtree_b200 import device
+    rng = np.random.default_rng(17)
+    q, r = cdr3(rng, 77), cdr3(rng, 515)
+    m = st.SubstitutionMatrix.blosum62()
+    prior = prior_by_name("central21")
+    host = as_np(st.score_matrix(q, r, m, gap_open=8, gap_prior=prior))
+    qs, rs = device.SeqSet(q), device.SeqSet(r)
+    width = max(map(len, q + r))
+    out = torch.empty((len(q), len(r)), dtype=torch.int32, device="cuda")
+    for _ in range(2):  # second call reuses the cached plans
+        out.fill_(-1)
+        device.gapblock_into(qs, rs, out.data_ptr(), torch.cuda.current_stream().cuda_stream,
+                             matrix=m, gap_open=8, prior=st.gapblock.prior_cube(prior, width),
+                             prior_width=width)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), host)

@@ -1,0 +1,107 @@
+"""Host-side logic of the Python mirror: priors and the prior cube, matrices, the result
+buffer, argument parsing and packing.  No device needed."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from seqtree_b200 import _lib
+from seqtree_b200.gapblock import (UNREACHABLE, central_prior, frame_prior, gap_cost,
+                                   positions_prior, prior_cube, profile_prior)
+from seqtree_b200.matrix import (ScoreMatrix, SubstitutionMatrix, alphabet_symbols, amino_acids,
+                                 parse_align_mode, parse_alphabet)
+
+
+def test_alphabet_and_mode_names():
+    assert [parse_alphabet(a) for a in ("aa", "AMINO", "protein", "nt", "dna", "nucleotide",
+                                        "iupac", "nt_iupac")] == [0, 0, 0, 1, 1, 1, 2, 2]
+    with pytest.raises(ValueError, match="unknown alphabet"):
+        parse_alphabet("rna")
+    assert [parse_align_mode(m) for m in ("global", "NW", "needleman-wunsch", "local", "sw",
+                                          "Smith-Waterman")] == [0, 0, 0, 1, 1, 1]
+    with pytest.raises(ValueError, match="mode"):
+        parse_align_mode("semiglobal")
+    assert amino_acids() == "ARNDCQEGHILKMFPSTWYVBZX*" and alphabet_symbols("nt") == "ACGT"
+
+
+def test_prior_cube_layout_and_checks():
+    cp = central_prior(21)
+    cube = prior_cube(cp, 6)
+    w1 = 7
+    for m in range(w1):
+        for d in range(1, m + 1):
+            for i in range(m - d + 1):
+                assert cube[(m * w1 + d) * w1 + i] == cp(i, d, m)
+    assert all(cube[(m * w1) * w1 + i] == 0 for m in range(w1) for i in range(w1))
+    with pytest.raises(ValueError, match="negative"):
+        prior_cube(lambda i, d, m: -1, 3)
+    with pytest.raises(ValueError):
+        central_prior(-1)
+    with pytest.raises(ValueError):
+        frame_prior(1, -1)
+    with pytest.raises(ValueError):
+        positions_prior(())
+    assert profile_prior(10, [0.5] * 8)(1, 2, 8) == 10
+    assert positions_prior((2,))(0, 1, 5) == UNREACHABLE
+    assert gap_cost(2, 8, 1) == 9
+
+
+def test_priors_vanish_without_a_gap():
+    for p in (central_prior(20), frame_prior(21, 5), positions_prior((3, 4, -4, -3)),
+              profile_prior(21, lambda j, m: 1.0)):
+        for m in range(1, 12):
+            assert p(0, 0, m) == 0
+
+
+def test_substitution_matrix_views_and_errors():
+    m = SubstitutionMatrix.blosum62()
+    assert m.size() == 24 and m.similarity("A", "K") < 0 < m.penalty("A", "K")
+    assert m.penalty("W", "W") == m.penalty("C", "C") == 0
+    with pytest.raises(ValueError):
+        m.penalty("AA", "A")
+    with pytest.raises(ValueError, match="unknown amino acid"):
+        m.penalty("J", "A")
+    small = SubstitutionMatrix.unit(4)
+    with pytest.raises(ValueError, match="out of range"):
+        small.similarity("C", "G")  # index 4 in the amino-acid order
+    with pytest.raises(ValueError, match="square"):
+        SubstitutionMatrix.from_similarity([[1, 2], [3]])
+    with pytest.raises(ValueError):
+        SubstitutionMatrix.from_similarity([])
+    c = SubstitutionMatrix.from_similarity([[5, -1], [-1, 3]])
+    assert c.penalty_grid.tolist() == [[0, 10], [10, 0]]
+    assert SubstitutionMatrix.unit(1).scale() == 0
+
+
+def test_score_matrix_buffer_protocol_and_indexing():
+    a = np.arange(6, dtype=np.int32).reshape(2, 3)
+    sm = ScoreMatrix(a)
+    mv = memoryview(sm)
+    assert mv.format == "i" and mv.shape == (2, 3) and mv.c_contiguous and mv.readonly
+    assert np.asarray(sm).tolist() == a.tolist()
+    assert sm.shape == (2, 3) and len(sm) == 2 and sm[1, 2] == 5 and sm.row(0) == [0, 1, 2]
+    with pytest.raises(IndexError):
+        sm.row(2)
+    with pytest.raises(IndexError):
+        sm[2, 0]
+    with pytest.raises(IndexError):
+        sm[0, 3]
+    assert repr(sm) == "ScoreMatrix(2, 3)"
+
+
+def test_packing_offsets_and_utf8():
+    p = _lib.Packed(["CASS", "", "AB"])
+    assert p.offsets.tolist() == [0, 4, 4, 6] and bytes(p.data[:6]) == b"CASSAB"
+    p = _lib.Packed(["é", "ab"])  # byte lengths, as the reference's std::string sees them
+    assert p.offsets.tolist() == [0, 2, 4]
+    with pytest.raises(TypeError):
+        _lib.Packed([1, 2])
+
+
+def test_pinned_results_are_plain_int32_arrays():
+    a = _lib.pinned_int32(3, 4)
+    assert a.shape == (3, 4) and a.dtype == np.int32 and a.flags.c_contiguous
+    a[:] = 7
+    v = a[1:]
+    del a
+    assert int(v.sum()) == 7 * 8

@@ -1,0 +1,128 @@
+"""Gotoh NW / SW score and distance matrices on the GPU, mirroring the invariant and known-answer
+tests of the reference's tests/test_pairwise.py (its BioPython comparisons are replaced by the
+reference's own C++ through the golden vectors)."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import as_np, rand_seqs
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pw(cuda_ready):
+    from seqtree_b200 import pairwise
+    return pairwise
+
+
+@pytest.fixture(scope="module")
+def B62(cuda_ready):
+    from seqtree_b200 import SubstitutionMatrix
+    return SubstitutionMatrix.blosum62()
+
+
+def test_golden_vectors(pw, golden_align):
+    from seqtree_b200 import SubstitutionMatrix
+    for case in golden_align:
+        m = getattr(SubstitutionMatrix, case["matrix"])()
+        fn = pw.dist_matrix if case["dist"] else pw.score_matrix
+        if case["overflow"]:
+            with pytest.raises(OverflowError, match="distance" if case["dist"] else "score"):
+                fn(case["queries"], case["refs"], m, mode=case["mode"], gap_open=case["gap_open"],
+                   gap_extend=case["gap_extend"])
+            continue
+        got = as_np(fn(case["queries"], case["refs"], m, mode=case["mode"],
+                       gap_open=case["gap_open"], gap_extend=case["gap_extend"]))
+        assert got.tolist() == case["expected"], case["name"]
+
+
+def test_known_answers(pw, B62):
+    assert pw.score("CASSLGQAYEQYF", "CASSPGQAYEQF", B62) == 45
+    assert pw.score("CASSLGQAYEQYF", "CASSPGQAYEQF", B62, gap_open=12) == 44
+    for L in (1, 2, 3, 5):
+        assert pw.score("AAA", "AAA" + "A" * L, B62) == 12 - (11 + (L - 1))
+    for L in (1, 2, 3):
+        assert pw.score("AAA", "AAA" + "A" * L, B62, gap_open=5, gap_extend=5) == 12 - 5 * L
+    assert pw.score("AAA", "KKAAA", B62) == 0
+    assert pw.score("WWW", "KKK", B62, mode="local") == 0
+    assert pw.score("WWWAAAWWW", "KKKAAAKKK", B62, mode="local") == 12
+    assert pw.score("WWWAAAWWW", "KKKAAAKKK", B62, mode="global") < 0
+    s = "CASSLGQAYEQYF"
+    assert pw.score(s, s, B62, mode="local") == pw.score(s, s, B62, mode="global")
+
+
+def test_huge_gaps_do_not_wrap(pw, B62):
+    q, r = "CASSLGQAYEQYF", "CASSPGQAYEQF"
+    assert pw.score(q, r, B62, gap_open=10 ** 8) == -99_999_944
+    assert pw.score(q, r, B62, gap_open=2 ** 30) == -1_073_741_768
+    assert pw.score(q, r, B62, gap_open=2 ** 31 - 1) == -2_147_483_591
+
+
+def test_overflow_is_refused(pw, B62):
+    with pytest.raises(OverflowError, match="32 bits"):
+        pw.score("A" * 400, "W" * 600, B62, gap_open=2 ** 31 - 1, gap_extend=2 ** 31 - 1)
+    for threads in (1, 0, 4):
+        with pytest.raises(OverflowError):
+            pw.score_matrix(["A" * 100], ["C"], B62, gap_open=10 ** 8, gap_extend=10 ** 8,
+                            threads=threads)
+        with pytest.raises(OverflowError):
+            pw.dist_matrix(["A" * 100], ["C"], B62, gap_open=10 ** 8, gap_extend=10 ** 8,
+                           threads=threads)
+    with pytest.raises(OverflowError, match="distance"):
+        pw.dist_matrix(["AAA"], ["C"], B62, gap_open=2 ** 31 - 1, gap_extend=2 ** 31 - 1)
+
+
+def test_dist_is_a_distance_and_equals_the_gram_transform(pw, B62):
+    rng = np.random.default_rng(19)
+    seqs = rand_seqs(rng, 15, 10, 20)
+    D = as_np(pw.dist_matrix(seqs, seqs, B62))
+    assert (np.diagonal(D) == 0).all() and (D >= 0).all() and (D == D.T).all()
+    q, r = rand_seqs(rng, 6, 8, 16), rand_seqs(rng, 5, 8, 16)
+    D = as_np(pw.dist_matrix(q, r, B62))
+    for i, a in enumerate(q):
+        for j, b in enumerate(r):
+            assert D[i, j] == pw.score(a, a, B62) + pw.score(b, b, B62) - 2 * pw.score(a, b, B62)
+
+
+@pytest.mark.parametrize("mode", ["global", "local"])
+@pytest.mark.parametrize("go,ge", [(11, 1), (5, 5), (1, 3), (0, 0), (1, 10)])
+def test_against_oracle(pw, B62, mode, go, ge):
+    rng = np.random.default_rng(hash((mode, go, ge)) & 0xFFFF)
+    q, r = rand_seqs(rng, 23, 1, 40), rand_seqs(rng, 67, 1, 40)
+    for dist in (False, True):
+        fn = pw.dist_matrix if dist else pw.score_matrix
+        got = as_np(fn(q, r, B62, mode=mode, gap_open=go, gap_extend=ge))
+        exp = oracle.align_matrix(q, r, B62.similarity_grid, mode=mode, gap_open=go,
+                                  gap_extend=ge, dist=dist, threads=os.cpu_count() or 1)
+        assert np.array_equal(got, exp)
+
+
+@pytest.mark.parametrize("mode", ["global", "local"])
+def test_protein_lengths_against_oracle(pw, B62, mode):
+    """Log-normal protein lengths (median 180, clipped 50-500), a block of the workload."""
+    rng = np.random.default_rng(2)
+    lens = np.clip(np.round(rng.lognormal(np.log(180), 0.5, size=40)), 50, 500).astype(int)
+    seqs = ["".join(rng.choice(list("ACDEFGHIKLMNPQRSTVWY"), size=int(L))) for L in lens]
+    q, r = seqs[:16], seqs[16:]
+    got = as_np(pw.dist_matrix(q, r, B62, mode=mode))
+    exp = oracle.align_matrix(q, r, B62.similarity_grid, mode=mode, dist=True,
+                              threads=os.cpu_count() or 1)
+    assert np.array_equal(got, exp)
+
+
+def test_bad_arguments_raise(pw, B62):
+    with pytest.raises(ValueError, match="gap_open"):
+        pw.score("AA", "AA", B62, gap_open=-1)
+    with pytest.raises(ValueError, match="mode"):
+        pw.score("AA", "AA", B62, mode="semiglobal")
+    with pytest.raises(ValueError, match="alphabet|symbol"):
+        pw.score("AA#", "AA", B62)
+    assert pw.score_matrix([], ["A"], B62).shape == (0, 1)
+    assert pw.score("", "", B62) == 0
+    assert pw.score("", "AAA", B62) == -(11 + 2)
+    assert pw.score("", "AAA", B62, mode="local") == 0
