@@ -319,25 +319,27 @@ def main_ours(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
     B62 = stb.SubstitutionMatrix.blosum62()
 
+    cur = lambda: torch.cuda.current_stream().cuda_stream  # noqa: E731  (capture-aware)
     if w["kind"] == "gapblock":
         width = max(map(len, q + r))
-        cube = prior_cube(central_prior(21), width)
+        prior = central_prior(21)
+        cube = np.asarray(prior_cube(prior, width), dtype=np.int32)
         qs, rs = device.SeqSet(q, "aa"), device.SeqSet(r, "aa")
 
         def step():
-            device.gapblock_into(qs, rs, out.data_ptr(), stream.cuda_stream, matrix=B62,
+            device.gapblock_into(qs, rs, out.data_ptr(), cur(), matrix=B62,
                                  gap_open=8, gap_extend=1, prior=cube, prior_width=width)
 
         def e2e_call():
             return stb.gapblock.score_matrix(q, r, B62, gap_open=8, gap_extend=1,
-                                             gap_prior=central_prior(21))
+                                             gap_prior=prior)
     elif w["kind"] in ("hamming", "levenshtein"):
         qs, rs = device.SeqSet(q, None), device.SeqSet(r, None)
         into = device.hamming_into if w["kind"] == "hamming" else device.levenshtein_into
         api = stb.distance.hamming_matrix if w["kind"] == "hamming" else stb.distance.levenshtein_matrix
 
         def step():
-            into(qs, rs, out.data_ptr(), stream.cuda_stream)
+            into(qs, rs, out.data_ptr(), cur())
 
         def e2e_call():
             return api(q, r)
@@ -345,18 +347,37 @@ def main_ours(args):
         qs, rs = device.SeqSet(q, "aa"), device.SeqSet(r, "aa")
 
         def step():
-            device.align_into(qs, rs, out.data_ptr(), stream.cuda_stream, matrix=B62,
+            device.align_into(qs, rs, out.data_ptr(), cur(), matrix=B62,
                               mode=w["mode"], gap_open=11, gap_extend=1, dist=True)
 
         def e2e_call():
             return stb.pairwise.dist_matrix(q, r, B62, mode=w["mode"])
 
-    # warm-up (plans, workspace, module load)
-    for _ in range(max(args.warmup, 3) if args.warmup >= 3 else args.warmup):
+    # warm-up (plans, workspace, module load), then capture one step in a CUDA graph so the
+    # timed replays measure the device work alone (no host enqueue gaps inside the events)
+    for _ in range(max(args.warmup, 1)):
         step()
     torch.cuda.synchronize()
     launches = _lib.last_launch_count()
     kernel_name = _lib.last_kernel_name()
+    graph = None
+    if not args.no_graph:
+        try:
+            side = torch.cuda.Stream()
+            side.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(side):
+                step()
+            torch.cuda.current_stream().wait_stream(side)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph):
+                step()
+            torch.cuda.synchronize()
+            run_step = graph.replay
+        except Exception as e:  # not capturable on this path: time eager launches
+            graph = None
+            print(f"[bench] graph capture failed ({e}); timing eager launches", file=sys.stderr)
+    if graph is None:
+        run_step = step
 
     def barrier():
         if world > 1:
@@ -372,7 +393,7 @@ def main_ours(args):
         for i in range(args.steps):
             flush.zero_()  # evict the previous step's output from L2 (outside the events)
             ev[i][0].record(stream)
-            step()
+            run_step()
             ev[i][1].record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -424,6 +445,7 @@ def main_ours(args):
         "e2e": e2e,
         "gpu_launches": launches * args.steps,
         "kernel": kernel_name,
+        "cuda_graph": graph is not None,
         "clocks": sampler.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
@@ -449,6 +471,7 @@ def main(argv=None) -> int:
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="time eager launches instead")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return main_reference(args)

@@ -17,6 +17,7 @@
 //   or more than 64 distinct symbols, take a one-thread-per-pair DP with its row in global
 //   scratch (any length).
 #include <algorithm>
+#include <map>
 
 #include "common.cuh"
 
@@ -54,8 +55,28 @@ __global__ void presence_kernel(const uint8_t* __restrict__ bytes, int64_t n,
     if (threadIdx.x < 8 && s[threadIdx.x]) atomicOr(&present[threadIdx.x], s[threadIdx.x]);
 }
 
-int compute_codes(st_seqset_s& a, st_seqset_s& b, cudaStream_t stream, Context& ctx,
-                  uint8_t** a_codes, uint8_t** b_codes) {
+// Dense codes of a (set, set) pair, cached by the sets' uids so that repeated calls on
+// device-resident sets enqueue no host round trip (and can be captured in a CUDA graph).
+struct DistCache {
+    uint64_t a_uid = 0, b_uid = 0;
+    int sigma = 0;
+    DevBuf ac, bc;             // codes of a and b
+    int packB = 0, packW = 0;  // Hamming packing built for (bits, words); 0 = none
+    DevBuf qp, rp;             // packed words
+};
+
+DistCache& dist_cache(int device) {
+    static std::mutex mu;
+    static std::map<int, std::unique_ptr<DistCache>> all;
+    std::lock_guard<std::mutex> lk(mu);
+    auto& p = all[device];
+    if (!p) p = std::make_unique<DistCache>();
+    return *p;
+}
+
+DistCache& compute_codes(st_seqset_s& a, st_seqset_s& b, cudaStream_t stream, Context& ctx) {
+    DistCache& dc = dist_cache(ctx.device);
+    if (dc.a_uid == a.uid && dc.b_uid == b.uid && a.uid != 0) return dc;
     auto* present = reinterpret_cast<unsigned int*>(ctx.flags_d + 16);
     STB_CUDA(cudaMemsetAsync(present, 0, 32, stream));
     for (st_seqset_s* s : {&a, &b}) {
@@ -73,8 +94,7 @@ int compute_codes(st_seqset_s& a, st_seqset_s& b, cudaStream_t stream, Context& 
     int sigma = 0;
     for (int c = 0; c < 256; ++c)
         if (bits[c >> 5] & (1u << (c & 31))) lut.v[c] = uint8_t(sigma++);
-    DevBuf* bufs[2] = {&ctx.q_codes, &ctx.r_codes};
-    uint8_t** outs[2] = {a_codes, b_codes};
+    DevBuf* bufs[2] = {&dc.ac, &dc.bc};
     st_seqset_s* sets[2] = {&a, &b};
     for (int t = 0; t < 2; ++t) {
         st_seqset_s* s = sets[t];
@@ -86,9 +106,12 @@ int compute_codes(st_seqset_s& a, st_seqset_s& b, cudaStream_t stream, Context& 
             STB_CUDA(cudaGetLastError());
             note_launch(nullptr);
         }
-        *outs[t] = dst;
     }
-    return sigma;
+    dc.sigma = sigma;
+    dc.a_uid = a.uid;
+    dc.b_uid = b.uid;
+    dc.packB = dc.packW = 0;
+    return dc;
 }
 
 // ---------------------------------------------------------------------------- Hamming -------
@@ -313,18 +336,24 @@ void hamming_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream_t s
                             std::to_string(a.h_len[size_t(bi)]) + " and " +
                             std::to_string(b.h_len[size_t(bk)]) + ")");
     Context& ctx = context();
-    uint8_t *ac = nullptr, *bc = nullptr;
-    const int sigma = compute_codes(a, b, stream, ctx, &ac, &bc);
+    DistCache& dc = compute_codes(a, b, stream, ctx);
+    const int sigma = dc.sigma;
     const int B = sigma <= 2 ? 1 : sigma <= 4 ? 2 : sigma <= 16 ? 4 : 8;
     const int per = 32 / B;
     const int W = std::max(1, int(ceil_div(L, per)));
-    uint32_t* qp = ctx.work_a.as<uint32_t>(size_t(N) * W);
-    uint32_t* rp = ctx.work_b.as<uint32_t>(size_t(K) * W);
-    pack_kernel<<<unsigned(ceil_div(N, 256)), 256, 0, stream>>>(ac, a.d_off, N, L, B, W, qp);
-    STB_CUDA(cudaGetLastError());
-    pack_kernel<<<unsigned(ceil_div(K, 256)), 256, 0, stream>>>(bc, b.d_off, K, L, B, W, rp);
-    STB_CUDA(cudaGetLastError());
-    note_launch(nullptr, 2);
+    uint32_t* qp = dc.qp.as<uint32_t>(size_t(N) * W);
+    uint32_t* rp = dc.rp.as<uint32_t>(size_t(K) * W);
+    if (dc.packB != B || dc.packW != W) {
+        const uint8_t* ac = static_cast<uint8_t*>(dc.ac.ptr);
+        const uint8_t* bc = static_cast<uint8_t*>(dc.bc.ptr);
+        pack_kernel<<<unsigned(ceil_div(N, 256)), 256, 0, stream>>>(ac, a.d_off, N, L, B, W, qp);
+        STB_CUDA(cudaGetLastError());
+        pack_kernel<<<unsigned(ceil_div(K, 256)), 256, 0, stream>>>(bc, b.d_off, K, L, B, W, rp);
+        STB_CUDA(cudaGetLastError());
+        note_launch(nullptr, 2);
+        dc.packB = B;
+        dc.packW = W;
+    }
     const char* name;
     switch (B) {
         case 1: name = launch_hamming<1>(qp, rp, N, K, W, out_d, stream, ctx.num_sms); break;
@@ -341,8 +370,10 @@ void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream
     const int64_t N = a.count, K = b.count;
     if (N == 0 || K == 0) return;
     Context& ctx = context();
-    uint8_t *ac = nullptr, *bc = nullptr;
-    const int sigma = std::max(1, compute_codes(a, b, stream, ctx, &ac, &bc));
+    DistCache& dc = compute_codes(a, b, stream, ctx);
+    const int sigma = std::max(1, dc.sigma);
+    const uint8_t* ac = static_cast<uint8_t*>(dc.ac.ptr);
+    const uint8_t* bc = static_cast<uint8_t*>(dc.bc.ptr);
     const dim3 grid(unsigned(ceil_div(K, kLevWarps * 32)), unsigned(ceil_div(N, kLevRows)));
     if (b.max_len <= 64 && sigma <= 64 && grid.y <= 65535) {
         const size_t smem = size_t(kLevWarps) * sigma * 32 * 8;

@@ -10,12 +10,23 @@
 // result is the same integer as the reference's (integer sums, no reassociation hazard while
 // the reference itself does not overflow int32).
 //
-// Fast path (every length <= 64, L*max_pen <= 8191): two queries of equal length share a
-// warp-uniform row of a (q1, q2, r) pair table in shared memory, so one 32-bit LDS returns the
-// two penalties as int16x2 and one DPX __viaddmin_s16x2 keeps both running minima.  Refs of a
-// 1024-column chunk are processed in groups of equal length (d, L and the prior row are then
-// warp-uniform and the table row read is bank-conflict free); results go through a shared
-// tile so that global stores stay coalesced in the original column order.
+// Fast path (every length <= 64, min(m,n) <= 32, L*max_pen <= 8191):
+//   * Queries are sorted by length and paired; the penalties of a pair against one ref residue
+//     travel as int16x2.  A query profile QP[pair][j][b] = pen(q1[j], b) | pen(q2[j], b) << 16
+//     (32 words per row: one pass over the banks) is built once per call in global memory.
+//   * Refs are cut into chunks of RC columns (original order); inside a chunk they are grouped
+//     by length into warp tasks of <= 32 refs, so d, L and the prior row are warp-uniform.  The
+//     refs' codes are laid out per task as [j][lane] bytes holding 4*code (a byte offset into a
+//     profile row), also once per call.
+//   * A CTA owns (chunk, 8 query pairs).  Two bulk (TMA) copies stage its 8-pair profile slab
+//     and the chunk's code slab into shared memory, completing on one mbarrier.  A warp unit is
+//     (task, slice of 4 pairs of one length); the 4 pairs are swept together, and every lookup
+//     is LDS [lane register + compile-time immediate]: the register is the residue's byte offset
+//     and the immediate ((slice*4 + pair)*LQ + j)*128.  Both penalties of two pairs arrive in
+//     one LDS, the running sums are plain 32-bit adds on halves kept in [0, 2^15), and one DPX
+//     __viaddmin_s16x2 updates both running minima.
+//   * Results go through a shared tile so that global stores are coalesced 16-byte vectors in
+//     the original column order; the per-(m,n) term (prior minimum + gap cost) is added there.
 // General path: one thread per pair in int32 for any lengths and penalty magnitudes.
 #include <algorithm>
 #include <map>
@@ -27,39 +38,42 @@ namespace stb {
 
 namespace {
 
-constexpr int kRC = 1024;    // refs per chunk (columns of one CTA tile)
-constexpr int kGP = 8;       // query pairs per CTA (rows of one CTA tile = 16)
+constexpr int kGP = 8;          // query pairs per CTA (tile rows = 16 queries)
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
+constexpr int kRow = 32;        // words per profile row
+constexpr int kPairsPerSlice = 4;
 
 // ---------------------------------------------------------------------------- plans ---------
-// Launch plans depend only on the lengths of a set, so a device-resident set builds them once;
-// transient sets (host-buffer calls) rebuild them in place inside the context's plan objects,
-// whose device buffers only grow.
+// Plans depend only on the lengths (and codes) of a set, so a device-resident set builds them
+// once; transient sets (host-buffer calls) rebuild them in place inside the context's plan
+// objects, whose device buffers only grow.
 struct QueryPlan {
     uint64_t uid = 0;                    // set the plan was built for
-    int64_t P = 0;                       // query pairs
-    std::vector<int2> pairs;             // original indices (second may be -1)
+    int64_t P = 0;                       // query pairs, a multiple of 4
+    std::vector<int2> pairs;             // original indices (-1 marks an empty slot)
     std::vector<int32_t> plen;           // m of each pair
     DevBuf d_pairs, d_plen;
+    std::vector<uint8_t> prof_key;       // (A, LQ, penalty grid) the profile was built for
+    DevBuf d_prof;                       // [P][LQ][32] uint32
 };
 
 struct RefPlan {
     uint64_t uid = 0;
+    int rc = 0;                          // columns per chunk
     int64_t nchunks = 0;
     int64_t ntasks = 0;
+    int64_t max_slab = 0;                // largest per-chunk code slab (bytes)
     std::vector<int32_t> sorted;
-    std::vector<int4> tasks;
-    std::vector<int32_t> task_off;
-    DevBuf d_sorted;                     // global ref index, sorted by length inside each chunk
-    DevBuf d_tasks;                      // int4 (n, start in sorted, count <= 32, chunk)
-    DevBuf d_task_off;                   // nchunks + 1
+    std::vector<int4> tasks;             // (n, start in sorted, count <= 32, slab byte offset)
+    std::vector<int32_t> task_off;       // nchunks + 1
+    DevBuf d_sorted, d_tasks, d_task_off;
+    DevBuf d_slab;                       // per task: n rows of 32 bytes (4*code per lane)
 };
 
 // Queries sorted by length (stable) and paired within each length; an odd one out is paired
-// with a dummy (-1).  Each length's pairs are padded with dummy pairs (-1, -1) to a multiple
-// of 4, so that every slice of 4 consecutive pairs has one length.  Dummy results are never
-// stored.
+// with -1.  Each length's pairs are padded with (-1, -1) to a multiple of 4, so that every slice
+// of 4 consecutive pairs has one length.  Empty slots are computed and never stored.
 void build_query_plan(QueryPlan& plan, const st_seqset_s& q, cudaStream_t stream) {
     const int64_t N = q.count;
     std::vector<int32_t> order(static_cast<size_t>(N));
@@ -75,7 +89,7 @@ void build_query_plan(QueryPlan& plan, const st_seqset_s& q, cudaStream_t stream
         const size_t first = plan.pairs.size();
         for (int64_t t = i; t < e; t += 2)
             plan.pairs.push_back(make_int2(order[size_t(t)], t + 1 < e ? order[size_t(t + 1)] : -1));
-        while ((plan.pairs.size() - first) % 4) plan.pairs.push_back(make_int2(-1, -1));
+        while ((plan.pairs.size() - first) % kPairsPerSlice) plan.pairs.push_back(make_int2(-1, -1));
         plan.plen.resize(plan.pairs.size(), m);
         i = e;
     }
@@ -84,34 +98,44 @@ void build_query_plan(QueryPlan& plan, const st_seqset_s& q, cudaStream_t stream
                              sizeof(int2) * size_t(plan.P), cudaMemcpyHostToDevice, stream));
     STB_CUDA(cudaMemcpyAsync(plan.d_plen.as<int32_t>(size_t(plan.P)), plan.plen.data(),
                              sizeof(int32_t) * size_t(plan.P), cudaMemcpyHostToDevice, stream));
+    plan.prof_key.clear();
     plan.uid = q.uid;
 }
 
-// Refs in chunks of kRC columns (original order); inside a chunk a counting sort by length
-// yields warp tasks of <= 32 refs of one length.
-void build_ref_plan(RefPlan& plan, const st_seqset_s& r, cudaStream_t stream) {
+// Refs in chunks of rc columns (original order); inside a chunk a counting sort by length
+// yields warp tasks of <= 32 refs of one length.  Each task's code rows occupy n*32 bytes of
+// the slab, so a chunk's slab is one contiguous range.
+void build_ref_plan(RefPlan& plan, const st_seqset_s& r, int rc, cudaStream_t stream) {
     const int64_t K = r.count;
-    plan.nchunks = ceil_div(K, kRC);
+    plan.rc = rc;
+    plan.nchunks = ceil_div(K, rc);
     plan.sorted.resize(size_t(K));
     plan.tasks.clear();
     plan.task_off.assign(size_t(plan.nchunks + 1), 0);
+    plan.max_slab = 0;
     std::vector<int32_t> cnt(size_t(r.max_len) + 2);
     std::vector<int32_t> start(cnt.size());
+    int64_t slab = 0;
     for (int64_t c = 0; c < plan.nchunks; ++c) {
-        const int64_t k0 = c * kRC, k1 = std::min<int64_t>(K, k0 + kRC);
+        const int64_t k0 = c * rc, k1 = std::min<int64_t>(K, k0 + rc);
         std::fill(cnt.begin(), cnt.end(), 0);
         for (int64_t k = k0; k < k1; ++k) cnt[size_t(r.h_len[size_t(k)]) + 1]++;
         for (size_t l = 1; l < cnt.size(); ++l) cnt[l] += cnt[l - 1];
         std::copy(cnt.begin(), cnt.end(), start.begin());
         for (int64_t k = k0; k < k1; ++k)
             plan.sorted[size_t(k0 + start[size_t(r.h_len[size_t(k)])]++)] = int32_t(k);
+        const int64_t slab0 = slab;
         for (int32_t l = 0; l <= r.max_len; ++l) {
             const int32_t b = cnt[size_t(l)], e = cnt[size_t(l) + 1];
-            for (int32_t s = b; s < e; s += 32)
-                plan.tasks.push_back(make_int4(l, int32_t(k0) + s, std::min(32, e - s), int32_t(c)));
+            for (int32_t s = b; s < e; s += 32) {
+                plan.tasks.push_back(make_int4(l, int32_t(k0) + s, std::min(32, e - s), int32_t(slab)));
+                slab += int64_t(l) * 32;
+            }
         }
+        plan.max_slab = std::max(plan.max_slab, slab - slab0);
         plan.task_off[size_t(c + 1)] = int32_t(plan.tasks.size());
     }
+    if (slab > INT32_MAX) fail(ST_EINVAL, "seqtree_b200: reference set too large for one call");
     plan.ntasks = int64_t(plan.tasks.size());
     STB_CUDA(cudaMemcpyAsync(plan.d_sorted.as<int32_t>(size_t(K)), plan.sorted.data(),
                              sizeof(int32_t) * size_t(K), cudaMemcpyHostToDevice, stream));
@@ -120,6 +144,7 @@ void build_ref_plan(RefPlan& plan, const st_seqset_s& r, cudaStream_t stream) {
     STB_CUDA(cudaMemcpyAsync(plan.d_task_off.as<int32_t>(plan.task_off.size()),
                              plan.task_off.data(), sizeof(int32_t) * plan.task_off.size(),
                              cudaMemcpyHostToDevice, stream));
+    plan.d_slab.as<uint8_t>(size_t(slab) + 16);
     plan.uid = r.uid;
 }
 
@@ -130,40 +155,58 @@ Plan& plan_slot(std::shared_ptr<void>& own, std::shared_ptr<void>& shared, bool 
     return *static_cast<Plan*>(slot.get());
 }
 
-// ---------------------------------------------------------------------------- fast kernel ---
-// Shared-memory query profile: for the CTA's query pair p and position j, the 32-word row
-// QP[p][j][b] = pen(q1[j], b) | pen(q2[j], b) << 16 (b < A, zero padded) -- one pass over the
-// 32 banks.  A warp unit is (32 refs of one length) x (a slice of 4 pairs of one length); the
-// four pairs are swept together, so every lookup address is a per-lane register (the ref
-// residue's byte offset, with the slice base folded in) plus a compile-time immediate
-// ((pair * LQ + j) * 128).  Query-longer and ref-longer pairs then share one inner loop: the
-// diagonal-d offset is either shifted by d rows (query longer) or taken from the ref residue
-// d positions further on (ref longer).
-constexpr int kRow = 32;        // words per profile row
-constexpr int kPairsPerSlice = 4;
+// QP[p][j][b] for b < 32 (zero beyond A, beyond the pair's length and for empty slots).
+__global__ void profile_kernel(const uint8_t* __restrict__ codes, const int64_t* __restrict__ off,
+                               const int2* __restrict__ pairs, const int32_t* __restrict__ plen,
+                               const int32_t* __restrict__ pen, int A, int LQ, int64_t total,
+                               uint32_t* __restrict__ prof) {
+    const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    const int64_t p = idx / (int64_t(LQ) * kRow);
+    const int j = int((idx / kRow) % LQ);
+    const int b = int(idx % kRow);
+    const int2 pr = pairs[p];
+    uint32_t v = 0;
+    if (b < A && j < plen[p] && pr.x >= 0) {
+        const int c1 = codes[off[pr.x] + j];
+        const int c2 = codes[off[pr.y >= 0 ? pr.y : pr.x] + j];
+        v = uint32_t(pen[c1 * A + b]) | (uint32_t(pen[c2 * A + b]) << 16);
+    }
+    prof[idx] = v;
+}
 
+// Per task: n rows of 32 lane bytes, each 4*code (lanes past the task's count repeat lane 0).
+__global__ void ref_slab_kernel(const uint8_t* __restrict__ codes, const int64_t* __restrict__ off,
+                                const int32_t* __restrict__ sorted, const int4* __restrict__ tasks,
+                                uint8_t* __restrict__ slab) {
+    const int4 t = tasks[blockIdx.x];
+    for (int idx = threadIdx.x; idx < t.x * 32; idx += blockDim.x) {
+        const int j = idx >> 5, l = idx & 31;
+        const int k = sorted[t.y + (l < t.z ? l : 0)];
+        slab[int64_t(t.w) + idx] = uint8_t(codes[off[k] + j] * 4);
+    }
+}
+
+// ---------------------------------------------------------------------------- fast kernel ---
 struct FastArgs {
-    const int32_t* pen;      // A*A penalty grid (padded to a multiple of 4 words)
-    int pen_words;
-    int A;
-    const uint8_t* qcodes;
-    const int64_t* qoff;
-    const uint8_t* rcodes;
-    const int64_t* roff;
+    const uint32_t* prof;    // [P][LQ][32]
+    const uint8_t* slab;     // ref code slab
     const int32_t* rlen;
     int64_t K;
-    const int2* pairs;       // (q1, q2); -1 marks a dummy slot
+    int rc;                  // columns per chunk
+    const int2* pairs;       // (q1, q2); -1 marks an empty slot
     const int32_t* plen;
-    int64_t P;               // a multiple of 4; every slice of 4 pairs has one length
+    int64_t P;
     const int32_t* ref_sorted;
     const int4* tasks;
     const int32_t* task_off;
+    int slab_cap;            // shared bytes reserved for a chunk's slab
     const uint32_t* prior2;  // [(M*W1 + d)*W1 + i], normalised, clamped, both halves; or null
     const int32_t* ftab;     // [m*W1 + n]: per-(m,n) additive term (prior minimum + gap cost)
     int W1;
     uint32_t bias2;          // BIAS in both halves
     int32_t* out;
-    unsigned long long* err; // set when the bounded wait for the staging copy gives up
+    unsigned long long* err; // set when the bounded wait for the staging copies gives up
 };
 
 // One non-blocking probe of an mbarrier phase (callers bound the number of probes).
@@ -177,46 +220,127 @@ __device__ __forceinline__ uint32_t mbar_try_wait(uint32_t bar, uint32_t parity)
     return ok;
 }
 
-template <int LQ, int LMAX, bool PRIOR>
-__global__ void __launch_bounds__(kThreads, 2) gapblock_fast_kernel(const FastArgs a) {
-    extern __shared__ __align__(128) uint8_t smem[];
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes,
+                                         uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+
+// One warp unit: the 4 pairs of one slice of the CTA against the 32 refs of one task.  The
+// sweep reads each residue offset straight from the staged code slab; the slice base and the
+// row offset j*128 are folded into two per-position addresses, so the 8 lookups of a position
+// are LDS [address + compile-time immediate (pair * LQ * 128)].  Query-longer pairs shift the
+// diagonal-d address by d rows; ref-longer pairs read the residue d positions further on.
+template <int LQ, bool PRIOR>
+__device__ __forceinline__ void run_unit(const FastArgs& a, const uint8_t* smem,
+                                         const uint8_t* s_codes, uint32_t* s_tile, int p0,
+                                         int slice, const int4 task, int tb, int64_t k0,
+                                         int lane) {
     constexpr int kRowB = kRow * 4;
     constexpr int kPairB = LQ * kRowB;
-    uint32_t* s_qp = reinterpret_cast<uint32_t*>(smem);                      // kGP*LQ rows
-    uint32_t* s_tile = reinterpret_cast<uint32_t*>(smem + kGP * kPairB);      // [kGP][kRC]
-    int32_t* s_ftab = reinterpret_cast<int32_t*>(s_tile + kGP * kRC);
-    int32_t* s_pen = s_ftab + ((a.W1 * a.W1 + 3) & ~3);
-    uint8_t* s_len = reinterpret_cast<uint8_t*>(s_pen + a.pen_words);
-    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_len + kRC);
+    const int n = task.x;
+    const int m = a.plen[p0 + slice * kPairsPerSlice];
+    const int L = min(m, n);
+    const int d = abs(m - n);
+    const int dq = m > n ? d : 0;   // query longer: diagonal d is d profile rows further down
+    const int dr = n > m ? d : 0;   // ref longer: diagonal d reads residue j + d
+    const uint8_t* rows0 = s_codes + tb + lane;
+    const uint8_t* rowsd = rows0 + dr * 32;
+    const uint32_t base0 = uint32_t(slice * kPairsPerSlice * kPairB);
+    const uint32_t based = base0 + uint32_t(dq * kRowB);
+    uint32_t res[kPairsPerSlice];
+    if (d == 0) {
+        uint32_t S[kPairsPerSlice] = {0u, 0u, 0u, 0u};
+#pragma unroll 4
+        for (int j = 0; j < L; ++j) {
+            const uint32_t a0 = base0 + uint32_t(j * kRowB) + rows0[j * 32];
+#pragma unroll
+            for (int q = 0; q < kPairsPerSlice; ++q)
+                S[q] += *reinterpret_cast<const uint32_t*>(smem + a0 + q * kPairB);
+        }
+#pragma unroll
+        for (int q = 0; q < kPairsPerSlice; ++q) res[q] = S[q];
+    } else {
+        const uint32_t* prow =
+            PRIOR ? a.prior2 + (size_t(max(m, n)) * a.W1 + d) * a.W1 : nullptr;
+        uint32_t S[kPairsPerSlice], Cb[kPairsPerSlice], best[kPairsPerSlice];
+        const uint32_t first = PRIOR ? a.bias2 + __ldg(prow) : a.bias2;
+#pragma unroll
+        for (int q = 0; q < kPairsPerSlice; ++q) {
+            S[q] = 0u;
+            Cb[q] = a.bias2;
+            best[q] = first;
+        }
+#pragma unroll 4
+        for (int j = 0; j < L; ++j) {
+            const uint32_t a0 = base0 + uint32_t(j * kRowB) + rows0[j * 32];
+            const uint32_t ad = based + uint32_t(j * kRowB) + rowsd[j * 32];
+            const uint32_t pr = PRIOR ? __ldg(prow + j + 1) : 0u;
+#pragma unroll
+            for (int q = 0; q < kPairsPerSlice; ++q) {
+                const uint32_t p0v = *reinterpret_cast<const uint32_t*>(smem + a0 + q * kPairB);
+                const uint32_t pdv = *reinterpret_cast<const uint32_t*>(smem + ad + q * kPairB);
+                S[q] += pdv;
+                Cb[q] = Cb[q] + p0v - pdv;  // per-half exact: halves stay in [0, 2^15)
+                best[q] = __viaddmin_s16x2(Cb[q], pr, best[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kPairsPerSlice; ++q) res[q] = S[q] + best[q] - a.bias2;
+    }
+    if (lane < task.z) {
+        const int col = int(a.ref_sorted[task.y + lane] - k0);
+#pragma unroll
+        for (int q = 0; q < kPairsPerSlice; ++q)
+            s_tile[(slice * kPairsPerSlice + q) * a.rc + col] = res[q];
+    }
+}
+
+template <int LQ, bool PRIOR>
+__global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastArgs a) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    constexpr int kProfB = kGP * LQ * kRow * 4;
+    uint8_t* s_codes = smem + kProfB;
+    uint32_t* s_tile = reinterpret_cast<uint32_t*>(s_codes + a.slab_cap);
+    int32_t* s_ftab = reinterpret_cast<int32_t*>(s_tile + kGP * a.rc);
+    uint8_t* s_len = reinterpret_cast<uint8_t*>(s_ftab + ((a.W1 * a.W1 + 3) & ~3));
+    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_len + ((a.rc + 15) & ~15));
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int chunk = blockIdx.x;
-    const int64_t k0 = int64_t(chunk) * kRC;
-    const int kcount = int(a.K - k0 < kRC ? a.K - k0 : kRC);
+    const int64_t k0 = int64_t(chunk) * a.rc;
+    const int kcount = int(a.K - k0 < a.rc ? a.K - k0 : a.rc);
     const int p0 = blockIdx.y * kGP;
     const int np = int(a.P - p0 < kGP ? a.P - p0 : kGP);
+    const int t0 = a.task_off[chunk], t1 = a.task_off[chunk + 1];
+    const int tw0 = a.tasks[t0].w;
+    const int slab_bytes = (t1 > t0 ? a.tasks[t1 - 1].w + a.tasks[t1 - 1].x * 32 : tw0) - tw0;
 
+    // Stage the CTA's profile slab and the chunk's code slab with two bulk (TMA) copies that
+    // complete on one mbarrier, while the other threads load the (m, n) terms and lengths.
     const uint32_t bar = uint32_t(__cvta_generic_to_shared(s_bar));
-    const uint32_t bytes = uint32_t(a.pen_words) * 4u;
-    // Stage the penalty grid with one bulk (TMA) copy that completes on an mbarrier, while the
-    // other threads load the per-chunk lengths and the (m, n) term table.
     if (tid == 0) {
+        const uint32_t prof_bytes = uint32_t(np) * LQ * kRow * 4;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                     "r"(prof_bytes + uint32_t(slab_bytes))
                      : "memory");
-        asm volatile(
-            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-                "r"(uint32_t(__cvta_generic_to_shared(s_pen))),
-            "l"(a.pen), "r"(bytes), "r"(bar)
-            : "memory");
+        bulk_g2s(uint32_t(__cvta_generic_to_shared(smem)),
+                 a.prof + size_t(p0) * LQ * kRow, prof_bytes, bar);
+        if (slab_bytes > 0)
+            bulk_g2s(uint32_t(__cvta_generic_to_shared(s_codes)), a.slab + tw0,
+                     uint32_t(slab_bytes), bar);
     }
     for (int i = tid; i < a.W1 * a.W1; i += kThreads) s_ftab[i] = a.ftab[i];
     for (int c = tid; c < kcount; c += kThreads) s_len[c] = uint8_t(a.rlen[k0 + c]);
     __syncthreads();
     {
         // Bounded wait on phase 0 by every thread.  If any thread runs out, the CTA records
-        // the failure, waits once more (bounded) for its copy in flight, and leaves as a
+        // the failure, waits once more (bounded) for its copies in flight, and leaves as a
         // whole -- the host then reports ST_ETIMEOUT and no tile is stored.
         uint32_t done = 0;
         for (int it = 0; it < (1 << 20) && !done; ++it) done = mbar_try_wait(bar, 0);
@@ -227,131 +351,45 @@ __global__ void __launch_bounds__(kThreads, 2) gapblock_fast_kernel(const FastAr
             return;
         }
     }
-    // Query profile of the CTA's pairs (rows past a pair's length and dummy pairs are zero).
-    {
-        const int A = a.A;
-        for (int idx = tid; idx < np * LQ * kRow; idx += kThreads) {
-            const int pl = idx / (LQ * kRow);
-            const int j = (idx / kRow) % LQ;
-            const int b = idx % kRow;
-            const int2 pr = a.pairs[p0 + pl];
-            const int m = a.plen[p0 + pl];
-            uint32_t v = 0;
-            if (b < A && j < m && pr.x >= 0) {
-                const int c1 = a.qcodes[a.qoff[pr.x] + j];
-                const int c2 = a.qcodes[a.qoff[pr.y >= 0 ? pr.y : pr.x] + j];
-                v = uint32_t(s_pen[c1 * A + b]) | (uint32_t(s_pen[c2 * A + b]) << 16);
-            }
-            s_qp[idx] = v;
-        }
-    }
-    __syncthreads();
 
-    const int t0 = a.task_off[chunk], t1 = a.task_off[chunk + 1];
     const int nslices = np / kPairsPerSlice;
     const int units = (t1 - t0) * nslices;
     for (int u = warp; u < units; u += kWarps) {
-        const int4 task = a.tasks[t0 + u / nslices];
-        const int slice = u - (u / nslices) * nslices;
-        const int n = task.x;
-        const int m = a.plen[p0 + slice * kPairsPerSlice];
-        const bool valid = lane < task.z;
-        const int k = a.ref_sorted[task.y + (valid ? lane : 0)];
-        const int col = int(k - k0);
-        const uint8_t* rb = a.rcodes + a.roff[k];
-        const int L = min(m, n);
-        const int d = abs(m - n);
-        const uint32_t sbase = uint32_t(slice * kPairsPerSlice * kPairB);
-        uint32_t r0[LMAX], rd[LMAX];
-#pragma unroll
-        for (int j = 0; j < LMAX; ++j) {
-            if (j < L) {
-                r0[j] = sbase + uint32_t(rb[j]) * 4u;
-                rd[j] = m > n ? r0[j] + uint32_t(d * kRowB) : sbase + uint32_t(rb[j + d]) * 4u;
-            }
-        }
-        uint32_t res[kPairsPerSlice];
-        if (d == 0) {
-            uint32_t S[kPairsPerSlice] = {0u, 0u, 0u, 0u};
-#pragma unroll
-            for (int j = 0; j < LMAX; ++j) {
-                if (j < L) {
-#pragma unroll
-                    for (int q = 0; q < kPairsPerSlice; ++q)
-                        S[q] += *reinterpret_cast<const uint32_t*>(smem + r0[j] + (q * LQ + j) * kRowB);
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < kPairsPerSlice; ++q) res[q] = S[q];
-        } else {
-            uint32_t pr[PRIOR ? LMAX + 1 : 1];
-            if constexpr (PRIOR) {
-                const uint32_t* row = a.prior2 + (size_t(max(m, n)) * a.W1 + d) * a.W1;
-#pragma unroll
-                for (int j = 0; j <= LMAX; ++j)
-                    if (j <= L) pr[j] = row[j];
-            }
-            uint32_t S[kPairsPerSlice], Cb[kPairsPerSlice], best[kPairsPerSlice];
-#pragma unroll
-            for (int q = 0; q < kPairsPerSlice; ++q) {
-                S[q] = 0u;
-                Cb[q] = a.bias2;
-                if constexpr (PRIOR) best[q] = a.bias2 + pr[0];
-                else best[q] = a.bias2;
-            }
-#pragma unroll
-            for (int j = 0; j < LMAX; ++j) {
-                if (j < L) {
-#pragma unroll
-                    for (int q = 0; q < kPairsPerSlice; ++q) {
-                        const uint32_t p0v =
-                            *reinterpret_cast<const uint32_t*>(smem + r0[j] + (q * LQ + j) * kRowB);
-                        const uint32_t pdv =
-                            *reinterpret_cast<const uint32_t*>(smem + rd[j] + (q * LQ + j) * kRowB);
-                        S[q] += pdv;
-                        Cb[q] = Cb[q] + p0v - pdv;  // per-half exact: halves stay in [0, 2^15)
-                        if constexpr (PRIOR)
-                            best[q] = __viaddmin_s16x2(Cb[q], pr[j + 1], best[q]);
-                        else
-                            best[q] = __viaddmin_s16x2(Cb[q], 0u, best[q]);
-                    }
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < kPairsPerSlice; ++q) res[q] = S[q] + best[q] - a.bias2;
-        }
-        if (valid) {
-#pragma unroll
-            for (int q = 0; q < kPairsPerSlice; ++q)
-                s_tile[(slice * kPairsPerSlice + q) * kRC + col] = res[q];
-        }
+        const int ti = u / nslices;
+        const int4 task = a.tasks[t0 + ti];
+        const int tb = task.w - tw0;
+        run_unit<LQ, PRIOR>(a, smem, s_codes, s_tile, p0, u - ti * nslices, task, tb, k0, lane);
     }
     __syncthreads();
 
     // Coalesced write-out of the (2*np) x kcount tile, adding the per-(m,n) term.
     const bool vec = (a.K & 3) == 0;
-    const int cols4 = (kcount + 3) / 4;
-    for (int idx = tid; idx < 2 * np * cols4; idx += kThreads) {
-        const int s = idx / cols4;
-        const int c = (idx - s * cols4) * 4;
-        const int2 pr = a.pairs[p0 + s / 2];
+    const int cols4 = (kcount + 3) >> 2;
+    for (int s = warp; s < 2 * np; s += kWarps) {
+        const int2 pr = a.pairs[p0 + (s >> 1)];
         const int orig = (s & 1) ? pr.y : pr.x;
         if (orig < 0) continue;
-        const int m = a.plen[p0 + s / 2];
-        const int32_t* frow = s_ftab + m * a.W1;
+        const int32_t* frow = s_ftab + a.plen[p0 + (s >> 1)] * a.W1;
         const int sh = (s & 1) * 16;
-        int32_t* dst = a.out + int64_t(orig) * a.K + k0 + c;
-        const uint32_t* src = s_tile + (s / 2) * kRC + c;
-        if (vec && c + 4 <= kcount) {
-            int4 v;
-            v.x = int32_t(((src[0] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + 0]]));
-            v.y = int32_t(((src[1] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + 1]]));
-            v.z = int32_t(((src[2] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + 2]]));
-            v.w = int32_t(((src[3] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + 3]]));
-            *reinterpret_cast<int4*>(dst) = v;
-        } else {
-            for (int t = 0; t < 4 && c + t < kcount; ++t)
-                dst[t] = int32_t(((src[t] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + t]]));
+        int32_t* dst_row = a.out + int64_t(orig) * a.K + k0;
+        const uint32_t* src_row = s_tile + (s >> 1) * a.rc;
+        for (int c4 = lane; c4 < cols4; c4 += 32) {
+            const int c = c4 * 4;
+            const uint32_t* src = src_row + c;
+            int32_t* dst = dst_row + c;
+            if (vec && c + 4 <= kcount) {
+                const uint4 t = *reinterpret_cast<const uint4*>(src);
+                const uint32_t l4 = *reinterpret_cast<const uint32_t*>(s_len + c);
+                int4 v;
+                v.x = int32_t(((t.x >> sh) & 0xFFFFu) + uint32_t(frow[l4 & 0xFF]));
+                v.y = int32_t(((t.y >> sh) & 0xFFFFu) + uint32_t(frow[(l4 >> 8) & 0xFF]));
+                v.z = int32_t(((t.z >> sh) & 0xFFFFu) + uint32_t(frow[(l4 >> 16) & 0xFF]));
+                v.w = int32_t(((t.w >> sh) & 0xFFFFu) + uint32_t(frow[l4 >> 24]));
+                *reinterpret_cast<int4*>(dst) = v;
+            } else {
+                for (int t = 0; t < 4 && c + t < kcount; ++t)
+                    dst[t] = int32_t(((src[t] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + t]]));
+            }
         }
     }
 }
@@ -411,34 +449,25 @@ __global__ void __launch_bounds__(256) gapblock_general_kernel(const GeneralArgs
     }
 }
 
-template <int LQ, int LMAX, bool PRIOR>
+template <int LQ, bool PRIOR>
 const char* launch_fast(const FastArgs& args, dim3 grid, size_t smem, cudaStream_t stream) {
-    auto kern = gapblock_fast_kernel<LQ, LMAX, PRIOR>;
+    auto kern = gapblock_fast_kernel<LQ, PRIOR>;
     STB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     kern<<<grid, kThreads, smem, stream>>>(args);
     STB_CUDA(cudaGetLastError());
     return "gapblock_fast_kernel";
 }
 
-template <int LQ, bool PRIOR>
-const char* dispatch_lmax(int lmax, const FastArgs& args, dim3 grid, size_t smem,
-                          cudaStream_t stream) {
-    if (lmax <= 8) return launch_fast<LQ, 8, PRIOR>(args, grid, smem, stream);
-    if (lmax <= 16) return launch_fast<LQ, 16, PRIOR>(args, grid, smem, stream);
-    if (lmax <= 24) return launch_fast<LQ, 24, PRIOR>(args, grid, smem, stream);
-    return launch_fast<LQ, 32, PRIOR>(args, grid, smem, stream);
-}
-
-// Profile height LQ >= longest query (32 or 64), LMAX >= longest min(m, n).
+// Profile height LQ >= longest query (32 or 64).
 int profile_height(int longest_query) { return longest_query <= 32 ? 32 : 64; }
 
-const char* dispatch_fast(int lq, int lmax, bool prior, const FastArgs& args, dim3 grid,
-                          size_t smem, cudaStream_t stream) {
+const char* dispatch_fast(int lq, bool prior, const FastArgs& args, dim3 grid, size_t smem,
+                          cudaStream_t stream) {
     if (lq == 32)
-        return prior ? dispatch_lmax<32, true>(lmax, args, grid, smem, stream)
-                     : dispatch_lmax<32, false>(lmax, args, grid, smem, stream);
-    return prior ? dispatch_lmax<64, true>(lmax, args, grid, smem, stream)
-                 : dispatch_lmax<64, false>(lmax, args, grid, smem, stream);
+        return prior ? launch_fast<32, true>(args, grid, smem, stream)
+                     : launch_fast<32, false>(args, grid, smem, stream);
+    return prior ? launch_fast<64, true>(args, grid, smem, stream)
+                 : launch_fast<64, false>(args, grid, smem, stream);
 }
 
 // Device-side tables of the fast path and the arguments they were built from.
@@ -456,16 +485,13 @@ GbTables& gb_tables(int device) {
     return *p;
 }
 
-// Penalty grid (padded to 16 bytes for the bulk copy); per-(M,d) prior rows shifted by their
-// minimum (added back through ftab) and clamped at CAP = 2*BIAS + 1 -- a clamped position can
-// never win, because the position holding the row's minimum scores at most BIAS while a
-// clamped one scores above it; ftab[m][n] = prior minimum + gap_open + (d-1)*gap_extend
-// (int32 wrap, as the reference's int32 arithmetic).
-void build_tables(GbTables& tb, const std::vector<int32_t>& pen, int A, int32_t go, int32_t ge,
-                  int W, int32_t bias, const int32_t* prior, int64_t W1p, cudaStream_t stream) {
-    const int pen_words = int((size_t(A) * A + 3) & ~size_t(3));
-    std::vector<int32_t> pen_padded(size_t(pen_words), 0);
-    std::copy(pen.begin(), pen.end(), pen_padded.begin());
+// Penalty grid; per-(M,d) prior rows shifted by their minimum (added back through ftab) and
+// clamped at CAP = 2*BIAS + 1 -- a clamped position can never win, because the position holding
+// the row's minimum scores at most BIAS while a clamped one scores above it;
+// ftab[m][n] = prior minimum + gap_open + (d-1)*gap_extend (int32 wrap, as the reference's
+// int32 arithmetic).
+void build_tables(GbTables& tb, const std::vector<int32_t>& pen, int32_t go, int32_t ge, int W,
+                  int32_t bias, const int32_t* prior, int64_t W1p, cudaStream_t stream) {
     const int W1 = W + 1;
     const int32_t cap = 2 * bias + 1;
     std::vector<int32_t> ftab(size_t(W1) * W1, 0);
@@ -489,13 +515,19 @@ void build_tables(GbTables& tb, const std::vector<int32_t>& pen, int A, int32_t 
             ftab[size_t(m) * W1 + n] = int32_t(uint32_t(pmin) + uint32_t(go) +
                                                uint32_t(d - 1) * uint32_t(ge));
         }
-    STB_CUDA(cudaMemcpyAsync(tb.pen.as<int32_t>(pen_padded.size()), pen_padded.data(),
-                             pen_padded.size() * 4, cudaMemcpyHostToDevice, stream));
+    STB_CUDA(cudaMemcpyAsync(tb.pen.as<int32_t>(pen.size()), pen.data(), pen.size() * 4,
+                             cudaMemcpyHostToDevice, stream));
     STB_CUDA(cudaMemcpyAsync(tb.ftab.as<int32_t>(ftab.size()), ftab.data(), ftab.size() * 4,
                              cudaMemcpyHostToDevice, stream));
     if (prior)
         STB_CUDA(cudaMemcpyAsync(tb.prior2.as<uint32_t>(prior2.size()), prior2.data(),
                                  prior2.size() * 4, cudaMemcpyHostToDevice, stream));
+}
+
+// Shared memory of one CTA for a given chunk width.
+size_t fast_smem(int lq, int64_t slab_cap, int rc, int W1) {
+    return size_t(kGP) * lq * kRow * 4 + size_t(slab_cap) + size_t(kGP) * rc * 4 +
+           size_t((W1 * W1 + 3) & ~3) * 4 + size_t((rc + 15) & ~15) + 16;
 }
 
 }  // namespace
@@ -534,7 +566,34 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
     }
     const int32_t Lmax = std::min(qs.max_len, rs.max_len);
     const int64_t lmaxpen = int64_t(Lmax) * maxpen;
-    const bool fast = nonneg && longest <= 64 && Lmax <= 32 && lmaxpen <= 8191;
+    bool fast = nonneg && longest <= 64 && lmaxpen <= 8191;
+
+    const int W = longest, W1 = W + 1;
+    const int lq = profile_height(qs.max_len);
+    RefPlan* rpp = nullptr;
+    size_t smem = 0;
+    if (fast) {
+        RefPlan& rp = plan_slot<RefPlan>(rs.gb_ref_plan, ctx.tmp_ref_plan, rs.owns);
+        if (rp.uid != rs.uid) {
+            // Widest chunk whose CTA fits in shared memory (narrower chunks fill warps worse).
+            for (int rc : {1024, 512, 256}) {
+                build_ref_plan(rp, rs, rc, stream);
+                smem = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rc, W1);
+                if (smem <= size_t(ctx.max_smem_optin)) break;
+            }
+            const unsigned blocks = unsigned(rp.ntasks);
+            if (blocks) {
+                ref_slab_kernel<<<blocks, 128, 0, stream>>>(
+                    rs.d_bytes, rs.d_off, static_cast<int32_t*>(rp.d_sorted.ptr),
+                    static_cast<int4*>(rp.d_tasks.ptr), static_cast<uint8_t*>(rp.d_slab.ptr));
+                STB_CUDA(cudaGetLastError());
+                note_launch(nullptr);
+            }
+        }
+        smem = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rp.rc, W1);
+        fast = smem <= size_t(ctx.max_smem_optin);
+        rpp = &rp;
+    }
 
     if (!fast) {
         int32_t* d_pen = ctx.table_buf.as<int32_t>(pen.size());
@@ -553,18 +612,12 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
         note_launch("gapblock_general_kernel");
         return;
     }
+    RefPlan& rp = *rpp;
 
-    // ---- fast path planning ----
-    QueryPlan& qp = plan_slot<QueryPlan>(qs.gb_query_plan, ctx.tmp_query_plan, qs.owns);
-    RefPlan& rp = plan_slot<RefPlan>(rs.gb_ref_plan, ctx.tmp_ref_plan, rs.owns);
-    if (qp.uid != qs.uid) build_query_plan(qp, qs, stream);
-    if (rp.uid != rs.uid) build_ref_plan(rp, rs, stream);
-    // Device tables for this (matrix, gaps, prior, lengths): rebuilt only when they change, so
-    // repeated calls with the same arguments enqueue nothing but the kernel.
+    // Tables for this (matrix, gaps, prior, lengths): rebuilt only when they change, so repeated
+    // calls with the same arguments enqueue nothing but the kernel.
     GbTables& tb = gb_tables(ctx.device);
-    const int W = longest, W1 = W + 1;
     const int32_t bias = int32_t(std::max<int64_t>(lmaxpen, 1));
-    const int pen_words = int((size_t(A) * A + 3) & ~size_t(3));
     {
         std::vector<uint8_t> key;
         auto put = [&key](const void* p, size_t n) {
@@ -575,45 +628,56 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
         put(hdr, sizeof hdr);
         put(pen.data(), pen.size() * 4);
         if (has_prior) put(prior, size_t(prior_len) * 4);
-        if (!same_as_last(tb.key, key.data(), key.size())) build_tables(tb, pen, A, go, ge, W, bias,
-                                                                      has_prior ? prior : nullptr,
-                                                                      W1p, stream);
+        if (!same_as_last(tb.key, key.data(), key.size()))
+            build_tables(tb, pen, go, ge, W, bias, has_prior ? prior : nullptr, W1p, stream);
     }
-    int32_t* d_pen = static_cast<int32_t*>(tb.pen.ptr);
-    int32_t* d_ftab = static_cast<int32_t*>(tb.ftab.ptr);
-    uint32_t* d_prior2 = has_prior ? static_cast<uint32_t*>(tb.prior2.ptr) : nullptr;
+
+    // Query pairs and their profile (rebuilt when the set or the penalty grid changes).
+    QueryPlan& qp = plan_slot<QueryPlan>(qs.gb_query_plan, ctx.tmp_query_plan, qs.owns);
+    if (qp.uid != qs.uid) build_query_plan(qp, qs, stream);
+    {
+        std::vector<uint8_t> key(sizeof(int) * 2 + pen.size() * 4);
+        const int hdr[2] = {A, lq};
+        std::memcpy(key.data(), hdr, sizeof hdr);
+        std::memcpy(key.data() + sizeof hdr, pen.data(), pen.size() * 4);
+        if (!same_as_last(qp.prof_key, key.data(), key.size())) {
+            const int64_t total = qp.P * lq * kRow;
+            uint32_t* prof = qp.d_prof.as<uint32_t>(size_t(total));
+            profile_kernel<<<unsigned(ceil_div(total, 256)), 256, 0, stream>>>(
+                qs.d_bytes, qs.d_off, static_cast<int2*>(qp.d_pairs.ptr),
+                static_cast<int32_t*>(qp.d_plen.ptr), static_cast<int32_t*>(tb.pen.ptr), A, lq,
+                total, prof);
+            STB_CUDA(cudaGetLastError());
+            note_launch(nullptr);
+        }
+    }
+
     auto* err = reinterpret_cast<unsigned long long*>(ctx.flags_d + 8);
     STB_CUDA(cudaMemsetAsync(err, 0, 8, stream));
 
     FastArgs fa{};
-    fa.pen = d_pen;
-    fa.pen_words = pen_words;
-    fa.A = A;
-    fa.qcodes = qs.d_bytes;
-    fa.qoff = qs.d_off;
-    fa.rcodes = rs.d_bytes;
-    fa.roff = rs.d_off;
+    fa.prof = static_cast<uint32_t*>(qp.d_prof.ptr);
+    fa.slab = static_cast<uint8_t*>(rp.d_slab.ptr);
     fa.rlen = rs.d_len;
     fa.K = K;
+    fa.rc = rp.rc;
     fa.pairs = static_cast<int2*>(qp.d_pairs.ptr);
     fa.plen = static_cast<int32_t*>(qp.d_plen.ptr);
     fa.P = qp.P;
     fa.ref_sorted = static_cast<int32_t*>(rp.d_sorted.ptr);
     fa.tasks = static_cast<int4*>(rp.d_tasks.ptr);
     fa.task_off = static_cast<int32_t*>(rp.d_task_off.ptr);
-    fa.prior2 = d_prior2;
-    fa.ftab = d_ftab;
+    fa.slab_cap = int((rp.max_slab + 15) & ~int64_t(15));
+    fa.prior2 = has_prior ? static_cast<uint32_t*>(tb.prior2.ptr) : nullptr;
+    fa.ftab = static_cast<int32_t*>(tb.ftab.ptr);
     fa.W1 = W1;
     fa.bias2 = uint32_t(bias) * 0x10001u;
     fa.out = out_d;
     fa.err = err;
 
-    const int lq = profile_height(qs.max_len);
-    const size_t smem = size_t(kGP) * lq * kRow * 4 + size_t(kGP) * kRC * 4 +
-                        size_t((W1 * W1 + 3) & ~3) * 4 + size_t(pen_words) * 4 + kRC + 16;
     const dim3 grid(unsigned(rp.nchunks), unsigned(ceil_div(qp.P, kGP)));
     if (grid.y > 65535) fail(ST_EINVAL, "seqtree_b200: too many query pairs for one launch");
-    const char* name = dispatch_fast(lq, Lmax, has_prior, fa, grid, smem, stream);
+    const char* name = dispatch_fast(lq, has_prior, fa, grid, smem, stream);
     note_launch(name);
     // The timeout flag is read by the caller after its synchronisation point.
 }
