@@ -104,20 +104,26 @@ class Packed:
     __slots__ = ("data", "offsets", "struct")
 
     def __init__(self, seqs):
-        seqs = list(seqs)
-        for s in seqs:
-            if not isinstance(s, (str, bytes)):
-                raise TypeError("sequences must be str")
-        joined = "".join(s if isinstance(s, str) else s.decode("latin-1") for s in seqs)
-        data = joined.encode("utf-8")
-        lens = np.fromiter((len(s) for s in seqs), dtype=np.int64, count=len(seqs))
-        if len(data) != int(lens.sum()):  # non-ASCII text: byte lengths differ from len()
-            enc = [s.encode("utf-8") if isinstance(s, str) else s for s in seqs]
+        seqs = seqs if isinstance(seqs, list) else list(seqs)
+        try:
+            data = "".join(seqs).encode("utf-8")
+            lens = np.fromiter(map(len, seqs), dtype=np.int64, count=len(seqs))
+            if len(data) != int(lens.sum()):  # non-ASCII text: use byte lengths
+                raise UnicodeError
+        except (TypeError, UnicodeError):
+            enc = []
+            for s in seqs:
+                if isinstance(s, str):
+                    enc.append(s.encode("utf-8"))
+                elif isinstance(s, (bytes, bytearray)):
+                    enc.append(bytes(s))
+                else:
+                    raise TypeError("sequences must be str") from None
             data = b"".join(enc)
-            lens = np.fromiter((len(b) for b in enc), dtype=np.int64, count=len(enc))
+            lens = np.fromiter(map(len, enc), dtype=np.int64, count=len(enc))
         off = np.zeros(len(seqs) + 1, dtype=np.int64)
         np.cumsum(lens, out=off[1:])
-        self.data = np.frombuffer(data + b"\0", dtype=np.uint8)
+        self.data = np.frombuffer(data, dtype=np.uint8) if data else np.zeros(1, np.uint8)
         self.offsets = off
         self.struct = st_strings(self.data.ctypes.data, self.offsets.ctypes.data, len(seqs))
 

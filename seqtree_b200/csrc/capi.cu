@@ -131,13 +131,23 @@ int32_t st_gapblock_matrix(const st_strings* queries, const st_strings* refs, in
         clear_flags(ctx);
         // src/gapblock.cpp:85-94: queries are encoded before refs.
         Transient t;
-        t.q.reset(make_seqset(queries, alphabet, ctx.stream, nullptr, nullptr, ctx.tq));
-        t.r.reset(make_seqset(refs, alphabet, ctx.stream, nullptr, nullptr, ctx.tr));
+        {
+            Phase ph("upload+encode");
+            t.q.reset(make_seqset(queries, alphabet, ctx.stream, nullptr, nullptr, ctx.tq));
+            t.r.reset(make_seqset(refs, alphabet, ctx.stream, nullptr, nullptr, ctx.tr));
+        }
         int32_t* out_d = ctx.out_buf.as<int32_t>(size_t(N) * size_t(K));
-        gapblock_sets(*t.q, *t.r, penalty, matrix_size, gap_open, gap_extend, prior, prior_len,
-                      prior_width, out_d, ctx.stream);
-        finish(ctx, out, N, K, out_d);
+        {
+            Phase ph("plan+launch");
+            gapblock_sets(*t.q, *t.r, penalty, matrix_size, gap_open, gap_extend, prior, prior_len,
+                          prior_width, out_d, ctx.stream);
+        }
+        {
+            Phase ph("kernel+d2h");
+            finish(ctx, out, N, K, out_d);
+        }
         check_timeout(ctx);
+        trace_report("st_gapblock_matrix");
     });
 }
 
@@ -172,9 +182,16 @@ static int32_t align_common(const st_strings* queries, const st_strings* refs,
         t.r.reset(make_seqset(refs, alphabet, ctx.stream, &bad, &bc, ctx.tr));
         if (bad >= 0) fail(ST_EINVAL, std::string("invalid symbol '") + bc + "' in sequence");
         int32_t* out_d = ctx.out_buf.as<int32_t>(size_t(N) * size_t(K));
-        align_sets(*t.q, *t.r, similarity, matrix_size, mode, gap_open, gap_extend, dist, out_d,
-                   ctx.stream);
-        finish(ctx, out, N, K, out_d);
+        {
+            Phase ph("plan+launch");
+            align_sets(*t.q, *t.r, similarity, matrix_size, mode, gap_open, gap_extend, dist, out_d,
+                       ctx.stream);
+        }
+        {
+            Phase ph("kernel+d2h");
+            finish(ctx, out, N, K, out_d);
+        }
+        trace_report(dist ? "st_align_dist_matrix" : "st_align_score_matrix");
         check_timeout(ctx);
         if (ctx.flags_h[9] != 0)
             fail(ST_EOVERFLOW, std::string("seqtree: the alignment ") + (dist ? "distance" : "score") +
@@ -214,14 +231,24 @@ static int32_t distance_common(const st_strings* a, const st_strings* b, bool le
         std::lock_guard<std::mutex> lk(ctx.mu);
         clear_flags(ctx);
         Transient t;
-        t.q.reset(make_seqset(a, -1, ctx.stream, nullptr, nullptr, ctx.tq));
-        t.r.reset(make_seqset(b, -1, ctx.stream, nullptr, nullptr, ctx.tr));
+        {
+            Phase ph("upload");
+            t.q.reset(make_seqset(a, -1, ctx.stream, nullptr, nullptr, ctx.tq));
+            t.r.reset(make_seqset(b, -1, ctx.stream, nullptr, nullptr, ctx.tr));
+        }
         int32_t* out_d = ctx.out_buf.as<int32_t>(size_t(N) * size_t(K));
-        if (lev)
-            levenshtein_sets(*t.q, *t.r, out_d, ctx.stream);
-        else
-            hamming_sets(*t.q, *t.r, out_d, ctx.stream);
-        finish(ctx, out, N, K, out_d);
+        {
+            Phase ph("plan+launch");
+            if (lev)
+                levenshtein_sets(*t.q, *t.r, out_d, ctx.stream);
+            else
+                hamming_sets(*t.q, *t.r, out_d, ctx.stream);
+        }
+        {
+            Phase ph("kernel+d2h");
+            finish(ctx, out, N, K, out_d);
+        }
+        trace_report(lev ? "st_levenshtein_matrix" : "st_hamming_matrix");
     });
 }
 

@@ -1,8 +1,13 @@
 // Per-device context, workspace, pinned host cache and sequence-set upload/encoding.
 #include "common.cuh"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <map>
 
 namespace stb {
@@ -23,6 +28,41 @@ void reset_launches() {
 }
 int last_launches() { return t_launches; }
 const char* last_kernel() { return t_kernel; }
+
+// ----------------------------------------------------------------------------- tracing ------
+namespace {
+bool trace_on() {
+    static const bool on = [] {
+        const char* v = std::getenv("SEQTREE_B200_TRACE");
+        return v && *v && *v != '0';
+    }();
+    return on;
+}
+double now_ms() {
+    using namespace std::chrono;
+    return duration<double, std::milli>(steady_clock::now().time_since_epoch()).count();
+}
+thread_local std::string t_trace;
+}  // namespace
+
+Phase::Phase(const char* n) : name(n), t0(0) {
+    nvtxRangePushA(n);
+    if (trace_on()) t0 = now_ms();
+}
+
+Phase::~Phase() {
+    nvtxRangePop();
+    if (trace_on()) {
+        char buf[96];
+        std::snprintf(buf, sizeof buf, " %s=%.3fms", name, now_ms() - t0);
+        t_trace += buf;
+    }
+}
+
+void trace_report(const char* call) {
+    if (trace_on() && !t_trace.empty()) std::fprintf(stderr, "[seqtree_b200] %s:%s\n", call, t_trace.c_str());
+    t_trace.clear();
+}
 
 // ----------------------------------------------------------------------------- buffers ------
 void* DevBuf::get(size_t bytes) {

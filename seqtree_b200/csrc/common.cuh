@@ -40,6 +40,17 @@ struct StError : std::runtime_error {
 void note_launch(const char* kernel_name, int count = 1);
 void reset_launches();
 
+// Host-side phase tracing.  Every Phase opens an NVTX range (visible to Nsight tools, free
+// otherwise); with SEQTREE_B200_TRACE=1 in the environment the wall time of each phase is also
+// recorded and trace_report() prints one line per call to stderr.
+struct Phase {
+    const char* name;
+    double t0;
+    explicit Phase(const char* n);
+    ~Phase();
+};
+void trace_report(const char* call);
+
 // ----------------------------------------------------------------------------- context ------
 // A device buffer that only grows; reused across calls so steady-state calls allocate nothing.
 struct DevBuf {

@@ -201,7 +201,8 @@ struct FastArgs {
     const int4* tasks;
     const int32_t* task_off;
     int slab_cap;            // shared bytes reserved for a chunk's slab
-    const uint32_t* prior2;  // [(M*W1 + d)*W1 + i], normalised, clamped, both halves; or null
+    const uint32_t* prior2;  // rows (M*W1 + d) of pstride words, value i at i + 3; or null
+    int pstride;
     const int32_t* ftab;     // [m*W1 + n]: per-(m,n) additive term (prior minimum + gap cost)
     int W1;
     uint32_t bias2;          // BIAS in both halves
@@ -264,21 +265,20 @@ __device__ __forceinline__ void run_unit(const FastArgs& a, const uint8_t* smem,
 #pragma unroll
         for (int q = 0; q < kPairsPerSlice; ++q) res[q] = S[q];
     } else {
-        const uint32_t* prow =
-            PRIOR ? a.prior2 + (size_t(max(m, n)) * a.W1 + d) * a.W1 : nullptr;
+        // Prior row of (max(m,n), d): value i at prow[i + 3], so values j+1..j+4 of an aligned
+        // group of four positions are one 16-byte load.
+        const uint32_t* prow = PRIOR ? a.prior2 + (size_t(max(m, n)) * a.W1 + d) * a.pstride : nullptr;
         uint32_t S[kPairsPerSlice], Cb[kPairsPerSlice], best[kPairsPerSlice];
-        const uint32_t first = PRIOR ? a.bias2 + __ldg(prow) : a.bias2;
+        const uint32_t first = PRIOR ? a.bias2 + __ldg(prow + 3) : a.bias2;
 #pragma unroll
         for (int q = 0; q < kPairsPerSlice; ++q) {
             S[q] = 0u;
             Cb[q] = a.bias2;
             best[q] = first;
         }
-#pragma unroll 4
-        for (int j = 0; j < L; ++j) {
+        auto step = [&](int j, uint32_t pr) {
             const uint32_t a0 = base0 + uint32_t(j * kRowB) + rows0[j * 32];
             const uint32_t ad = based + uint32_t(j * kRowB) + rowsd[j * 32];
-            const uint32_t pr = PRIOR ? __ldg(prow + j + 1) : 0u;
 #pragma unroll
             for (int q = 0; q < kPairsPerSlice; ++q) {
                 const uint32_t p0v = *reinterpret_cast<const uint32_t*>(smem + a0 + q * kPairB);
@@ -287,7 +287,17 @@ __device__ __forceinline__ void run_unit(const FastArgs& a, const uint8_t* smem,
                 Cb[q] = Cb[q] + p0v - pdv;  // per-half exact: halves stay in [0, 2^15)
                 best[q] = __viaddmin_s16x2(Cb[q], pr, best[q]);
             }
+        };
+        int j = 0;
+        for (; j + 4 <= L; j += 4) {
+            uint4 pv = make_uint4(0u, 0u, 0u, 0u);
+            if constexpr (PRIOR) pv = __ldg(reinterpret_cast<const uint4*>(prow + j + 4));
+            step(j, pv.x);
+            step(j + 1, pv.y);
+            step(j + 2, pv.z);
+            step(j + 3, pv.w);
         }
+        for (; j < L; ++j) step(j, PRIOR ? __ldg(prow + j + 4) : 0u);
 #pragma unroll
         for (int q = 0; q < kPairsPerSlice; ++q) res[q] = S[q] + best[q] - a.bias2;
     }
@@ -303,7 +313,9 @@ template <int LQ, bool PRIOR>
 __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastArgs a) {
     extern __shared__ __align__(128) uint8_t smem[];
     constexpr int kProfB = kGP * LQ * kRow * 4;
-    uint8_t* s_codes = smem + kProfB;
+    const int prof_area = kProfB > (kGP / kPairsPerSlice) * a.rc * 4 ? kProfB
+                                                                    : (kGP / kPairsPerSlice) * a.rc * 4;
+    uint8_t* s_codes = smem + prof_area;
     uint32_t* s_tile = reinterpret_cast<uint32_t*>(s_codes + a.slab_cap);
     int32_t* s_ftab = reinterpret_cast<int32_t*>(s_tile + kGP * a.rc);
     uint8_t* s_len = reinterpret_cast<uint8_t*>(s_ftab + ((a.W1 * a.W1 + 3) & ~3));
@@ -362,33 +374,41 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
     }
     __syncthreads();
 
-    // Coalesced write-out of the (2*np) x kcount tile, adding the per-(m,n) term.
+    // Per-slice column terms fcol[slice][c] = ftab[m_slice][len(c)], written over the profile
+    // (no longer read), then the coalesced write-out: each thread takes one pair and four
+    // columns, reads the packed tile and the terms once and stores both queries' rows as
+    // 16-byte vectors.
+    int32_t* s_fcol = reinterpret_cast<int32_t*>(smem);
+    for (int i = tid; i < nslices * a.rc; i += kThreads) {
+        const int sl = i / a.rc, c = i - sl * a.rc;
+        s_fcol[i] = c < kcount ? s_ftab[a.plen[p0 + sl * kPairsPerSlice] * a.W1 + s_len[c]] : 0;
+    }
+    __syncthreads();
     const bool vec = (a.K & 3) == 0;
     const int cols4 = (kcount + 3) >> 2;
-    for (int s = warp; s < 2 * np; s += kWarps) {
-        const int2 pr = a.pairs[p0 + (s >> 1)];
-        const int orig = (s & 1) ? pr.y : pr.x;
-        if (orig < 0) continue;
-        const int32_t* frow = s_ftab + a.plen[p0 + (s >> 1)] * a.W1;
-        const int sh = (s & 1) * 16;
-        int32_t* dst_row = a.out + int64_t(orig) * a.K + k0;
-        const uint32_t* src_row = s_tile + (s >> 1) * a.rc;
-        for (int c4 = lane; c4 < cols4; c4 += 32) {
-            const int c = c4 * 4;
-            const uint32_t* src = src_row + c;
-            int32_t* dst = dst_row + c;
-            if (vec && c + 4 <= kcount) {
-                const uint4 t = *reinterpret_cast<const uint4*>(src);
-                const uint32_t l4 = *reinterpret_cast<const uint32_t*>(s_len + c);
-                int4 v;
-                v.x = int32_t(((t.x >> sh) & 0xFFFFu) + uint32_t(frow[l4 & 0xFF]));
-                v.y = int32_t(((t.y >> sh) & 0xFFFFu) + uint32_t(frow[(l4 >> 8) & 0xFF]));
-                v.z = int32_t(((t.z >> sh) & 0xFFFFu) + uint32_t(frow[(l4 >> 16) & 0xFF]));
-                v.w = int32_t(((t.w >> sh) & 0xFFFFu) + uint32_t(frow[l4 >> 24]));
-                *reinterpret_cast<int4*>(dst) = v;
-            } else {
-                for (int t = 0; t < 4 && c + t < kcount; ++t)
-                    dst[t] = int32_t(((src[t] >> sh) & 0xFFFFu) + uint32_t(frow[s_len[c + t]]));
+    for (int i = tid; i < np * cols4; i += kThreads) {
+        const int pl = i / cols4;
+        const int c = (i - pl * cols4) * 4;
+        const int2 pr = a.pairs[p0 + pl];
+        if (pr.x < 0) continue;
+        const uint32_t* src = s_tile + pl * a.rc + c;
+        const int32_t* fc = s_fcol + (pl / kPairsPerSlice) * a.rc + c;
+        int32_t* d1 = a.out + int64_t(pr.x) * a.K + k0 + c;
+        int32_t* d2 = pr.y >= 0 ? a.out + int64_t(pr.y) * a.K + k0 + c : nullptr;
+        if (vec && c + 4 <= kcount) {
+            const uint4 t = *reinterpret_cast<const uint4*>(src);
+            const int4 f = *reinterpret_cast<const int4*>(fc);
+            *reinterpret_cast<int4*>(d1) =
+                make_int4(int32_t((t.x & 0xFFFFu) + uint32_t(f.x)), int32_t((t.y & 0xFFFFu) + uint32_t(f.y)),
+                          int32_t((t.z & 0xFFFFu) + uint32_t(f.z)), int32_t((t.w & 0xFFFFu) + uint32_t(f.w)));
+            if (d2)
+                *reinterpret_cast<int4*>(d2) =
+                    make_int4(int32_t((t.x >> 16) + uint32_t(f.x)), int32_t((t.y >> 16) + uint32_t(f.y)),
+                              int32_t((t.z >> 16) + uint32_t(f.z)), int32_t((t.w >> 16) + uint32_t(f.w)));
+        } else {
+            for (int u = 0; u < 4 && c + u < kcount; ++u) {
+                d1[u] = int32_t((src[u] & 0xFFFFu) + uint32_t(fc[u]));
+                if (d2) d2[u] = int32_t((src[u] >> 16) + uint32_t(fc[u]));
             }
         }
     }
@@ -458,17 +478,34 @@ const char* launch_fast(const FastArgs& args, dim3 grid, size_t smem, cudaStream
     return "gapblock_fast_kernel";
 }
 
-// Profile height LQ >= longest query (32 or 64).
-int profile_height(int longest_query) { return longest_query <= 32 ? 32 : 64; }
+// Profile height LQ >= longest query: rows per pair in shared memory.
+int profile_height(int longest_query) {
+    for (int h : {16, 24, 32, 48})
+        if (longest_query <= h) return h;
+    return 64;
+}
+
+template <int LQ>
+const char* dispatch_prior(bool prior, const FastArgs& args, dim3 grid, size_t smem,
+                           cudaStream_t stream) {
+    return prior ? launch_fast<LQ, true>(args, grid, smem, stream)
+                 : launch_fast<LQ, false>(args, grid, smem, stream);
+}
 
 const char* dispatch_fast(int lq, bool prior, const FastArgs& args, dim3 grid, size_t smem,
                           cudaStream_t stream) {
-    if (lq == 32)
-        return prior ? launch_fast<32, true>(args, grid, smem, stream)
-                     : launch_fast<32, false>(args, grid, smem, stream);
-    return prior ? launch_fast<64, true>(args, grid, smem, stream)
-                 : launch_fast<64, false>(args, grid, smem, stream);
+    switch (lq) {
+        case 16: return dispatch_prior<16>(prior, args, grid, smem, stream);
+        case 24: return dispatch_prior<24>(prior, args, grid, smem, stream);
+        case 32: return dispatch_prior<32>(prior, args, grid, smem, stream);
+        case 48: return dispatch_prior<48>(prior, args, grid, smem, stream);
+        default: return dispatch_prior<64>(prior, args, grid, smem, stream);
+    }
 }
+
+// Words per prior row: value i at i + 3, rounded up so that every row is 16-byte aligned and
+// the last aligned group of four stays inside the row.
+int prior_stride(int W1) { return (W1 + 3 + 4 + 3) & ~3; }
 
 // Device-side tables of the fast path and the arguments they were built from.
 struct GbTables {
@@ -495,8 +532,9 @@ void build_tables(GbTables& tb, const std::vector<int32_t>& pen, int32_t go, int
     const int W1 = W + 1;
     const int32_t cap = 2 * bias + 1;
     std::vector<int32_t> ftab(size_t(W1) * W1, 0);
+    const int pstride = prior_stride(W1);
     std::vector<uint32_t> prior2;
-    if (prior) prior2.assign(size_t(W1) * W1 * W1, 0);
+    if (prior) prior2.assign(size_t(W1) * W1 * pstride, 0);
     for (int m = 0; m <= W; ++m)
         for (int n = 0; n <= W; ++n) {
             const int M = std::max(m, n), d = std::abs(m - n), L = std::min(m, n);
@@ -507,7 +545,7 @@ void build_tables(GbTables& tb, const std::vector<int32_t>& pen, int32_t go, int
                 pmin = row[0];
                 for (int i = 1; i <= L; ++i) pmin = std::min(pmin, row[i]);
                 if (m >= n) {  // fill each (M, d) row once
-                    uint32_t* dst = prior2.data() + (size_t(M) * W1 + d) * W1;
+                    uint32_t* dst = prior2.data() + (size_t(M) * W1 + d) * pstride + 3;
                     for (int i = 0; i <= L; ++i)
                         dst[i] = uint32_t(std::min<int64_t>(int64_t(row[i]) - pmin, cap)) * 0x10001u;
                 }
@@ -525,9 +563,25 @@ void build_tables(GbTables& tb, const std::vector<int32_t>& pen, int32_t go, int
 }
 
 // Shared memory of one CTA for a given chunk width.
+// CTAs per SM the fast kernel's registers allow (256 threads x <= 80 registers).
+constexpr int kTargetBlocks = 3;
+
+const void* fast_kernel_ptr(int lq, bool prior) {
+#define STB_K(LQ)                                                                             \
+    if (lq == LQ)                                                                             \
+        return prior ? reinterpret_cast<const void*>(gapblock_fast_kernel<LQ, true>)          \
+                     : reinterpret_cast<const void*>(gapblock_fast_kernel<LQ, false>);
+    STB_K(16) STB_K(24) STB_K(32) STB_K(48)
+#undef STB_K
+    return prior ? reinterpret_cast<const void*>(gapblock_fast_kernel<64, true>)
+                 : reinterpret_cast<const void*>(gapblock_fast_kernel<64, false>);
+}
+
+// The profile area is reused for the per-slice column terms at write-out time.
 size_t fast_smem(int lq, int64_t slab_cap, int rc, int W1) {
-    return size_t(kGP) * lq * kRow * 4 + size_t(slab_cap) + size_t(kGP) * rc * 4 +
-           size_t((W1 * W1 + 3) & ~3) * 4 + size_t((rc + 15) & ~15) + 16;
+    const size_t prof = std::max(size_t(kGP) * lq * kRow * 4, size_t(kGP / kPairsPerSlice) * rc * 4);
+    return prof + size_t(slab_cap) + size_t(kGP) * rc * 4 + size_t((W1 * W1 + 3) & ~3) * 4 +
+           size_t((rc + 15) & ~15) + 16;
 }
 
 }  // namespace
@@ -575,12 +629,26 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
     if (fast) {
         RefPlan& rp = plan_slot<RefPlan>(rs.gb_ref_plan, ctx.tmp_ref_plan, rs.owns);
         if (rp.uid != rs.uid) {
-            // Widest chunk whose CTA fits in shared memory (narrower chunks fill warps worse).
-            for (int rc : {1024, 512, 256}) {
+            Phase ph("ref_plan");
+            // Chunk width: the widest (best warp fill) that still reaches the highest CTA
+            // residency the kernel's registers allow, checked with the occupancy calculator.
+            const void* kern = fast_kernel_ptr(lq, has_prior);
+            int best_rc = 0, best_blocks = -1;
+            for (int rc : {1024, 896, 768, 640, 512, 384, 256}) {
                 build_ref_plan(rp, rs, rc, stream);
-                smem = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rc, W1);
-                if (smem <= size_t(ctx.max_smem_optin)) break;
+                const size_t sm = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rc, W1);
+                if (sm > size_t(ctx.max_smem_optin)) continue;
+                int blocks = 0;
+                STB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              ctx.max_smem_optin));
+                STB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, kThreads, sm));
+                if (blocks > best_blocks) {
+                    best_blocks = blocks;
+                    best_rc = rc;
+                }
+                if (blocks >= kTargetBlocks) break;
             }
+            if (best_rc && rp.rc != best_rc) build_ref_plan(rp, rs, best_rc, stream);
             const unsigned blocks = unsigned(rp.ntasks);
             if (blocks) {
                 ref_slab_kernel<<<blocks, 128, 0, stream>>>(
@@ -628,13 +696,17 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
         put(hdr, sizeof hdr);
         put(pen.data(), pen.size() * 4);
         if (has_prior) put(prior, size_t(prior_len) * 4);
+        Phase ph("tables");
         if (!same_as_last(tb.key, key.data(), key.size()))
             build_tables(tb, pen, go, ge, W, bias, has_prior ? prior : nullptr, W1p, stream);
     }
 
     // Query pairs and their profile (rebuilt when the set or the penalty grid changes).
     QueryPlan& qp = plan_slot<QueryPlan>(qs.gb_query_plan, ctx.tmp_query_plan, qs.owns);
-    if (qp.uid != qs.uid) build_query_plan(qp, qs, stream);
+    if (qp.uid != qs.uid) {
+        Phase ph("query_plan");
+        build_query_plan(qp, qs, stream);
+    }
     {
         std::vector<uint8_t> key(sizeof(int) * 2 + pen.size() * 4);
         const int hdr[2] = {A, lq};
@@ -671,6 +743,7 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
     fa.prior2 = has_prior ? static_cast<uint32_t*>(tb.prior2.ptr) : nullptr;
     fa.ftab = static_cast<int32_t*>(tb.ftab.ptr);
     fa.W1 = W1;
+    fa.pstride = prior_stride(W1);
     fa.bias2 = uint32_t(bias) * 0x10001u;
     fa.out = out_d;
     fa.err = err;

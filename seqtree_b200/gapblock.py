@@ -14,6 +14,8 @@ from __future__ import annotations
 
 from collections.abc import Callable, Iterable, Sequence
 
+import numpy as np
+
 from ._core import gapblock_matrix as _gapblock_matrix
 from .matrix import ScoreMatrix, SubstitutionMatrix
 
@@ -35,6 +37,13 @@ def gap_cost(d: int, gap_open: int, gap_extend: int) -> int:
     return 0 if d == 0 else gap_open + (d - 1) * gap_extend
 
 
+def _cube_index(width: int):
+    """(i, d, m) grids of the reachable cells of a width-``width`` cube (d >= 1, i <= m - d)."""
+    w1 = width + 1
+    m, d, i = np.meshgrid(np.arange(w1), np.arange(w1), np.arange(w1), indexing="ij")
+    return i, d, m, (d >= 1) & (i <= m - d)
+
+
 def central_prior(lam: int) -> GapPrior:
     """``lam * |block midpoint - m/2|`` as ``int(lam * |2i + d - m| // 2)``; 0 at d == 0."""
     if lam < 0:
@@ -43,6 +52,15 @@ def central_prior(lam: int) -> GapPrior:
     def prior(i: int, d: int, m: int) -> int:
         return 0 if d == 0 else int(lam * abs(2 * i + d - m) // 2)
 
+    def cube(width: int) -> np.ndarray:
+        # Same arithmetic as prior() in int64 (an int lam) or float64 (a float lam): a floor
+        # division of a non-negative value, then truncation, exactly as int(...) of it.
+        i, d, m, ok = _cube_index(width)
+        x = np.abs(2 * i + d - m)
+        v = (lam * x) // 2 if isinstance(lam, (int, np.integer)) else np.floor_divide(lam * x, 2)
+        return np.where(ok, v, 0).astype(np.int64)
+
+    prior.cube = cube
     return prior
 
 
@@ -68,6 +86,12 @@ def frame_prior(lam: int, c: int) -> GapPrior:
     def prior(i: int, d: int, m: int) -> int:
         return 0 if d == 0 else lam * abs(i - c)
 
+    def cube(width: int) -> np.ndarray:
+        i, d, m, ok = _cube_index(width)
+        return np.where(ok, lam * np.abs(i - c), 0).astype(np.int64)
+
+    if isinstance(lam, (int, np.integer)) and isinstance(c, (int, np.integer)):
+        prior.cube = cube
     return prior
 
 
@@ -95,12 +119,23 @@ def _default_gap_open(matrix: SubstitutionMatrix | None) -> int:
     return 2 * matrix.scale() if matrix is not None else 1
 
 
-def prior_cube(prior: GapPrior, width: int) -> list[int]:
+def prior_cube(prior: GapPrior, width: int):
     """Flatten ``prior`` to ``[m][d][i]`` with stride ``width + 1``.
 
     Only reachable cells are filled -- ``d >= 1`` and ``i <= m - d`` -- the rest stay zero and
-    are never read.  A negative prior value raises ValueError naming the cell.
+    are never read.  A negative prior value raises ValueError naming the cell.  The built-in
+    central and frame priors fill the cube with numpy (same values); any other callable is
+    evaluated cell by cell.
     """
+    fast = getattr(prior, "cube", None)
+    if fast is not None:
+        c = fast(width)
+        if (c < 0).any():
+            mm, dd, ii = (int(x[0]) for x in np.nonzero(c < 0))
+            raise ValueError(f"gap_prior({ii}, {dd}, {mm}) = {int(c[mm, dd, ii])} is negative")
+        if c.max(initial=0) >= 2 ** 31:
+            raise TypeError("prior entries must fit a 32-bit signed integer")
+        return c.astype(np.int32).ravel()
     w1 = width + 1
     cube = [0] * (w1 * w1 * w1)
     for m in range(w1):
@@ -132,6 +167,6 @@ def score_matrix(queries: Sequence[str], refs: Sequence[str],
         gap_open = _default_gap_open(matrix)
     if gap_open < 0 or gap_extend < 0:
         raise ValueError("gap_open and gap_extend must be >= 0")
-    width = max((len(s) for s in q + r), default=0)
+    width = max(max(map(len, q), default=0), max(map(len, r), default=0))
     cube = prior_cube(gap_prior, width) if gap_prior is not None else []
     return _gapblock_matrix(q, r, alphabet, matrix, gap_open, gap_extend, cube, width, threads)
