@@ -7,14 +7,28 @@ dense matrix calls.
 * :mod:`seqtree_b200.device` -- the same computations on device-resident sequence sets.
 
 Everything runs on the current CUDA device through ``libseqtree_b200.so``; there is no CPU
-fallback.  Results are bit-identical to seqtree 0.6.0's C++ on the same inputs.
+fallback.  Results are bit-identical to seqtree 0.6.0's C++ on the same inputs.  The compiled
+library is loaded on first use of a module that needs it, so ``python -m seqtree_b200.build``
+works before it exists.
 """
-from . import _core, distance, gapblock, pairwise
-from .gapblock import central_prior, frame_prior, positions_prior, profile_prior, score_matrix
+import importlib
+
 from .matrix import ScoreMatrix, SubstitutionMatrix, alphabet_symbols, amino_acids
 
 __version__ = "0.1.0"
 
+_MODULES = {"distance", "gapblock", "pairwise", "device", "_core", "_lib"}
+_FROM_GAPBLOCK = {"score_matrix", "central_prior", "frame_prior", "positions_prior",
+                  "profile_prior"}
+
 __all__ = ["distance", "gapblock", "pairwise", "score_matrix", "central_prior", "frame_prior",
            "positions_prior", "profile_prior", "ScoreMatrix", "SubstitutionMatrix",
            "alphabet_symbols", "amino_acids"]
+
+
+def __getattr__(name):
+    if name in _MODULES:
+        return importlib.import_module(f".{name}", __name__)
+    if name in _FROM_GAPBLOCK:
+        return getattr(importlib.import_module(".gapblock", __name__), name)
+    raise AttributeError(f"module 'seqtree_b200' has no attribute '{name}'")
