@@ -150,6 +150,24 @@ int32_t st_hamming_matrix_sets(st_seqset a, st_seqset b, int32_t *out_device, vo
 int32_t st_levenshtein_matrix_sets(st_seqset a, st_seqset b, int32_t *out_device,
                                    void *cuda_stream, st_error *err);
 
+/*
+ * Levenshtein matrix that allocates nothing, for callers that cannot let a library allocate
+ * device memory (their device memory is owned by their own allocator or reserved to a fixed
+ * budget, or an allocation's latency or failure is unacceptable on their path).  No counterpart
+ * in the reference.  All pointers are DEVICE memory owned by the caller: the concatenated raw
+ * bytes and count+1 int64 offsets of each side, and the a_count*b_count int32 row-major output.
+ * Same results as st_levenshtein_matrix.  The kernel's scratch is a fixed 32 MiB array inside
+ * the library (held by every GPU that loads it); inputs whose DP row (shorter length + 1 words)
+ * does not fit it for 256 threads are rejected with ST_EINVAL.  The first call on a device looks
+ * up the array's address (make it before any stream capture).  The call synchronises
+ * cuda_stream once (to size the launch) and returns with the matrix kernel enqueued on it.
+ * Calls share the array: calls whose work overlaps on the GPU race.
+ */
+int32_t st_levenshtein_matrix_noalloc(const char *a_bytes, const int64_t *a_offsets,
+                                      int64_t a_count, const char *b_bytes,
+                                      const int64_t *b_offsets, int64_t b_count, int32_t *out,
+                                      void *cuda_stream, st_error *err);
+
 /* Launch statistics of the last *_sets / host call on this thread: how many kernels of this
  * library it launched and the name of the main kernel variant it chose. */
 int32_t st_last_launch_count(void);

@@ -61,6 +61,9 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
     ("st_levenshtein_matrix_sets", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_levenshtein_matrix_noalloc", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, _ep]),
     ("st_last_launch_count", ctypes.c_int32, []),
     ("st_last_kernel_name", ctypes.c_char_p, []),
     ("st_host_alloc", ctypes.c_void_p, [ctypes.c_uint64]),
