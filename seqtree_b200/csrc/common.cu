@@ -83,6 +83,16 @@ DevBuf::~DevBuf() {
     // Contexts live until process exit; the driver reclaims device memory then.
 }
 
+void h2d(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+    if (bytes == 0) return;
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    STB_CUDA(cudaStreamIsCapturing(stream, &st));
+    if (st != cudaStreamCaptureStatusNone)
+        fail(ST_EINVAL, "seqtree_b200: this call has tables or plans to upload; make the same call "
+                        "once before capturing it into a CUDA graph");
+    STB_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+}
+
 bool same_as_last(std::vector<uint8_t>& slot, const void* data, size_t bytes) {
     if (slot.size() == bytes && (bytes == 0 || std::memcmp(slot.data(), data, bytes) == 0))
         return true;

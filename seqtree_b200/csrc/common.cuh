@@ -79,12 +79,18 @@ struct Context {
     // storage of the transient sets made by the host-buffer entry points
     DevBuf tq[3], tr[3];  // bytes, offsets, lengths
     // plans reused by transient sets (rebuilt in place for every call)
-    std::shared_ptr<void> tmp_query_plan, tmp_ref_plan;
+    std::shared_ptr<void> tmp_query_plan, tmp_ref_plan, tmp_wave_plan[2];
 };
 
 // Context of the current CUDA device (created on first use).  Fails with ST_ENODEV when no
 // device is usable.
 Context& context();
+
+// Host -> device copy of per-call tables or plans.  Refuses to run while `stream` is being
+// captured into a CUDA graph: the captured copy would read host memory that is gone when the
+// graph is replayed.  Plans and tables are cached, so a call made once before capturing leaves
+// nothing to upload inside the capture.
+void h2d(void* dst, const void* src, size_t bytes, cudaStream_t stream);
 
 // Byte-exact content cache: returns true when `bytes` equals what was uploaded last time
 // under `slot`, so re-uploads of unchanged tables are skipped.
@@ -109,7 +115,7 @@ struct st_seqset_s {
     bool owns = true;           // false: storage borrowed from the context (transient set)
     uint64_t uid = 0;           // unique per set; plans record the uid they were built for
     // plan caches (opaque; transient sets share the context's)
-    std::shared_ptr<void> gb_query_plan, gb_ref_plan;
+    std::shared_ptr<void> gb_query_plan, gb_ref_plan, wave_plan;
     ~st_seqset_s();
 };
 

@@ -64,6 +64,7 @@ struct RefPlan {
     int64_t nchunks = 0;
     int64_t ntasks = 0;
     int64_t max_slab = 0;                // largest per-chunk code slab (bytes)
+    int64_t slab_bytes = 0;              // whole slab
     std::vector<int32_t> sorted;
     std::vector<int4> tasks;             // (n, start in sorted, count <= 32, slab byte offset)
     std::vector<int32_t> task_off;       // nchunks + 1
@@ -94,10 +95,10 @@ void build_query_plan(QueryPlan& plan, const st_seqset_s& q, cudaStream_t stream
         i = e;
     }
     plan.P = int64_t(plan.pairs.size());
-    STB_CUDA(cudaMemcpyAsync(plan.d_pairs.as<int2>(size_t(plan.P)), plan.pairs.data(),
-                             sizeof(int2) * size_t(plan.P), cudaMemcpyHostToDevice, stream));
-    STB_CUDA(cudaMemcpyAsync(plan.d_plen.as<int32_t>(size_t(plan.P)), plan.plen.data(),
-                             sizeof(int32_t) * size_t(plan.P), cudaMemcpyHostToDevice, stream));
+    h2d(plan.d_pairs.as<int2>(size_t(plan.P)), plan.pairs.data(),
+                             sizeof(int2) * size_t(plan.P), stream);
+    h2d(plan.d_plen.as<int32_t>(size_t(plan.P)), plan.plen.data(),
+                             sizeof(int32_t) * size_t(plan.P), stream);
     plan.prof_key.clear();
     plan.uid = q.uid;
 }
@@ -105,7 +106,8 @@ void build_query_plan(QueryPlan& plan, const st_seqset_s& q, cudaStream_t stream
 // Refs in chunks of rc columns (original order); inside a chunk a counting sort by length
 // yields warp tasks of <= 32 refs of one length.  Each task's code rows occupy n*32 bytes of
 // the slab, so a chunk's slab is one contiguous range.
-void build_ref_plan(RefPlan& plan, const st_seqset_s& r, int rc, cudaStream_t stream) {
+void build_ref_plan(RefPlan& plan, const st_seqset_s& r, int rc, cudaStream_t stream,
+                    bool upload = true) {
     const int64_t K = r.count;
     plan.rc = rc;
     plan.nchunks = ceil_div(K, rc);
@@ -137,13 +139,14 @@ void build_ref_plan(RefPlan& plan, const st_seqset_s& r, int rc, cudaStream_t st
     }
     if (slab > INT32_MAX) fail(ST_EINVAL, "seqtree_b200: reference set too large for one call");
     plan.ntasks = int64_t(plan.tasks.size());
-    STB_CUDA(cudaMemcpyAsync(plan.d_sorted.as<int32_t>(size_t(K)), plan.sorted.data(),
-                             sizeof(int32_t) * size_t(K), cudaMemcpyHostToDevice, stream));
-    STB_CUDA(cudaMemcpyAsync(plan.d_tasks.as<int4>(plan.tasks.size()), plan.tasks.data(),
-                             sizeof(int4) * plan.tasks.size(), cudaMemcpyHostToDevice, stream));
-    STB_CUDA(cudaMemcpyAsync(plan.d_task_off.as<int32_t>(plan.task_off.size()),
-                             plan.task_off.data(), sizeof(int32_t) * plan.task_off.size(),
-                             cudaMemcpyHostToDevice, stream));
+    plan.slab_bytes = slab;
+    if (!upload) return;
+    h2d(plan.d_sorted.as<int32_t>(size_t(K)), plan.sorted.data(),
+                             sizeof(int32_t) * size_t(K), stream);
+    h2d(plan.d_tasks.as<int4>(plan.tasks.size()), plan.tasks.data(),
+                             sizeof(int4) * plan.tasks.size(), stream);
+    h2d(plan.d_task_off.as<int32_t>(plan.task_off.size()),
+                             plan.task_off.data(), sizeof(int32_t) * plan.task_off.size(), stream);
     plan.d_slab.as<uint8_t>(size_t(slab) + 16);
     plan.uid = r.uid;
 }
@@ -553,13 +556,11 @@ void build_tables(GbTables& tb, const std::vector<int32_t>& pen, int32_t go, int
             ftab[size_t(m) * W1 + n] = int32_t(uint32_t(pmin) + uint32_t(go) +
                                                uint32_t(d - 1) * uint32_t(ge));
         }
-    STB_CUDA(cudaMemcpyAsync(tb.pen.as<int32_t>(pen.size()), pen.data(), pen.size() * 4,
-                             cudaMemcpyHostToDevice, stream));
-    STB_CUDA(cudaMemcpyAsync(tb.ftab.as<int32_t>(ftab.size()), ftab.data(), ftab.size() * 4,
-                             cudaMemcpyHostToDevice, stream));
+    h2d(tb.pen.as<int32_t>(pen.size()), pen.data(), pen.size() * 4, stream);
+    h2d(tb.ftab.as<int32_t>(ftab.size()), ftab.data(), ftab.size() * 4, stream);
     if (prior)
-        STB_CUDA(cudaMemcpyAsync(tb.prior2.as<uint32_t>(prior2.size()), prior2.data(),
-                                 prior2.size() * 4, cudaMemcpyHostToDevice, stream));
+        h2d(tb.prior2.as<uint32_t>(prior2.size()), prior2.data(),
+                                 prior2.size() * 4, stream);
 }
 
 // Shared memory of one CTA for a given chunk width.
@@ -635,7 +636,7 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
             const void* kern = fast_kernel_ptr(lq, has_prior);
             int best_rc = 0, best_blocks = -1;
             for (int rc : {1024, 896, 768, 640, 512, 384, 256}) {
-                build_ref_plan(rp, rs, rc, stream);
+                build_ref_plan(rp, rs, rc, stream, /*upload=*/false);
                 const size_t sm = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rc, W1);
                 if (sm > size_t(ctx.max_smem_optin)) continue;
                 int blocks = 0;
@@ -648,7 +649,7 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
                 }
                 if (blocks >= kTargetBlocks) break;
             }
-            if (best_rc && rp.rc != best_rc) build_ref_plan(rp, rs, best_rc, stream);
+            if (best_rc) build_ref_plan(rp, rs, best_rc, stream);
             const unsigned blocks = unsigned(rp.ntasks);
             if (blocks) {
                 ref_slab_kernel<<<blocks, 128, 0, stream>>>(
@@ -665,12 +666,11 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
 
     if (!fast) {
         int32_t* d_pen = ctx.table_buf.as<int32_t>(pen.size());
-        STB_CUDA(cudaMemcpyAsync(d_pen, pen.data(), pen.size() * 4, cudaMemcpyHostToDevice, stream));
+        h2d(d_pen, pen.data(), pen.size() * 4, stream);
         int32_t* d_prior = nullptr;
         if (has_prior) {
             d_prior = ctx.prior_buf.as<int32_t>(size_t(prior_len));
-            STB_CUDA(cudaMemcpyAsync(d_prior, prior, size_t(prior_len) * 4, cudaMemcpyHostToDevice,
-                                     stream));
+            h2d(d_prior, prior, size_t(prior_len) * 4, stream);
         }
         GeneralArgs g{qs.d_bytes, qs.d_off, rs.d_bytes, rs.d_off, N, K, d_pen, A, go, ge,
                       d_prior, W1p, out_d};
@@ -697,8 +697,14 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
         put(pen.data(), pen.size() * 4);
         if (has_prior) put(prior, size_t(prior_len) * 4);
         Phase ph("tables");
-        if (!same_as_last(tb.key, key.data(), key.size()))
-            build_tables(tb, pen, go, ge, W, bias, has_prior ? prior : nullptr, W1p, stream);
+        if (!same_as_last(tb.key, key.data(), key.size())) {
+            try {
+                build_tables(tb, pen, go, ge, W, bias, has_prior ? prior : nullptr, W1p, stream);
+            } catch (...) {
+                tb.key.clear();  // not uploaded: the next call builds them again
+                throw;
+            }
+        }
     }
 
     // Query pairs and their profile (rebuilt when the set or the penalty grid changes).
@@ -713,6 +719,7 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
         std::memcpy(key.data(), hdr, sizeof hdr);
         std::memcpy(key.data() + sizeof hdr, pen.data(), pen.size() * 4);
         if (!same_as_last(qp.prof_key, key.data(), key.size())) {
+            qp.prof_key.clear();  // set again once the profile kernel is enqueued
             const int64_t total = qp.P * lq * kRow;
             uint32_t* prof = qp.d_prof.as<uint32_t>(size_t(total));
             profile_kernel<<<unsigned(ceil_div(total, 256)), 256, 0, stream>>>(
@@ -721,6 +728,7 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
                 total, prof);
             STB_CUDA(cudaGetLastError());
             note_launch(nullptr);
+            qp.prof_key = key;
         }
     }
 

@@ -11,6 +11,9 @@
 // 2^31-1 gap costs the reference's tests pin.
 #include <algorithm>
 #include <climits>
+#include <map>
+#include <numeric>
+#include <tuple>
 
 #include "common.cuh"
 
@@ -140,6 +143,311 @@ void launch_exact(Context& ctx, ExactArgs a, int64_t work, cudaStream_t stream) 
     note_launch("gotoh_exact_kernel");
 }
 
+// ------------------------------------------------------------------------- wavefront path ---
+// Warp-cooperative anti-diagonal wavefront.  A warp scores one query against two refs at once
+// (int16x2 halves).  Lane t owns query rows t*R+1 .. t*R+R and at step s processes column
+// j = s - t + 1, so the row above its first row (lane t-1's last row, same column) was finished
+// one step earlier and arrives by one shuffle, together with the column's two ref residues.
+// Cells are updated with DPX max-plus ops on both halves; the substitution scores of a cell pair
+// come from one shared-memory word T[q][r1][r2] = s(q,r1) | s(q,r2) << 16, where the extra code
+// A pads rows past the query and columns past the shorter ref with NEG.
+//
+// With gap_extend <= gap_open the vertical gap is max(H_up - open, X_up - extend): H includes X,
+// and X_up - open <= X_up - extend, so adding it to the opening term never changes the maximum --
+// this is the reference's max(M_up - open, Y_up - open, X_up - extend) (pairwise.cpp:113), and
+// likewise for the horizontal gap (:114).  Otherwise (EXACT) the opening terms use max(M, Y) and
+// max(M, X) as the reference does.
+//
+// int16 safety: the host admits a call only when every finite cell lies within +-14000
+// (|s| * L + open + extend * (rows + cols) <= 14000, |s| <= 2000); then NEG = -16384 and every
+// NEG-derived candidate stays below every finite one without wrapping.
+constexpr int kWaveThreads = 256;
+constexpr uint32_t kNeg2 = 0xC000C000u;  // -16384 in both halves
+
+struct WaveArgs {
+    const uint8_t* qc;
+    const int64_t* qoff;
+    const uint8_t* rc;
+    const int64_t* roff;
+    const int32_t* qlist;   // queries of this launch (all of one row bucket)
+    int64_t nq;
+    const int2* rpairs;     // ref pairs of similar length (x == y for an odd one out)
+    int64_t nrp;
+    const uint32_t* table;  // A1^3 words
+    int A1;                 // alphabet size + 1 (the last code pads)
+    int32_t go, ge;
+    int self;               // 1: each query against itself, int64 result to self_out
+    int64_t* self_out;
+    int dist;
+    const int64_t* q_self;
+    const int64_t* r_self;
+    int32_t* out;
+    int64_t K;
+    unsigned int* overflow;
+};
+
+__device__ __forceinline__ uint32_t dup2(int v) { return (uint32_t(uint16_t(int16_t(v))) * 0x10001u); }
+__device__ __forceinline__ int lo16(uint32_t v) { return int(int16_t(uint16_t(v & 0xFFFFu))); }
+__device__ __forceinline__ int hi16(uint32_t v) { return int(int16_t(uint16_t(v >> 16))); }
+
+template <int R, bool LOCAL, bool EXACT>
+__global__ void __launch_bounds__(kWaveThreads) gotoh_wave_kernel(const WaveArgs a) {
+    extern __shared__ uint32_t s_tab[];
+    const int A1 = a.A1, pad = A1 - 1;
+    for (int i = threadIdx.x; i < A1 * A1 * A1; i += blockDim.x) s_tab[i] = a.table[i];
+    __syncthreads();
+    const unsigned full = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const int64_t gwarp = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    const int64_t ntasks = a.self ? a.nq : a.nq * a.nrp;
+    const uint32_t mgo2 = dup2(-a.go), mge2 = dup2(-a.ge);
+
+    for (int64_t task = gwarp; task < ntasks; task += nwarps) {
+        const int64_t qi_idx = a.self ? task : task / a.nrp;
+        const int qi = a.qlist[qi_idx];
+        int k1 = qi, k2 = qi;
+        if (!a.self) {
+            const int2 rp = a.rpairs[task - qi_idx * a.nrp];
+            k1 = rp.x;
+            k2 = rp.y;
+        }
+        const uint8_t* q = a.qc + a.qoff[qi];
+        const int m = int(a.qoff[qi + 1] - a.qoff[qi]);
+        const uint8_t* rbase = a.self ? a.qc : a.rc;
+        const int64_t* roff = a.self ? a.qoff : a.roff;
+        const uint8_t* r1 = rbase + roff[k1];
+        const uint8_t* r2 = rbase + roff[k2];
+        const int n1 = int(roff[k1 + 1] - roff[k1]);
+        const int n2 = int(roff[k2 + 1] - roff[k2]);
+        const int nmax = max(n1, n2);
+
+        // Rows of this lane: 1-indexed i = lane*R + r + 1; column 0 state per row.
+        uint32_t qb[R], Hl[R], Yl[R], MXl[EXACT ? R : 1];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int row = lane * R + r;  // 0-indexed query position
+            qb[r] = uint32_t((row < m ? q[row] : pad) * A1 * A1);
+            const int gr = a.go + row * a.ge;  // gap_run(row + 1)
+            Hl[r] = LOCAL ? 0u : dup2(-gr);
+            Yl[r] = kNeg2;
+            if constexpr (EXACT) MXl[r] = Hl[r];
+        }
+        // H[lane*R][0]: the row above this lane's first row, at column 0.
+        uint32_t diag = (lane == 0 || LOCAL) ? 0u : dup2(-(a.go + (lane * R - 1) * a.ge));
+        uint32_t best = 0u, cap = 0u;
+        uint32_t outH = 0u, outX = kNeg2, outMY = 0u;
+        int outRes = 0;
+        const int cap_lane = (m - 1) / R, cap_r = (m - 1) - cap_lane * R;
+        const int steps = nmax + 31;
+        for (int s = 0; s < steps; ++s) {
+            uint32_t upH = __shfl_up_sync(full, outH, 1);
+            uint32_t upX = __shfl_up_sync(full, outX, 1);
+            uint32_t upMY = EXACT ? __shfl_up_sync(full, outMY, 1) : 0u;
+            int res = __shfl_up_sync(full, outRes, 1);
+            const int j = s - lane + 1;
+            if (lane == 0) {  // the virtual row 0 at column j
+                const uint32_t h0 = LOCAL ? 0u : dup2(-(a.go + (j - 1) * a.ge));
+                upH = h0;
+                upX = kNeg2;
+                upMY = h0;
+                res = (j <= n1 ? int(r1[j - 1]) : pad) | ((j <= n2 ? int(r2[j - 1]) : pad) << 8);
+            }
+            if (j >= 1 && j <= nmax) {
+                const uint32_t col = uint32_t((res & 0xFF) * A1 + (res >> 8));
+                const uint32_t top = upH;
+                uint32_t d = diag;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    const uint32_t sc = s_tab[qb[r] + col];
+                    const uint32_t M = LOCAL ? __viaddmax_s16x2_relu(d, sc, kNeg2)
+                                             : __viaddmax_s16x2(d, sc, kNeg2);
+                    uint32_t X, Y;
+                    if constexpr (EXACT) {
+                        X = __viaddmax_s16x2(upMY, mgo2, __viaddmax_s16x2(upX, mge2, kNeg2));
+                        Y = __viaddmax_s16x2(MXl[r], mgo2, __viaddmax_s16x2(Yl[r], mge2, kNeg2));
+                    } else {
+                        X = __viaddmax_s16x2(upH, mgo2, __viaddmax_s16x2(upX, mge2, kNeg2));
+                        Y = __viaddmax_s16x2(Hl[r], mgo2, __viaddmax_s16x2(Yl[r], mge2, kNeg2));
+                    }
+                    const uint32_t H = __vimax3_s16x2(M, X, Y);
+                    if constexpr (LOCAL) best = __vimax3_s16x2(best, M, kNeg2);
+                    d = Hl[r];
+                    Hl[r] = H;
+                    Yl[r] = Y;
+                    upH = H;
+                    upX = X;
+                    if constexpr (EXACT) {
+                        MXl[r] = __vimax3_s16x2(M, X, kNeg2);
+                        upMY = __vimax3_s16x2(M, Y, kNeg2);
+                    }
+                }
+                diag = top;
+                outH = upH;
+                outX = upX;
+                outMY = upMY;
+                outRes = res;
+                if (!LOCAL && lane == cap_lane && (j == n1 || j == n2)) {
+                    uint32_t h = 0u;
+#pragma unroll
+                    for (int r = 0; r < R; ++r)
+                        if (r == cap_r) h = Hl[r];
+                    if (j == n1) cap = (cap & 0xFFFF0000u) | (h & 0xFFFFu);
+                    if (j == n2) cap = (cap & 0xFFFFu) | (h & 0xFFFF0000u);
+                }
+            }
+        }
+        int v1, v2;
+        if constexpr (LOCAL) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1)
+                best = __vimax3_s16x2(best, __shfl_xor_sync(full, best, off), kNeg2);
+            v1 = lo16(best);
+            v2 = hi16(best);
+        } else {
+            cap = __shfl_sync(full, cap, cap_lane);
+            v1 = lo16(cap);
+            v2 = hi16(cap);
+        }
+        if (lane == 0) {
+            if (a.self) {
+                a.self_out[qi] = v1;
+            } else {
+                for (int t = 0; t < (k2 != k1 ? 2 : 1); ++t) {
+                    const int k = t ? k2 : k1;
+                    const int64_t sv = t ? v2 : v1;
+                    const int64_t v = a.dist ? a.q_self[qi] + a.r_self[k] - 2 * sv : sv;
+                    if (v < INT32_MIN || v > INT32_MAX)
+                        atomicOr(a.overflow, 1u);
+                    else
+                        a.out[int64_t(qi) * a.K + k] = int32_t(v);
+                }
+            }
+        }
+    }
+}
+
+constexpr int kRowBuckets[] = {2, 4, 6, 8, 10, 12, 14, 16};
+
+int rows_per_lane(int m) {
+    for (int r : kRowBuckets)
+        if (m <= 32 * r) return r;
+    return 0;
+}
+
+template <int R>
+const void* wave_kernel_ptr(bool local, bool exact) {
+    if (local)
+        return exact ? reinterpret_cast<const void*>(gotoh_wave_kernel<R, true, true>)
+                     : reinterpret_cast<const void*>(gotoh_wave_kernel<R, true, false>);
+    return exact ? reinterpret_cast<const void*>(gotoh_wave_kernel<R, false, true>)
+                 : reinterpret_cast<const void*>(gotoh_wave_kernel<R, false, false>);
+}
+
+const void* wave_kernel(int R, bool local, bool exact) {
+    switch (R) {
+        case 2: return wave_kernel_ptr<2>(local, exact);
+        case 4: return wave_kernel_ptr<4>(local, exact);
+        case 6: return wave_kernel_ptr<6>(local, exact);
+        case 8: return wave_kernel_ptr<8>(local, exact);
+        case 10: return wave_kernel_ptr<10>(local, exact);
+        case 12: return wave_kernel_ptr<12>(local, exact);
+        case 14: return wave_kernel_ptr<14>(local, exact);
+        default: return wave_kernel_ptr<16>(local, exact);
+    }
+}
+
+// Substitution table of the wavefront path, per device, and the grid it was built from.
+struct WaveState {
+    std::vector<uint8_t> key;
+    DevBuf table;
+};
+
+// Per-set launch plan (depends only on the lengths): the set's indices grouped by rows per
+// lane, with the (R, offset, count) of each group, and the set's sequences sorted by length and
+// paired with their neighbour (used when the set is the ref side).
+struct WavePlan {
+    uint64_t uid = 0;
+    std::vector<std::tuple<int, int64_t, int64_t>> groups;
+    int64_t npairs = 0;
+    DevBuf list, pairs;
+};
+
+WavePlan& wave_plan(st_seqset_s& s, Context& ctx, int slot, cudaStream_t stream) {
+    std::shared_ptr<void>& holder = s.owns ? s.wave_plan : ctx.tmp_wave_plan[slot];
+    if (!holder) holder = std::make_shared<WavePlan>();
+    WavePlan& p = *static_cast<WavePlan*>(holder.get());
+    if (p.uid == s.uid) return p;
+    std::vector<std::vector<int32_t>> b(17);
+    for (int64_t i = 0; i < s.count; ++i)
+        b[size_t(rows_per_lane(s.h_len[size_t(i)]))].push_back(int32_t(i));
+    std::vector<int32_t> all;
+    all.reserve(size_t(s.count));
+    p.groups.clear();
+    for (int R = 1; R <= 16; ++R)
+        if (!b[size_t(R)].empty()) {
+            p.groups.emplace_back(R, int64_t(all.size()), int64_t(b[size_t(R)].size()));
+            all.insert(all.end(), b[size_t(R)].begin(), b[size_t(R)].end());
+        }
+    std::vector<int32_t> order(static_cast<size_t>(s.count));
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
+        return s.h_len[size_t(x)] < s.h_len[size_t(y)];
+    });
+    std::vector<int32_t> pairs;
+    pairs.reserve(order.size() + 1);
+    for (size_t i = 0; i < order.size(); i += 2) {
+        pairs.push_back(order[i]);
+        pairs.push_back(i + 1 < order.size() ? order[i + 1] : order[i]);
+    }
+    p.npairs = int64_t(pairs.size() / 2);
+    // (a pageable-source copy has consumed the host vectors by the time it returns)
+    h2d(p.list.as<int32_t>(all.size()), all.data(), all.size() * 4, stream);
+    h2d(p.pairs.as<int32_t>(pairs.size()), pairs.data(), pairs.size() * 4, stream);
+    p.uid = s.uid;
+    return p;
+}
+
+WaveState& wave_state(int device) {
+    static std::mutex mu;
+    static std::map<int, std::unique_ptr<WaveState>> all;
+    std::lock_guard<std::mutex> lk(mu);
+    auto& p = all[device];
+    if (!p) p = std::make_unique<WaveState>();
+    return *p;
+}
+
+// Every finite cell of every pair within +-14000 (see the kernel's note), lengths 1..512.
+bool wave_eligible(const st_seqset_s& qs, const st_seqset_s& rs, const int32_t* sim, int A,
+                   int32_t go, int32_t ge) {
+    for (const st_seqset_s* s : {&qs, &rs})
+        for (int32_t l : s->h_len)
+            if (l < 1) return false;
+    if (qs.max_len > 512 || rs.max_len > 512) return false;
+    int64_t maxabs = 0;
+    for (int i = 0; i < A * A; ++i) maxabs = std::max<int64_t>(maxabs, std::llabs(int64_t(sim[i])));
+    if (maxabs > 2000) return false;
+    const int64_t rows = 512, cols = std::max(qs.max_len, rs.max_len);
+    const int64_t bound = maxabs * rows + int64_t(go) + int64_t(ge) * (rows + cols);
+    return bound <= 14000;
+}
+
+// Launches one wavefront pass: `list` queries (one row bucket) against `pairs` (or themselves).
+void launch_wave(Context& ctx, WaveArgs wa, int R, bool local, bool exact, cudaStream_t stream) {
+    const void* kern = wave_kernel(R, local, exact);
+    const size_t smem = size_t(wa.A1) * wa.A1 * wa.A1 * 4;
+    STB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    int per_sm = 0;
+    STB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWaveThreads, smem));
+    const int64_t ntasks = wa.self ? wa.nq : wa.nq * wa.nrp;
+    const int64_t warps_per_block = kWaveThreads / 32;
+    const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>(
+        ceil_div(ntasks, warps_per_block), int64_t(ctx.num_sms) * std::max(per_sm, 1)));
+    void* args[] = {&wa};
+    STB_CUDA(cudaLaunchKernel(kern, dim3(unsigned(blocks)), dim3(kWaveThreads), args, smem, stream));
+    note_launch("gotoh_wave_kernel");
+}
+
 }  // namespace
 
 void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int32_t matrix_size,
@@ -157,12 +465,88 @@ void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
     const int64_t N = qs.count, K = rs.count;
     if (N == 0 || K == 0) return;
     Context& ctx = context();
-    int32_t* d_sim = ctx.table_buf.as<int32_t>(size_t(A) * A);
-    STB_CUDA(cudaMemcpyAsync(d_sim, similarity, size_t(A) * A * 4, cudaMemcpyHostToDevice, stream));
     // Word 9 of the context flags: set when a result does not fit int32.
     auto* ovf = reinterpret_cast<unsigned int*>(ctx.flags_d + 9);
     STB_CUDA(cudaMemsetAsync(ovf, 0, 8, stream));
 
+    if (wave_eligible(qs, rs, similarity, A, go, ge)) {
+        WaveState& ws = wave_state(ctx.device);
+        const int A1 = A + 1;
+        {
+            // T[(q*A1 + r1)*A1 + r2] = s(q,r1) | s(q,r2) << 16, the pad code scoring NEG.
+            std::vector<uint8_t> key(size_t(A) * A * 4);
+            std::memcpy(key.data(), similarity, key.size());
+            if (!same_as_last(ws.key, key.data(), key.size())) {
+                std::vector<uint32_t> tab(size_t(A1) * A1 * A1);
+                auto sv = [&](int x, int y) -> int32_t {
+                    return (x == A || y == A) ? -16384 : similarity[x * A + y];
+                };
+                for (int x = 0; x < A1; ++x)
+                    for (int y1 = 0; y1 < A1; ++y1)
+                        for (int y2 = 0; y2 < A1; ++y2)
+                            tab[(size_t(x) * A1 + y1) * A1 + y2] =
+                                uint32_t(uint16_t(int16_t(sv(x, y1)))) |
+                                (uint32_t(uint16_t(int16_t(sv(x, y2)))) << 16);
+                try {
+                    h2d(ws.table.as<uint32_t>(tab.size()), tab.data(), tab.size() * 4, stream);
+                } catch (...) {
+                    ws.key.clear();  // not uploaded: the next call builds it again
+                    throw;
+                }
+            }
+        }
+        WavePlan& qp = wave_plan(qs, ctx, 0, stream);
+        WavePlan& rp = wave_plan(rs, ctx, 1, stream);
+        const bool local = mode == ST_MODE_LOCAL;
+        const bool exact = ge > go;
+        WaveArgs wa{};
+        wa.table = static_cast<uint32_t*>(ws.table.ptr);
+        wa.A1 = A1;
+        wa.go = go;
+        wa.ge = ge;
+        wa.overflow = ovf;
+        wa.K = K;
+        int64_t* q_self = nullptr;
+        int64_t* r_self = nullptr;
+        if (dist) {
+            q_self = ctx.work_b.as<int64_t>(size_t(N + K));
+            r_self = q_self + N;
+            for (int t = 0; t < 2; ++t) {
+                const st_seqset_s& s = t == 0 ? qs : rs;
+                const WavePlan& p = t == 0 ? qp : rp;
+                for (auto& [R, off, cnt] : p.groups) {
+                    WaveArgs sa = wa;
+                    sa.qc = s.d_bytes;
+                    sa.qoff = s.d_off;
+                    sa.qlist = static_cast<int32_t*>(p.list.ptr) + off;
+                    sa.nq = cnt;
+                    sa.self = 1;
+                    sa.self_out = t == 0 ? q_self : r_self;
+                    launch_wave(ctx, sa, R, local, exact, stream);
+                }
+            }
+        }
+        for (auto& [R, off, cnt] : qp.groups) {
+            WaveArgs ma = wa;
+            ma.qc = qs.d_bytes;
+            ma.qoff = qs.d_off;
+            ma.rc = rs.d_bytes;
+            ma.roff = rs.d_off;
+            ma.qlist = static_cast<int32_t*>(qp.list.ptr) + off;
+            ma.nq = cnt;
+            ma.rpairs = static_cast<int2*>(rp.pairs.ptr);
+            ma.nrp = rp.npairs;
+            ma.dist = dist;
+            ma.q_self = q_self;
+            ma.r_self = r_self;
+            ma.out = out_d;
+            launch_wave(ctx, ma, R, local, exact, stream);
+        }
+        return;
+    }
+
+    int32_t* d_sim = ctx.table_buf.as<int32_t>(size_t(A) * A);
+    h2d(d_sim, similarity, size_t(A) * A * 4, stream);
     ExactArgs a{};
     a.sim = d_sim;
     a.A = A;
