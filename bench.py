@@ -37,6 +37,14 @@ sys.path.insert(0, str(ROOT))
 AA20 = "ACDEFGHIKLMNPQRSTVWY"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes (read + write) per launch of the dominant kernel on the named workload, from the ncu
+# captures summarised in profiles/ (None until captured).
+TRAFFIC: dict[str, float | None] = {
+    "gapblock": 2.02e6,     # 1.89 MB read + 0.13 MB write (the result stays in L2)
+    "hamming": 1.31e9,      # 262 MB per 4,000 rows, scaled to 20,000 rows
+    "levenshtein": 1.03e9,  # 102.5 MB per 2,000 rows, scaled to 20,000 rows
+    "align": 1.05e6,        # one row-bucket launch of the wavefront kernel
+}
 
 
 # ----------------------------------------------------------------------------- workloads ----
@@ -85,8 +93,19 @@ def proteins(seed: int, n: int) -> list[str]:
     return out
 
 
-def make_workload(name: str, rank: int):
-    """Returns dict(queries, refs, kind, params, metric, cells_fn)."""
+def make_workload(name: str, rank: int, nq: int | None = None, nr: int | None = None):
+    """The named workload (queries, refs, kind, config, metric); nq / nr shrink it for
+    profiling captures of the same kernels on a smaller case."""
+    w = _make_workload(name, rank)
+    if nq is not None or nr is not None:
+        w["queries"] = w["queries"][:nq] if nq is not None else w["queries"]
+        w["refs"] = w["refs"][:nr] if nr is not None else w["refs"]
+        w["config"] = dict(w["config"], queries=len(w["queries"]), refs=len(w["refs"]),
+                           workload="REDUCED " + w["config"]["workload"])
+    return w
+
+
+def _make_workload(name: str, rank: int):
     qseed = 1 + 1000 * rank  # rank 0 scores exactly the named workload
     if name == "gapblock":
         return dict(kind="gapblock", queries=cdr3(qseed, 1000), refs=cdr3(0, 10000),
@@ -194,6 +213,33 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def kernel_roofline(w, cells: float, seconds: float, clocks) -> dict | None:
+    """The dominant kernel's own bound (the contract's roofline object above is the HBM one).
+
+    gap block: shared-memory bandwidth.  Every cell needs one 2-byte penalty; the kernel reads
+    them as conflict-free 32-bit words, two cells (two queries) per word, so the algorithmic
+    traffic is 2 B/cell against 128 B/clk/SM.
+    alignment: ALU pipe.  A DPX instruction updates one int16x2 cell pair, and the recurrence
+    needs 6 of them per pair (M, X, Y, H and the two gap extends) -- 3 per cell -- against
+    64 lanes/clk/SM.
+    """
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    sms = 148
+    if w["kind"] == "gapblock":
+        achieved = 2.0 * cells / seconds / 1e9
+        peak = sms * 128 * mhz * 1e6 / 1e9
+        return {"bound": "smem", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "work": "2 B of penalty per cell",
+                "peak_basis": f"148 SMs x 128 B/clk at {mhz:.0f} MHz"}
+    if w["kind"] == "align":
+        achieved = 3.0 * cells / seconds / 1e9
+        peak = sms * 64 * mhz * 1e6 / 1e9
+        return {"bound": "alu", "achieved": achieved, "peak": peak, "unit": "Glane-op/s",
+                "frac": achieved / peak, "work": "3 DPX lane-ops per cell (6 per int16x2 pair)",
+                "peak_basis": f"148 SMs x 64 ALU lanes/clk at {mhz:.0f} MHz"}
+    return None
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -265,7 +311,7 @@ def main_reference(args):
     world, rank, _ = dist_env()
     if rank != 0:
         return 0
-    w = make_workload(args.workload, 0)
+    w = make_workload(args.workload, 0, args.queries, args.refs)
     call, kind = cpu_reference_call(w, 0)
     # Each step is a bounded sample of the workload sized so the whole run stays in minutes.
     budget = float(os.environ.get("SEQTREE_B200_REF_STEP_S", "5"))
@@ -311,7 +357,7 @@ def main_ours(args):
     from seqtree_b200 import _lib, device
     from seqtree_b200.gapblock import central_prior, prior_cube
 
-    w = make_workload(args.workload, rank)
+    w = make_workload(args.workload, rank, args.queries, args.refs)
     q, r = w["queries"], w["refs"]
     N, K = len(q), len(r)
     stream = torch.cuda.current_stream()
@@ -439,9 +485,10 @@ def main_ours(args):
                        parallelism=f"{world} independent query blocks" if world > 1 else "single GPU"),
         "gcups": cells * world * args.steps / (total_ms / 1e3) / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
-                     "note": f"algorithmic bytes = 4 B/pair output + input residues; peak {src}; "
-                             "the gap-block kernel is integer-issue bound, see profiles/"},
+                     "frac": achieved / hbm, "traffic": TRAFFIC.get(w["kind"]),
+                     "note": f"algorithmic bytes = 4 B/pair output + input residues; peak {src} "
+                             "(of measured); traffic = ncu dram read+write per launch (profiles/)"},
+        "kernel_roofline": kernel_roofline(w, cells, per_launch_s, sampler.summary()),
         "e2e": e2e,
         "gpu_launches": launches * args.steps,
         "kernel": kernel_name,
@@ -472,6 +519,9 @@ def main(argv=None) -> int:
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="time eager launches instead")
+    ap.add_argument("--queries", type=int, default=None,
+                    help="use only the first N queries (smaller case for profiling captures)")
+    ap.add_argument("--refs", type=int, default=None, help="use only the first N refs")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return main_reference(args)
