@@ -17,7 +17,7 @@ from .matrix import ScoreMatrix, SubstitutionMatrix, alphabet_symbols, amino_aci
 
 __version__ = "0.1.0"
 
-_MODULES = {"distance", "gapblock", "pairwise", "device", "_core", "_lib"}
+_MODULES = {"distance", "gapblock", "pairwise", "device", "shard", "_core", "_lib"}
 _FROM_GAPBLOCK = {"score_matrix", "central_prior", "frame_prior", "positions_prior",
                   "profile_prior"}
 
