@@ -41,7 +41,7 @@ enum {
 /* Alphabet codes: the reference's enum class Alphabet (include/seqtree/types.hpp:9). */
 enum { ST_ALPHABET_AA = 0, ST_ALPHABET_NT = 1, ST_ALPHABET_IUPAC = 2 };
 
-/* Alignment modes: the reference's enum class AlignMode (include/seqtree/seqtree.hpp:182). */
+/* Alignment modes: the reference's enum class AlignMode (include/seqtree/seqtree.hpp:186). */
 enum { ST_MODE_GLOBAL = 0, ST_MODE_LOCAL = 1 };
 
 typedef struct st_strings {
@@ -103,7 +103,7 @@ int32_t st_align_dist_matrix(const st_strings *queries, const st_strings *refs,
 
 /*
  * Dense Hamming matrix over raw bytes, case-sensitive.
- * Replaces seqtree::hamming_matrix (include/seqtree/seqtree.hpp:237-238,
+ * Replaces seqtree::hamming_matrix (include/seqtree/seqtree.hpp:239-240,
  * src/distance.cpp:97-102) and _core.hamming_matrix (src/_bindings.cpp:586-600).
  * Fails with ST_EINVAL when any (a[i], b[k]) pair differs in length.
  */
@@ -112,7 +112,7 @@ int32_t st_hamming_matrix(const st_strings *a, const st_strings *b, int32_t thre
 
 /*
  * Dense Levenshtein (unit-cost edit distance) matrix over raw bytes, case-sensitive.
- * Replaces seqtree::levenshtein_matrix (include/seqtree/seqtree.hpp:239-240,
+ * Replaces seqtree::levenshtein_matrix (include/seqtree/seqtree.hpp:241-242,
  * src/distance.cpp:104-109) and _core.levenshtein_matrix (src/_bindings.cpp:602-615).
  */
 int32_t st_levenshtein_matrix(const st_strings *a, const st_strings *b, int32_t threads,
@@ -167,6 +167,16 @@ int32_t st_levenshtein_matrix_noalloc(const char *a_bytes, const int64_t *a_offs
                                       int64_t a_count, const char *b_bytes,
                                       const int64_t *b_offsets, int64_t b_count, int32_t *out,
                                       void *cuda_stream, st_error *err);
+
+/*
+ * The raw similarity grid of a built-in amino-acid matrix ("blosum62", "blosum45", "blosum80",
+ * "pam250", "pam100", "structural"), row-major 24*24 in the AminoAcid codec order, the numbers
+ * behind seqtree::SubstitutionMatrix::blosum62() etc. (include/seqtree/seqtree.hpp:48-53,
+ * src/substitution_matrix.cpp:52-74).  Writes *size = 24 and, when `out` is not NULL, the 576
+ * entries (capacity must be >= 576).  Host-only: needs no GPU.
+ */
+int32_t st_builtin_similarity(const char *name, int32_t *out, int32_t capacity, int32_t *size,
+                              st_error *err);
 
 /* Launch statistics of the last *_sets / host call on this thread: how many kernels of this
  * library it launched and the name of the main kernel variant it chose. */

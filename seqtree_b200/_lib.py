@@ -64,6 +64,8 @@ SIGNATURES = [
     ("st_levenshtein_matrix_noalloc", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_builtin_similarity", ctypes.c_int32,
+     [ctypes.c_char_p, _i32p, ctypes.c_int32, _i32p, _ep]),
     ("st_last_launch_count", ctypes.c_int32, []),
     ("st_last_kernel_name", ctypes.c_char_p, []),
     ("st_host_alloc", ctypes.c_void_p, [ctypes.c_uint64]),

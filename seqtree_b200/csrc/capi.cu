@@ -4,6 +4,7 @@
 // fails with the same message: gap costs, alphabet, matrix size, empty shapes (no further
 // checks, as in the reference), symbol encoding (queries before refs), then per-family checks.
 #include <algorithm>
+#include <cstring>
 #include <memory>
 
 #include "common.cuh"
@@ -101,6 +102,27 @@ int32_t st_device_count(void) {
         return 0;
     }
     return n;
+}
+
+namespace {
+#include "builtin_tables.inc"
+}  // namespace
+
+int32_t st_builtin_similarity(const char* name, int32_t* out, int32_t capacity, int32_t* size,
+                              st_error* err) {
+    return guard(err, [&] {
+        if (!name) fail(ST_EINVAL, "matrix name is NULL");
+        for (size_t m = 0; m < sizeof(kBuiltinNames) / sizeof(kBuiltinNames[0]); ++m) {
+            if (std::strcmp(name, kBuiltinNames[m]) != 0) continue;
+            if (size) *size = 24;
+            if (out) {
+                if (capacity < 24 * 24) fail(ST_EINVAL, "output holds fewer than 576 entries");
+                std::memcpy(out, kBuiltinSimilarity[m], sizeof(kBuiltinSimilarity[m]));
+            }
+            return;
+        }
+        fail(ST_EINVAL, std::string("unknown built-in matrix '") + name + "'");
+    });
 }
 
 int32_t st_last_launch_count(void) { return last_launches(); }

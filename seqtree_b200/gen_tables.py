@@ -1,4 +1,5 @@
-"""Regenerate ``seqtree_b200/_tables.py`` from the reference's similarity grids.
+"""Regenerate ``seqtree_b200/_tables.py`` and ``seqtree_b200/csrc/builtin_tables.inc`` from the
+reference's similarity grids.
 
 The six built-in amino-acid similarity matrices must hold exactly the reference's numbers for
 results to be bit-identical (seqtree 0.6.0 ``src/blosum62.inc``, ``blosum45.inc``,
@@ -42,6 +43,27 @@ def main(ref_root: str) -> None:
         out.append("    ),")
     out.append("}")
     (Path(__file__).parent / "_tables.py").write_text("\n".join(out) + "\n")
+    write_c_include(Path(__file__).parent / "csrc" / "builtin_tables.inc")
+
+
+def write_c_include(path: Path) -> None:
+    """The same grids as a C array for the library's ``st_builtin_similarity``."""
+    from importlib import util
+    spec = util.spec_from_file_location("_tables", Path(__file__).parent / "_tables.py")
+    mod = util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    out = ["// Built-in similarity grids, row/column order ARNDCQEGHILKMFPSTWYVBZX*.",
+           "// Generated by gen_tables.py; do not edit by hand.",
+           "static const char* const kBuiltinNames[] = {" +
+           ", ".join(f'"{n}"' for n in NAMES) + "};",
+           f"static const int32_t kBuiltinSimilarity[{len(NAMES)}][24 * 24] = {{"]
+    for name in NAMES:
+        out.append(f"    {{  // {name}")
+        for r in mod.SIMILARITY[name]:
+            out.append("        " + ", ".join(f"{v:3d}" for v in r) + ",")
+        out.append("    },")
+    out.append("};")
+    path.write_text("\n".join(out) + "\n")
 
 
 if __name__ == "__main__":
