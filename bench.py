@@ -7,7 +7,11 @@ uniform 10-20; numpy PCG64 seed 1 for queries, seed 0 for refs), BLOSUM62 penalt
 gap_open 8, gap_extend 1, central_prior(21); int32 output bit-identical to seqtree's C++.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload gapblock|hamming|
-                    levenshtein|nw|sw] [--impl ours|reference]
+                    levenshtein|nw|sw|sparse|sparse_structural] [--impl ours|reference]
+
+Other workloads: ``hamming`` / ``levenshtein`` (20,000 x 20,000 ACGT), ``nw`` / ``sw`` (4,096 x
+4,096 proteins, distance matrix), ``sparse`` / ``sparse_structural`` (100,000 x 1,000,000
+CDR3-like, thresholded at max_penalty 24 into CSR rows; the dense matrix would be 400 GB).
 
 * ``value``: pairs/s with inputs resident in HBM (device sets) and the result written to HBM,
   device-timed with CUDA events on the launching stream; the L2 is flushed (a 256 MiB write)
@@ -105,8 +109,36 @@ def make_workload(name: str, rank: int, nq: int | None = None, nr: int | None = 
     return w
 
 
+def cdr3_skewed(seed: int, n: int) -> list[str]:
+    """CDR3-like junctions 'CASS' + uniform middle + 'F' with length 8-25, mode 14: P(L) is a
+    Gaussian around 14 with sigma 2.5 below and 3.5 above (right-skewed, like TRB junctions)."""
+    rng = np.random.default_rng(seed)
+    L = np.arange(8, 26)
+    sig = np.where(L < 14, 2.5, 3.5)
+    p = np.exp(-0.5 * ((L - 14) / sig) ** 2)
+    lens = rng.choice(L, size=n, p=p / p.sum())
+    mids = rng.integers(0, 20, size=int((lens - 5).sum()), dtype=np.uint8)
+    letters = np.frombuffer(AA20.encode(), np.uint8)[mids].tobytes().decode()
+    out, o = [], 0
+    for length in lens:
+        k = int(length) - 5
+        out.append("CASS" + letters[o:o + k] + "F")
+        o += k
+    return out
+
+
 def _make_workload(name: str, rank: int):
     qseed = 1 + 1000 * rank  # rank 0 scores exactly the named workload
+    if name in ("sparse", "sparse_structural"):
+        mat = "blosum62" if name == "sparse" else "structural"
+        return dict(kind="sparse", matrix=mat, thresh=24, queries=cdr3_skewed(qseed, 100000),
+                    refs=cdr3_skewed(0, 1000000),
+                    config={"workload": f"gapblock score_sparse 100000x1000000 CDR3-like (len 8-25, "
+                                        f"mode 14), {mat}, gap_open 8, gap_extend 1, no prior, "
+                                        "max_penalty 24, CSR (ref_id int32, score int32) output",
+                            "queries": 100000, "refs": 1000000, "matrix": mat, "gap_open": 8,
+                            "gap_extend": 1, "prior": None, "max_penalty": 24},
+                    metric="gapblock thresholded sparse pairs/s")
     if name == "gapblock":
         return dict(kind="gapblock", queries=cdr3(qseed, 1000), refs=cdr3(0, 10000),
                     config={"workload": "gapblock score_matrix 1000x10000 CDR3 junctions (len 10-20), "
@@ -138,7 +170,7 @@ def cells_of(w) -> float:
     """Algorithmic cells: gap block 2*min(m,n) (min(m,n) at d == 0); DP m*n; Hamming L."""
     lq = np.array([len(s) for s in w["queries"]], dtype=np.float64)
     lr = np.array([len(s) for s in w["refs"]], dtype=np.float64)
-    if w["kind"] == "gapblock":
+    if w["kind"] in ("gapblock", "sparse"):
         vq, cq = np.unique(lq, return_counts=True)
         vr, cr = np.unique(lr, return_counts=True)
         L = np.minimum(vq[:, None], vr[None, :])
@@ -225,7 +257,7 @@ def kernel_roofline(w, cells: float, seconds: float, clocks) -> dict | None:
     """
     mhz = (clocks or {}).get("sm_mhz") or 1965.0
     sms = 148
-    if w["kind"] == "gapblock":
+    if w["kind"] in ("gapblock", "sparse"):
         achieved = 2.0 * cells / seconds / 1e9
         peak = sms * 128 * mhz * 1e6 / 1e9
         return {"bound": "smem", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -250,6 +282,23 @@ def dist_env():
 # ----------------------------------------------------------------------------- reference ----
 def cpu_reference_call(w, threads: int):
     import oracle
+    if w["kind"] == "sparse":
+        # The reference has no sparse form: its dense matrix over the sampled rows, thresholded.
+        t = w["thresh"]
+        if oracle.ref_available():
+            def ref_sparse(q):
+                d = oracle.ref_gapblock_matrix(q, w["refs"], matrix=w["matrix"], gap_open=8,
+                                               gap_extend=1, threads=threads)
+                return np.nonzero(d <= t)
+            return ref_sparse, "reference"
+        from seqtree_b200.matrix import SubstitutionMatrix
+        pen = getattr(SubstitutionMatrix, w["matrix"])().penalty_grid
+
+        def port_sparse(q):
+            d = oracle.gapblock_matrix(q, w["refs"], pen, gap_open=8,
+                                       threads=threads or os.cpu_count())
+            return np.nonzero(d <= t)
+        return port_sparse, "port"
     if w["kind"] == "gapblock":
         from seqtree_b200.gapblock import central_prior, prior_cube
         width = max(map(len, w["queries"] + w["refs"]))
@@ -361,7 +410,7 @@ def main_ours(args):
     q, r = w["queries"], w["refs"]
     N, K = len(q), len(r)
     stream = torch.cuda.current_stream()
-    out = torch.empty((N, K), dtype=torch.int32, device="cuda")
+    out = None if w["kind"] == "sparse" else torch.empty((N, K), dtype=torch.int32, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.int32, device="cuda")
     B62 = stb.SubstitutionMatrix.blosum62()
 
@@ -379,6 +428,19 @@ def main_ours(args):
         def e2e_call():
             return stb.gapblock.score_matrix(q, r, B62, gap_open=8, gap_extend=1,
                                              gap_prior=prior)
+    elif w["kind"] == "sparse":
+        from seqtree_b200.gapblock import score_sparse
+        M = getattr(stb.SubstitutionMatrix, w["matrix"])()
+        qs, rs = device.SeqSet(q, "aa"), device.SeqSet(r, "aa")
+        hits = device.Hits()
+        nnz_seen = []
+
+        def step():
+            nnz_seen.append(device.gapblock_sparse_into(qs, rs, hits, cur(), max_penalty=w["thresh"],
+                                                        matrix=M, gap_open=8, gap_extend=1))
+
+        def e2e_call():
+            return score_sparse(q, r, w["thresh"], M, gap_open=8, gap_extend=1)
     elif w["kind"] in ("hamming", "levenshtein"):
         qs, rs = device.SeqSet(q, None), device.SeqSet(r, None)
         into = device.hamming_into if w["kind"] == "hamming" else device.levenshtein_into
@@ -407,7 +469,8 @@ def main_ours(args):
     launches = _lib.last_launch_count()
     kernel_name = _lib.last_kernel_name()
     graph = None
-    if not args.no_graph:
+    # The sparse step reads its hit count back to size the sort, so it is timed eagerly.
+    if not args.no_graph and w["kind"] != "sparse":
         try:
             side = torch.cuda.Stream()
             side.wait_stream(torch.cuda.current_stream())
@@ -461,8 +524,11 @@ def main_ours(args):
     value = pairs_rank * world * args.steps / (total_ms / 1e3)
     e2e_s = statistics.median(e2e_times) if e2e_times else float("nan")
     in_bytes = sum(len(s) for s in q + r) + 8 * (N + K + 2)
+    out_bytes_host = 4 * pairs_rank
+    if w["kind"] == "sparse":
+        out_bytes_host = 8 * (N + 1) + 8 * nnz_seen[-1]
     e2e = {"value": pairs_rank / e2e_s, "unit": "pairs/s", "h2d_bytes_per_step": in_bytes,
-           "d2h_bytes_per_step": 4 * pairs_rank, "seconds_per_step": e2e_s}
+           "d2h_bytes_per_step": out_bytes_host, "seconds_per_step": e2e_s}
 
     if rank != 0:
         if world > 1:
@@ -472,7 +538,7 @@ def main_ours(args):
 
     hbm, src = peaks()
     per_launch_s = (total_ms / args.steps) / 1e3
-    out_bytes = 4.0 * pairs_rank
+    out_bytes = 4.0 * pairs_rank if w["kind"] != "sparse" else float(out_bytes_host)
     in_dev_bytes = float(sum(len(s) for s in q + r))
     achieved = (out_bytes + in_dev_bytes) / per_launch_s / 1e9
     cells = cells_of(w)
@@ -495,6 +561,10 @@ def main_ours(args):
         "cuda_graph": graph is not None,
         "clocks": sampler.summary(),
     }
+    if w["kind"] == "sparse":
+        line["nnz"] = nnz_seen[-1]
+        line["roofline"]["note"] = ("algorithmic bytes = CSR output (8 B/hit + 8 B/row) + input "
+                                    "residues; the scoring kernel is bound on chip (kernel_roofline)")
     if world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = run_cpu_baseline(w, budget_s=args.cpu_seconds, threads=0)
@@ -514,7 +584,8 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="gapblock",
-                    choices=["gapblock", "hamming", "levenshtein", "nw", "sw"])
+                    choices=["gapblock", "hamming", "levenshtein", "nw", "sw", "sparse",
+                             "sparse_structural"])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

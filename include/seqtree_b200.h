@@ -118,6 +118,31 @@ int32_t st_hamming_matrix(const st_strings *a, const st_strings *b, int32_t thre
 int32_t st_levenshtein_matrix(const st_strings *a, const st_strings *b, int32_t threads,
                               int32_t *out, st_error *err);
 
+/*
+ * Thresholded sparse gap-block matrix: only the cells with score <= max_penalty, as CSR rows
+ * over the queries.  Row i holds the refs k (ascending) with gapblock_matrix[i][k] <= max_penalty
+ * and their scores -- exactly the dense matrix's entries that pass, for matrices too large to
+ * hold densely (e.g. 1e5 x 1e6).  An addition to the reference's API: it is the dense call of
+ * seqtree::gapblock_matrix (include/seqtree/seqtree.hpp:218-222) filtered the way
+ * GapBlockIndex.search filters (python/seqtree/gapblock.py:611-634: keep score <= max_penalty,
+ * ValueError "max_penalty must be >= 0"), without that index's |m-n| cap.  Arguments and checks
+ * are st_gapblock_matrix's.  The library allocates the three arrays (pinned host memory);
+ * release them with st_sparse_free.
+ */
+typedef struct st_sparse {
+    int64_t rows, cols, nnz;
+    int64_t *indptr;  /* rows + 1 */
+    int32_t *ref_ids; /* nnz */
+    int32_t *scores;  /* nnz */
+} st_sparse;
+
+int32_t st_gapblock_sparse(const st_strings *queries, const st_strings *refs, int32_t alphabet,
+                           const int32_t *penalty, int32_t matrix_size, int32_t gap_open,
+                           int32_t gap_extend, const int32_t *prior, int64_t prior_len,
+                           uint32_t prior_width, int32_t max_penalty, int32_t threads,
+                           st_sparse *out, st_error *err);
+void st_sparse_free(st_sparse *sparse);
+
 /* ------------------------------------------------------------------------------------------
  * Device-resident form.  For callers whose sequences stay on the GPU across many calls (and
  * for measuring the kernels alone): a sequence set is uploaded and encoded once, and the
@@ -138,6 +163,27 @@ int32_t st_gapblock_matrix_sets(st_seqset queries, st_seqset refs, const int32_t
                                 int32_t matrix_size, int32_t gap_open, int32_t gap_extend,
                                 const int32_t *prior, int64_t prior_len, uint32_t prior_width,
                                 int32_t *out_device, void *cuda_stream, st_error *err);
+
+/* Sparse result kept on the device (CSR over the query set; see st_gapblock_sparse).  Its
+ * buffers belong to the handle and are reused by the next call that fills it. */
+typedef struct st_hits_s *st_hits;
+int32_t st_hits_create(st_hits *out, st_error *err);
+void st_hits_destroy(st_hits hits);
+int32_t st_hits_info(st_hits hits, int64_t *rows, int64_t *cols, int64_t *nnz,
+                     const int64_t **indptr_device, const int32_t **ref_ids_device,
+                     const int32_t **scores_device);
+/* Copy a hits handle's rows into host arrays of rows + 1 / nnz / nnz entries (any may be NULL);
+ * synchronous. */
+int32_t st_hits_download(st_hits hits, int64_t *indptr, int32_t *ref_ids, int32_t *scores,
+                         st_error *err);
+
+/* Sparse gap-block matrix of two device sets into `out`.  Synchronises cuda_stream once (to
+ * read the hit count), then enqueues the sort and the row build on it. */
+int32_t st_gapblock_sparse_sets(st_seqset queries, st_seqset refs, const int32_t *penalty,
+                                int32_t matrix_size, int32_t gap_open, int32_t gap_extend,
+                                const int32_t *prior, int64_t prior_len, uint32_t prior_width,
+                                int32_t max_penalty, st_hits out, void *cuda_stream,
+                                st_error *err);
 
 int32_t st_align_matrix_sets(st_seqset queries, st_seqset refs, const int32_t *similarity,
                              int32_t matrix_size, int32_t mode, int32_t gap_open,

@@ -15,7 +15,7 @@ import numpy as np
 from . import _lib
 from .matrix import ScoreMatrix, SubstitutionMatrix, parse_align_mode, parse_alphabet
 
-__all__ = ["gapblock_matrix", "align_score_matrix", "align_dist_matrix", "hamming_matrix",
+__all__ = ["gapblock_matrix", "gapblock_sparse", "align_score_matrix", "align_dist_matrix", "hamming_matrix",
            "levenshtein_matrix", "align_score", "hamming", "levenshtein", "ScoreMatrix",
            "SubstitutionMatrix"]
 
@@ -44,10 +44,7 @@ def gapblock_matrix(queries, refs, alphabet: str = "aa", matrix: SubstitutionMat
     alph = parse_alphabet(alphabet)
     q, r = _lib.Packed(queries), _lib.Packed(refs)
     pen = None if matrix is None else np.ascontiguousarray(matrix.penalty_grid, np.int32)
-    pr = np.ascontiguousarray(np.asarray(prior, dtype=np.int64), dtype=np.int64).ravel()
-    if pr.size and (pr.min() < _INT32[0] or pr.max() > _INT32[1]):
-        raise TypeError("prior entries must fit a 32-bit signed integer")
-    pr32 = pr.astype(np.int32)
+    pr32 = _prior32(prior)
     out = _result(q.count, r.count)
     err = _lib.st_error()
     code = _lib.lib.st_gapblock_matrix(
@@ -57,6 +54,38 @@ def gapblock_matrix(queries, refs, alphabet: str = "aa", matrix: SubstitutionMat
         int(threads), out.ctypes.data, ctypes.byref(err))
     _lib.check(code, err)
     return ScoreMatrix(out)
+
+
+def _prior32(prior) -> np.ndarray:
+    pr = np.ascontiguousarray(np.asarray(prior, dtype=np.int64), dtype=np.int64).ravel()
+    if pr.size and (pr.min() < _INT32[0] or pr.max() > _INT32[1]):
+        raise TypeError("prior entries must fit a 32-bit signed integer")
+    return pr.astype(np.int32)
+
+
+def gapblock_sparse(queries, refs, max_penalty: int, alphabet: str = "aa",
+                    matrix: SubstitutionMatrix | None = None, gap_open: int = 1,
+                    gap_extend: int = 1, prior=(), prior_width: int = 0, threads: int = 0):
+    """The cells of :func:`gapblock_matrix` with score <= ``max_penalty``, as CSR arrays
+    ``(indptr int64[N+1], ref_ids int32[nnz], scores int32[nnz])``; refs ascend within a row."""
+    alph = parse_alphabet(alphabet)
+    q, r = _lib.Packed(queries), _lib.Packed(refs)
+    pen = None if matrix is None else np.ascontiguousarray(matrix.penalty_grid, np.int32)
+    pr32 = _prior32(prior)
+    res = _lib.st_sparse()
+    err = _lib.st_error()
+    code = _lib.lib.st_gapblock_sparse(
+        q.ref(), r.ref(), alph, _lib.i32_ptr(pen), 0 if pen is None else pen.shape[0],
+        _i32("gap_open", gap_open), _i32("gap_extend", gap_extend),
+        _lib.i32_ptr(pr32) if pr32.size else None, int(pr32.size), int(prior_width),
+        _i32("max_penalty", max_penalty), int(threads), ctypes.byref(res), ctypes.byref(err))
+    _lib.check(code, err)
+    # the arrays take over the library's pinned blocks (no copy of a possibly huge result)
+    n, nnz = int(res.rows), int(res.nnz)
+    indptr = _lib.adopt_pinned(res.indptr, n + 1, ctypes.c_int64, np.int64)
+    ref_ids = _lib.adopt_pinned(res.ref_ids, nnz, ctypes.c_int32, np.int32)
+    scores = _lib.adopt_pinned(res.scores, nnz, ctypes.c_int32, np.int32)
+    return indptr, ref_ids, scores
 
 
 def _align(queries, refs, matrix: SubstitutionMatrix, mode: str, gap_open: int, gap_extend: int,

@@ -28,6 +28,13 @@ class st_error(ctypes.Structure):
     _fields_ = [("code", ctypes.c_int32), ("message", ctypes.c_char * 256)]
 
 
+class st_sparse(ctypes.Structure):
+    _fields_ = [("rows", ctypes.c_int64), ("cols", ctypes.c_int64), ("nnz", ctypes.c_int64),
+                ("indptr", ctypes.POINTER(ctypes.c_int64)),
+                ("ref_ids", ctypes.POINTER(ctypes.c_int32)),
+                ("scores", ctypes.POINTER(ctypes.c_int32))]
+
+
 _i32p = ctypes.POINTER(ctypes.c_int32)
 _sp = ctypes.POINTER(st_strings)
 _ep = ctypes.POINTER(st_error)
@@ -47,6 +54,23 @@ SIGNATURES = [
       ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, _ep]),
     ("st_hamming_matrix", ctypes.c_int32, [_sp, _sp, ctypes.c_int32, ctypes.c_void_p, _ep]),
     ("st_levenshtein_matrix", ctypes.c_int32, [_sp, _sp, ctypes.c_int32, ctypes.c_void_p, _ep]),
+    ("st_gapblock_sparse", ctypes.c_int32,
+     [_sp, _sp, ctypes.c_int32, _i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p,
+      ctypes.c_int64, ctypes.c_uint32, ctypes.c_int32, ctypes.c_int32,
+      ctypes.POINTER(st_sparse), _ep]),
+    ("st_sparse_free", None, [ctypes.POINTER(st_sparse)]),
+    ("st_hits_create", ctypes.c_int32, [ctypes.POINTER(ctypes.c_void_p), _ep]),
+    ("st_hits_destroy", None, [ctypes.c_void_p]),
+    ("st_hits_info", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+      ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_void_p),
+      ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_void_p)]),
+    ("st_hits_download", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_gapblock_sparse_sets", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, _i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+      _i32p, ctypes.c_int64, ctypes.c_uint32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+      _ep]),
     ("st_seqset_create", ctypes.c_int32,
      [_sp, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p), _ep]),
     ("st_seqset_destroy", None, [ctypes.c_void_p]),
@@ -169,6 +193,17 @@ def pinned_int32(rows: int, cols: int) -> np.ndarray:
     buf = (ctypes.c_int32 * n).from_address(ptr)
     buf._owner = _PinnedOwner(ptr)  # the ctypes array is the numpy base; it owns the block
     return np.frombuffer(buf, dtype=np.int32, count=n).reshape(rows, cols)
+
+
+def adopt_pinned(ptr, n: int, ctype, dtype) -> np.ndarray:
+    """A numpy view of n elements of a pinned block the library allocated; the view owns the
+    block (it returns to the cache when the last view is gone)."""
+    addr = ctypes.cast(ptr, ctypes.c_void_p).value
+    if not addr:
+        return np.zeros(n, dtype)
+    buf = (ctype * max(n, 1)).from_address(addr)
+    buf._owner = _PinnedOwner(addr)
+    return np.frombuffer(buf, dtype=dtype, count=n)
 
 
 def i32_ptr(a: np.ndarray | None):

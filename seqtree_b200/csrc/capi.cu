@@ -13,6 +13,10 @@ namespace stb {
 void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int32_t matrix_size,
                    int32_t go, int32_t ge, const int32_t* prior, int64_t prior_len,
                    uint32_t prior_width, int32_t* out_d, cudaStream_t stream);
+void gapblock_sparse_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty,
+                          int32_t matrix_size, int32_t go, int32_t ge, const int32_t* prior,
+                          int64_t prior_len, uint32_t prior_width, int32_t max_penalty,
+                          st_hits_s& hits, cudaStream_t stream);
 void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int32_t matrix_size,
                 int32_t mode, int32_t go, int32_t ge, int32_t dist, int32_t* out_d,
                 cudaStream_t stream);
@@ -173,6 +177,90 @@ int32_t st_gapblock_matrix(const st_strings* queries, const st_strings* refs, in
     });
 }
 
+int32_t st_gapblock_sparse(const st_strings* queries, const st_strings* refs, int32_t alphabet,
+                           const int32_t* penalty, int32_t matrix_size, int32_t gap_open,
+                           int32_t gap_extend, const int32_t* prior, int64_t prior_len,
+                           uint32_t prior_width, int32_t max_penalty, int32_t threads,
+                           st_sparse* out, st_error* err) {
+    (void)threads;
+    return guard(err, [&] {
+        reset_launches();
+        if (!out) fail(ST_EINVAL, "seqtree_b200: null output");
+        *out = st_sparse{};
+        check_strings(queries);
+        check_strings(refs);
+        if (max_penalty < 0) fail(ST_EINVAL, "max_penalty must be >= 0");
+        // the dense call's checks, in its order (src/gapblock.cpp:71-81)
+        if (gap_open < 0 || gap_extend < 0) fail(ST_EINVAL, "gap_open and gap_extend must be >= 0");
+        const int A = alphabet_size(alphabet);
+        if (A == 0) fail(ST_EINVAL, "unknown alphabet code " + std::to_string(alphabet));
+        if (penalty && matrix_size != A) fail(ST_EINVAL, "matrix size does not match the alphabet");
+        const int64_t N = count_of(queries), K = count_of(refs);
+        st_sparse res{};
+        res.rows = N;
+        res.cols = K;
+        auto release = [&res] {
+            host_free(res.indptr);
+            host_free(res.ref_ids);
+            host_free(res.scores);
+        };
+        res.indptr = static_cast<int64_t*>(host_alloc(sizeof(int64_t) * size_t(N + 1)));
+        if (!res.indptr) fail(ST_ENOMEM, "seqtree_b200: pinned host allocation failed");
+        if (N == 0 || K == 0) {
+            std::memset(res.indptr, 0, sizeof(int64_t) * size_t(N + 1));
+            *out = res;
+            return;
+        }
+        try {
+            Context& ctx = context();
+            std::lock_guard<std::mutex> lk(ctx.mu);
+            clear_flags(ctx);
+            Transient t;
+            {
+                Phase ph("upload+encode");
+                t.q.reset(make_seqset(queries, alphabet, ctx.stream, nullptr, nullptr, ctx.tq));
+                t.r.reset(make_seqset(refs, alphabet, ctx.stream, nullptr, nullptr, ctx.tr));
+            }
+            if (!ctx.tmp_hits) ctx.tmp_hits = std::make_shared<st_hits_s>();
+            st_hits_s& h = *static_cast<st_hits_s*>(ctx.tmp_hits.get());
+            {
+                Phase ph("kernel+sort");
+                gapblock_sparse_sets(*t.q, *t.r, penalty, matrix_size, gap_open, gap_extend, prior,
+                                     prior_len, prior_width, max_penalty, h, ctx.stream);
+            }
+            Phase ph("d2h");
+            res.nnz = h.nnz;
+            const size_t nb = size_t(std::max<int64_t>(h.nnz, 1));
+            res.ref_ids = static_cast<int32_t*>(host_alloc(sizeof(int32_t) * nb));
+            res.scores = static_cast<int32_t*>(host_alloc(sizeof(int32_t) * nb));
+            if (!res.ref_ids || !res.scores)
+                fail(ST_ENOMEM, "seqtree_b200: pinned host allocation failed");
+            STB_CUDA(cudaMemcpyAsync(res.indptr, h.indptr.ptr, sizeof(int64_t) * size_t(N + 1),
+                                     cudaMemcpyDeviceToHost, ctx.stream));
+            if (h.nnz > 0) {
+                STB_CUDA(cudaMemcpyAsync(res.ref_ids, h.ref_ids.ptr, sizeof(int32_t) * size_t(h.nnz),
+                                         cudaMemcpyDeviceToHost, ctx.stream));
+                STB_CUDA(cudaMemcpyAsync(res.scores, h.scores.ptr, sizeof(int32_t) * size_t(h.nnz),
+                                         cudaMemcpyDeviceToHost, ctx.stream));
+            }
+            STB_CUDA(cudaStreamSynchronize(ctx.stream));
+        } catch (...) {
+            release();
+            throw;
+        }
+        *out = res;
+        trace_report("st_gapblock_sparse");
+    });
+}
+
+void st_sparse_free(st_sparse* s) {
+    if (!s) return;
+    host_free(s->indptr);
+    host_free(s->ref_ids);
+    host_free(s->scores);
+    *s = st_sparse{};
+}
+
 static int32_t align_common(const st_strings* queries, const st_strings* refs,
                             const int32_t* similarity, int32_t matrix_size, int32_t alphabet,
                             int32_t mode, int32_t gap_open, int32_t gap_extend, int32_t dist,
@@ -324,6 +412,84 @@ int32_t st_gapblock_matrix_sets(st_seqset queries, st_seqset refs, const int32_t
         auto stream = static_cast<cudaStream_t>(cuda_stream);
         gapblock_sets(*queries, *refs, penalty, matrix_size, gap_open, gap_extend, prior, prior_len,
                       prior_width, out_device, stream);
+    });
+}
+
+int32_t st_hits_create(st_hits* out, st_error* err) {
+    return guard(err, [&] {
+        if (!out) fail(ST_EINVAL, "seqtree_b200: null output handle");
+        *out = nullptr;
+        auto h = std::make_unique<st_hits_s>();
+        STB_CUDA(cudaGetDevice(&h->device));
+        *out = h.release();
+    });
+}
+
+void st_hits_destroy(st_hits hits) {
+    if (!hits) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    const int home = hits->device;
+    if (prev != home) cudaSetDevice(home);
+    delete hits;  // frees its device buffers on their device
+    if (prev >= 0 && prev != home) cudaSetDevice(prev);
+}
+
+int32_t st_hits_info(st_hits hits, int64_t* rows, int64_t* cols, int64_t* nnz,
+                     const int64_t** indptr_device, const int32_t** ref_ids_device,
+                     const int32_t** scores_device) {
+    if (!hits) return ST_EINVAL;
+    if (rows) *rows = hits->rows;
+    if (cols) *cols = hits->cols;
+    if (nnz) *nnz = hits->nnz;
+    if (indptr_device) *indptr_device = static_cast<const int64_t*>(hits->indptr.ptr);
+    if (ref_ids_device) *ref_ids_device = static_cast<const int32_t*>(hits->ref_ids.ptr);
+    if (scores_device) *scores_device = static_cast<const int32_t*>(hits->scores.ptr);
+    return ST_OK;
+}
+
+int32_t st_hits_download(st_hits hits, int64_t* indptr, int32_t* ref_ids, int32_t* scores,
+                         st_error* err) {
+    return guard(err, [&] {
+        if (!hits) fail(ST_EINVAL, "seqtree_b200: null hits handle");
+        int dev = -1;
+        STB_CUDA(cudaGetDevice(&dev));
+        if (dev != hits->device) fail(ST_EINVAL, "seqtree_b200: hits handle lives on another device");
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        if (indptr && hits->indptr.ptr)
+            STB_CUDA(cudaMemcpyAsync(indptr, hits->indptr.ptr, sizeof(int64_t) * size_t(hits->rows + 1),
+                                     cudaMemcpyDeviceToHost, ctx.stream));
+        if (hits->nnz > 0) {
+            if (ref_ids)
+                STB_CUDA(cudaMemcpyAsync(ref_ids, hits->ref_ids.ptr, sizeof(int32_t) * size_t(hits->nnz),
+                                         cudaMemcpyDeviceToHost, ctx.stream));
+            if (scores)
+                STB_CUDA(cudaMemcpyAsync(scores, hits->scores.ptr, sizeof(int32_t) * size_t(hits->nnz),
+                                         cudaMemcpyDeviceToHost, ctx.stream));
+        }
+        STB_CUDA(cudaStreamSynchronize(ctx.stream));
+    });
+}
+
+int32_t st_gapblock_sparse_sets(st_seqset queries, st_seqset refs, const int32_t* penalty,
+                                int32_t matrix_size, int32_t gap_open, int32_t gap_extend,
+                                const int32_t* prior, int64_t prior_len, uint32_t prior_width,
+                                int32_t max_penalty, st_hits out, void* cuda_stream,
+                                st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_set(queries);
+        check_set(refs);
+        if (!out) fail(ST_EINVAL, "seqtree_b200: null hits handle");
+        int dev = -1;
+        STB_CUDA(cudaGetDevice(&dev));
+        if (dev != out->device) fail(ST_EINVAL, "seqtree_b200: hits handle lives on another device");
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        gapblock_sparse_sets(*queries, *refs, penalty, matrix_size, gap_open, gap_extend, prior,
+                             prior_len, prior_width, max_penalty, *out,
+                             static_cast<cudaStream_t>(cuda_stream));
     });
 }
 

@@ -79,6 +79,33 @@ void* DevBuf::get(size_t bytes) {
     return ptr;
 }
 
+void* DevBuf::grow_keep(size_t bytes, size_t keep, cudaStream_t stream) {
+    if (bytes <= cap) return ptr;
+    size_t want = std::max<size_t>(bytes + bytes / 2, 4096);
+    want = (want + 255) & ~size_t(255);
+    void* fresh = nullptr;
+    STB_CUDA(cudaMalloc(&fresh, want));
+    if (ptr && keep) {
+        const cudaError_t e = cudaMemcpyAsync(fresh, ptr, std::min(keep, cap),
+                                              cudaMemcpyDeviceToDevice, stream);
+        if (e != cudaSuccess) {
+            cudaFree(fresh);
+            STB_CUDA(e);
+        }
+        STB_CUDA(cudaStreamSynchronize(stream));
+    }
+    if (ptr) cudaFree(ptr);
+    ptr = fresh;
+    cap = want;
+    return ptr;
+}
+
+void DevBuf::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+}
+
 DevBuf::~DevBuf() {
     // Contexts live until process exit; the driver reclaims device memory then.
 }
@@ -343,11 +370,22 @@ void* host_alloc(uint64_t bytes) {
     return p;
 }
 
+// Returned blocks stay pinned for reuse up to kPinCacheBytes in total; beyond that they are
+// unpinned and freed (a huge one-off result does not stay locked in host memory).
+constexpr size_t kPinCacheBytes = size_t(8) << 30;
+
 void host_free(void* p) {
     if (!p) return;
     std::lock_guard<std::mutex> lk(g_pin_mu);
     auto it = g_pin_size.find(p);
     if (it == g_pin_size.end()) return;
+    size_t cached = 0;
+    for (const auto& kv : g_pin_free) cached += kv.first;
+    if (cached + it->second > kPinCacheBytes) {
+        g_pin_size.erase(it);
+        cudaFreeHost(p);
+        return;
+    }
     g_pin_free.emplace(it->second, p);
 }
 }  // namespace stb

@@ -59,6 +59,9 @@ struct DevBuf {
     void* get(size_t bytes);
     template <class T>
     T* as(size_t count) { return static_cast<T*>(get(count * sizeof(T))); }
+    // Grows to at least `bytes`, keeping the first `keep` bytes (device-to-device on `stream`).
+    void* grow_keep(size_t bytes, size_t keep, cudaStream_t stream);
+    void release();  // frees the memory now (owners that do not live until exit)
     ~DevBuf();
 };
 
@@ -76,10 +79,16 @@ struct Context {
     int64_t* flags_h = nullptr;
     // named scratch, grow-only
     DevBuf out_buf, q_codes, r_codes, table_buf, prior_buf, ftab_buf, work_a, work_b, work_c;
+    // sparse output: unsorted hit keys and scores, sorted keys, radix-sort scratch
+    DevBuf sp_keys, sp_vals, sp_sorted, sp_temp;
     // storage of the transient sets made by the host-buffer entry points
     DevBuf tq[3], tr[3];  // bytes, offsets, lengths
     // plans reused by transient sets (rebuilt in place for every call)
     std::shared_ptr<void> tmp_query_plan, tmp_ref_plan, tmp_wave_plan[2];
+    // query plan of a row block (sparse calls whose hits are taken in several blocks)
+    std::shared_ptr<void> tmp_block_plan;
+    // sparse result of the host-buffer sparse call (an st_hits_s)
+    std::shared_ptr<void> tmp_hits;
 };
 
 // Context of the current CUDA device (created on first use).  Fails with ST_ENODEV when no
@@ -117,6 +126,22 @@ struct st_seqset_s {
     // plan caches (opaque; transient sets share the context's)
     std::shared_ptr<void> gb_query_plan, gb_ref_plan, wave_plan;
     ~st_seqset_s();
+};
+
+// A thresholded sparse result resident on one device: CSR rows over the query set.
+struct st_hits_s {
+    int device = 0;
+    int64_t rows = 0, cols = 0, nnz = 0;
+    uint64_t cap_hint = 0;       // hit-buffer size that the next call starts from
+    int64_t block_rows_hint = 0; // query rows per block the last call needed (0: one block)
+    stb::DevBuf indptr;          // rows + 1 int64
+    stb::DevBuf ref_ids;         // nnz int32, ascending within a row
+    stb::DevBuf scores;          // nnz int32
+    ~st_hits_s() {
+        indptr.release();
+        ref_ids.release();
+        scores.release();
+    }
 };
 
 namespace stb {

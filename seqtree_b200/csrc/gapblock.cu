@@ -28,11 +28,20 @@
 //   * Results go through a shared tile so that global stores are coalesced 16-byte vectors in
 //     the original column order; the per-(m,n) term (prior minimum + gap cost) is added there.
 // General path: one thread per pair in int32 for any lengths and penalty magnitudes.
+//
+// Thresholded sparse form (for matrices too large to hold densely): the same kernels keep only
+// the cells with score <= max_penalty.  Hits are appended as (query << shift | ref, score) with one
+// atomic per warp, then radix-sorted by key and turned into CSR rows (indptr, ref ids, scores):
+// exactly the entries of the dense matrix's rows that pass the threshold, in ref order.
 #include <algorithm>
+#include <cstdlib>
 #include <map>
 #include <numeric>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "common.cuh"
+#include "sparse.cuh"
 
 namespace stb {
 
@@ -50,6 +59,7 @@ constexpr int kPairsPerSlice = 4;
 // objects, whose device buffers only grow.
 struct QueryPlan {
     uint64_t uid = 0;                    // set the plan was built for
+    int64_t r0 = 0, r1 = -1;             // its rows [r0, r1) (r1 = -1: the whole set)
     int64_t P = 0;                       // query pairs, a multiple of 4
     std::vector<int2> pairs;             // original indices (-1 marks an empty slot)
     std::vector<int32_t> plen;           // m of each pair
@@ -72,13 +82,15 @@ struct RefPlan {
     DevBuf d_slab;                       // per task: n rows of 32 bytes (4*code per lane)
 };
 
-// Queries sorted by length (stable) and paired within each length; an odd one out is paired
-// with -1.  Each length's pairs are padded with (-1, -1) to a multiple of 4, so that every slice
-// of 4 consecutive pairs has one length.  Empty slots are computed and never stored.
-void build_query_plan(QueryPlan& plan, const st_seqset_s& q, cudaStream_t stream) {
-    const int64_t N = q.count;
+// Queries (rows [r0, r1) of the set; r1 = -1 for all) sorted by length (stable) and paired
+// within each length; an odd one out is paired with -1.  Each length's pairs are padded with
+// (-1, -1) to a multiple of 4, so that every slice of 4 consecutive pairs has one length.  Empty
+// slots are computed and never stored.
+void build_query_plan(QueryPlan& plan, const st_seqset_s& q, cudaStream_t stream, int64_t r0 = 0,
+                      int64_t r1 = -1) {
+    const int64_t N = (r1 < 0 ? q.count : r1) - r0;
     std::vector<int32_t> order(static_cast<size_t>(N));
-    std::iota(order.begin(), order.end(), 0);
+    std::iota(order.begin(), order.end(), int32_t(r0));
     std::stable_sort(order.begin(), order.end(),
                      [&](int32_t a, int32_t b) { return q.h_len[size_t(a)] < q.h_len[size_t(b)]; });
     plan.pairs.clear();
@@ -101,6 +113,8 @@ void build_query_plan(QueryPlan& plan, const st_seqset_s& q, cudaStream_t stream
                              sizeof(int32_t) * size_t(plan.P), stream);
     plan.prof_key.clear();
     plan.uid = q.uid;
+    plan.r0 = r0;
+    plan.r1 = r1;
 }
 
 // Refs in chunks of rc columns (original order); inside a chunk a counting sort by length
@@ -209,8 +223,9 @@ struct FastArgs {
     const int32_t* ftab;     // [m*W1 + n]: per-(m,n) additive term (prior minimum + gap cost)
     int W1;
     uint32_t bias2;          // BIAS in both halves
-    int32_t* out;
+    int32_t* out;            // dense output (unused by the sparse form)
     unsigned long long* err; // set when the bounded wait for the staging copies gives up
+    SparseSink sink;         // sparse output (unused by the dense form)
 };
 
 // One non-blocking probe of an mbarrier phase (callers bound the number of probes).
@@ -312,7 +327,7 @@ __device__ __forceinline__ void run_unit(const FastArgs& a, const uint8_t* smem,
     }
 }
 
-template <int LQ, bool PRIOR>
+template <int LQ, bool PRIOR, bool SPARSE>
 __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastArgs a) {
     extern __shared__ __align__(128) uint8_t smem[];
     constexpr int kProfB = kGP * LQ * kRow * 4;
@@ -387,8 +402,42 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
         s_fcol[i] = c < kcount ? s_ftab[a.plen[p0 + sl * kPairsPerSlice] * a.W1 + s_len[c]] : 0;
     }
     __syncthreads();
-    const bool vec = (a.K & 3) == 0;
     const int cols4 = (kcount + 3) >> 2;
+    if constexpr (SPARSE) {
+        // Every lane runs the same number of rounds (sink_append is warp-collective).
+        const int total = np * cols4;
+        for (int i0 = 0; i0 < total; i0 += kThreads) {
+            const int i = i0 + tid;
+            uint32_t hits = 0;
+            int pl = 0, c = 0;
+            int2 pr = make_int2(-1, -1);
+            if (i < total) {
+                pl = i / cols4;
+                c = (i - pl * cols4) * 4;
+                pr = a.pairs[p0 + pl];
+            }
+            const uint32_t* src = s_tile + pl * a.rc + c;
+            const int32_t* fc = s_fcol + (pl / kPairsPerSlice) * a.rc + c;
+            if (pr.x >= 0) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (c + u >= kcount) break;
+                    const uint32_t t = src[u];
+                    const uint32_t f = uint32_t(fc[u]);
+                    if (int32_t((t & 0xFFFFu) + f) <= a.sink.thresh) hits |= 1u << u;
+                    if (pr.y >= 0 && int32_t((t >> 16) + f) <= a.sink.thresh) hits |= 16u << u;
+                }
+            }
+            sink_append(a.sink, hits, lane, [&](int b, unsigned long long& key, int32_t& val) {
+                const int u = b & 3;
+                const uint32_t t = src[u];
+                val = int32_t((b < 4 ? (t & 0xFFFFu) : (t >> 16)) + uint32_t(fc[u]));
+                key = sink_key(a.sink, b < 4 ? pr.x : pr.y, k0 + c + u);
+            });
+        }
+        return;
+    }
+    const bool vec = (a.K & 3) == 0;
     for (int i = tid; i < np * cols4; i += kThreads) {
         const int pl = i / cols4;
         const int c = (i - pl * cols4) * 4;
@@ -423,24 +472,32 @@ struct GeneralArgs {
     const int64_t* qoff;
     const uint8_t* rcodes;
     const int64_t* roff;
-    int64_t N, K;
+    int64_t row0;         // first query row (row blocks of the sparse form)
+    int64_t N, K;         // rows in this launch, refs
     const int32_t* pen;   // A*A
     int A;
     int32_t go, ge;
     const int32_t* prior; // (pw+1)^3 or null
     int64_t pw1;
-    int32_t* out;
+    int32_t* out;         // dense output (unused by the sparse form)
+    SparseSink sink;      // sparse output (unused by the dense form)
 };
 
-// One thread per (i, k) in row-major order, int32 arithmetic with the reference's wrap.
+// One thread per (i, k) in row-major order, int32 arithmetic with the reference's wrap.  The
+// loop runs the same number of rounds on every lane (the sparse append is warp-collective).
+template <bool SPARSE>
 __global__ void __launch_bounds__(256) gapblock_general_kernel(const GeneralArgs a) {
     extern __shared__ int32_t s_pen[];
     for (int i = threadIdx.x; i < a.A * a.A; i += blockDim.x) s_pen[i] = a.pen[i];
     __syncthreads();
     const int64_t total = a.N * a.K;
-    for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total;
-         idx += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t i = idx / a.K, k = idx - i * a.K;
+    for (int64_t base = int64_t(blockIdx.x) * blockDim.x; base < total;
+         base += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t idx = base + threadIdx.x;
+        if (!SPARSE && idx >= total) break;
+        const bool live = idx < total;
+        const int64_t il = live ? idx / a.K : 0, k = live ? idx - il * a.K : 0;
+        const int64_t i = a.row0 + il;
         const uint8_t* q = a.qcodes + a.qoff[i];
         const uint8_t* r = a.rcodes + a.roff[k];
         const int m = int(a.qoff[i + 1] - a.qoff[i]);
@@ -468,17 +525,26 @@ __global__ void __launch_bounds__(256) gapblock_general_kernel(const GeneralArgs
             v = int32_t(uint32_t(S) + uint32_t(best) + uint32_t(a.go) +
                         uint32_t(d - 1) * uint32_t(a.ge));
         }
-        a.out[idx] = v;
+        if constexpr (SPARSE) {
+            sink_append(a.sink, live && v <= a.sink.thresh ? 1u : 0u, int(threadIdx.x & 31),
+                        [&](int, unsigned long long& key, int32_t& val) {
+                            key = sink_key(a.sink, i, k);
+                            val = v;
+                        });
+        } else {
+            a.out[idx] = v;
+        }
     }
 }
 
 template <int LQ, bool PRIOR>
 const char* launch_fast(const FastArgs& args, dim3 grid, size_t smem, cudaStream_t stream) {
-    auto kern = gapblock_fast_kernel<LQ, PRIOR>;
+    auto kern = args.sink.keys ? gapblock_fast_kernel<LQ, PRIOR, true>
+                               : gapblock_fast_kernel<LQ, PRIOR, false>;
     STB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     kern<<<grid, kThreads, smem, stream>>>(args);
     STB_CUDA(cudaGetLastError());
-    return "gapblock_fast_kernel";
+    return args.sink.keys ? "gapblock_fast_kernel<sparse>" : "gapblock_fast_kernel";
 }
 
 // Profile height LQ >= longest query: rows per pair in shared memory.
@@ -567,15 +633,17 @@ void build_tables(GbTables& tb, const std::vector<int32_t>& pen, int32_t go, int
 // CTAs per SM the fast kernel's registers allow (256 threads x <= 80 registers).
 constexpr int kTargetBlocks = 3;
 
+// The dense variant stands in for both forms when sizing (same registers and shared memory,
+// apart from the epilogue).
 const void* fast_kernel_ptr(int lq, bool prior) {
 #define STB_K(LQ)                                                                             \
     if (lq == LQ)                                                                             \
-        return prior ? reinterpret_cast<const void*>(gapblock_fast_kernel<LQ, true>)          \
-                     : reinterpret_cast<const void*>(gapblock_fast_kernel<LQ, false>);
+        return prior ? reinterpret_cast<const void*>(gapblock_fast_kernel<LQ, true, false>)   \
+                     : reinterpret_cast<const void*>(gapblock_fast_kernel<LQ, false, false>);
     STB_K(16) STB_K(24) STB_K(32) STB_K(48)
 #undef STB_K
-    return prior ? reinterpret_cast<const void*>(gapblock_fast_kernel<64, true>)
-                 : reinterpret_cast<const void*>(gapblock_fast_kernel<64, false>);
+    return prior ? reinterpret_cast<const void*>(gapblock_fast_kernel<64, true, false>)
+                 : reinterpret_cast<const void*>(gapblock_fast_kernel<64, false, false>);
 }
 
 // The profile area is reused for the per-slice column terms at write-out time.
@@ -587,10 +655,15 @@ size_t fast_smem(int lq, int64_t slab_cap, int rc, int W1) {
 
 }  // namespace
 
-// Validated inputs -> device matrix.  `out_d` is device memory of N*K int32.
-void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int32_t matrix_size,
-                   int32_t go, int32_t ge, const int32_t* prior, int64_t prior_len,
-                   uint32_t prior_width, int32_t* out_d, cudaStream_t stream) {
+namespace {
+
+// Validated inputs -> the dense matrix in `out_d` (device, N*K int32), or, when `sink` is given,
+// the cells that pass its threshold appended to it.
+// `r0`, `r1` restrict the queries to rows [r0, r1) (sparse form only; r1 = -1: all rows).
+void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int32_t matrix_size,
+                  int32_t go, int32_t ge, const int32_t* prior, int64_t prior_len,
+                  uint32_t prior_width, int32_t* out_d, const SparseSink* sink,
+                  cudaStream_t stream, int64_t r0 = 0, int64_t r1 = -1) {
     if (go < 0 || ge < 0) fail(ST_EINVAL, "gap_open and gap_extend must be >= 0");
     if (qs.alphabet < 0 || qs.alphabet != rs.alphabet)
         fail(ST_EINVAL, "seqtree_b200: gap-block sets must be encoded with one alphabet");
@@ -672,12 +745,16 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
             d_prior = ctx.prior_buf.as<int32_t>(size_t(prior_len));
             h2d(d_prior, prior, size_t(prior_len) * 4, stream);
         }
-        GeneralArgs g{qs.d_bytes, qs.d_off, rs.d_bytes, rs.d_off, N, K, d_pen, A, go, ge,
-                      d_prior, W1p, out_d};
-        const int64_t blocks = std::min<int64_t>(ceil_div(N * K, 256), int64_t(ctx.num_sms) * 16);
-        gapblock_general_kernel<<<unsigned(blocks), 256, size_t(A) * A * 4, stream>>>(g);
+        const int64_t rows = (r1 < 0 ? N : r1) - r0;
+        GeneralArgs g{qs.d_bytes, qs.d_off, rs.d_bytes, rs.d_off, r0, rows, K, d_pen, A, go, ge,
+                      d_prior, W1p, out_d, sink ? *sink : SparseSink{}};
+        const int64_t blocks = std::min<int64_t>(ceil_div(rows * K, 256), int64_t(ctx.num_sms) * 16);
+        if (sink)
+            gapblock_general_kernel<true><<<unsigned(blocks), 256, size_t(A) * A * 4, stream>>>(g);
+        else
+            gapblock_general_kernel<false><<<unsigned(blocks), 256, size_t(A) * A * 4, stream>>>(g);
         STB_CUDA(cudaGetLastError());
-        note_launch("gapblock_general_kernel");
+        note_launch(sink ? "gapblock_general_kernel<sparse>" : "gapblock_general_kernel");
         return;
     }
     RefPlan& rp = *rpp;
@@ -708,10 +785,12 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
     }
 
     // Query pairs and their profile (rebuilt when the set or the penalty grid changes).
-    QueryPlan& qp = plan_slot<QueryPlan>(qs.gb_query_plan, ctx.tmp_query_plan, qs.owns);
-    if (qp.uid != qs.uid) {
+    const bool row_block = r0 != 0 || (r1 >= 0 && r1 != N);
+    QueryPlan& qp = row_block ? plan_slot<QueryPlan>(ctx.tmp_block_plan, ctx.tmp_block_plan, false)
+                              : plan_slot<QueryPlan>(qs.gb_query_plan, ctx.tmp_query_plan, qs.owns);
+    if (qp.uid != qs.uid || qp.r0 != r0 || qp.r1 != (row_block ? r1 : -1)) {
         Phase ph("query_plan");
-        build_query_plan(qp, qs, stream);
+        build_query_plan(qp, qs, stream, r0, row_block ? r1 : -1);
     }
     {
         std::vector<uint8_t> key(sizeof(int) * 2 + pen.size() * 4);
@@ -755,12 +834,176 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
     fa.bias2 = uint32_t(bias) * 0x10001u;
     fa.out = out_d;
     fa.err = err;
+    if (sink) fa.sink = *sink;
 
     const dim3 grid(unsigned(rp.nchunks), unsigned(ceil_div(qp.P, kGP)));
     if (grid.y > 65535) fail(ST_EINVAL, "seqtree_b200: too many query pairs for one launch");
     const char* name = dispatch_fast(lq, has_prior, fa, grid, smem, stream);
     note_launch(name);
     // The timeout flag is read by the caller after its synchronisation point.
+}
+
+}  // namespace
+
+void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int32_t matrix_size,
+                   int32_t go, int32_t ge, const int32_t* prior, int64_t prior_len,
+                   uint32_t prior_width, int32_t* out_d, cudaStream_t stream) {
+    gapblock_run(qs, rs, penalty, matrix_size, go, ge, prior, prior_len, prior_width, out_d,
+                 nullptr, stream);
+}
+
+// ---------------------------------------------------------------------------- sparse --------
+namespace {
+
+int bits_for(int64_t n) {  // bits to hold 0..n-1 (at least 1)
+    int b = 1;
+    while (b < 62 && (int64_t(1) << b) < n) ++b;
+    return b;
+}
+
+}  // namespace
+
+// Hits of one query-row block: the kernel appends (key, score) pairs, a radix sort orders them by
+// key (row-major), and csr_block_kernel writes the block's rows of indptr (offset by `base`) and ref ids.
+// The block's ref ids and scores land at `base` in the result arrays.
+namespace {
+
+__global__ void csr_block_kernel(const unsigned long long* __restrict__ keys, int64_t H, int shift,
+                                 int64_t row0, int64_t rows, int64_t base,
+                                 int64_t* __restrict__ indptr, int32_t* __restrict__ ref_ids) {
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    const unsigned long long mask = (1ull << shift) - 1;
+    for (int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; t <= rows || t < H;
+         t += stride) {
+        if (t <= rows) {
+            const unsigned long long want = static_cast<unsigned long long>(row0 + t) << shift;
+            int64_t lo = 0, hi = H;
+            while (lo < hi) {
+                const int64_t mid = (lo + hi) >> 1;
+                if (keys[mid] < want) lo = mid + 1;
+                else hi = mid;
+            }
+            indptr[row0 + t] = base + lo;
+        }
+        if (t < H) ref_ids[base + t] = int32_t(keys[t] & mask);
+    }
+}
+
+// Hits one sort takes at most (2^28, about 10 GB of scratch); larger outputs are produced in
+// query-row blocks.  SEQTREE_B200_SPARSE_BLOCK_HITS lowers it (at least 1024), e.g. to bound the
+// scratch memory.
+uint64_t max_block_hits() {
+    uint64_t v = uint64_t(1) << 28;
+    if (const char* e = std::getenv("SEQTREE_B200_SPARSE_BLOCK_HITS")) {
+        const long long x = std::atoll(e);
+        if (x > 0) v = std::min<uint64_t>(v, std::max<uint64_t>(uint64_t(x), 1024));
+    }
+    return v;
+}
+
+}  // namespace
+
+void gapblock_sparse_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty,
+                          int32_t matrix_size, int32_t go, int32_t ge, const int32_t* prior,
+                          int64_t prior_len, uint32_t prior_width, int32_t max_penalty,
+                          st_hits_s& hits, cudaStream_t stream) {
+    if (max_penalty < 0) fail(ST_EINVAL, "max_penalty must be >= 0");
+    Context& ctx = context();
+    const int64_t N = qs.count, K = rs.count;
+    hits.rows = N;
+    hits.cols = K;
+    hits.nnz = 0;
+    int64_t* indptr = hits.indptr.as<int64_t>(size_t(N) + 1);
+    if (N == 0 || K == 0) {
+        // the dense call's checks still apply (they come before its empty-shape return)
+        gapblock_run(qs, rs, penalty, matrix_size, go, ge, prior, prior_len, prior_width, nullptr,
+                     nullptr, stream);
+        STB_CUDA(cudaMemsetAsync(indptr, 0, sizeof(int64_t) * size_t(N + 1), stream));
+        return;
+    }
+    const int shift = bits_for(K);
+    if (shift + bits_for(N) > 63) fail(ST_EINVAL, "seqtree_b200: matrix too large for sparse keys");
+    const int end_bit = shift + bits_for(N);
+    const uint64_t kMaxBlockHits = max_block_hits();
+    auto* count = reinterpret_cast<unsigned long long*>(ctx.flags_d + 10);
+
+    // One block of all rows when the hits fit one sort (the usual case: the set's cached plans
+    // are used and nothing is copied); otherwise blocks sized from the hit density seen so far.
+    int64_t r0 = 0, rows = hits.block_rows_hint > 0 ? hits.block_rows_hint : N;
+    int64_t first_rows = 0, nblocks = 0;
+    uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(hits.cap_hint, uint64_t(1) << 20),
+                                      kMaxBlockHits);
+    int64_t total = 0;
+    bool exact_retry = false;
+    while (r0 < N) {
+        const int64_t r1 = std::min<int64_t>(N, r0 + rows);
+        SparseSink sink{};
+        sink.keys = ctx.sp_keys.as<unsigned long long>(size_t(cap));
+        sink.vals = ctx.sp_vals.as<int32_t>(size_t(cap));
+        sink.count = count;
+        sink.cap = cap;
+        sink.shift = shift;
+        sink.thresh = max_penalty;
+        STB_CUDA(cudaMemsetAsync(ctx.flags_d + 8, 0, 8 * sizeof(int64_t), stream));
+        gapblock_run(qs, rs, penalty, matrix_size, go, ge, prior, prior_len, prior_width, nullptr,
+                     &sink, stream, r0, r1 == N && r0 == 0 ? -1 : r1);
+        STB_CUDA(cudaMemcpyAsync(ctx.flags_h + 8, ctx.flags_d + 8, 8 * sizeof(int64_t),
+                                 cudaMemcpyDeviceToHost, stream));
+        STB_CUDA(cudaStreamSynchronize(stream));
+        if (ctx.flags_h[8] != 0)
+            fail(ST_ETIMEOUT, "seqtree_b200: a bounded device-side wait gave up (shared-memory staging)");
+        const uint64_t H = static_cast<uint64_t>(ctx.flags_h[10]);
+        if (H > cap) {
+            if (exact_retry) fail(ST_ECUDA, "seqtree_b200: sparse hit count changed between passes");
+            const int64_t nrows = r1 - r0;
+            if (H <= kMaxBlockHits || nrows == 1) {
+                // same block at its exact size (a single row may exceed the block cap: its hits
+                // are at most K < 2^31, what one sort takes)
+                cap = H <= kMaxBlockHits ? std::min<uint64_t>(H + H / 8, kMaxBlockHits) : H;
+                exact_retry = true;
+            } else {  // fewer rows, sized to about 3/4 of a full sort
+                const double per_row = double(H) / double(nrows);
+                rows = std::max<int64_t>(
+                    1, std::min<int64_t>(nrows - 1, int64_t(0.75 * double(kMaxBlockHits) / per_row)));
+                cap = kMaxBlockHits;
+            }
+            continue;
+        }
+        exact_retry = false;
+        // room for this block's results after the previous blocks'
+        const size_t need = size_t(total + int64_t(H) + 1);
+        hits.ref_ids.grow_keep(need * sizeof(int32_t), size_t(total) * sizeof(int32_t), stream);
+        hits.scores.grow_keep(need * sizeof(int32_t), size_t(total) * sizeof(int32_t), stream);
+        auto* ref_ids = static_cast<int32_t*>(hits.ref_ids.ptr);
+        auto* scores = static_cast<int32_t*>(hits.scores.ptr);
+        auto* sorted = ctx.sp_sorted.as<unsigned long long>(size_t(std::max<uint64_t>(H, 1)));
+        if (H > 0) {
+            size_t temp = 0;
+            STB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, sink.keys, sorted, sink.vals,
+                                                     scores + total, int(H), 0, end_bit, stream));
+            void* d_temp = ctx.sp_temp.as<uint8_t>(temp + 16);
+            STB_CUDA(cub::DeviceRadixSort::SortPairs(d_temp, temp, sink.keys, sorted, sink.vals,
+                                                     scores + total, int(H), 0, end_bit, stream));
+        }
+        const int64_t work = std::max<int64_t>(r1 - r0 + 1, int64_t(H));
+        const unsigned blocks =
+            unsigned(std::min<int64_t>(ceil_div(work, 256), int64_t(ctx.num_sms) * 8));
+        csr_block_kernel<<<blocks, 256, 0, stream>>>(sorted, int64_t(H), shift, r0, r1 - r0, total,
+                                                     indptr, ref_ids);
+        STB_CUDA(cudaGetLastError());
+        note_launch(nullptr);
+        total += int64_t(H);
+        if (nblocks++ == 0) first_rows = r1 - r0;
+        // next block: as many rows as this block's density says fit 3/4 of a sort
+        const double per_row = double(std::max<uint64_t>(H, 1)) / double(r1 - r0);
+        rows = std::max<int64_t>(1, int64_t(0.75 * double(kMaxBlockHits) / per_row));
+        cap = std::min<uint64_t>(std::max<uint64_t>(cap, uint64_t(per_row * double(rows) * 1.25) + 1024),
+                                 kMaxBlockHits);
+        r0 = r1;
+    }
+    hits.nnz = total;
+    hits.block_rows_hint = nblocks > 1 ? first_rows : 0;
+    hits.cap_hint = std::max<uint64_t>(hits.cap_hint, std::min<uint64_t>(uint64_t(total) + uint64_t(total) / 8, kMaxBlockHits));
 }
 
 }  // namespace stb

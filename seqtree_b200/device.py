@@ -56,6 +56,68 @@ def gapblock_into(queries: SeqSet, refs: SeqSet, out_ptr: int, stream: int = 0,
     _lib.check(code, err)
 
 
+class Hits:
+    """A thresholded sparse result kept on the current CUDA device (``st_hits``): CSR rows of
+    device pointers, refilled in place by :func:`gapblock_sparse_into`."""
+
+    def __init__(self):
+        self._h = ctypes.c_void_p()
+        err = _lib.st_error()
+        _lib.check(_lib.lib.st_hits_create(ctypes.byref(self._h), ctypes.byref(err)), err)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> dict:
+        """rows, cols, nnz and the device pointers of indptr / ref_ids / scores."""
+        rows, cols, nnz = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        ip, ri, sc = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        code = _lib.lib.st_hits_info(self._h, ctypes.byref(rows), ctypes.byref(cols),
+                                     ctypes.byref(nnz), ctypes.byref(ip), ctypes.byref(ri),
+                                     ctypes.byref(sc))
+        if code:
+            raise ValueError("invalid hits handle")
+        return {"rows": rows.value, "cols": cols.value, "nnz": nnz.value,
+                "indptr": ip.value or 0, "ref_ids": ri.value or 0, "scores": sc.value or 0}
+
+    def to_host(self):
+        """(indptr int64[rows+1], ref_ids int32[nnz], scores int32[nnz]) as numpy arrays."""
+        info = self.info()
+        indptr = np.zeros(info["rows"] + 1, np.int64)
+        ref_ids = np.zeros(info["nnz"], np.int32)
+        scores = np.zeros(info["nnz"], np.int32)
+        err = _lib.st_error()
+        code = _lib.lib.st_hits_download(self._h, indptr.ctypes.data, ref_ids.ctypes.data,
+                                         scores.ctypes.data, ctypes.byref(err))
+        _lib.check(code, err)
+        return indptr, ref_ids, scores
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            _lib.lib.st_hits_destroy(h)
+            self._h = ctypes.c_void_p()
+
+
+def gapblock_sparse_into(queries: SeqSet, refs: SeqSet, hits: Hits, stream: int = 0, *,
+                         max_penalty: int, matrix: SubstitutionMatrix | None = None,
+                         gap_open: int = 1, gap_extend: int = 1, prior=(),
+                         prior_width: int = 0) -> int:
+    """Fill ``hits`` with the cells of the gap-block matrix scoring <= ``max_penalty``; returns
+    the hit count.  Synchronises ``stream`` once (to size the sort)."""
+    pen = None if matrix is None else np.ascontiguousarray(matrix.penalty_grid, np.int32)
+    pr = np.ascontiguousarray(np.asarray(prior, dtype=np.int64).astype(np.int32)).ravel()
+    err = _lib.st_error()
+    code = _lib.lib.st_gapblock_sparse_sets(
+        queries.handle, refs.handle, _lib.i32_ptr(pen), 0 if pen is None else pen.shape[0],
+        gap_open, gap_extend, _lib.i32_ptr(pr) if pr.size else None, int(pr.size),
+        int(prior_width), int(max_penalty), hits.handle, ctypes.c_void_p(stream),
+        ctypes.byref(err))
+    _lib.check(code, err)
+    return hits.info()["nnz"]
+
+
 def align_into(queries: SeqSet, refs: SeqSet, out_ptr: int, stream: int = 0, *,
                matrix: SubstitutionMatrix, mode: str = "global", gap_open: int = 11,
                gap_extend: int = 1, dist: bool = False) -> None:

@@ -17,10 +17,11 @@ from collections.abc import Callable, Iterable, Sequence
 import numpy as np
 
 from ._core import gapblock_matrix as _gapblock_matrix
+from ._core import gapblock_sparse as _gapblock_sparse
 from .matrix import ScoreMatrix, SubstitutionMatrix
 
-__all__ = ["score_matrix", "central_prior", "profile_prior", "frame_prior", "positions_prior",
-           "gap_cost", "ScoreMatrix", "UNREACHABLE"]
+__all__ = ["score_matrix", "score_sparse", "SparseScores", "central_prior", "profile_prior",
+           "frame_prior", "positions_prior", "gap_cost", "ScoreMatrix", "UNREACHABLE"]
 
 #: A prior large enough that no layout carrying it wins, small enough not to overflow int32
 #: once a substitution cost is added (python/seqtree/gapblock.py:48-50).
@@ -170,3 +171,66 @@ def score_matrix(queries: Sequence[str], refs: Sequence[str],
     width = max(max(map(len, q), default=0), max(map(len, r), default=0))
     cube = prior_cube(gap_prior, width) if gap_prior is not None else []
     return _gapblock_matrix(q, r, alphabet, matrix, gap_open, gap_extend, cube, width, threads)
+
+
+class SparseScores:
+    """Thresholded gap-block matrix in CSR form: row ``i`` lists the refs ``k`` (ascending) whose
+    score against query ``i`` is <= ``max_penalty``, with those scores.
+
+    ``indptr`` (int64, rows + 1), ``ref_ids`` and ``scores`` (int32, nnz) are numpy arrays, the
+    layout of ``scipy.sparse.csr_matrix((scores, ref_ids, indptr), shape)``.
+    """
+
+    def __init__(self, indptr, ref_ids, scores, shape, max_penalty: int):
+        self.indptr, self.ref_ids, self.scores = indptr, ref_ids, scores
+        self.shape = tuple(shape)
+        self.max_penalty = max_penalty
+
+    @property
+    def nnz(self) -> int:
+        return int(self.ref_ids.size)
+
+    def row(self, i: int):
+        """(ref_ids, scores) of query ``i``."""
+        if not -self.shape[0] <= i < self.shape[0]:
+            raise IndexError("row index out of range")
+        i %= self.shape[0]
+        a, b = int(self.indptr[i]), int(self.indptr[i + 1])
+        return self.ref_ids[a:b], self.scores[a:b]
+
+    def to_dense(self, fill: int = -1):
+        """The (rows, cols) int32 matrix with ``fill`` where a cell did not pass."""
+        out = np.full(self.shape, fill, np.int32)
+        rows = np.repeat(np.arange(self.shape[0]), np.diff(self.indptr))
+        out[rows, self.ref_ids] = self.scores
+        return out
+
+    def __repr__(self) -> str:
+        return (f"SparseScores(shape={self.shape}, nnz={self.nnz}, "
+                f"max_penalty={self.max_penalty})")
+
+
+def score_sparse(queries: Sequence[str], refs: Sequence[str], max_penalty: int,
+                 matrix: SubstitutionMatrix | None = None, gap_open: int | None = None,
+                 gap_extend: int = 1, gap_prior: GapPrior | None = None, alphabet: str = "aa",
+                 threads: int = 0) -> SparseScores:
+    """Every (query, ref) pair with gap-block penalty <= ``max_penalty``, on the GPU.
+
+    The same scores as :func:`score_matrix` (same arguments and defaults), keeping only the cells
+    that pass the threshold, the way ``GapBlockIndex.search`` keeps its hits; nothing of size
+    ``len(queries) * len(refs)`` is ever materialised, so it runs on sets whose dense matrix
+    would not fit in memory (1e5 x 1e6 and beyond).  Raises ``ValueError`` when
+    ``max_penalty < 0``.
+    """
+    if max_penalty < 0:
+        raise ValueError("max_penalty must be >= 0")
+    q, r = list(queries), list(refs)
+    if gap_open is None:
+        gap_open = _default_gap_open(matrix)
+    if gap_open < 0 or gap_extend < 0:
+        raise ValueError("gap_open and gap_extend must be >= 0")
+    width = max(max(map(len, q), default=0), max(map(len, r), default=0))
+    cube = prior_cube(gap_prior, width) if gap_prior is not None else []
+    indptr, ref_ids, scores = _gapblock_sparse(q, r, max_penalty, alphabet, matrix, gap_open,
+                                              gap_extend, cube, width, threads)
+    return SparseScores(indptr, ref_ids, scores, (len(q), len(r)), max_penalty)
