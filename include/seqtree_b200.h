@@ -185,6 +185,45 @@ int32_t st_gapblock_sparse_sets(st_seqset queries, st_seqset refs, const int32_t
                                 int32_t max_penalty, st_hits out, void *cuda_stream,
                                 st_error *err);
 
+/* Gap-block scores of listed pairs: out_device[p] = score(queries[query_idx[p]], refs[ref_idx[p]])
+ * (index arrays and output in device memory).  The dense call's arithmetic and checks
+ * (src/gapblock.cpp:39-62, 66-81) on a pair list instead of the full product -- the exact rescore
+ * of the learned proposals and the labeller of the encoder's training pairs.  No counterpart in
+ * the reference. */
+int32_t st_gapblock_pairs_sets(st_seqset queries, st_seqset refs, const int32_t *query_idx,
+                               const int32_t *ref_idx, int64_t n, const int32_t *penalty,
+                               int32_t matrix_size, int32_t gap_open, int32_t gap_extend,
+                               const int32_t *prior, int64_t prior_len, uint32_t prior_width,
+                               int32_t *out_device, void *cuda_stream, st_error *err);
+
+/* ------------------------------------------------------------------------------------------
+ * Sequence encoder of the learned-proposal path (no counterpart in the reference).  One-hot
+ * amino-acid codes padded to 32 positions -> 2 conv layers -> 2 attention layers (width 128) ->
+ * mean pool -> 64-d unit vector; trained so that |z_a - z_b|^2 tracks the exact gap-block score.
+ * Parameters are a flat fp32 array of st_encoder_param_count() values.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct st_encoder_s *st_encoder;
+int64_t st_encoder_param_count(void);
+/* params: host array of st_encoder_param_count() floats (NULL: all zero). */
+int32_t st_encoder_create(const float *params, st_encoder *out, st_error *err);
+void st_encoder_destroy(st_encoder enc);
+int32_t st_encoder_get_params(st_encoder enc, float *out, st_error *err);
+/* A batch is S sequences (S even; pairs are (2i, 2i+1)) as host arrays: codes [S][32] (0..23,
+ * zero beyond the length), lens [S] (1..32), scores [S/2] (exact gap-block scores).  loss_grad
+ * returns the mean pair loss and, when grad is not NULL, its gradient; train_step also applies
+ * one Adam step with learning rate lr. */
+int32_t st_encoder_loss_grad(st_encoder enc, const uint8_t *codes, const int32_t *lens,
+                             const int32_t *scores, int32_t S, float *loss, float *grad,
+                             st_error *err);
+int32_t st_encoder_train_step(st_encoder enc, const uint8_t *codes, const int32_t *lens,
+                              const int32_t *scores, int32_t S, float lr, float *loss,
+                              st_error *err);
+/* Embeddings of a device set (amino acids, lengths 1..32) into out_device: layout 0 = fp32
+ * [n][64]; layout 1 = bf16 [n][64] with the 16-byte chunks of row r stored at chunk ^ (r & 7)
+ * (the operand layout of the proposal kernel). */
+int32_t st_encoder_embed(st_encoder enc, st_seqset set, void *out_device, int32_t layout,
+                         void *cuda_stream, st_error *err);
+
 int32_t st_align_matrix_sets(st_seqset queries, st_seqset refs, const int32_t *similarity,
                              int32_t matrix_size, int32_t mode, int32_t gap_open,
                              int32_t gap_extend, int32_t dist, int32_t *out_device,

@@ -71,6 +71,22 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_void_p, _i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
       _i32p, ctypes.c_int64, ctypes.c_uint32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
       _ep]),
+    ("st_gapblock_pairs_sets", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, _i32p,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_int64, ctypes.c_uint32,
+      ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_encoder_param_count", ctypes.c_int64, []),
+    ("st_encoder_create", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), _ep]),
+    ("st_encoder_destroy", None, [ctypes.c_void_p]),
+    ("st_encoder_get_params", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_encoder_loss_grad", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.POINTER(ctypes.c_float), ctypes.c_void_p, _ep]),
+    ("st_encoder_train_step", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
+      ctypes.c_float, ctypes.POINTER(ctypes.c_float), _ep]),
+    ("st_encoder_embed", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, _ep]),
     ("st_seqset_create", ctypes.c_int32,
      [_sp, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p), _ep]),
     ("st_seqset_destroy", None, [ctypes.c_void_p]),

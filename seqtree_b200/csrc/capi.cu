@@ -22,6 +22,20 @@ void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
                 cudaStream_t stream);
 void hamming_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream_t stream);
 void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream_t stream);
+void gapblock_pairs_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* qi_d, const int32_t* ri_d,
+                         int64_t n, const int32_t* penalty, int32_t matrix_size, int32_t go,
+                         int32_t ge, const int32_t* prior, int64_t prior_len, uint32_t prior_width,
+                         int32_t* out_d, cudaStream_t stream);
+struct Encoder;
+int64_t encoder_param_count();
+Encoder* encoder_create(const float* params);
+void encoder_destroy(Encoder* m);
+void encoder_params(Encoder& m, float* out);
+float encoder_loss_grad(Encoder& m, const uint8_t* codes, const int32_t* lens, const int32_t* scores,
+                        int S, float* grad_out);
+float encoder_train_step(Encoder& m, const uint8_t* codes, const int32_t* lens, const int32_t* scores,
+                         int S, float lr);
+void encoder_embed(Encoder& m, const st_seqset_s& set, void* out, int layout, cudaStream_t st);
 int last_launches();
 const char* last_kernel();
 void* host_alloc(uint64_t bytes);
@@ -490,6 +504,111 @@ int32_t st_gapblock_sparse_sets(st_seqset queries, st_seqset refs, const int32_t
         gapblock_sparse_sets(*queries, *refs, penalty, matrix_size, gap_open, gap_extend, prior,
                              prior_len, prior_width, max_penalty, *out,
                              static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int32_t st_gapblock_pairs_sets(st_seqset queries, st_seqset refs, const int32_t* query_idx,
+                               const int32_t* ref_idx, int64_t n, const int32_t* penalty,
+                               int32_t matrix_size, int32_t gap_open, int32_t gap_extend,
+                               const int32_t* prior, int64_t prior_len, uint32_t prior_width,
+                               int32_t* out_device, void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_set(queries);
+        check_set(refs);
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        gapblock_pairs_sets(*queries, *refs, query_idx, ref_idx, n, penalty, matrix_size, gap_open,
+                            gap_extend, prior, prior_len, prior_width, out_device,
+                            static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+// ---------------------------------------------------------------------------- encoder -------
+struct st_encoder_s {
+    int device = 0;
+    stb::Encoder* impl = nullptr;
+};
+
+int64_t st_encoder_param_count(void) { return encoder_param_count(); }
+
+int32_t st_encoder_create(const float* params, st_encoder* out, st_error* err) {
+    return guard(err, [&] {
+        if (!out) fail(ST_EINVAL, "seqtree_b200: null output handle");
+        *out = nullptr;
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        auto h = std::make_unique<st_encoder_s>();
+        h->device = ctx.device;
+        h->impl = encoder_create(params);
+        *out = h.release();
+    });
+}
+
+void st_encoder_destroy(st_encoder enc) {
+    if (!enc) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    const int home = enc->device;
+    if (prev != home) cudaSetDevice(home);
+    encoder_destroy(enc->impl);
+    delete enc;
+    if (prev >= 0 && prev != home) cudaSetDevice(prev);
+}
+
+static Context& encoder_ctx(st_encoder enc) {
+    if (!enc || !enc->impl) fail(ST_EINVAL, "seqtree_b200: null encoder");
+    int dev = -1;
+    STB_CUDA(cudaGetDevice(&dev));
+    if (dev != enc->device) fail(ST_EINVAL, "seqtree_b200: encoder lives on another device");
+    return context();
+}
+
+int32_t st_encoder_get_params(st_encoder enc, float* out, st_error* err) {
+    return guard(err, [&] {
+        Context& ctx = encoder_ctx(enc);
+        if (!out) fail(ST_EINVAL, "seqtree_b200: null output");
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        encoder_params(*enc->impl, out);
+    });
+}
+
+int32_t st_encoder_loss_grad(st_encoder enc, const uint8_t* codes, const int32_t* lens,
+                             const int32_t* scores, int32_t S, float* loss, float* grad,
+                             st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        Context& ctx = encoder_ctx(enc);
+        if (!codes || !lens || !scores) fail(ST_EINVAL, "seqtree_b200: null batch");
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        const float l = encoder_loss_grad(*enc->impl, codes, lens, scores, S, grad);
+        if (loss) *loss = l;
+    });
+}
+
+int32_t st_encoder_train_step(st_encoder enc, const uint8_t* codes, const int32_t* lens,
+                              const int32_t* scores, int32_t S, float lr, float* loss,
+                              st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        Context& ctx = encoder_ctx(enc);
+        if (!codes || !lens || !scores) fail(ST_EINVAL, "seqtree_b200: null batch");
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        const float l = encoder_train_step(*enc->impl, codes, lens, scores, S, lr);
+        if (loss) *loss = l;
+    });
+}
+
+int32_t st_encoder_embed(st_encoder enc, st_seqset set, void* out_device, int32_t layout,
+                         void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        Context& ctx = encoder_ctx(enc);
+        check_set(set);
+        if (!out_device) fail(ST_EINVAL, "seqtree_b200: null output");
+        if (layout != 0 && layout != 1) fail(ST_EINVAL, "seqtree_b200: embedding layout is 0 or 1");
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        encoder_embed(*enc->impl, *set, out_device, layout, static_cast<cudaStream_t>(cuda_stream));
     });
 }
 

@@ -483,6 +483,51 @@ struct GeneralArgs {
     SparseSink sink;      // sparse output (unused by the dense form)
 };
 
+// The gap-block score of one pair in int32 arithmetic with the reference's wrap
+// (src/gapblock.cpp:39-62, in the single-sweep form S + min_i(C_i + p_i)).
+__device__ __forceinline__ int32_t gapblock_cell(const uint8_t* q, int m, const uint8_t* r, int n,
+                                                 const int32_t* s_pen, int A, int32_t go, int32_t ge,
+                                                 const int32_t* prior, int64_t pw1) {
+    const int L = min(m, n), d = abs(m - n);
+    if (d == 0) {
+        uint32_t s = 0;
+        for (int j = 0; j < L; ++j) s += uint32_t(s_pen[q[j] * A + r[j]]);
+        return int32_t(s);
+    }
+    const bool ql = m > n;
+    const int32_t* prow = prior ? prior + (int64_t(max(m, n)) * pw1 + d) * pw1 : nullptr;
+    int32_t S = 0, C = 0;
+    int32_t best = prow ? prow[0] : 0;
+    for (int j = 0; j < L; ++j) {
+        const int32_t p0v = s_pen[q[j] * A + r[j]];
+        const int32_t pdv = ql ? s_pen[q[j + d] * A + r[j]] : s_pen[q[j] * A + r[j + d]];
+        S += pdv;
+        C += p0v - pdv;
+        const int32_t cand = C + (prow ? prow[j + 1] : 0);
+        best = cand < best ? cand : best;
+    }
+    return int32_t(uint32_t(S) + uint32_t(best) + uint32_t(go) + uint32_t(d - 1) * uint32_t(ge));
+}
+
+// One thread per listed pair (qi[p], ri[p]); out[p] = its score.
+__global__ void __launch_bounds__(256) gapblock_pairs_kernel(
+    const uint8_t* __restrict__ qcodes, const int64_t* __restrict__ qoff,
+    const uint8_t* __restrict__ rcodes, const int64_t* __restrict__ roff,
+    const int32_t* __restrict__ qi, const int32_t* __restrict__ ri, int64_t n,
+    const int32_t* __restrict__ pen, int A, int32_t go, int32_t ge,
+    const int32_t* __restrict__ prior, int64_t pw1, int32_t* __restrict__ out) {
+    extern __shared__ int32_t s_pen[];
+    for (int i = threadIdx.x; i < A * A; i += blockDim.x) s_pen[i] = pen[i];
+    __syncthreads();
+    for (int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; p < n;
+         p += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t i = qi[p], k = ri[p];
+        const int m = int(qoff[i + 1] - qoff[i]), nn = int(roff[k + 1] - roff[k]);
+        out[p] = gapblock_cell(qcodes + qoff[i], m, rcodes + roff[k], nn, s_pen, A, go, ge, prior,
+                               pw1);
+    }
+}
+
 // One thread per (i, k) in row-major order, int32 arithmetic with the reference's wrap.  The
 // loop runs the same number of rounds on every lane (the sparse append is warp-collective).
 template <bool SPARSE>
@@ -498,33 +543,10 @@ __global__ void __launch_bounds__(256) gapblock_general_kernel(const GeneralArgs
         const bool live = idx < total;
         const int64_t il = live ? idx / a.K : 0, k = live ? idx - il * a.K : 0;
         const int64_t i = a.row0 + il;
-        const uint8_t* q = a.qcodes + a.qoff[i];
-        const uint8_t* r = a.rcodes + a.roff[k];
         const int m = int(a.qoff[i + 1] - a.qoff[i]);
         const int n = int(a.roff[k + 1] - a.roff[k]);
-        const int L = min(m, n), d = abs(m - n);
-        int32_t v;
-        if (d == 0) {
-            uint32_t s = 0;
-            for (int j = 0; j < L; ++j) s += uint32_t(s_pen[q[j] * a.A + r[j]]);
-            v = int32_t(s);
-        } else {
-            const bool ql = m > n;
-            const int32_t* prow =
-                a.prior ? a.prior + (int64_t(max(m, n)) * a.pw1 + d) * a.pw1 : nullptr;
-            int32_t S = 0, C = 0;
-            int32_t best = prow ? prow[0] : 0;
-            for (int j = 0; j < L; ++j) {
-                const int32_t p0v = s_pen[q[j] * a.A + r[j]];
-                const int32_t pdv = ql ? s_pen[q[j + d] * a.A + r[j]] : s_pen[q[j] * a.A + r[j + d]];
-                S += pdv;
-                C += p0v - pdv;
-                const int32_t cand = C + (prow ? prow[j + 1] : 0);
-                best = cand < best ? cand : best;
-            }
-            v = int32_t(uint32_t(S) + uint32_t(best) + uint32_t(a.go) +
-                        uint32_t(d - 1) * uint32_t(a.ge));
-        }
+        const int32_t v = gapblock_cell(a.qcodes + a.qoff[i], m, a.rcodes + a.roff[k], n, s_pen,
+                                        a.A, a.go, a.ge, a.prior, a.pw1);
         if constexpr (SPARSE) {
             sink_append(a.sink, live && v <= a.sink.thresh ? 1u : 0u, int(threadIdx.x & 31),
                         [&](int, unsigned long long& key, int32_t& val) {
@@ -850,6 +872,70 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
                    uint32_t prior_width, int32_t* out_d, cudaStream_t stream) {
     gapblock_run(qs, rs, penalty, matrix_size, go, ge, prior, prior_len, prior_width, out_d,
                  nullptr, stream);
+}
+
+// Scores of listed pairs (device index arrays) into out_d; the general int32 kernel's
+// arithmetic, so any lengths and penalties.
+void gapblock_pairs_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* qi_d, const int32_t* ri_d,
+                         int64_t n, const int32_t* penalty, int32_t matrix_size, int32_t go,
+                         int32_t ge, const int32_t* prior, int64_t prior_len, uint32_t prior_width,
+                         int32_t* out_d, cudaStream_t stream) {
+    if (go < 0 || ge < 0) fail(ST_EINVAL, "gap_open and gap_extend must be >= 0");
+    if (qs.alphabet < 0 || qs.alphabet != rs.alphabet)
+        fail(ST_EINVAL, "seqtree_b200: gap-block sets must be encoded with one alphabet");
+    const int A = alphabet_size(qs.alphabet);
+    if (penalty && matrix_size != A) fail(ST_EINVAL, "matrix size does not match the alphabet");
+    if (n < 0) fail(ST_EINVAL, "seqtree_b200: negative pair count");
+    if (n == 0) return;
+    const int64_t W1p = int64_t(prior_width) + 1;
+    const bool has_prior = prior && prior_len > 0;
+    if (has_prior) {
+        if (prior_len != W1p * W1p * W1p)
+            fail(ST_EINVAL, "prior table must have (prior_width + 1)^3 entries");
+        if (uint32_t(std::max(qs.max_len, rs.max_len)) > prior_width)
+            fail(ST_EINVAL, "a sequence is longer than the prior table's width");
+    }
+    Context& ctx = context();
+    std::vector<int32_t> pen(size_t(A) * A);
+    for (int x = 0; x < A; ++x)
+        for (int y = 0; y < A; ++y) pen[size_t(x) * A + y] = penalty ? penalty[x * A + y] : int32_t(x != y);
+    // Tables cached per device by content, so repeated calls upload nothing (and can be
+    // captured in a CUDA graph once warmed up).
+    struct PairTables {
+        std::vector<uint8_t> key;
+        DevBuf pen, prior;
+    };
+    static std::mutex mu;
+    static std::map<int, std::unique_ptr<PairTables>> all;
+    PairTables* pt;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        auto& slot = all[ctx.device];
+        if (!slot) slot = std::make_unique<PairTables>();
+        pt = slot.get();
+    }
+    {
+        std::vector<uint8_t> key(pen.size() * 4 + (has_prior ? size_t(prior_len) * 4 : 0) + 8);
+        const int64_t hdr = has_prior ? prior_len : -1;
+        std::memcpy(key.data(), &hdr, 8);
+        std::memcpy(key.data() + 8, pen.data(), pen.size() * 4);
+        if (has_prior) std::memcpy(key.data() + 8 + pen.size() * 4, prior, size_t(prior_len) * 4);
+        if (!same_as_last(pt->key, key.data(), key.size())) {
+            pt->key.clear();
+            h2d(pt->pen.as<int32_t>(pen.size()), pen.data(), pen.size() * 4, stream);
+            if (has_prior)
+                h2d(pt->prior.as<int32_t>(size_t(prior_len)), prior, size_t(prior_len) * 4, stream);
+            pt->key = key;
+        }
+    }
+    const int32_t* d_pen = static_cast<const int32_t*>(pt->pen.ptr);
+    const int32_t* d_prior = has_prior ? static_cast<const int32_t*>(pt->prior.ptr) : nullptr;
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), int64_t(ctx.num_sms) * 16);
+    gapblock_pairs_kernel<<<unsigned(blocks), 256, size_t(A) * A * 4, stream>>>(
+        qs.d_bytes, qs.d_off, rs.d_bytes, rs.d_off, qi_d, ri_d, n, d_pen, A, go, ge, d_prior, W1p,
+        out_d);
+    STB_CUDA(cudaGetLastError());
+    note_launch("gapblock_pairs_kernel");
 }
 
 // ---------------------------------------------------------------------------- sparse --------

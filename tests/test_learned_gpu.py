@@ -1,0 +1,116 @@
+"""The learned-proposal path on the GPU: the encoder's training kernels against the float64
+oracle (loss, every gradient, the forward embedding), training progress, and the exact pair
+scorer against the oracle."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+import oracle.encoder as oenc
+from conftest import cdr3
+from seqtree_b200.matrix import SubstitutionMatrix
+
+
+def _batch(rng, S):
+    from seqtree_b200.learned import pad_codes
+    seqs = cdr3(rng, S, 8, 25)
+    codes, lens = pad_codes(seqs)
+    return seqs, codes, lens, rng.integers(0, 90, size=S // 2).astype(np.int32)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("S", [16, 258])
+def test_encoder_gradients_match_the_oracle(cuda_ready, S):
+    from seqtree_b200.learned import Encoder
+    rng = np.random.default_rng(S)
+    _, codes, lens, scores = _batch(rng, S)
+    flat = (oenc.init_params(5) + rng.normal(0, 0.05, oenc.param_count())).astype(np.float32)
+    enc = Encoder(flat)
+    loss, g = enc.loss_grad(codes, lens, scores)
+    want_loss, want_g = oenc.backward(flat.astype(np.float64), codes, lens, scores)
+    assert loss == pytest.approx(want_loss, rel=1e-4)
+    # fp32 against float64: every block within 1e-3 of its largest gradient
+    o = 0
+    for name, shape in oenc.SHAPES:
+        n = int(np.prod(shape))
+        a, b = g[o:o + n], want_g[o:o + n]
+        scale = max(np.abs(b).max(), 1e-12)
+        assert np.abs(a - b).max() <= 2e-3 * scale, (name, np.abs(a - b).max(), scale)
+        o += n
+
+
+@pytest.mark.gpu
+def test_encoder_embeddings_match_the_oracle_forward(cuda_ready):
+    import torch
+
+    from seqtree_b200 import device
+    from seqtree_b200.learned import Encoder, pad_codes
+    rng = np.random.default_rng(9)
+    seqs = cdr3(rng, 300, 8, 25) + ["C", "CASSLGQGAYEQYFCASSLGQGAYEQYFWWW"]
+    flat = oenc.init_params(11)
+    enc = Encoder(flat)
+    ss = device.SeqSet(seqs, "aa")
+    z32 = torch.empty((len(seqs), 64), dtype=torch.float32, device="cuda")
+    zbf = torch.empty((len(seqs), 64), dtype=torch.bfloat16, device="cuda")
+    enc.embed_into(ss, z32.data_ptr(), 0, torch.cuda.current_stream().cuda_stream)
+    enc.embed_into(ss, zbf.data_ptr(), 1, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    codes, lens = pad_codes(seqs)
+    want = oenc.forward(flat.astype(np.float64), codes, lens)
+    np.testing.assert_allclose(z32.cpu().numpy(), want, atol=2e-5)
+    # layout 1: row r's 16-byte chunk c sits at chunk c ^ (r & 7)
+    raw = zbf.float().cpu().numpy().reshape(len(seqs), 8, 8)
+    rows = np.arange(len(seqs))[:, None]
+    unswz = raw[rows, np.arange(8)[None, :] ^ (rows & 7)].reshape(len(seqs), 64)
+    np.testing.assert_allclose(unswz, want, atol=8e-3)
+    with pytest.raises(ValueError, match="1..32 residues"):
+        enc.embed_into(device.SeqSet(["C" * 33], "aa"), z32.data_ptr(), 0)
+
+
+@pytest.mark.gpu
+def test_training_lowers_the_loss(cuda_ready):
+    from seqtree_b200.learned import Encoder, pad_codes, training_pairs
+    rng = np.random.default_rng(1)
+    a, b = training_pairs(3, 4096)
+    m = SubstitutionMatrix.blosum62()
+    pen = m.penalty_grid
+    sc = np.array([oracle.gapblock_matrix([x], [y], pen, gap_open=8)[0, 0] for x, y in zip(a, b)],
+                  np.int32)
+    seqs = [s for pair in zip(a, b) for s in pair]
+    codes, lens = pad_codes(seqs)
+    enc = Encoder(seed=0)
+    first = None
+    for epoch in range(6):
+        losses = []
+        for i in range(0, len(seqs), 512):
+            losses.append(enc.train_step(codes[i:i + 512], lens[i:i + 512], sc[i // 2:(i + 512) // 2],
+                                         lr=1e-3))
+        first = first if first is not None else np.mean(losses)
+    assert np.mean(losses) < 0.5 * first
+    assert np.all(np.isfinite(enc.params()))
+
+
+@pytest.mark.gpu
+def test_pair_scorer_matches_the_oracle(cuda_ready):
+    import torch
+
+    from seqtree_b200 import device
+    from seqtree_b200.gapblock import central_prior, prior_cube
+    from seqtree_b200.learned import pair_scores
+    rng = np.random.default_rng(4)
+    q, r = cdr3(rng, 70, 8, 25), cdr3(rng, 90, 8, 25) + ["C" * 70]
+    qi = rng.integers(0, len(q), 5000).astype(np.int32)
+    ri = rng.integers(0, len(r), 5000).astype(np.int32)
+    m = SubstitutionMatrix.blosum62()
+    width = 70
+    cube = np.asarray(prior_cube(central_prior(21), width), np.int32).ravel()
+    dense = oracle.gapblock_matrix(q, r, m.penalty_grid, gap_open=8, gap_extend=1, prior=cube,
+                                   prior_width=width)
+    qs, rs = device.SeqSet(q, "aa"), device.SeqSet(r, "aa")
+    tq, tr = torch.from_numpy(qi).cuda(), torch.from_numpy(ri).cuda()
+    out = torch.empty(5000, dtype=torch.int32, device="cuda")
+    pair_scores(qs, rs, tq.data_ptr(), tr.data_ptr(), 5000, out.data_ptr(), matrix=m, gap_open=8,
+                prior=cube, prior_width=width)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(out.cpu().numpy(), dense[qi, ri])
