@@ -224,6 +224,22 @@ int32_t st_encoder_train_step(st_encoder enc, const uint8_t *codes, const int32_
 int32_t st_encoder_embed(st_encoder enc, st_seqset set, void *out_device, int32_t layout,
                          void *cuda_stream, st_error *err);
 
+/* Learned candidate proposal (no counterpart in the reference): for every query, the k refs with
+ * the largest embedding dot product, computed on the tensor cores without materialising the
+ * nq x nr similarity matrix.  query_emb / ref_emb are device arrays of st_encoder_embed layout 1
+ * (bf16 [n][64], 16-byte aligned).  ids_device[q*k + i] (and scores_device, which may be NULL)
+ * receive the i-th best ref of query q, best first (score descending, ties by ascending ref
+ * id); slots beyond nr refs hold -1 / -inf.  k is 1..256.  Asynchronous on cuda_stream; a
+ * bounded device wait that gave up is reported by st_stream_status. */
+int32_t st_propose_topk(const void *query_emb, int64_t nq, const void *ref_emb, int64_t nr,
+                        int32_t k, int32_t *ids_device, float *scores_device, void *cuda_stream,
+                        st_error *err);
+
+/* Synchronises cuda_stream and reports (then clears) the device error words written by the
+ * asynchronous *_sets and proposal calls since the last check: ST_ETIMEOUT when a bounded
+ * device-side wait gave up. */
+int32_t st_stream_status(void *cuda_stream, st_error *err);
+
 int32_t st_align_matrix_sets(st_seqset queries, st_seqset refs, const int32_t *similarity,
                              int32_t matrix_size, int32_t mode, int32_t gap_open,
                              int32_t gap_extend, int32_t dist, int32_t *out_device,

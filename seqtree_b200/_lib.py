@@ -87,6 +87,10 @@ SIGNATURES = [
       ctypes.c_float, ctypes.POINTER(ctypes.c_float), _ep]),
     ("st_encoder_embed", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, _ep]),
+    ("st_propose_topk", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_stream_status", ctypes.c_int32, [ctypes.c_void_p, _ep]),
     ("st_seqset_create", ctypes.c_int32,
      [_sp, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p), _ep]),
     ("st_seqset_destroy", None, [ctypes.c_void_p]),

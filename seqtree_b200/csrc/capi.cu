@@ -36,6 +36,8 @@ float encoder_loss_grad(Encoder& m, const uint8_t* codes, const int32_t* lens, c
 float encoder_train_step(Encoder& m, const uint8_t* codes, const int32_t* lens, const int32_t* scores,
                          int S, float lr);
 void encoder_embed(Encoder& m, const st_seqset_s& set, void* out, int layout, cudaStream_t st);
+void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, int k, int32_t* ids,
+                  float* scores, cudaStream_t stream);
 int last_launches();
 const char* last_kernel();
 void* host_alloc(uint64_t bytes);
@@ -609,6 +611,32 @@ int32_t st_encoder_embed(st_encoder enc, st_seqset set, void* out_device, int32_
         if (layout != 0 && layout != 1) fail(ST_EINVAL, "seqtree_b200: embedding layout is 0 or 1");
         std::lock_guard<std::mutex> lk(ctx.mu);
         encoder_embed(*enc->impl, *set, out_device, layout, static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int32_t st_propose_topk(const void* query_emb, int64_t nq, const void* ref_emb, int64_t nr,
+                        int32_t k, int32_t* ids_device, float* scores_device, void* cuda_stream,
+                        st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        propose_topk(query_emb, nq, ref_emb, nr, k, ids_device, scores_device,
+                     static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int32_t st_stream_status(void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+        STB_CUDA(cudaStreamSynchronize(st));
+        STB_CUDA(cudaMemcpyAsync(ctx.flags_h + 8, ctx.flags_d + 8, 8 * sizeof(int64_t),
+                                 cudaMemcpyDeviceToHost, st));
+        STB_CUDA(cudaMemsetAsync(ctx.flags_d + 8, 0, 8 * sizeof(int64_t), st));
+        STB_CUDA(cudaStreamSynchronize(st));
+        check_timeout(ctx);
     });
 }
 

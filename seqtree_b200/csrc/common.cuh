@@ -81,6 +81,8 @@ struct Context {
     DevBuf out_buf, q_codes, r_codes, table_buf, prior_buf, ftab_buf, work_a, work_b, work_c;
     // sparse output: unsorted hit keys and scores, sorted keys, radix-sort scratch
     DevBuf sp_keys, sp_vals, sp_sorted, sp_temp;
+    // candidate lists of the learned-proposal kernel
+    DevBuf topk_cand;
     // storage of the transient sets made by the host-buffer entry points
     DevBuf tq[3], tr[3];  // bytes, offsets, lengths
     // plans reused by transient sets (rebuilt in place for every call)

@@ -1,0 +1,578 @@
+// Learned candidate proposal: the top-k refs of every query by embedding dot product, on the
+// 5th-generation tensor cores, without ever materialising the query x ref similarity matrix.
+//
+// Inputs are the encoder's 64-d unit embeddings in bf16, stored [n][64] with the eight 16-byte
+// chunks of row r at chunk ^ (r & 7).  That is the 128-byte-swizzled K-major operand layout, so a
+// linear bulk copy of 128 consecutive rows into 1024-byte-aligned shared memory is a ready
+// tcgen05 operand tile and no tensor map is needed.
+//
+// One persistent CTA per SM (320 threads) walks query tiles of 256 rows:
+//   warp 0     bulk-copies the tile's query rows once, then streams ref tiles of 128 rows
+//              through a 6-stage shared-memory ring (cp.async.bulk + mbarrier complete_tx);
+//   warp 1     allocates 512 TMEM columns and, from one thread, issues per ref tile two
+//              M=128 N=128 K=64 bf16 MMAs (4 x tcgen05.mma K=16 each) into one of two
+//              256-column fp32 accumulators, committing the stage and the accumulator to
+//              mbarriers;
+//   warps 2-9  own one query row each (TMEM lane = row, warp % 4 selects the lane quarter,
+//              warps 2-5 read the first query half and 6-9 the second).  Each reads its row's
+//              128 fp32 scores with tcgen05.ld, rejects a 32-column group with one 3-input max
+//              against the running threshold, and appends the survivors to the query's
+//              candidate list in global scratch as 64-bit keys
+//              (orderable score << 32 | ~ref_id: larger score first, then smaller ref id).
+//              When a list passes kCap - 128 entries, the warp cooperatively radix-selects its
+//              k-th largest key, keeps exactly k keys and raises the threshold to the smallest
+//              kept score.  After the last ref tile each list is cut to k, sorted by key in
+//              shared memory and written out.
+//
+// Refs are scanned in ascending id order, so a later ref with a score equal to the k-th kept
+// one never ranks above it: the strict "score > threshold" test loses no member of the exact
+// top-k under that order.  Every wait is bounded (a few seconds of %globaltimer); on time-out
+// the CTA records the failure, drains its copies and MMAs with bounded waits, frees TMEM and
+// returns.
+#include <cuda_bf16.h>
+
+#include <cfloat>
+#include <algorithm>
+#include <cstdint>
+#include <mutex>
+
+#include "common.cuh"
+
+namespace stb {
+
+namespace {
+
+constexpr int kRowB = 128;                     // one 64-d bf16 embedding row
+constexpr int kQT = 256;                       // queries per tile (two M=128 accumulators)
+constexpr int kRT = 128;                       // refs per stage (MMA N)
+constexpr int kStages = 6;
+constexpr int kCap = 640;                      // candidate keys per query list
+constexpr int kPer = kCap / 32;                // keys per lane in a cooperative pass
+constexpr int kMaxK = 256;
+constexpr int kThreads = 320;
+constexpr int kEpiWarps = 8;
+constexpr uint32_t kTmemCols = 512;
+constexpr int kTileB = kRT * kRowB;            // 16 KB
+
+constexpr int kSmA = 0;                                   // 32 KB: the query tile
+constexpr int kSmB = kSmA + kQT * kRowB;                  // 96 KB: the ref ring
+constexpr int kSmWarp = kSmB + kStages * kTileB;          // 8 x 2 KB: histogram / sort space
+constexpr int kSmBar = kSmWarp + kEpiWarps * 2048;        // mbarriers and flags
+constexpr int kSmTotal = kSmBar + 256;
+constexpr size_t kSmemBytes = size_t(kSmTotal) + 1024;    // + alignment slack
+
+// bf16 x bf16 -> fp32, both operands K-major, M = 128, N = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kRT >> 3) << 17) |
+                            (uint32_t(128 >> 4) << 24);
+
+constexpr uint64_t kWaitNs = 4000000000ull;               // bound of every wait
+
+struct ProposeArgs {
+    const uint8_t* qemb;
+    const uint8_t* remb;
+    int64_t nq, nr;
+    int k;
+    unsigned long long* cand;  // [gridDim.x][kQT][kCap]
+    int32_t* out_ids;          // [nq][k]
+    float* out_scores;         // [nq][k] or null
+    unsigned long long* err;
+};
+
+// ------------------------------------------------------------------ PTX wrappers ------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return uint32_t(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ uint64_t now_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ bool bar_test(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for the phase of `parity` to complete.  Gives up (returns false) when the CTA's
+// abort word is set or after kWaitNs, setting the abort word and the host-visible error word.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, volatile int* abort,
+                                         unsigned long long* err) {
+    if (bar_test(bar, parity)) return true;
+    const uint64_t t0 = now_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (bar_test(bar, parity)) return true;
+        if ((it & 255) == 0) {
+            if (*abort) return false;
+            if (now_ns() - t0 > kWaitNs) {
+                *abort = 1;
+                atomicExch(err, 1ull);
+                return false;
+            }
+        }
+    }
+}
+// Bounded wait that ignores the abort word (draining in-flight work before exit).
+__device__ __forceinline__ void bar_drain(uint32_t bar, uint32_t parity) {
+    const uint64_t t0 = now_ns();
+    while (!bar_test(bar, parity) && now_ns() - t0 < kWaitNs) {
+    }
+}
+__device__ __forceinline__ void bar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void bar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes,
+                                          uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(dst),
+        "l"(src), "r"(bytes), "r"(bar)
+        : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     bar)
+                 : "memory");
+}
+// K-major operand in the 128-byte swizzle: rows of 128 B, 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t(1) << 16) | (uint64_t(1024 >> 4) << 32) |
+           (uint64_t(1) << 46) | (uint64_t(2) << 61);
+}
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+          "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+          "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+          "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+    float m;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(m) : "f"(a), "f"(b), "f"(c));
+    return m;
+}
+
+// Score <-> key half: an unsigned order that matches the float order (non-NaN).
+__device__ __forceinline__ uint32_t ord_of(uint32_t u) {
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float score_of(uint32_t o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7FFFFFFFu) : ~o);
+}
+// Acceptance threshold for keys above `min_kept`: any score whose key can exceed it passes
+// "s > thr" (a -0.0 threshold is lowered so that +0.0 passes; the test is a superset).
+__device__ __forceinline__ float threshold_of(unsigned long long min_kept) {
+    const float t = score_of(uint32_t(min_kept >> 32));
+    return (t == 0.0f) ? -FLT_TRUE_MIN : t;
+}
+
+// ------------------------------------------------------------- warp selection ---------------
+// The k-th largest of the n (<= kCap, distinct) keys at `list`, by one warp: 8-bit radix passes
+// from the top with a 256-bin shared-memory histogram, stopping as soon as the bin holding the
+// k-th key is entirely inside the top k.  Returns T with exactly k keys >= T.
+__device__ unsigned long long warp_kth_largest(const unsigned long long (&key)[kPer], int n, int k,
+                                               uint32_t* hist, int lane) {
+    unsigned long long prefix = 0, pmask = 0;
+    int krem = k;
+#pragma unroll 1
+    for (int shift = 56; shift >= 0; shift -= 8) {
+        for (int i = lane; i < 256; i += 32) hist[i] = 0;
+        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            const int idx = lane + 32 * i;
+            if (idx < n && (key[i] & pmask) == prefix)
+                atomicAdd(&hist[uint32_t(key[i] >> shift) & 255u], 1u);
+        }
+        __syncwarp();
+        // lane l owns bins 255-8l .. 248-8l, highest first
+        uint32_t c[8], sum = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            c[j] = hist[255 - 8 * lane - j];
+            sum += c[j];
+        }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const uint32_t excl = incl - sum;
+        const uint32_t owner = __ballot_sync(0xffffffffu, excl < uint32_t(krem) && uint32_t(krem) <= incl);
+        const int L = __ffs(owner) - 1;
+        uint32_t bin = 0, above = 0, cb = 0;
+        if (lane == L) {
+            uint32_t acc = excl;
+            bool found = false;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                if (!found && acc + c[j] >= uint32_t(krem)) {
+                    found = true;
+                    bin = uint32_t(255 - 8 * lane - j);
+                    above = acc;
+                    cb = c[j];
+                }
+                acc += c[j];
+            }
+        }
+        bin = __shfl_sync(0xffffffffu, bin, L);
+        above = __shfl_sync(0xffffffffu, above, L);
+        cb = __shfl_sync(0xffffffffu, cb, L);
+        krem -= int(above);
+        prefix |= (unsigned long long)bin << shift;
+        pmask |= 0xFFull << shift;
+        __syncwarp();
+        if (int(cb) == krem) break;
+    }
+    return prefix;
+}
+
+// Cuts the list of n > k keys to exactly its k largest (kept in list order) and returns the
+// smallest kept key.  Warp-collective.
+__device__ unsigned long long warp_cut(unsigned long long* list, int n, int k, uint32_t* hist,
+                                       int lane) {
+    unsigned long long key[kPer];
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int idx = lane + 32 * i;
+        key[i] = idx < n ? list[idx] : 0ull;
+    }
+    __syncwarp();
+    const unsigned long long T = warp_kth_largest(key, n, k, hist, lane);
+    unsigned long long mn = ~0ull;
+    int base = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int idx = lane + 32 * i;
+        const bool keep = idx < n && key[i] >= T;
+        const uint32_t b = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+            list[base + __popc(b & ((1u << lane) - 1u))] = key[i];
+            mn = key[i] < mn ? key[i] : mn;
+        }
+        base += __popc(b);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, mn, o);
+        mn = t < mn ? t : mn;
+    }
+    __syncwarp();
+    return mn;
+}
+
+// Descending bitonic sort of 256 keys in shared memory by one warp.
+__device__ void warp_sort256_desc(unsigned long long* s, int lane) {
+#pragma unroll 1
+    for (int k = 2; k <= 256; k <<= 1) {
+#pragma unroll 1
+        for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+            for (int t = lane; t < 128; t += 32) {
+                const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+                const int p = i + j;
+                const unsigned long long a = s[i], b = s[p];
+                const bool desc = (i & k) == 0;
+                if (desc ? (a < b) : (a > b)) {
+                    s[i] = b;
+                    s[p] = a;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// ------------------------------------------------------------------------ kernel ------------
+__global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((uintptr_t(smem_raw) + 1023) & ~uintptr_t(1023));
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + kSmBar);
+    // bars: [0,6) full, [6,12) empty, 12 a_full, 13 a_empty, 14-15 acc_full, 16-17 acc_empty,
+    // 18 done
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + kSmBar + 8 * 20);
+    volatile int* s_abort = reinterpret_cast<volatile int*>(smem + kSmBar + 8 * 20 + 4);
+    const uint32_t bar0 = smem_u32(bars);
+    auto BAR = [&](int i) { return bar0 + 8u * uint32_t(i); };
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t ntq = (a.nq + kQT - 1) / kQT, ntr = (a.nr + kRT - 1) / kRT;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            bar_init(BAR(s), 1);
+            bar_init(BAR(kStages + s), 1);
+        }
+        bar_init(BAR(12), 1);
+        bar_init(BAR(13), 1);
+        bar_init(BAR(14), 1);
+        bar_init(BAR(15), 1);
+        bar_init(BAR(16), kEpiWarps);
+        bar_init(BAR(17), kEpiWarps);
+        bar_init(BAR(18), 1);
+        *s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(s_tmem)),
+                     "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *s_tmem;
+
+    if (warp == 0 && lane == 0) {
+        // ---------------------------------------------------------------- producer --------
+        const uint32_t sA = smem_u32(smem + kSmA), sB = smem_u32(smem + kSmB);
+        uint32_t stage = 0, sphase = 0, aphase = 0;
+        uint32_t issued = 0, par = 0;  // per stage: issued at least once, parity of last issue
+        bool a_issued = false;
+        uint32_t a_par = 0;
+        for (int64_t qt = blockIdx.x; qt < ntq; qt += gridDim.x) {
+            if (!bar_wait(BAR(13), aphase ^ 1u, s_abort, a.err)) break;
+            const uint32_t rows = uint32_t((a.nq - qt * kQT < kQT ? a.nq - qt * kQT : kQT));
+            bar_expect_tx(BAR(12), rows * kRowB);
+            bulk_load(sA, a.qemb + qt * kQT * kRowB, rows * kRowB, BAR(12));
+            a_issued = true;
+            a_par = aphase;
+            aphase ^= 1u;
+            bool ok = true;
+            for (int64_t rt = 0; rt < ntr; ++rt) {
+                if (!bar_wait(BAR(kStages + stage), sphase ^ 1u, s_abort, a.err)) {
+                    ok = false;
+                    break;
+                }
+                const uint32_t rr = uint32_t((a.nr - rt * kRT < kRT ? a.nr - rt * kRT : kRT));
+                bar_expect_tx(BAR(stage), rr * kRowB);
+                bulk_load(sB + stage * kTileB, a.remb + rt * kRT * kRowB, rr * kRowB, BAR(stage));
+                issued |= 1u << stage;
+                par = sphase ? (par | (1u << stage)) : (par & ~(1u << stage));
+                if (++stage == kStages) {
+                    stage = 0;
+                    sphase ^= 1u;
+                }
+            }
+            if (!ok) break;
+        }
+        // Drain: every copy this CTA issued has landed before the CTA can exit.
+        for (int s = 0; s < kStages; ++s)
+            if (issued & (1u << s)) bar_drain(BAR(s), (par >> s) & 1u);
+        if (a_issued) bar_drain(BAR(12), a_par);
+    } else if (warp == 1 && lane == 0) {
+        // ------------------------------------------------------------- MMA issuer ---------
+        const uint32_t sA = smem_u32(smem + kSmA), sB = smem_u32(smem + kSmB);
+        uint32_t stage = 0, sphase = 0, aphase = 0, acc = 0, accphase = 0;
+        for (int64_t qt = blockIdx.x; qt < ntq; qt += gridDim.x) {
+            if (!bar_wait(BAR(12), aphase, s_abort, a.err)) break;
+            aphase ^= 1u;
+            tc_fence_after();
+            bool ok = true;
+            for (int64_t rt = 0; rt < ntr; ++rt) {
+                if (!bar_wait(BAR(16 + acc), accphase ^ 1u, s_abort, a.err) ||
+                    !bar_wait(BAR(stage), sphase, s_abort, a.err)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t bbase = sB + stage * kTileB;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t d = tmem + acc * 256u + uint32_t(h) * 128u;
+                    const uint32_t abase = sA + uint32_t(h) * kTileB;
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk)
+                        tc_mma(d, sw128_desc(abase + 32u * kk), sw128_desc(bbase + 32u * kk),
+                               kk > 0 ? 1u : 0u);
+                }
+                tc_commit(BAR(kStages + stage));  // stage free once these MMAs finish
+                tc_commit(BAR(14 + acc));         // accumulator ready
+                if (++stage == kStages) {
+                    stage = 0;
+                    sphase ^= 1u;
+                }
+                acc ^= 1u;
+                if (acc == 0) accphase ^= 1u;
+            }
+            tc_commit(BAR(13));  // query tile free once the last MMA reading it finishes
+            if (!ok) break;
+        }
+        tc_commit(BAR(18));
+        bar_drain(BAR(18), 0);
+    } else if (warp >= 2) {
+        // --------------------------------------------------------------- selection --------
+        const int ew = warp - 2, grp = ew >> 2, quarter = warp & 3;
+        const int row = quarter * 32 + lane;
+        uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kSmWarp + ew * 2048);
+        unsigned long long* sortbuf = reinterpret_cast<unsigned long long*>(hist);
+        unsigned long long* lists =
+            a.cand + (int64_t(blockIdx.x) * kQT + grp * 128 + quarter * 32) * kCap;
+        unsigned long long* mine = lists + int64_t(lane) * kCap;
+        const uint32_t tlane = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(grp) * 128u;
+        uint32_t acc = 0, accphase = 0;
+        bool ok = true;
+        for (int64_t qt = blockIdx.x; qt < ntq && ok; qt += gridDim.x) {
+            const int64_t q = qt * kQT + grp * 128 + row;
+            float thr = q < a.nq ? -INFINITY : INFINITY;
+            int count = 0;
+            for (int64_t rt = 0; rt < ntr; ++rt) {
+                if (!bar_wait(BAR(14 + acc), accphase, s_abort, a.err)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const int64_t r0 = rt * kRT;
+                const int nvalid = int((a.nr - r0 < kRT ? a.nr - r0 : kRT));
+#pragma unroll 1
+                for (int c = 0; c < kRT / 32; ++c) {
+                    uint32_t v[32];
+                    __syncwarp();
+                    tmem_ld32(tlane + acc * 256u + uint32_t(c) * 32u, v);
+                    if (c * 32 + 32 > nvalid) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (c * 32 + j >= nvalid) v[j] = 0xFF800000u;  // -inf
+                    }
+                    float m[11];
+#pragma unroll
+                    for (int j = 0; j < 10; ++j)
+                        m[j] = fmax3(__uint_as_float(v[3 * j]), __uint_as_float(v[3 * j + 1]),
+                                     __uint_as_float(v[3 * j + 2]));
+                    m[10] = fmaxf(__uint_as_float(v[30]), __uint_as_float(v[31]));
+                    const float mx = fmaxf(fmax3(fmax3(m[0], m[1], m[2]), fmax3(m[3], m[4], m[5]),
+                                                 fmax3(m[6], m[7], m[8])),
+                                           fmax3(m[9], m[10], -INFINITY));
+                    if (mx > thr) {
+                        const uint32_t rbase = uint32_t(r0 + c * 32);
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            if (__uint_as_float(v[j]) > thr) {
+                                mine[count++] = ((unsigned long long)ord_of(v[j]) << 32) |
+                                                (unsigned long long)(~(rbase + uint32_t(j)));
+                            }
+                        }
+                    }
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) bar_arrive(BAR(16 + acc));
+                acc ^= 1u;
+                if (acc == 0) accphase ^= 1u;
+                // Lists about to overflow are cut back to k (room for a full tile remains).
+                uint32_t need = __ballot_sync(0xffffffffu, count > kCap - kRT);
+                while (need) {
+                    const int L = __ffs(need) - 1;
+                    need &= need - 1;
+                    const int n = __shfl_sync(0xffffffffu, count, L);
+                    const unsigned long long mn =
+                        warp_cut(lists + int64_t(L) * kCap, n, a.k, hist, lane);
+                    if (lane == L) {
+                        count = a.k;
+                        thr = threshold_of(mn);
+                    }
+                }
+            }
+            if (!ok) break;
+            // Final lists: cut to k, sort by key (score descending, then ref ascending), store.
+            __syncwarp();
+            for (int L = 0; L < 32; ++L) {
+                const int64_t qL = qt * kQT + grp * 128 + quarter * 32 + L;
+                if (qL >= a.nq) break;
+                int n = __shfl_sync(0xffffffffu, count, L);
+                unsigned long long* list = lists + int64_t(L) * kCap;
+                if (n > a.k) {
+                    warp_cut(list, n, a.k, hist, lane);
+                    n = a.k;
+                }
+                for (int i = lane; i < kMaxK; i += 32) sortbuf[i] = i < n ? list[i] : 0ull;
+                __syncwarp();
+                warp_sort256_desc(sortbuf, lane);
+                for (int i = lane; i < a.k; i += 32) {
+                    const unsigned long long key = sortbuf[i];
+                    a.out_ids[qL * a.k + i] = i < n ? int32_t(~uint32_t(key)) : -1;
+                    if (a.out_scores)
+                        a.out_scores[qL * a.k + i] = i < n ? score_of(uint32_t(key >> 32)) : -INFINITY;
+                }
+                __syncwarp();
+            }
+        }
+    }
+
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        __syncwarp();
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(kTmemCols));
+    }
+}
+
+}  // namespace
+
+// Top-k refs of every query by dot product of the swizzled bf16 embeddings (device memory, 16-byte
+// aligned).  ids[q][i] / scores[q][i] hold the i-th best ref of query q (score descending, ties by
+// ascending ref id); entries past the number of refs are -1 / -inf.
+void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, int k, int32_t* ids,
+                  float* scores, cudaStream_t stream) {
+    if (nq < 0 || nr < 0) fail(ST_EINVAL, "seqtree_b200: negative embedding count");
+    if (k < 1 || k > kMaxK) fail(ST_EINVAL, "seqtree_b200: k must be in 1..256");
+    if (nr >= (int64_t(1) << 31)) fail(ST_EINVAL, "seqtree_b200: at most 2^31 - 1 refs");
+    if (nq == 0) return;
+    if (!qemb || !ids || (nr > 0 && !remb)) fail(ST_EINVAL, "seqtree_b200: null embedding or output");
+    if ((uintptr_t(qemb) | uintptr_t(remb)) & 15)
+        fail(ST_EINVAL, "seqtree_b200: embeddings must be 16-byte aligned");
+    Context& ctx = context();
+    static std::once_flag once;
+    std::call_once(once, [] {
+        STB_CUDA(cudaFuncSetAttribute(propose_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(kSmemBytes)));
+    });
+    const int64_t ntq = (nq + kQT - 1) / kQT;
+    const int grid = int(std::min<int64_t>(ntq, ctx.num_sms));
+    ProposeArgs a;
+    a.qemb = static_cast<const uint8_t*>(qemb);
+    a.remb = static_cast<const uint8_t*>(remb);
+    a.nq = nq;
+    a.nr = nr;
+    a.k = k;
+    a.cand = ctx.topk_cand.as<unsigned long long>(size_t(grid) * kQT * kCap);
+    a.out_ids = ids;
+    a.out_scores = scores;
+    a.err = reinterpret_cast<unsigned long long*>(ctx.flags_d + 8);
+    propose_topk_kernel<<<grid, kThreads, kSmemBytes, stream>>>(a);
+    STB_CUDA(cudaGetLastError());
+    note_launch("propose_topk_kernel");
+}
+
+}  // namespace stb

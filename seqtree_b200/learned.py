@@ -144,6 +144,51 @@ def pair_scores(qset, rset, qi_ptr: int, ri_ptr: int, n: int, out_ptr: int, stre
     _lib.check(code, err)
 
 
+def swizzle_rows(x):
+    """bf16 [n][64] rows in the proposal kernel's operand layout: the eight 16-byte chunks of row
+    r stored at chunk ^ (r & 7) (what ``Encoder.embed_into(..., layout=1)`` writes)."""
+    import torch
+    n = x.shape[0]
+    if x.dim() != 2 or x.shape[1] != 64:
+        raise ValueError("embeddings must be [n, 64]")
+    chunks = x.to(torch.bfloat16).reshape(n, 8, 8)
+    perm = torch.arange(8, device=x.device)[None, :] ^ (torch.arange(n, device=x.device)[:, None] & 7)
+    out = torch.empty_like(chunks)
+    out.scatter_(1, perm[:, :, None].expand(n, 8, 8), chunks)
+    return out.reshape(n, 64).contiguous()
+
+
+def propose_topk_into(q_ptr: int, nq: int, r_ptr: int, nr: int, k: int, ids_ptr: int,
+                      scores_ptr: int = 0, stream: int = 0) -> None:
+    """``st_propose_topk`` on device pointers (swizzled bf16 embeddings in, [nq][k] out)."""
+    err = _lib.st_error()
+    _lib.check(_lib.lib.st_propose_topk(ctypes.c_void_p(q_ptr), int(nq), ctypes.c_void_p(r_ptr),
+                                        int(nr), int(k), ctypes.c_void_p(ids_ptr),
+                                        ctypes.c_void_p(scores_ptr or None),
+                                        ctypes.c_void_p(stream), ctypes.byref(err)), err)
+
+
+def propose_topk(q_emb, r_emb, k: int = 256):
+    """Top-k refs per query by dot product of swizzled bf16 embeddings (torch CUDA tensors
+    [n][64]); returns (ids int32 [nq][k], scores float32 [nq][k]), best first."""
+    import torch
+    nq, nr = q_emb.shape[0], r_emb.shape[0]
+    ids = torch.empty((nq, k), dtype=torch.int32, device=q_emb.device)
+    scores = torch.empty((nq, k), dtype=torch.float32, device=q_emb.device)
+    stream = torch.cuda.current_stream(q_emb.device).cuda_stream
+    propose_topk_into(q_emb.data_ptr(), nq, r_emb.data_ptr(), nr, k, ids.data_ptr(),
+                      scores.data_ptr(), stream)
+    stream_status(stream)
+    return ids, scores
+
+
+def stream_status(stream: int = 0) -> None:
+    """Synchronise ``stream`` and raise if a bounded device-side wait gave up since the last
+    check."""
+    err = _lib.st_error()
+    _lib.check(_lib.lib.st_stream_status(ctypes.c_void_p(stream), ctypes.byref(err)), err)
+
+
 # ----------------------------------------------------------------------------- data ---------
 def cdr3_like(seed: int, n: int) -> list[str]:
     """'CASS' + uniform middle + 'F', length 8-25 with mode 14 (a Gaussian around 14 with sigma
