@@ -282,6 +282,8 @@ int32_t st_builtin_similarity(const char *name, int32_t *out, int32_t capacity, 
 /* Launch statistics of the last *_sets / host call on this thread: how many kernels of this
  * library it launched and the name of the main kernel variant it chose. */
 int32_t st_last_launch_count(void);
+/* Kernels of this library launched by the whole process so far (all threads, all calls). */
+int64_t st_total_launch_count(void);
 const char *st_last_kernel_name(void);
 
 /* Pinned host buffers from a per-device cache.  A result written into one of these travels

@@ -111,6 +111,7 @@ SIGNATURES = [
     ("st_builtin_similarity", ctypes.c_int32,
      [ctypes.c_char_p, _i32p, ctypes.c_int32, _i32p, _ep]),
     ("st_last_launch_count", ctypes.c_int32, []),
+    ("st_total_launch_count", ctypes.c_int64, []),
     ("st_last_kernel_name", ctypes.c_char_p, []),
     ("st_host_alloc", ctypes.c_void_p, [ctypes.c_uint64]),
     ("st_host_free", None, [ctypes.c_void_p]),
@@ -176,6 +177,16 @@ class Packed:
         self.offsets = off
         self.struct = st_strings(self.data.ctypes.data, self.offsets.ctypes.data, len(seqs))
 
+    @classmethod
+    def from_arrays(cls, data: np.ndarray, offsets: np.ndarray) -> "Packed":
+        """Sequences already concatenated: ``data`` (uint8) and ``offsets`` (int64, count + 1)."""
+        self = cls.__new__(cls)
+        self.data = np.ascontiguousarray(data, np.uint8) if len(data) else np.zeros(1, np.uint8)
+        self.offsets = np.ascontiguousarray(offsets, np.int64)
+        self.struct = st_strings(self.data.ctypes.data, self.offsets.ctypes.data,
+                                 len(self.offsets) - 1)
+        return self
+
     @property
     def count(self) -> int:
         return int(self.struct.count)
@@ -187,14 +198,15 @@ class Packed:
 class _PinnedOwner:
     """Returns a pinned block to the library's cache when the last view is gone."""
 
-    __slots__ = ("ptr",)
+    __slots__ = ("ptr", "_free")
 
     def __init__(self, ptr: int):
         self.ptr = ptr
+        self._free = lib.st_host_free
 
     def __del__(self):
         if self.ptr:
-            lib.st_host_free(ctypes.c_void_p(self.ptr))
+            self._free(ctypes.c_void_p(self.ptr))
             self.ptr = 0
 
 
@@ -234,6 +246,10 @@ def i32_ptr(a: np.ndarray | None):
 
 def last_launch_count() -> int:
     return int(lib.st_last_launch_count())
+
+
+def total_launch_count() -> int:
+    return int(lib.st_total_launch_count())
 
 
 def last_kernel_name() -> str:

@@ -39,6 +39,7 @@ void encoder_embed(Encoder& m, const st_seqset_s& set, void* out, int layout, cu
 void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, int k, int32_t* ids,
                   float* scores, cudaStream_t stream);
 int last_launches();
+int64_t total_launches();
 const char* last_kernel();
 void* host_alloc(uint64_t bytes);
 void host_free(void* p);
@@ -146,6 +147,8 @@ int32_t st_builtin_similarity(const char* name, int32_t* out, int32_t capacity, 
 }
 
 int32_t st_last_launch_count(void) { return last_launches(); }
+
+int64_t st_total_launch_count(void) { return total_launches(); }
 const char* st_last_kernel_name(void) { return last_kernel(); }
 
 void* st_host_alloc(uint64_t bytes) { return host_alloc(bytes); }

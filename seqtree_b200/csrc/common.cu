@@ -16,10 +16,12 @@ namespace stb {
 namespace {
 thread_local int t_launches = 0;
 thread_local const char* t_kernel = "";
+std::atomic<int64_t> g_launches{0};
 }  // namespace
 
 void note_launch(const char* kernel_name, int count) {
     t_launches += count;
+    g_launches.fetch_add(count, std::memory_order_relaxed);
     if (kernel_name && *kernel_name) t_kernel = kernel_name;
 }
 void reset_launches() {
@@ -27,6 +29,7 @@ void reset_launches() {
     t_kernel = "";
 }
 int last_launches() { return t_launches; }
+int64_t total_launches() { return g_launches.load(std::memory_order_relaxed); }
 const char* last_kernel() { return t_kernel; }
 
 // ----------------------------------------------------------------------------- tracing ------

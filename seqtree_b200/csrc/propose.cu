@@ -37,6 +37,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "tc.cuh"
 
 namespace stb {
 
@@ -62,10 +63,8 @@ constexpr int kSmTotal = kSmBar + 256;
 constexpr size_t kSmemBytes = size_t(kSmTotal) + 1024;    // + alignment slack
 
 // bf16 x bf16 -> fp32, both operands K-major, M = 128, N = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(kRT >> 3) << 17) |
-                            (uint32_t(128 >> 4) << 24);
+constexpr uint32_t kIdesc = idesc_bf16(128, kRT);
 
-constexpr uint64_t kWaitNs = 4000000000ull;               // bound of every wait
 
 struct ProposeArgs {
     const uint8_t* qemb;
@@ -78,101 +77,6 @@ struct ProposeArgs {
     unsigned long long* err;
 };
 
-// ------------------------------------------------------------------ PTX wrappers ------------
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return uint32_t(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ uint64_t now_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-__device__ __forceinline__ bool bar_test(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for the phase of `parity` to complete.  Gives up (returns false) when the CTA's
-// abort word is set or after kWaitNs, setting the abort word and the host-visible error word.
-__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, volatile int* abort,
-                                         unsigned long long* err) {
-    if (bar_test(bar, parity)) return true;
-    const uint64_t t0 = now_ns();
-    for (uint32_t it = 1;; ++it) {
-        if (bar_test(bar, parity)) return true;
-        if ((it & 255) == 0) {
-            if (*abort) return false;
-            if (now_ns() - t0 > kWaitNs) {
-                *abort = 1;
-                atomicExch(err, 1ull);
-                return false;
-            }
-        }
-    }
-}
-// Bounded wait that ignores the abort word (draining in-flight work before exit).
-__device__ __forceinline__ void bar_drain(uint32_t bar, uint32_t parity) {
-    const uint64_t t0 = now_ns();
-    while (!bar_test(bar, parity) && now_ns() - t0 < kWaitNs) {
-    }
-}
-__device__ __forceinline__ void bar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
-}
-__device__ __forceinline__ void bar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void bar_arrive(uint32_t bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes,
-                                          uint32_t bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
-            "r"(dst),
-        "l"(src), "r"(bytes), "r"(bar)
-        : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     bar)
-                 : "memory");
-}
-// K-major operand in the 128-byte swizzle: rows of 128 B, 8-row groups 1024 B apart.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
-    return uint64_t((addr >> 4) & 0x3FFFu) | (uint64_t(1) << 16) | (uint64_t(1024 >> 4) << 32) |
-           (uint64_t(1) << 46) | (uint64_t(2) << 61);
-}
-__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
-        : "memory");
-}
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-        "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-          "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
-          "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
-          "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
 __device__ __forceinline__ float fmax3(float a, float b, float c) {
     float m;
     asm("max.f32 %0, %1, %2, %3;" : "=f"(m) : "f"(a), "f"(b), "f"(c));
@@ -413,7 +317,7 @@ __global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk)
                         tc_mma(d, sw128_desc(abase + 32u * kk), sw128_desc(bbase + 32u * kk),
-                               kk > 0 ? 1u : 0u);
+                               kIdesc, kk > 0 ? 1u : 0u);
                 }
                 tc_commit(BAR(kStages + stage));  // stage free once these MMAs finish
                 tc_commit(BAR(14 + acc));         // accumulator ready

@@ -20,7 +20,8 @@ class SeqSet:
     """Sequences resident on the current CUDA device (encoded, or raw bytes when alphabet=None)."""
 
     def __init__(self, seqs, alphabet: str | None = "aa"):
-        packed = _lib.Packed(seqs)
+        self._free = _lib.lib.st_seqset_destroy  # kept: module globals are gone at exit
+        packed = seqs if isinstance(seqs, _lib.Packed) else _lib.Packed(seqs)
         self.alphabet = None if alphabet is None else parse_alphabet(alphabet)
         self._h = ctypes.c_void_p()
         err = _lib.st_error()
@@ -39,7 +40,7 @@ class SeqSet:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _lib.lib.st_seqset_destroy(h)
+            self._free(h)
             self._h = ctypes.c_void_p()
 
 
@@ -61,6 +62,7 @@ class Hits:
     device pointers, refilled in place by :func:`gapblock_sparse_into`."""
 
     def __init__(self):
+        self._free = _lib.lib.st_hits_destroy
         self._h = ctypes.c_void_p()
         err = _lib.st_error()
         _lib.check(_lib.lib.st_hits_create(ctypes.byref(self._h), ctypes.byref(err)), err)
@@ -96,7 +98,7 @@ class Hits:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _lib.lib.st_hits_destroy(h)
+            self._free(h)
             self._h = ctypes.c_void_p()
 
 

@@ -75,6 +75,7 @@ class Encoder:
         p = init_params(seed) if params is None else np.ascontiguousarray(params, np.float32)
         if p.size != param_count():
             raise ValueError(f"expected {param_count()} parameters, got {p.size}")
+        self._free = _lib.lib.st_encoder_destroy
         self._h = ctypes.c_void_p()
         err = _lib.st_error()
         _lib.check(_lib.lib.st_encoder_create(p.ctypes.data, ctypes.byref(self._h),
@@ -125,7 +126,7 @@ class Encoder:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _lib.lib.st_encoder_destroy(h)
+            self._free(h)
             self._h = ctypes.c_void_p()
 
 
@@ -190,52 +191,480 @@ def stream_status(stream: int = 0) -> None:
 
 
 # ----------------------------------------------------------------------------- data ---------
-def cdr3_like(seed: int, n: int) -> list[str]:
-    """'CASS' + uniform middle + 'F', length 8-25 with mode 14 (a Gaussian around 14 with sigma
-    2.5 below and 3.5 above)."""
-    rng = np.random.default_rng(seed)
+_LETTER = np.frombuffer(AA24.encode(), np.uint8)             # code -> ASCII
+_AA20_CODES = _CODE[np.frombuffer(AA20.encode(), np.uint8)]  # the 20 standard residues as codes
+_C, _A, _S, _F = (int(_CODE[ord(x)]) for x in "CASF")
+
+
+def cdr3_lengths(rng, n: int) -> np.ndarray:
+    """Junction lengths 8-25 with mode 14: P(L) is a Gaussian around 14 with sigma 2.5 below and
+    3.5 above (right-skewed, like TRB junctions)."""
     L = np.arange(8, 26)
     sig = np.where(L < 14, 2.5, 3.5)
     p = np.exp(-0.5 * ((L - 14) / sig) ** 2)
-    lens = rng.choice(L, size=n, p=p / p.sum())
-    mids = rng.integers(0, 20, size=int((lens - 5).sum()), dtype=np.uint8)
-    letters = np.frombuffer(AA20.encode(), np.uint8)[mids].tobytes().decode()
-    out, o = [], 0
-    for length in lens:
-        k = int(length) - 5
-        out.append("CASS" + letters[o:o + k] + "F")
-        o += k
-    return out
+    return rng.choice(L, size=n, p=p / p.sum()).astype(np.int32)
+
+
+def cdr3_codes(seed: int, n: int) -> tuple[np.ndarray, np.ndarray]:
+    """n CDR3-like junctions 'CASS' + uniform middle + 'F' (lengths from :func:`cdr3_lengths`)
+    as amino-acid codes [n, 32] (zero past each length) and lengths [n]."""
+    rng = np.random.default_rng(seed)
+    lens = cdr3_lengths(rng, n)
+    codes = _AA20_CODES[rng.integers(0, 20, size=(n, PAD), dtype=np.uint8)]
+    codes[:, :4] = (_C, _A, _S, _S)
+    codes[np.arange(n), lens - 1] = _F
+    codes[np.arange(PAD)[None, :] >= lens[:, None]] = 0
+    return codes, lens
+
+
+def codes_to_packed(codes: np.ndarray, lens: np.ndarray) -> _lib.Packed:
+    """Codes [n, 32] + lengths as one concatenated letter buffer (for ``device.SeqSet``)."""
+    lens = np.asarray(lens, np.int64)
+    data = _LETTER[codes[np.arange(PAD)[None, :] < lens[:, None]]]
+    off = np.zeros(lens.size + 1, np.int64)
+    np.cumsum(lens, out=off[1:])
+    return _lib.Packed.from_arrays(data, off)
+
+
+def codes_to_strings(codes: np.ndarray, lens: np.ndarray) -> list[str]:
+    p = codes_to_packed(codes, lens)
+    text = p.data.tobytes().decode() if p.offsets[-1] else ""
+    return [text[a:b] for a, b in zip(p.offsets[:-1].tolist(), p.offsets[1:].tolist())]
+
+
+def cdr3_like(seed: int, n: int) -> list[str]:
+    """:func:`cdr3_codes` as strings."""
+    return codes_to_strings(*cdr3_codes(seed, n))
+
+
+def mutate_codes(codes: np.ndarray, lens: np.ndarray, rng) -> tuple[np.ndarray, np.ndarray]:
+    """Near neighbours: 1-3 random substitutions, then one random indel block of 1-3 residues at
+    a random position (a deletion or an insertion with equal odds, whichever keeps 1..32
+    residues; a deletion near the end removes what is there)."""
+    n = lens.size
+    out = codes.copy()
+    rows = np.arange(n)
+    nsub = rng.integers(1, 4, size=n)
+    for t in range(3):
+        pos = np.minimum((rng.random(n) * lens).astype(np.int64), lens - 1)
+        aa = _AA20_CODES[rng.integers(0, 20, size=n)]
+        m = t < nsub
+        out[rows[m], pos[m]] = aa[m]
+    blk = rng.integers(1, 4, size=n)
+    pos = np.minimum((rng.random(n) * (lens + 1)).astype(np.int64), lens)
+    want_del = rng.random(n) < 0.5
+    dele = want_del & (lens - blk >= 1)
+    ins = ~dele & (lens + blk <= PAD)
+    gone = np.minimum(blk, lens - pos)
+    j = np.arange(PAD)[None, :]
+    p, b, g = pos[:, None], blk[:, None], gone[:, None]
+    src = np.where(dele[:, None], np.where(j < p, j, j + g),
+                   np.where(ins[:, None], np.where(j < p, j, j - b), j))
+    res = np.take_along_axis(out, np.clip(src, 0, PAD - 1), axis=1)
+    new = ins[:, None] & (j >= p) & (j < p + b)
+    res[new] = _AA20_CODES[rng.integers(0, 20, size=int(new.sum()))]
+    nl = np.where(dele, lens - gone, np.where(ins, lens + blk, lens)).astype(np.int32)
+    res[j >= nl[:, None]] = 0
+    return res, nl
 
 
 def mutate(seqs, rng) -> list[str]:
-    """Near neighbours: 1-3 random substitutions and one random indel block (a deletion or an
-    insertion of 1-3 residues at a random position), kept within 1..32 residues."""
-    out = []
-    nsub = rng.integers(1, 4, size=len(seqs))
-    for s, k in zip(seqs, nsub):
-        b = bytearray(s.encode())
-        for _ in range(int(k)):
-            b[int(rng.integers(0, len(b)))] = ord(AA20[int(rng.integers(0, 20))])
-        blk = int(rng.integers(1, 4))
-        pos = int(rng.integers(0, len(b) + 1))
-        if rng.random() < 0.5 and len(b) - blk >= 1:
-            del b[pos:pos + blk]
-        elif len(b) + blk <= PAD:
-            b[pos:pos] = bytes(ord(AA20[int(x)]) for x in rng.integers(0, 20, size=blk))
-        out.append(b.decode())
-    return out
+    """:func:`mutate_codes` on strings."""
+    codes, lens = pad_codes(list(seqs))
+    return codes_to_strings(*mutate_codes(codes, lens, rng))
 
 
-def training_pairs(seed: int, n_pairs: int, pool: list[str] | None = None):
-    """n_pairs (a, b) string pairs: half near neighbours made by :func:`mutate`, half random
-    pairs drawn from the pool (default: fresh CDR3-like strings)."""
+def training_pairs_codes(seed: int, n_pairs: int) -> tuple[np.ndarray, np.ndarray]:
+    """n_pairs seeded pairs as interleaved codes [2n, 32] / lengths [2n] (rows 2i and 2i+1 are
+    one pair): the first half near neighbours made by :func:`mutate_codes`, the second half two
+    independent CDR3-like junctions."""
     rng = np.random.default_rng(seed)
-    if pool is None:
-        pool = cdr3_like(seed + 7, max(2 * n_pairs, 1000))
+    a, la = cdr3_codes(seed * 2 + 1, n_pairs)
     near = n_pairs // 2
-    idx = rng.integers(0, len(pool), size=(n_pairs, 2))
-    a = [pool[i] for i in idx[:, 0]]
-    b = [pool[i] for i in idx[:, 1]]
-    b[:near] = mutate(a[:near], rng)
-    return a, b
+    b, lb = cdr3_codes(seed * 2 + 2, n_pairs)
+    b[:near], lb[:near] = mutate_codes(a[:near], la[:near], rng)
+    codes = np.empty((2 * n_pairs, PAD), np.uint8)
+    lens = np.empty(2 * n_pairs, np.int32)
+    codes[0::2], codes[1::2] = a, b
+    lens[0::2], lens[1::2] = la, lb
+    return codes, lens
+
+
+def training_pairs(seed: int, n_pairs: int):
+    """:func:`training_pairs_codes` as two lists of strings (a[i], b[i])."""
+    codes, lens = training_pairs_codes(seed, n_pairs)
+    s = codes_to_strings(codes, lens)
+    return s[0::2], s[1::2]
+
+
+# ------------------------------------------------------------------------- training ---------
+def label_pairs(codes: np.ndarray, lens: np.ndarray, *, matrix, gap_open: int,
+                gap_extend: int = 1) -> np.ndarray:
+    """Exact gap-block scores of the interleaved pairs (rows 2i, 2i+1), by the GPU pair scorer."""
+    import torch
+
+    from .device import SeqSet
+    n = lens.size // 2
+    ss = SeqSet(codes_to_packed(codes, lens), "aa")
+    qi = torch.arange(0, 2 * n, 2, dtype=torch.int32, device="cuda")
+    ri = qi + 1
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    pair_scores(ss, ss, qi.data_ptr(), ri.data_ptr(), n, out.data_ptr(), stream, matrix=matrix,
+                gap_open=gap_open, gap_extend=gap_extend)
+    return out.cpu().numpy()
+
+
+def mine_partners(codes: np.ndarray, lens: np.ndarray, rows: np.ndarray, *, seed: int, tries: int,
+                  matrix, gap_open: int, gap_extend: int = 1) -> None:
+    """Replaces the partner (odd row) of every pair in ``rows`` by the best-scoring of ``tries``
+    random CDR3-like junctions (exact gap-block score, lowest wins), in place.  The pairs become
+    'hard' random pairs whose scores sit near the search threshold instead of far above it."""
+    import torch
+
+    from .device import SeqSet
+    n = rows.size
+    if n == 0 or tries < 1:
+        return
+    pool_n = max(4096, min(1 << 20, n * tries // 4))
+    pc, pl = cdr3_codes(seed, pool_n)
+    a_codes, a_lens = codes[2 * rows], lens[2 * rows]
+    aset = SeqSet(codes_to_packed(a_codes, a_lens), "aa")
+    pset = SeqSet(codes_to_packed(pc, pl), "aa")
+    rng = np.random.default_rng(seed + 1)
+    cand = rng.integers(0, pool_n, size=(n, tries)).astype(np.int32)
+    qi = torch.arange(n, dtype=torch.int32, device="cuda").repeat_interleave(tries)
+    ri = torch.from_numpy(cand.ravel()).cuda()
+    sc = torch.empty(n * tries, dtype=torch.int32, device="cuda")
+    pair_scores(aset, pset, qi.data_ptr(), ri.data_ptr(), n * tries, sc.data_ptr(),
+                torch.cuda.current_stream().cuda_stream, matrix=matrix, gap_open=gap_open,
+                gap_extend=gap_extend)
+    best = sc.view(n, tries).argmin(dim=1).cpu().numpy()
+    pick = cand[np.arange(n), best]
+    codes[2 * rows + 1] = pc[pick]
+    lens[2 * rows + 1] = pl[pick]
+
+
+def train(enc: Encoder, n_pairs: int, *, seed: int, matrix, gap_open: int, gap_extend: int = 1,
+          batch_pairs: int = 2048, lr: float = 2e-3, lr_final: float = 1e-4,
+          chunk_pairs: int = 1 << 20, mine: int = 0, log=None) -> list[float]:
+    """Trains ``enc`` for one pass over ``n_pairs`` fresh seeded pairs labelled by the exact
+    kernel (Adam, cosine learning-rate decay from ``lr`` to ``lr_final``).  Half the pairs are
+    near neighbours (:func:`mutate_codes`); the other half are random pairs, each the best of
+    ``mine`` random partners when ``mine`` > 0 (:func:`mine_partners`).  Returns the mean loss
+    of every chunk."""
+    steps = max(1, -(-n_pairs // batch_pairs))
+    t, losses = 0, []
+    for c0 in range(0, n_pairs, chunk_pairs):
+        m = min(chunk_pairs, n_pairs - c0)
+        cseed = seed * 7919 + c0 // chunk_pairs
+        codes, lens = training_pairs_codes(cseed, m)
+        if mine:
+            mine_partners(codes, lens, np.arange(m // 2, m), seed=cseed * 31 + 5, tries=mine,
+                          matrix=matrix, gap_open=gap_open, gap_extend=gap_extend)
+        perm = np.random.default_rng(cseed + 3).permutation(m)  # mix the two halves
+        codes = codes.reshape(m, 2, PAD)[perm].reshape(2 * m, PAD)
+        lens = lens.reshape(m, 2)[perm].reshape(2 * m)
+        scores = label_pairs(codes, lens, matrix=matrix, gap_open=gap_open, gap_extend=gap_extend)
+        acc = []
+        for b0 in range(0, m, batch_pairs):
+            b1 = min(m, b0 + batch_pairs)
+            if b1 - b0 < 2:
+                continue
+            cur = lr_final + (lr - lr_final) * 0.5 * (1.0 + np.cos(np.pi * t / steps))
+            acc.append(enc.train_step(codes[2 * b0:2 * b1], lens[2 * b0:2 * b1], scores[b0:b1],
+                                      lr=float(cur)))
+            t += 1
+        losses.append(float(np.mean(acc)) if acc else float("nan"))
+        if log:
+            log(f"pairs {c0 + m}/{n_pairs}: loss {losses[-1]:.4f}")
+    return losses
+
+
+# -------------------------------------------------------------------------- search ----------
+class _DeviceArray:
+    """A borrowed device buffer exposed through ``__cuda_array_interface__`` (for torch views)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr,
+                                         "data": (ptr or 0, False), "version": 3, "strides": None}
+
+
+def _hits_tensors(hits):
+    """(indptr int64, ref_ids int32, scores int32) torch copies of a device ``Hits``."""
+    import torch
+    info = hits.info()
+    rows, nnz = info["rows"], info["nnz"]
+
+    def view(ptr, n, ts, dt):
+        if n == 0:
+            return torch.zeros(0, dtype=dt, device="cuda")
+        return torch.as_tensor(_DeviceArray(ptr, n, ts), device="cuda").clone()
+
+    return (view(info["indptr"], rows + 1, "<i8", torch.int64),
+            view(info["ref_ids"], nnz, "<i4", torch.int32),
+            view(info["scores"], nnz, "<i4", torch.int32))
+
+
+def _subset(codes, lens, rows):
+    from .device import SeqSet
+    return SeqSet(codes_to_packed(codes[rows], lens[rows]), "aa") if rows.size else None
+
+
+class QueryBatch:
+    """Queries resident on the device for :meth:`LearnedIndex.search`, split by the index's
+    query-length fallback: ``learn`` rows go through the proposals, ``fb`` rows through the
+    exhaustive kernel."""
+
+    def __init__(self, index: "LearnedIndex", codes: np.ndarray, lens: np.ndarray):
+        import torch
+        self.lens = np.asarray(lens, np.int32)
+        self.count = int(self.lens.size)
+        fb = index.query_fallback[np.clip(self.lens, 0, PAD)]
+        self.fb_rows = np.flatnonzero(fb).astype(np.int64)
+        self.learn_rows = np.flatnonzero(~fb).astype(np.int64)
+        self.fb_set = _subset(codes, self.lens, self.fb_rows)
+        self.learn_set = _subset(codes, self.lens, self.learn_rows)
+        self.fb_rows_t = torch.from_numpy(self.fb_rows).cuda()
+        self.learn_rows_t = torch.from_numpy(self.learn_rows).cuda()
+
+
+class LearnedIndex:
+    """Thresholded gap-block search by learned proposal + exact rescore.
+
+    The refs outside the ref-length fallback are embedded once (:meth:`embed_refs`).
+    :meth:`search` embeds the queries outside the query-length fallback, proposes the top ``k``
+    of those refs for each by embedding similarity (``st_propose_topk``), rescores every
+    proposal with the exact gap-block kernel and keeps those with score <= ``max_penalty``.  The
+    exhaustive sparse kernel answers the two fallback parts exactly: fallback-length queries
+    against every ref, and the other queries against the fallback-length refs.  Every reported
+    score is exact; rows are CSR with refs ascending, the format of ``score_sparse``.
+    :meth:`calibrate` chooses the fallback lengths on a held-out batch.
+    """
+
+    def __init__(self, encoder: Encoder, ref_codes: np.ndarray, ref_lens: np.ndarray, *, matrix,
+                 gap_open: int, gap_extend: int = 1, max_penalty: int = 24, k: int = 256):
+        from .device import SeqSet
+        if max_penalty < 0:
+            raise ValueError("max_penalty must be >= 0")
+        self.encoder, self.matrix = encoder, matrix
+        self.gap_open, self.gap_extend, self.max_penalty, self.k = gap_open, gap_extend, max_penalty, k
+        self.ref_codes = np.ascontiguousarray(ref_codes, np.uint8)
+        self.ref_lens = np.asarray(ref_lens, np.int32)
+        self.nr = int(self.ref_lens.size)
+        self.refs = SeqSet(codes_to_packed(self.ref_codes, self.ref_lens), "aa")
+        self.query_fallback = np.zeros(PAD + 1, bool)
+        self.ref_fallback = np.zeros(PAD + 1, bool)
+        self._hits = None
+        self._build()
+
+    def set_fallback(self, query_lengths=(), ref_lengths=()) -> None:
+        self.query_fallback[:] = False
+        self.ref_fallback[:] = False
+        self.query_fallback[list(query_lengths)] = True
+        self.ref_fallback[list(ref_lengths)] = True
+        self._build()
+
+    def _build(self) -> None:
+        import torch
+        fb = self.ref_fallback[np.clip(self.ref_lens, 0, PAD)]
+        learn = np.flatnonzero(~fb).astype(np.int64)
+        fbr = np.flatnonzero(fb).astype(np.int64)
+        self.learn_ids = torch.from_numpy(learn.astype(np.int32)).cuda()
+        self.fb_ref_ids = torch.from_numpy(fbr.astype(np.int32)).cuda()
+        self.learn_refs = _subset(self.ref_codes, self.ref_lens, learn)
+        self.fb_refs = _subset(self.ref_codes, self.ref_lens, fbr)
+        self.n_learn = int(learn.size)
+        self.r_emb = torch.empty((self.n_learn, 64), dtype=torch.bfloat16, device="cuda")
+        self.embed_refs()
+
+    def embed_refs(self) -> None:
+        import torch
+        if self.learn_refs is not None:
+            self.encoder.embed_into(self.learn_refs, self.r_emb.data_ptr(), 1,
+                                    torch.cuda.current_stream().cuda_stream)
+
+    def queries(self, codes: np.ndarray, lens: np.ndarray) -> QueryBatch:
+        return QueryBatch(self, codes, lens)
+
+    def _sparse(self, qset, rset):
+        """Exhaustive sparse hits of qset x rset as (local row int64, local ref int32, score)."""
+        import torch
+
+        from .device import Hits, gapblock_sparse_into
+        if self._hits is None:
+            self._hits = Hits()
+        gapblock_sparse_into(qset, rset, self._hits, torch.cuda.current_stream().cuda_stream,
+                             max_penalty=self.max_penalty, matrix=self.matrix,
+                             gap_open=self.gap_open, gap_extend=self.gap_extend)
+        ip, rr, sc = _hits_tensors(self._hits)
+        return torch_rows(ip), rr, sc
+
+    def search(self, qb: QueryBatch, phases: dict | None = None):
+        """CSR (indptr int64 [nq+1], ref_ids int32, scores int32) torch tensors on the device.
+        With ``phases`` (a dict), CUDA events bracketing embed / propose / rescore /
+        exhaustive / merge are appended under those names."""
+        import torch
+        parts = []
+        stream = torch.cuda.current_stream().cuda_stream
+
+        def mark(name):
+            if phases is not None:
+                e = torch.cuda.Event(enable_timing=True)
+                e.record()
+                phases.setdefault(name, []).append(e)
+
+        mark("start")
+        if qb.learn_set is not None and self.n_learn:
+            n = len(qb.learn_set)
+            q_emb = torch.empty((n, 64), dtype=torch.bfloat16, device="cuda")
+            self.encoder.embed_into(qb.learn_set, q_emb.data_ptr(), 1, stream)
+            mark("embed")
+            ids = torch.empty((n, self.k), dtype=torch.int32, device="cuda")
+            propose_topk_into(q_emb.data_ptr(), n, self.r_emb.data_ptr(), self.n_learn, self.k,
+                              ids.data_ptr(), 0, stream)
+            mark("propose")
+            qi = torch.arange(n, dtype=torch.int32, device="cuda").repeat_interleave(self.k)
+            ri = ids.view(-1)
+            keep = ri >= 0
+            qi, ri = qi[keep], ri[keep]
+            sc = torch.empty(qi.numel(), dtype=torch.int32, device="cuda")
+            if qi.numel():
+                pair_scores(qb.learn_set, self.learn_refs, qi.data_ptr(), ri.data_ptr(), qi.numel(),
+                            sc.data_ptr(), stream, matrix=self.matrix, gap_open=self.gap_open,
+                            gap_extend=self.gap_extend)
+            hit = sc <= self.max_penalty
+            parts.append((qb.learn_rows_t[qi[hit].long()], self.learn_ids[ri[hit].long()], sc[hit]))
+            mark("rescore")
+        if qb.learn_set is not None and self.fb_refs is not None:
+            rows, rr, sc = self._sparse(qb.learn_set, self.fb_refs)
+            parts.append((qb.learn_rows_t[rows], self.fb_ref_ids[rr.long()], sc))
+        if qb.fb_set is not None and self.nr:
+            rows, rr, sc = self._sparse(qb.fb_set, self.refs)
+            parts.append((qb.fb_rows_t[rows], rr, sc))
+        mark("exhaustive")
+        if parts:
+            qi = torch.cat([p[0] for p in parts])
+            ri = torch.cat([p[1] for p in parts])
+            sc = torch.cat([p[2] for p in parts])
+        else:
+            qi = torch.zeros(0, dtype=torch.int64, device="cuda")
+            ri = torch.zeros(0, dtype=torch.int32, device="cuda")
+            sc = torch.zeros(0, dtype=torch.int32, device="cuda")
+        key, order = torch.sort(qi * max(self.nr, 1) + ri.long())
+        counts = torch.bincount(qi, minlength=qb.count)
+        indptr = torch.zeros(qb.count + 1, dtype=torch.int64, device="cuda")
+        torch.cumsum(counts, 0, out=indptr[1:])
+        out = indptr, ri[order], sc[order]
+        mark("merge")
+        return out
+
+    def search_strings(self, queries) -> "SparseScores":
+        """The public call: thresholded hits of host query strings against the index's refs, as
+        host CSR (``gapblock.SparseScores``, the format of ``score_sparse``)."""
+        from .gapblock import SparseScores
+        codes, lens = pad_codes(list(queries))
+        ip, ri, sc = self.search(self.queries(codes, lens))
+        return SparseScores(ip.cpu().numpy(), ri.cpu().numpy(), sc.cpu().numpy(),
+                            (len(lens), self.nr), self.max_penalty)
+
+    def exhaustive(self, qb: QueryBatch, codes: np.ndarray):
+        """The exhaustive sparse kernel's CSR for the same queries (the exact answer)."""
+        from .device import SeqSet
+        qset = SeqSet(codes_to_packed(codes, qb.lens), "aa")
+        from .device import Hits, gapblock_sparse_into
+        import torch
+        hits = Hits()
+        gapblock_sparse_into(qset, self.refs, hits, torch.cuda.current_stream().cuda_stream,
+                             max_penalty=self.max_penalty, matrix=self.matrix,
+                             gap_open=self.gap_open, gap_extend=self.gap_extend)
+        return _hits_tensors(hits)
+
+    def recall(self, codes: np.ndarray, lens: np.ndarray) -> dict:
+        """Found / exact hit counts against the exhaustive kernel, overall and per (query length,
+        ref length) cell; also checks that every reported hit is an exact hit, score included."""
+        import torch
+        qb = self.queries(codes, lens)
+        ip, ri, sc = self.search(qb)
+        eip, eri, esc = self.exhaustive(qb, codes)
+        nr = max(self.nr, 1)
+        rows, erows = torch_rows(ip), torch_rows(eip)
+        got, want = rows * nr + ri.long(), erows * nr + eri.long()
+        if got.numel() == 0:
+            ok = True
+        elif want.numel() == 0:
+            ok = False
+        else:
+            pos = torch.searchsorted(want, got).clamp(max=want.numel() - 1)
+            ok = bool(torch.equal(want[pos], got)) and bool(torch.equal(esc[pos], sc))
+        ql = torch.from_numpy(qb.lens.astype(np.int64)).cuda()
+        rl = torch.from_numpy(self.ref_lens.astype(np.int64)).cuda()
+        cells = lambda r, c: torch.bincount(ql[r] * (PAD + 1) + rl[c.long()],  # noqa: E731
+                                            minlength=(PAD + 1) ** 2).view(PAD + 1, PAD + 1)
+        found = cells(rows, ri).cpu().numpy()
+        exact = cells(erows, eri).cpu().numpy()
+        tf, te = int(found.sum()), int(exact.sum())
+        return {"found": tf, "exact": te, "recall": tf / te if te else 1.0, "found_cells": found,
+                "exact_cells": exact, "subset_of_exact": ok}
+
+    def calibrate(self, codes: np.ndarray, lens: np.ndarray, bound: float = 0.99,
+                  margin: float = 0.003) -> dict:
+        """Chooses the fallback lengths on a held-out calibration batch.
+
+        Without fallback, the proposals' found / exact hit counts are measured per (query
+        length, ref length) cell.  A cell is covered (answered exactly) once its query length or
+        its ref length falls back.  Lengths are added greedily -- each time the query or ref
+        length with the most recovered hits per exhaustively scored pair (pairs estimated from
+        the calibration batch's query lengths and the refs' lengths) -- until the estimated
+        recall reaches ``bound + margin``.  The recall with the chosen fallback is then measured
+        on the same batch."""
+        self.set_fallback()
+        r0 = self.recall(codes, lens)
+        f, e = r0["found_cells"].astype(np.float64), r0["exact_cells"].astype(np.float64)
+        wq = np.bincount(np.asarray(lens, np.int64), minlength=PAD + 1)[:PAD + 1] / max(len(lens), 1)
+        wr = np.bincount(self.ref_lens.astype(np.int64), minlength=PAD + 1)[:PAD + 1] / max(self.nr, 1)
+        covered = np.zeros((PAD + 1, PAD + 1), bool)
+        q_fb, ref_fb = [], []
+        total = e.sum()
+        while total:
+            rec = (e[covered].sum() + f[~covered].sum()) / total
+            if rec >= bound + margin:
+                break
+            best, pick = 0.0, None
+            for a in range(PAD + 1):
+                if a in q_fb or not wq[a]:
+                    continue
+                open_ = ~covered[a]
+                gain, cost = (e[a] - f[a])[open_].sum(), wq[a] * wr[open_].sum()
+                if gain > 0 and cost > 0 and gain / cost > best:
+                    best, pick = gain / cost, ("q", a)
+            for b in range(PAD + 1):
+                if b in ref_fb or not wr[b]:
+                    continue
+                open_ = ~covered[:, b]
+                gain, cost = (e[:, b] - f[:, b])[open_].sum(), wr[b] * wq[open_].sum()
+                if gain > 0 and cost > 0 and gain / cost > best:
+                    best, pick = gain / cost, ("r", b)
+            if pick is None:
+                break
+            if pick[0] == "q":
+                q_fb.append(pick[1])
+                covered[pick[1], :] = True
+            else:
+                ref_fb.append(pick[1])
+                covered[:, pick[1]] = True
+        q_fb, ref_fb = sorted(q_fb), sorted(ref_fb)
+        self.set_fallback(q_fb, ref_fb)
+        r2 = self.recall(codes, lens)
+        share = float(wq[q_fb].sum() + (1.0 - wq[q_fb].sum()) * wr[ref_fb].sum())
+        return {"ref_fallback": ref_fb, "query_fallback": q_fb, "recall_no_fallback": r0["recall"],
+                "recall": r2["recall"], "found": r2["found"], "exact": r2["exact"],
+                "subset_of_exact": r2["subset_of_exact"], "exhaustive_share": share,
+                "cells_no_fallback": (r0["found_cells"], r0["exact_cells"])}
+
+
+def torch_rows(indptr):
+    """Row index of every CSR entry."""
+    import torch
+    n = indptr.numel() - 1
+    return torch.arange(n, device=indptr.device).repeat_interleave(indptr[1:] - indptr[:-1])
