@@ -218,9 +218,11 @@ int32_t st_encoder_loss_grad(st_encoder enc, const uint8_t *codes, const int32_t
 int32_t st_encoder_train_step(st_encoder enc, const uint8_t *codes, const int32_t *lens,
                               const int32_t *scores, int32_t S, float lr, float *loss,
                               st_error *err);
-/* Embeddings of a device set (amino acids, lengths 1..32) into out_device: layout 0 = fp32
- * [n][64]; layout 1 = bf16 [n][64] with the 16-byte chunks of row r stored at chunk ^ (r & 7)
- * (the operand layout of the proposal kernel). */
+/* Embeddings of a device set (amino acids, lengths 1..32) into out_device.
+ *   layout 0: fp32 [n][64] from the fp32 forward (the training kernels' numbers);
+ *   layout 1: bf16 [n][64] from the bf16 tensor-core inference kernels, the 16-byte chunks of
+ *             row r stored at chunk ^ (r & 7) (the operand layout of st_propose_topk);
+ *   layout 2: the fp32 forward stored in layout 1's format. */
 int32_t st_encoder_embed(st_encoder enc, st_seqset set, void *out_device, int32_t layout,
                          void *cuda_stream, st_error *err);
 

@@ -611,7 +611,7 @@ int32_t st_encoder_embed(st_encoder enc, st_seqset set, void* out_device, int32_
         Context& ctx = encoder_ctx(enc);
         check_set(set);
         if (!out_device) fail(ST_EINVAL, "seqtree_b200: null output");
-        if (layout != 0 && layout != 1) fail(ST_EINVAL, "seqtree_b200: embedding layout is 0 or 1");
+        if (layout < 0 || layout > 2) fail(ST_EINVAL, "seqtree_b200: embedding layout is 0, 1 or 2");
         std::lock_guard<std::mutex> lk(ctx.mu);
         encoder_embed(*enc->impl, *set, out_device, layout, static_cast<cudaStream_t>(cuda_stream));
     });

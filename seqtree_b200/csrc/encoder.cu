@@ -15,21 +15,14 @@
 #include <memory>
 
 #include "common.cuh"
+#include "encoder_layout.cuh"
 
 namespace stb {
 
 namespace {
 
-constexpr int kA = 24, kW = 128, kE = 64, kP = 32;
+using namespace enc;
 constexpr float kClip = 64.0f;
-
-// flat parameter offsets
-constexpr int64_t oW1 = 0, ob1 = oW1 + 3 * kA * kW, oW2 = ob1 + kW, ob2 = oW2 + 3 * kW * kW;
-constexpr int64_t oL0 = ob2 + kW;                                   // attention layer 0
-constexpr int64_t kLayer = kW * 3 * kW + 3 * kW + kW * kW + kW;     // Wqkv, bqkv, Wo, bo
-constexpr int64_t oWout = oL0 + 2 * kLayer, obout = oWout + kW * kE;
-constexpr int64_t kParams = obout + kE;
-constexpr int64_t lWqkv = 0, lbqkv = kW * 3 * kW, lWo = lbqkv + 3 * kW, lbo = lWo + kW * kW;
 
 // ------------------------------------------------------------------------------ SGEMM -------
 // C[M x N] (op) = opA(A) * opB(B); A is [M x K] (or [K x M] when TA), B is [K x N] (or [N x K]
@@ -562,7 +555,8 @@ __global__ void store_embed_kernel(const float* __restrict__ z, int S, int64_t f
 struct Encoder {
     int device = 0;
     DevBuf params, grads, adam_m, adam_v, loss;
-    int64_t step = 0;
+    int64_t step = 0;            // Adam steps taken: also the version of the parameters
+    std::shared_ptr<void> bf16;  // weights and workspace of the bf16 inference path
     int S_cap = 0;  // sequences the workspace holds
     // forward activations (rows = 32 * S)
     DevBuf codes, lens, scores, pre1, h1, x2, pre2, hA, hB, hC, qkv0, qkv1, a0, a1, o0, o1, y, pool,
@@ -775,12 +769,19 @@ float encoder_train_step(Encoder& m, const uint8_t* codes, const int32_t* lens, 
     return loss;
 }
 
+void encoder_embed_bf16(const float* prm, int64_t version, std::shared_ptr<void>& state,
+                        const st_seqset_s& set, void* out, int layout, cudaStream_t st);
+
 // Embeddings of every sequence of a device set (amino-acid codes, lengths 1..32) into `out`.
 void encoder_embed(Encoder& m, const st_seqset_s& set, void* out, int layout, cudaStream_t st) {
     if (set.alphabet != ST_ALPHABET_AA)
         fail(ST_EINVAL, "seqtree_b200: the encoder takes amino-acid sets");
     for (int32_t L : set.h_len)
         if (L < 1 || L > kP) fail(ST_EINVAL, "seqtree_b200: encoder inputs must have 1..32 residues");
+    if (layout == 1) {
+        encoder_embed_bf16(P(m), m.step, m.bf16, set, out, layout, st);
+        return;
+    }
     Context& ctx = context();
     constexpr int kChunk = 16384;
     m.reserve(kChunk);
@@ -790,7 +791,8 @@ void encoder_embed(Encoder& m, const st_seqset_s& set, void* out, int layout, cu
                                                        static_cast<uint8_t*>(m.codes.ptr),
                                                        static_cast<int32_t*>(m.lens.ptr));
         forward(m, S, st, ctx.num_sms);
-        store_embed_kernel<<<unsigned(ceil_div(S, 8)), 256, 0, st>>>(F(m.z), S, first, layout, out);
+        store_embed_kernel<<<unsigned(ceil_div(S, 8)), 256, 0, st>>>(F(m.z), S, first, layout ? 1 : 0,
+                                                                    out);
         STB_CUDA(cudaGetLastError());
         note_launch(nullptr, 2);
     }

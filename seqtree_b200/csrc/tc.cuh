@@ -44,6 +44,20 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity, volatile
         }
     }
 }
+// Bounded wait that does not look at an abort word: every waiter of a barrier that completes
+// sees it complete, so a group of warps waiting on one phase either all pass or all time out
+// (after kWaitNs) -- none is left behind at a later rendezvous.
+__device__ __forceinline__ bool bar_wait_own(uint32_t bar, uint32_t parity, unsigned long long* err) {
+    if (bar_test(bar, parity)) return true;
+    const uint64_t t0 = now_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (bar_test(bar, parity)) return true;
+        if ((it & 255) == 0 && now_ns() - t0 > kWaitNs) {
+            atomicExch(err, 1ull);
+            return false;
+        }
+    }
+}
 // Bounded wait that ignores the abort word (draining in-flight work before exit).
 __device__ __forceinline__ void bar_drain(uint32_t bar, uint32_t parity) {
     const uint64_t t0 = now_ns();

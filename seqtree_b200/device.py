@@ -41,7 +41,7 @@ class SeqSet:
         h = getattr(self, "_h", None)
         if h is not None and h.value:
             self._free(h)
-            self._h = ctypes.c_void_p()
+            self._h = None
 
 
 def gapblock_into(queries: SeqSet, refs: SeqSet, out_ptr: int, stream: int = 0,
@@ -99,7 +99,7 @@ class Hits:
         h = getattr(self, "_h", None)
         if h is not None and h.value:
             self._free(h)
-            self._h = ctypes.c_void_p()
+            self._h = None
 
 
 def gapblock_sparse_into(queries: SeqSet, refs: SeqSet, hits: Hits, stream: int = 0, *,

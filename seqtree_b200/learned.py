@@ -117,7 +117,8 @@ class Encoder:
         return float(loss.value)
 
     def embed_into(self, seqset, out_ptr: int, layout: int = 0, stream: int = 0) -> None:
-        """Embeddings of a device set: layout 0 fp32 [n][64], 1 bf16 swizzled [n][64]."""
+        """Embeddings of a device set: layout 0 fp32 [n][64] (fp32 forward), 1 bf16 swizzled
+        [n][64] (bf16 tensor-core inference), 2 the fp32 forward in layout 1's format."""
         err = _lib.st_error()
         _lib.check(_lib.lib.st_encoder_embed(self._h, seqset.handle, ctypes.c_void_p(out_ptr),
                                              int(layout), ctypes.c_void_p(stream),
@@ -127,7 +128,7 @@ class Encoder:
         h = getattr(self, "_h", None)
         if h is not None and h.value:
             self._free(h)
-            self._h = ctypes.c_void_p()
+            self._h = None
 
 
 def pair_scores(qset, rset, qi_ptr: int, ri_ptr: int, n: int, out_ptr: int, stream: int = 0, *,

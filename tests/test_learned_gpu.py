@@ -69,6 +69,37 @@ def test_encoder_embeddings_match_the_oracle_forward(cuda_ready):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [300, 40000])
+def test_bf16_inference_tracks_the_fp32_forward(cuda_ready, n):
+    """The bf16 tensor-core embedding (layout 1) against the float64 forward: bf16 activations
+    with fp32 accumulation, so a tolerance -- every row within 0.03 per component and cosine
+    >= 0.998 to the exact unit vector.  40,000 sequences span two 32,768-sequence passes."""
+    import torch
+
+    from seqtree_b200 import device
+    from seqtree_b200.learned import Encoder, pad_codes
+    rng = np.random.default_rng(n)
+    seqs = cdr3(rng, n - 3, 8, 25) + ["C", "CASSLGQGAYEQYFCASSLGQGAYEQYFWWW", "WY"]
+    flat = (oenc.init_params(3) + rng.normal(0, 0.02, oenc.param_count())).astype(np.float32)
+    enc = Encoder(flat)
+    ss = device.SeqSet(seqs, "aa")
+    zbf = torch.empty((len(seqs), 64), dtype=torch.bfloat16, device="cuda")
+    enc.embed_into(ss, zbf.data_ptr(), 1, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    raw = zbf.float().cpu().numpy().reshape(len(seqs), 8, 8)
+    rows = np.arange(len(seqs))[:, None]
+    got = raw[rows, np.arange(8)[None, :] ^ (rows & 7)].reshape(len(seqs), 64)
+    check = np.arange(len(seqs)) if n <= 1000 else np.r_[np.arange(500), np.arange(n - 500, n),
+                                                           rng.integers(0, n, 500)]
+    codes, lens = pad_codes([seqs[i] for i in check])
+    want = oenc.forward(flat.astype(np.float64), codes, lens)
+    err = np.abs(got[check] - want).max(axis=1)
+    cos = (got[check] * want).sum(1) / np.linalg.norm(got[check], axis=1)
+    print(f"bf16 vs float64: max abs {err.max():.4f}, min cos {cos.min():.5f}")
+    assert err.max() <= 0.03 and cos.min() >= 0.998
+
+
+@pytest.mark.gpu
 def test_training_lowers_the_loss(cuda_ready):
     from seqtree_b200.learned import Encoder, pad_codes, training_pairs
     rng = np.random.default_rng(1)
