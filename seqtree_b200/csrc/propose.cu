@@ -16,8 +16,10 @@
 //   warps 2-9  own one query row each (TMEM lane = row, warp % 4 selects the lane quarter,
 //              warps 2-5 read the first query half and 6-9 the second).  Each reads its row's
 //              128 fp32 scores with tcgen05.ld, rejects a 32-column group with one 3-input max
-//              against the running threshold, and appends the survivors to the query's
-//              candidate list in global scratch as 64-bit keys
+//              tree against the running threshold, and otherwise builds the group's survivor bit
+//              mask, parks the 32 scores in its own shared-memory row and appends only the set
+//              bits (the loop stays small, which measured faster than unrolled or predicated
+//              appends) to the query's candidate list in global scratch as 64-bit keys
 //              (orderable score << 32 | ~ref_id: larger score first, then smaller ref id).
 //              When a list passes kCap - 128 entries, the warp cooperatively radix-selects its
 //              k-th largest key, keeps exactly k keys and raises the threshold to the smallest
@@ -58,7 +60,8 @@ constexpr int kTileB = kRT * kRowB;            // 16 KB
 constexpr int kSmA = 0;                                   // 32 KB: the query tile
 constexpr int kSmB = kSmA + kQT * kRowB;                  // 96 KB: the ref ring
 constexpr int kSmWarp = kSmB + kStages * kTileB;          // 8 x 2 KB: histogram / sort space
-constexpr int kSmBar = kSmWarp + kEpiWarps * 2048;        // mbarriers and flags
+constexpr int kSmPark = kSmWarp + kEpiWarps * 2048;       // 8 x 32 x 128 B: parked scores
+constexpr int kSmBar = kSmPark + kEpiWarps * 32 * 128;    // mbarriers and flags
 constexpr int kSmTotal = kSmBar + 256;
 constexpr size_t kSmemBytes = size_t(kSmTotal) + 1024;    // + alignment slack
 
@@ -342,6 +345,7 @@ __global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a
         unsigned long long* lists =
             a.cand + (int64_t(blockIdx.x) * kQT + grp * 128 + quarter * 32) * kCap;
         unsigned long long* mine = lists + int64_t(lane) * kCap;
+        uint32_t* park = reinterpret_cast<uint32_t*>(smem + kSmPark + (ew * 32 + lane) * 128);
         const uint32_t tlane = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(grp) * 128u;
         uint32_t acc = 0, accphase = 0;
         bool ok = true;
@@ -377,13 +381,24 @@ __global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a
                                                  fmax3(m[6], m[7], m[8])),
                                            fmax3(m[9], m[10], -INFINITY));
                     if (mx > thr) {
-                        const uint32_t rbase = uint32_t(r0 + c * 32);
+                        // survivors as a bit mask; the 32 values parked in this thread's
+                        // shared-memory row (16-byte chunks swizzled by lane) so that only the
+                        // set bits are visited
+                        uint32_t mask = 0;
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            if (__uint_as_float(v[j]) > thr) {
-                                mine[count++] = ((unsigned long long)ord_of(v[j]) << 32) |
-                                                (unsigned long long)(~(rbase + uint32_t(j)));
-                            }
+                        for (int j = 0; j < 32; ++j)
+                            mask |= (__uint_as_float(v[j]) > thr) ? (1u << j) : 0u;
+#pragma unroll
+                        for (int ch = 0; ch < 8; ++ch)
+                            *reinterpret_cast<uint4*>(park + ((ch ^ (lane & 7)) << 2)) =
+                                make_uint4(v[4 * ch], v[4 * ch + 1], v[4 * ch + 2], v[4 * ch + 3]);
+                        const uint32_t rbase = uint32_t(r0 + c * 32);
+                        while (mask) {
+                            const int j = __ffs(mask) - 1;
+                            mask &= mask - 1;
+                            const uint32_t x = park[(((j >> 2) ^ (lane & 7)) << 2) | (j & 3)];
+                            mine[count++] = ((unsigned long long)ord_of(x) << 32) |
+                                            (unsigned long long)(~(rbase + uint32_t(j)));
                         }
                     }
                 }
