@@ -286,6 +286,10 @@ int32_t st_builtin_similarity(const char *name, int32_t *out, int32_t capacity, 
 int32_t st_last_launch_count(void);
 /* Kernels of this library launched by the whole process so far (all threads, all calls). */
 int64_t st_total_launch_count(void);
+/* The launch autotuner's decisions so far, one line per shape key ("device|key -> choice
+ * (variant:time ...)"), written NUL-terminated into buf (truncated to capacity); returns the full
+ * length.  Shapes are tuned on first use unless SEQTREE_B200_TUNE=0 is set in the environment. */
+int64_t st_tuning_table(char *buf, int64_t capacity);
 const char *st_last_kernel_name(void);
 
 /* Pinned host buffers from a per-device cache.  A result written into one of these travels

@@ -112,6 +112,7 @@ SIGNATURES = [
      [ctypes.c_char_p, _i32p, ctypes.c_int32, _i32p, _ep]),
     ("st_last_launch_count", ctypes.c_int32, []),
     ("st_total_launch_count", ctypes.c_int64, []),
+    ("st_tuning_table", ctypes.c_int64, [ctypes.c_char_p, ctypes.c_int64]),
     ("st_last_kernel_name", ctypes.c_char_p, []),
     ("st_host_alloc", ctypes.c_void_p, [ctypes.c_uint64]),
     ("st_host_free", None, [ctypes.c_void_p]),
@@ -246,6 +247,14 @@ def i32_ptr(a: np.ndarray | None):
 
 def last_launch_count() -> int:
     return int(lib.st_last_launch_count())
+
+
+def tuning_table() -> str:
+    """The autotuner's decisions: one line per tuned shape key."""
+    n = int(lib.st_tuning_table(None, 0))
+    buf = ctypes.create_string_buffer(n + 1)
+    lib.st_tuning_table(buf, n + 1)
+    return buf.value.decode()
 
 
 def total_launch_count() -> int:

@@ -40,6 +40,7 @@ void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, in
                   float* scores, cudaStream_t stream);
 int last_launches();
 int64_t total_launches();
+std::string tuning_table();
 const char* last_kernel();
 void* host_alloc(uint64_t bytes);
 void host_free(void* p);
@@ -149,6 +150,16 @@ int32_t st_builtin_similarity(const char* name, int32_t* out, int32_t capacity, 
 int32_t st_last_launch_count(void) { return last_launches(); }
 
 int64_t st_total_launch_count(void) { return total_launches(); }
+
+int64_t st_tuning_table(char* buf, int64_t capacity) {
+    const std::string t = tuning_table();
+    if (buf && capacity > 0) {
+        const size_t n = std::min<size_t>(t.size(), size_t(capacity - 1));
+        std::memcpy(buf, t.data(), n);
+        buf[n] = 0;
+    }
+    return int64_t(t.size());
+}
 const char* st_last_kernel_name(void) { return last_kernel(); }
 
 void* st_host_alloc(uint64_t bytes) { return host_alloc(bytes); }

@@ -9,6 +9,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <map>
+#include <mutex>
+#include <string>
+#include <vector>
 
 namespace stb {
 
@@ -31,6 +34,95 @@ void reset_launches() {
 int last_launches() { return t_launches; }
 int64_t total_launches() { return g_launches.load(std::memory_order_relaxed); }
 const char* last_kernel() { return t_kernel; }
+
+// ----------------------------------------------------------------------------- tuning -------
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, int> g_tune;        // "device|key" -> choice
+std::map<std::string, std::string> g_tune_log;  // "device|key" -> measured times
+
+bool tune_on() {
+    static const bool on = [] {
+        const char* v = std::getenv("SEQTREE_B200_TUNE");
+        return !(v && *v == '0');
+    }();
+    return on;
+}
+std::string dev_key(const std::string& key) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return std::to_string(dev) + "|" + key;
+}
+}  // namespace
+
+int tuned_lookup(const std::string& key) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(dev_key(key));
+    return it == g_tune.end() ? -1 : it->second;
+}
+
+int tuned_run(const std::string& key, int n, int fallback, const std::function<void(int)>& run,
+              cudaStream_t stream) {
+    const std::string k = dev_key(key);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(k);
+        if (it != g_tune.end()) {
+            run(it->second);
+            return it->second;
+        }
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    STB_CUDA(cudaStreamIsCapturing(stream, &cs));
+    if (!tune_on() || n < 2 || cs != cudaStreamCaptureStatusNone) {
+        run(fallback);
+        return fallback;
+    }
+    cudaEvent_t e0, e1;
+    STB_CUDA(cudaEventCreate(&e0));
+    STB_CUDA(cudaEventCreate(&e1));
+    float best = 0.f;
+    int pick = fallback;
+    std::string log;
+    std::vector<float> ms(size_t(n), 0.f);
+    try {
+        for (int c = 0; c < n; ++c) {
+            run(c);  // untimed: first-use effects (plans, module loading, workspace growth)
+            STB_CUDA(cudaEventRecord(e0, stream));
+            run(c);
+            STB_CUDA(cudaEventRecord(e1, stream));
+            STB_CUDA(cudaEventSynchronize(e1));
+            STB_CUDA(cudaEventElapsedTime(&ms[size_t(c)], e0, e1));
+            if (c == 0 || ms[size_t(c)] < best) {
+                best = ms[size_t(c)];
+                pick = c;
+            }
+        }
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    char buf[64];
+    for (int c = 0; c < n; ++c) {
+        std::snprintf(buf, sizeof buf, "%s%d:%.3fms", c ? " " : "", c, double(ms[size_t(c)]));
+        log += buf;
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[k] = pick;
+    g_tune_log[k] = log;
+    return pick;
+}
+
+// One line per tuned key: "device|key -> choice (variant:time ...)".
+std::string tuning_table() {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    std::string out;
+    for (auto& [k, v] : g_tune) out += k + " -> " + std::to_string(v) + " (" + g_tune_log[k] + ")\n";
+    return out;
+}
 
 // ----------------------------------------------------------------------------- tracing ------
 namespace {

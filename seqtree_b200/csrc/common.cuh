@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -106,6 +107,28 @@ void h2d(void* dst, const void* src, size_t bytes, cudaStream_t stream);
 // Byte-exact content cache: returns true when `bytes` equals what was uploaded last time
 // under `slot`, so re-uploads of unchanged tables are skipped.
 bool same_as_last(std::vector<uint8_t>& slot, const void* data, size_t bytes);
+
+// ----------------------------------------------------------------------------- tuning -------
+// Measured choice among `n` launch variants that produce identical results.  The first time `key`
+// is seen on a device (and tuning is on and `stream` is not being captured), every variant runs
+// once untimed and once timed with CUDA events on `stream`, and the fastest is cached; every
+// call ends with the chosen variant's results in place.  Later calls with the key run the cached
+// choice directly.  Tuning is off with SEQTREE_B200_TUNE=0; then, and while `stream` is being
+// captured before the key was tuned, `run(fallback)` runs (`fallback` may be -1, the caller's
+// static choice).
+int tuned_run(const std::string& key, int n, int fallback, const std::function<void(int)>& run,
+              cudaStream_t stream);
+// The cached choice for `key` on the current device, or -1.
+int tuned_lookup(const std::string& key);
+// log2 bucket of a size, for shape keys.
+inline int size_bucket(int64_t n) {
+    int b = 0;
+    while (n > 1) {
+        n >>= 1;
+        ++b;
+    }
+    return b;
+}
 
 // ----------------------------------------------------------------------------- sets ---------
 // A sequence set resident on one device: the concatenated (encoded or raw) bytes, offsets and

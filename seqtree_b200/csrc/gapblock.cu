@@ -679,6 +679,18 @@ size_t fast_smem(int lq, int64_t slab_cap, int rc, int W1) {
 
 namespace {
 
+// Chunk widths the fast kernel may use.  The widest that reaches the best CTA residency is the
+// static choice; the autotuner (dense calls) measures all of them once per shape.
+constexpr int kRcCandidates[] = {1024, 768, 512, 384, 256};
+constexpr int kNumRc = int(sizeof(kRcCandidates) / sizeof(kRcCandidates[0]));
+thread_local int t_force_rc = 0;  // set while the autotuner times one chunk width
+
+std::string gb_shape_key(const st_seqset_s& qs, const st_seqset_s& rs, bool has_prior) {
+    return "gapblock|" + std::to_string(profile_height(qs.max_len)) + "|" +
+           std::to_string(int(has_prior)) + "|" + std::to_string(std::max(qs.max_len, rs.max_len)) +
+           "|" + std::to_string(size_bucket(qs.count)) + "|" + std::to_string(size_bucket(rs.count));
+}
+
 // Validated inputs -> the dense matrix in `out_d` (device, N*K int32), or, when `sink` is given,
 // the cells that pass its threshold appended to it.
 // `r0`, `r1` restrict the queries to rows [r0, r1) (sparse form only; r1 = -1: all rows).
@@ -724,13 +736,17 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
     size_t smem = 0;
     if (fast) {
         RefPlan& rp = plan_slot<RefPlan>(rs.gb_ref_plan, ctx.tmp_ref_plan, rs.owns);
-        if (rp.uid != rs.uid) {
+        const int tuned = t_force_rc ? -1 : tuned_lookup(gb_shape_key(qs, rs, has_prior));
+        const int want_rc = t_force_rc ? t_force_rc : (tuned >= 0 ? kRcCandidates[tuned] : 0);
+        if (rp.uid != rs.uid || (want_rc && rp.rc != want_rc)) {
             Phase ph("ref_plan");
-            // Chunk width: the widest (best warp fill) that still reaches the highest CTA
-            // residency the kernel's registers allow, checked with the occupancy calculator.
+            // Chunk width: the autotuner's measured choice when there is one; otherwise the
+            // widest (best warp fill) that still reaches the highest CTA residency the
+            // kernel's registers allow, checked with the occupancy calculator.
             const void* kern = fast_kernel_ptr(lq, has_prior);
             int best_rc = 0, best_blocks = -1;
             for (int rc : {1024, 896, 768, 640, 512, 384, 256}) {
+                if (want_rc && rc != want_rc) continue;
                 build_ref_plan(rp, rs, rc, stream, /*upload=*/false);
                 const size_t sm = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rc, W1);
                 if (sm > size_t(ctx.max_smem_optin)) continue;
@@ -870,8 +886,32 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
 void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int32_t matrix_size,
                    int32_t go, int32_t ge, const int32_t* prior, int64_t prior_len,
                    uint32_t prior_width, int32_t* out_d, cudaStream_t stream) {
-    gapblock_run(qs, rs, penalty, matrix_size, go, ge, prior, prior_len, prior_width, out_d,
-                 nullptr, stream);
+    auto run = [&] {
+        gapblock_run(qs, rs, penalty, matrix_size, go, ge, prior, prior_len, prior_width, out_d,
+                     nullptr, stream);
+    };
+    // Only the fast kernel has a chunk width to choose (non-negative penalties, lengths <= 64;
+    // the remaining range checks happen inside and fall back to the general kernel).
+    bool nonneg = true;
+    const int A = qs.alphabet >= 0 ? alphabet_size(qs.alphabet) : 0;
+    if (penalty && matrix_size == A)
+        for (int i = 0; i < A * A; ++i) nonneg &= penalty[i] >= 0;
+    if (!nonneg || qs.count == 0 || rs.count == 0 || std::max(qs.max_len, rs.max_len) > 64 ||
+        qs.alphabet < 0 || qs.alphabet != rs.alphabet || (penalty && matrix_size != A)) {
+        run();
+        return;
+    }
+    const bool has_prior = prior && prior_len > 0;
+    tuned_run(gb_shape_key(qs, rs, has_prior), kNumRc, -1, [&](int c) {
+        t_force_rc = c >= 0 ? kRcCandidates[c] : 0;  // -1: the static choice
+        try {
+            run();
+        } catch (...) {
+            t_force_rc = 0;
+            throw;
+        }
+        t_force_rc = 0;
+    }, stream);
 }
 
 // Scores of listed pairs (device index arrays) into out_d; the general int32 kernel's

@@ -12,6 +12,8 @@
 #include <algorithm>
 #include <climits>
 #include <map>
+#include <memory>
+#include <mutex>
 #include <numeric>
 #include <tuple>
 
@@ -141,6 +143,154 @@ void launch_exact(Context& ctx, ExactArgs a, int64_t work, cudaStream_t stream) 
     gotoh_exact_kernel<<<unsigned(T / 256), 256, size_t(a.A) * a.A * 4, stream>>>(a);
     STB_CUDA(cudaGetLastError());
     note_launch("gotoh_exact_kernel");
+}
+
+// --------------------------------------------------------------------- per-thread path -----
+// Short sequences (both sets at most NMAX long): one thread per (query, ref) pair, the whole DP
+// row (M, X, Y for ref columns 0..NMAX) in registers, so no scratch memory is touched.  The
+// recurrence and its order of evaluation are gotoh_pair's, in int32 with the sentinel kNeg32:
+// the host admits a launch only when every legitimate value is bounded by 2^27 in magnitude, so
+// sentinel-derived values (>= kNeg32 - 64 * (go + ge) > INT32_MIN) stay below every legitimate
+// one and the maxima -- hence the result -- are the int64 recurrence's.  Consecutive threads
+// take consecutive refs of one query, so a warp shares the query row and writes 128 contiguous
+// bytes.  The three-input maxima are Blackwell DPX instructions.
+constexpr int32_t kNeg32 = -(1 << 29);
+
+struct ThreadArgs {
+    const uint8_t* qc;
+    const int64_t* qoff;
+    const uint8_t* rc;
+    const int64_t* roff;
+    int64_t N, K;
+    const int32_t* sim;
+    int A;
+    int32_t go, ge;
+    int self;            // 1: self scores of the query set into self_out
+    int64_t* self_out;
+    int dist;
+    const int64_t* q_self;
+    const int64_t* r_self;
+    int32_t* out;
+    unsigned int* overflow;
+};
+
+__device__ __forceinline__ int32_t gap_run32(int L, int32_t open, int32_t extend) {
+    return L <= 0 ? 0 : open + (L - 1) * extend;
+}
+
+template <int NMAX, bool LOCAL>
+__global__ void __launch_bounds__(128) gotoh_thread_kernel(const ThreadArgs a) {
+    extern __shared__ int32_t s_sim[];
+    for (int i = threadIdx.x; i < a.A * a.A; i += blockDim.x) s_sim[i] = a.sim[i];
+    __syncthreads();
+    const int64_t total = a.self ? a.N : a.N * a.K;
+    const int64_t stride = int64_t(gridDim.x) * blockDim.x;
+    for (int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; idx < total; idx += stride) {
+        const int64_t i = a.self ? idx : idx / a.K;
+        const int64_t k = a.self ? idx : idx - i * a.K;
+        const uint8_t* q = a.qc + a.qoff[i];
+        const int m = int(a.qoff[i + 1] - a.qoff[i]);
+        const uint8_t* r = a.self ? q : a.rc + a.roff[k];
+        const int n = a.self ? m : int(a.roff[k + 1] - a.roff[k]);
+        int32_t score;
+        if (m == 0 || n == 0) {
+            score = LOCAL ? 0 : -gap_run32(m ? m : n, a.go, a.ge);
+        } else {
+            int rcode[NMAX];
+            int32_t M[NMAX + 1], X[NMAX + 1], Y[NMAX + 1];
+            M[0] = 0;
+            X[0] = kNeg32;
+            Y[0] = kNeg32;
+#pragma unroll
+            for (int j = 1; j <= NMAX; ++j) {
+                rcode[j - 1] = j <= n ? int(r[j - 1]) : 0;
+                M[j] = LOCAL ? 0 : kNeg32;
+                X[j] = kNeg32;
+                Y[j] = LOCAL ? kNeg32 : -gap_run32(j, a.go, a.ge);
+            }
+            int32_t best = LOCAL ? 0 : kNeg32;
+            int32_t lm = 0, lx = 0, ly = 0;
+            for (int ii = 1; ii <= m; ++ii) {
+                int32_t dm = M[0], dx = X[0], dy = Y[0];
+                lm = LOCAL ? 0 : kNeg32;
+                lx = LOCAL ? kNeg32 : -gap_run32(ii, a.go, a.ge);
+                ly = kNeg32;
+                M[0] = lm;
+                X[0] = lx;
+                Y[0] = ly;
+                const int32_t* srow = s_sim + int(q[ii - 1]) * a.A;
+                int32_t em = lm, ex = lx, ey = ly;  // row values at column n
+#pragma unroll
+                for (int j = 1; j <= NMAX; ++j) {
+                    if (j <= n) {
+                        const int32_t um = M[j], ux = X[j], uy = Y[j];
+                        int32_t mv = __vimax3_s32(dm, dx, dy) + srow[rcode[j - 1]];
+                        if (LOCAL) mv = max(mv, 0);
+                        const int32_t xv = __viaddmax_s32(max(um, uy), -a.go, ux - a.ge);
+                        const int32_t yv = __viaddmax_s32(max(lm, lx), -a.go, ly - a.ge);
+                        M[j] = mv;
+                        X[j] = xv;
+                        Y[j] = yv;
+                        if (LOCAL) best = max(best, mv);
+                        dm = um;
+                        dx = ux;
+                        dy = uy;
+                        lm = mv;
+                        lx = xv;
+                        ly = yv;
+                        em = mv;
+                        ex = xv;
+                        ey = yv;
+                    }
+                }
+                lm = em;
+                lx = ex;
+                ly = ey;
+            }
+            score = LOCAL ? best : __vimax3_s32(lm, lx, ly);
+        }
+        if (a.self) {
+            a.self_out[idx] = score;
+            continue;
+        }
+        const int64_t v = a.dist ? a.q_self[i] + a.r_self[k] - 2 * int64_t(score) : int64_t(score);
+        if (v < INT32_MIN || v > INT32_MAX) {
+            atomicOr(a.overflow, 1u);
+            continue;
+        }
+        a.out[idx] = int32_t(v);
+    }
+}
+
+// Largest legitimate |value| of the recurrence for sequences up to lq / lr long, or -1 when
+// the per-thread path does not apply (lengths beyond 32, an empty sequence is fine).
+int thread_nmax(const st_seqset_s& qs, const st_seqset_s& rs, const int32_t* sim, int A, int32_t go,
+                int32_t ge, bool self_q, bool self_r) {
+    int need = rs.max_len;
+    if (self_q) need = std::max(need, qs.max_len);
+    if (self_r) need = std::max(need, rs.max_len);
+    if (need > 32) return -1;
+    int64_t smax = 0;
+    for (int i = 0; i < A * A; ++i) smax = std::max<int64_t>(smax, std::llabs(int64_t(sim[i])));
+    const int64_t span = int64_t(std::max(qs.max_len, rs.max_len)) * 2;
+    const int64_t bound = span * (smax + int64_t(go) + int64_t(ge) * span);
+    if (bound >= (int64_t(1) << 27)) return -1;
+    return need <= 16 ? 16 : 32;
+}
+
+void launch_thread(Context& ctx, ThreadArgs a, int nmax, bool local, int64_t work, cudaStream_t stream) {
+    const int64_t blocks = std::min<int64_t>(ceil_div(std::max<int64_t>(work, 1), 128),
+                                             int64_t(ctx.num_sms) * 16);
+    const size_t smem = size_t(a.A) * a.A * 4;
+    if (nmax == 16) {
+        if (local) gotoh_thread_kernel<16, true><<<unsigned(blocks), 128, smem, stream>>>(a);
+        else gotoh_thread_kernel<16, false><<<unsigned(blocks), 128, smem, stream>>>(a);
+    } else {
+        if (local) gotoh_thread_kernel<32, true><<<unsigned(blocks), 128, smem, stream>>>(a);
+        else gotoh_thread_kernel<32, false><<<unsigned(blocks), 128, smem, stream>>>(a);
+    }
+    STB_CUDA(cudaGetLastError());
+    note_launch("gotoh_thread_kernel");
 }
 
 // ------------------------------------------------------------------------- wavefront path ---
@@ -450,6 +600,86 @@ void launch_wave(Context& ctx, WaveArgs wa, int R, bool local, bool exact, cudaS
 
 }  // namespace
 
+// The warp-wavefront path for every pair (int16x2 cells; the caller checked wave_eligible).
+void align_wave(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int A, int32_t mode,
+                int32_t go, int32_t ge, int32_t dist, int32_t* out_d, unsigned int* ovf,
+                cudaStream_t stream) {
+    Context& ctx = context();
+    const int64_t N = qs.count, K = rs.count;
+    WaveState& ws = wave_state(ctx.device);
+    const int A1 = A + 1;
+    {
+        // T[(q*A1 + r1)*A1 + r2] = s(q,r1) | s(q,r2) << 16, the pad code scoring NEG.
+        std::vector<uint8_t> key(size_t(A) * A * 4);
+        std::memcpy(key.data(), similarity, key.size());
+        if (!same_as_last(ws.key, key.data(), key.size())) {
+            std::vector<uint32_t> tab(size_t(A1) * A1 * A1);
+            auto sv = [&](int x, int y) -> int32_t {
+                return (x == A || y == A) ? -16384 : similarity[x * A + y];
+            };
+            for (int x = 0; x < A1; ++x)
+                for (int y1 = 0; y1 < A1; ++y1)
+                    for (int y2 = 0; y2 < A1; ++y2)
+                        tab[(size_t(x) * A1 + y1) * A1 + y2] =
+                            uint32_t(uint16_t(int16_t(sv(x, y1)))) |
+                            (uint32_t(uint16_t(int16_t(sv(x, y2)))) << 16);
+            try {
+                h2d(ws.table.as<uint32_t>(tab.size()), tab.data(), tab.size() * 4, stream);
+            } catch (...) {
+                ws.key.clear();  // not uploaded: the next call builds it again
+                throw;
+            }
+        }
+    }
+    WavePlan& qp = wave_plan(qs, ctx, 0, stream);
+    WavePlan& rp = wave_plan(rs, ctx, 1, stream);
+    const bool local = mode == ST_MODE_LOCAL;
+    const bool exact = ge > go;
+    WaveArgs wa{};
+    wa.table = static_cast<uint32_t*>(ws.table.ptr);
+    wa.A1 = A1;
+    wa.go = go;
+    wa.ge = ge;
+    wa.overflow = ovf;
+    wa.K = K;
+    int64_t* q_self = nullptr;
+    int64_t* r_self = nullptr;
+    if (dist) {
+        q_self = ctx.work_b.as<int64_t>(size_t(N + K));
+        r_self = q_self + N;
+        for (int t = 0; t < 2; ++t) {
+            const st_seqset_s& s = t == 0 ? qs : rs;
+            const WavePlan& p = t == 0 ? qp : rp;
+            for (auto& [R, off, cnt] : p.groups) {
+                WaveArgs sa = wa;
+                sa.qc = s.d_bytes;
+                sa.qoff = s.d_off;
+                sa.qlist = static_cast<int32_t*>(p.list.ptr) + off;
+                sa.nq = cnt;
+                sa.self = 1;
+                sa.self_out = t == 0 ? q_self : r_self;
+                launch_wave(ctx, sa, R, local, exact, stream);
+            }
+        }
+    }
+    for (auto& [R, off, cnt] : qp.groups) {
+        WaveArgs ma = wa;
+        ma.qc = qs.d_bytes;
+        ma.qoff = qs.d_off;
+        ma.rc = rs.d_bytes;
+        ma.roff = rs.d_off;
+        ma.qlist = static_cast<int32_t*>(qp.list.ptr) + off;
+        ma.nq = cnt;
+        ma.rpairs = static_cast<int2*>(rp.pairs.ptr);
+        ma.nrp = rp.npairs;
+        ma.dist = dist;
+        ma.q_self = q_self;
+        ma.r_self = r_self;
+        ma.out = out_d;
+        launch_wave(ctx, ma, R, local, exact, stream);
+    }
+}
+
 void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int32_t matrix_size,
                 int32_t mode, int32_t go, int32_t ge, int32_t dist, int32_t* out_d,
                 cudaStream_t stream) {
@@ -469,79 +699,85 @@ void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
     auto* ovf = reinterpret_cast<unsigned int*>(ctx.flags_d + 9);
     STB_CUDA(cudaMemsetAsync(ovf, 0, 8, stream));
 
-    if (wave_eligible(qs, rs, similarity, A, go, ge)) {
-        WaveState& ws = wave_state(ctx.device);
-        const int A1 = A + 1;
+    const int tn = thread_nmax(qs, rs, similarity, A, go, ge, dist != 0, dist != 0);
+    const bool wave_ok = wave_eligible(qs, rs, similarity, A, go, ge);
+    if (tn > 0) {
+        // Short sequences: one thread per pair (registers only) or the warp wavefront, whichever
+        // the autotuner measured faster for this shape.
+        // the similarity table, uploaded only when it changes (so warmed-up calls capture)
+        struct ThreadTable {
+            std::vector<uint8_t> key;
+            DevBuf sim;
+        };
+        static std::mutex tmu;
+        static std::map<int, std::unique_ptr<ThreadTable>> tables;
+        ThreadTable* tt;
         {
-            // T[(q*A1 + r1)*A1 + r2] = s(q,r1) | s(q,r2) << 16, the pad code scoring NEG.
-            std::vector<uint8_t> key(size_t(A) * A * 4);
-            std::memcpy(key.data(), similarity, key.size());
-            if (!same_as_last(ws.key, key.data(), key.size())) {
-                std::vector<uint32_t> tab(size_t(A1) * A1 * A1);
-                auto sv = [&](int x, int y) -> int32_t {
-                    return (x == A || y == A) ? -16384 : similarity[x * A + y];
-                };
-                for (int x = 0; x < A1; ++x)
-                    for (int y1 = 0; y1 < A1; ++y1)
-                        for (int y2 = 0; y2 < A1; ++y2)
-                            tab[(size_t(x) * A1 + y1) * A1 + y2] =
-                                uint32_t(uint16_t(int16_t(sv(x, y1)))) |
-                                (uint32_t(uint16_t(int16_t(sv(x, y2)))) << 16);
-                try {
-                    h2d(ws.table.as<uint32_t>(tab.size()), tab.data(), tab.size() * 4, stream);
-                } catch (...) {
-                    ws.key.clear();  // not uploaded: the next call builds it again
-                    throw;
-                }
+            std::lock_guard<std::mutex> lk(tmu);
+            auto& slot = tables[ctx.device];
+            if (!slot) slot = std::make_unique<ThreadTable>();
+            tt = slot.get();
+        }
+        int32_t* d_sim = tt->sim.as<int32_t>(size_t(A) * A);
+        if (!same_as_last(tt->key, similarity, size_t(A) * A * 4)) {
+            try {
+                h2d(d_sim, similarity, size_t(A) * A * 4, stream);
+            } catch (...) {
+                tt->key.clear();
+                throw;
             }
         }
-        WavePlan& qp = wave_plan(qs, ctx, 0, stream);
-        WavePlan& rp = wave_plan(rs, ctx, 1, stream);
-        const bool local = mode == ST_MODE_LOCAL;
-        const bool exact = ge > go;
-        WaveArgs wa{};
-        wa.table = static_cast<uint32_t*>(ws.table.ptr);
-        wa.A1 = A1;
-        wa.go = go;
-        wa.ge = ge;
-        wa.overflow = ovf;
-        wa.K = K;
-        int64_t* q_self = nullptr;
-        int64_t* r_self = nullptr;
-        if (dist) {
-            q_self = ctx.work_b.as<int64_t>(size_t(N + K));
-            r_self = q_self + N;
-            for (int t = 0; t < 2; ++t) {
-                const st_seqset_s& s = t == 0 ? qs : rs;
-                const WavePlan& p = t == 0 ? qp : rp;
-                for (auto& [R, off, cnt] : p.groups) {
-                    WaveArgs sa = wa;
-                    sa.qc = s.d_bytes;
-                    sa.qoff = s.d_off;
-                    sa.qlist = static_cast<int32_t*>(p.list.ptr) + off;
-                    sa.nq = cnt;
-                    sa.self = 1;
-                    sa.self_out = t == 0 ? q_self : r_self;
-                    launch_wave(ctx, sa, R, local, exact, stream);
+        auto run_thread = [&] {
+            ThreadArgs t{};
+            t.sim = d_sim;
+            t.A = A;
+            t.go = go;
+            t.ge = ge;
+            t.overflow = ovf;
+            int64_t* q_self = nullptr;
+            int64_t* r_self = nullptr;
+            if (dist) {
+                q_self = ctx.work_b.as<int64_t>(size_t(N + K));
+                r_self = q_self + N;
+                for (int side = 0; side < 2; ++side) {
+                    const st_seqset_s& s = side == 0 ? qs : rs;
+                    ThreadArgs b = t;
+                    b.qc = s.d_bytes;
+                    b.qoff = s.d_off;
+                    b.N = s.count;
+                    b.self = 1;
+                    b.self_out = side == 0 ? q_self : r_self;
+                    launch_thread(ctx, b, tn, mode == ST_MODE_LOCAL, s.count, stream);
                 }
             }
+            t.qc = qs.d_bytes;
+            t.qoff = qs.d_off;
+            t.rc = rs.d_bytes;
+            t.roff = rs.d_off;
+            t.N = N;
+            t.K = K;
+            t.dist = dist;
+            t.q_self = q_self;
+            t.r_self = r_self;
+            t.out = out_d;
+            launch_thread(ctx, t, tn, mode == ST_MODE_LOCAL, N * K, stream);
+        };
+        if (!wave_ok) {
+            run_thread();
+            return;
         }
-        for (auto& [R, off, cnt] : qp.groups) {
-            WaveArgs ma = wa;
-            ma.qc = qs.d_bytes;
-            ma.qoff = qs.d_off;
-            ma.rc = rs.d_bytes;
-            ma.roff = rs.d_off;
-            ma.qlist = static_cast<int32_t*>(qp.list.ptr) + off;
-            ma.nq = cnt;
-            ma.rpairs = static_cast<int2*>(rp.pairs.ptr);
-            ma.nrp = rp.npairs;
-            ma.dist = dist;
-            ma.q_self = q_self;
-            ma.r_self = r_self;
-            ma.out = out_d;
-            launch_wave(ctx, ma, R, local, exact, stream);
-        }
+        const std::string key = "align|" + std::to_string(mode) + "|" + std::to_string(dist) + "|" +
+                                std::to_string(A) + "|" + std::to_string(qs.max_len) + "|" +
+                                std::to_string(rs.max_len) + "|" + std::to_string(size_bucket(N)) +
+                                "|" + std::to_string(size_bucket(K));
+        tuned_run(key, 2, 0, [&](int c) {
+            if (c == 0) run_thread();
+            else align_wave(qs, rs, similarity, A, mode, go, ge, dist, out_d, ovf, stream);
+        }, stream);
+        return;
+    }
+    if (wave_ok) {
+        align_wave(qs, rs, similarity, A, mode, go, ge, dist, out_d, ovf, stream);
         return;
     }
 

@@ -126,3 +126,46 @@ def test_bad_arguments_raise(pw, B62):
     assert pw.score("", "", B62) == 0
     assert pw.score("", "AAA", B62) == -(11 + 2)
     assert pw.score("", "AAA", B62, mode="local") == 0
+
+
+@pytest.mark.parametrize("mode", ["global", "local"])
+@pytest.mark.parametrize("dist", [False, True])
+def test_short_pairs_thread_and_wavefront_paths(pw, B62, mode, dist):
+    """Junction-length sets (all <= 32) take the one-thread-per-pair kernel or the wavefront,
+    whichever the autotuner measured faster; the first call tunes (both run), the second runs
+    the cached choice.  Both calls are bit-exact against the oracle, empty strings included, as
+    are gap costs the int16 wavefront refuses (only the per-thread path takes those)."""
+    from seqtree_b200 import _lib
+    rng = np.random.default_rng(77 + dist + 2 * (mode == "local"))
+    q = rand_seqs(rng, 300, 1, 30) + [""]
+    r = rand_seqs(rng, 400, 1, 16) + ["", "W" * 32]
+    fn = pw.dist_matrix if dist else pw.score_matrix
+    want = oracle.align_matrix(q, r, B62.similarity_grid, mode=mode, dist=dist)
+    for _ in range(2):
+        got = as_np(fn(q, r, B62, mode=mode))
+        np.testing.assert_array_equal(got, want)
+    for go, ge in ((200, 30), (2000, 900)):
+        want = oracle.align_matrix(q[:60], r[:70], B62.similarity_grid, mode=mode, gap_open=go,
+                                   gap_extend=ge, dist=dist)
+        got = as_np(fn(q[:60], r[:70], B62, mode=mode, gap_open=go, gap_extend=ge))
+        np.testing.assert_array_equal(got, want)
+    assert "align|" in _lib.tuning_table() or os.environ.get("SEQTREE_B200_TUNE") == "0"
+
+
+def test_gapblock_chunk_width_is_tuned_and_exact(cuda_ready):
+    """The dense gap-block call times every chunk width once per shape and caches the fastest;
+    every variant gives the same matrix (checked against the oracle on both calls)."""
+    import seqtree_b200 as stb
+    from conftest import cdr3
+    from seqtree_b200 import _lib
+    rng = np.random.default_rng(5)
+    q, r = cdr3(rng, 257), cdr3(rng, 3001)
+    m = stb.SubstitutionMatrix.blosum62()
+    prior = stb.central_prior(21)
+    width = max(map(len, q + r))
+    want = oracle.gapblock_matrix(q, r, m.penalty_grid, gap_open=8,
+                                  prior=stb.gapblock.prior_cube(prior, width), prior_width=width)
+    for _ in range(2):
+        got = np.asarray(stb.score_matrix(q, r, m, gap_open=8, gap_prior=prior))
+        np.testing.assert_array_equal(got, want)
+    assert "gapblock|" in _lib.tuning_table() or os.environ.get("SEQTREE_B200_TUNE") == "0"
