@@ -196,6 +196,17 @@ int32_t st_gapblock_pairs_sets(st_seqset queries, st_seqset refs, const int32_t 
                                const int32_t *prior, int64_t prior_len, uint32_t prior_width,
                                int32_t *out_device, void *cuda_stream, st_error *err);
 
+/* The same pair scores plus, in pos_device[p], the position of the gap block that attains the
+ * minimum (the smallest such position, counted in residues of the shorter sequence; 0 for equal
+ * lengths): the (block_length, block_position) report of GapBlockIndex.search
+ * (python/seqtree/gapblock.py:607-661), where block_length is |m - n|. */
+int32_t st_gapblock_pairs_pos_sets(st_seqset queries, st_seqset refs, const int32_t *query_idx,
+                                   const int32_t *ref_idx, int64_t n, const int32_t *penalty,
+                                   int32_t matrix_size, int32_t gap_open, int32_t gap_extend,
+                                   const int32_t *prior, int64_t prior_len, uint32_t prior_width,
+                                   int32_t *out_device, int32_t *pos_device, void *cuda_stream,
+                                   st_error *err);
+
 /* ------------------------------------------------------------------------------------------
  * Sequence encoder of the learned-proposal path (no counterpart in the reference).  One-hot
  * amino-acid codes padded to 32 positions -> 2 conv layers -> 2 attention layers (width 128) ->

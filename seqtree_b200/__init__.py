@@ -4,7 +4,9 @@ dense matrix calls.
 * :mod:`seqtree_b200.gapblock` -- single-gap-block penalty matrix (``score_matrix``) and priors;
 * :mod:`seqtree_b200.pairwise` -- Gotoh Needleman-Wunsch / Smith-Waterman scores and distances;
 * :mod:`seqtree_b200.distance` -- Hamming and Levenshtein matrices;
-* :mod:`seqtree_b200.device` -- the same computations on device-resident sequence sets.
+* :mod:`seqtree_b200.device` -- the same computations on device-resident sequence sets;
+* :mod:`seqtree_b200.learned` -- learned candidate proposal + exact rescore for 1e6 x 1e6 searches;
+* ``GapBlockIndex`` -- thresholded gap-block search (the reference's index, on the GPU).
 
 Everything runs on the current CUDA device through ``libseqtree_b200.so``; there is no CPU
 fallback.  Results are bit-identical to seqtree 0.6.0's C++ on the same inputs.  The compiled
@@ -17,13 +19,13 @@ from .matrix import ScoreMatrix, SubstitutionMatrix, alphabet_symbols, amino_aci
 
 __version__ = "0.1.0"
 
-_MODULES = {"distance", "gapblock", "pairwise", "device", "shard", "_core", "_lib"}
-_FROM_GAPBLOCK = {"score_matrix", "central_prior", "frame_prior", "positions_prior",
-                  "profile_prior"}
+_MODULES = {"distance", "gapblock", "pairwise", "device", "shard", "learned", "_core", "_lib"}
+_FROM_GAPBLOCK = {"score_matrix", "score_sparse", "central_prior", "frame_prior",
+                  "positions_prior", "profile_prior", "GapBlockIndex"}
 
-__all__ = ["distance", "gapblock", "pairwise", "score_matrix", "central_prior", "frame_prior",
-           "positions_prior", "profile_prior", "ScoreMatrix", "SubstitutionMatrix",
-           "alphabet_symbols", "amino_acids"]
+__all__ = ["distance", "gapblock", "pairwise", "score_matrix", "score_sparse", "central_prior",
+           "frame_prior", "positions_prior", "profile_prior", "GapBlockIndex", "ScoreMatrix",
+           "SubstitutionMatrix", "alphabet_symbols", "amino_acids"]
 
 
 def __getattr__(name):

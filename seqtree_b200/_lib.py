@@ -75,6 +75,10 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, _i32p,
       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_int64, ctypes.c_uint32,
       ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_gapblock_pairs_pos_sets", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, _i32p,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_int64, ctypes.c_uint32,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
     ("st_encoder_param_count", ctypes.c_int64, []),
     ("st_encoder_create", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), _ep]),
     ("st_encoder_destroy", None, [ctypes.c_void_p]),

@@ -25,7 +25,7 @@ void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream
 void gapblock_pairs_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* qi_d, const int32_t* ri_d,
                          int64_t n, const int32_t* penalty, int32_t matrix_size, int32_t go,
                          int32_t ge, const int32_t* prior, int64_t prior_len, uint32_t prior_width,
-                         int32_t* out_d, cudaStream_t stream);
+                         int32_t* out_d, int32_t* pos_d, cudaStream_t stream);
 struct Encoder;
 int64_t encoder_param_count();
 Encoder* encoder_create(const float* params);
@@ -535,7 +535,26 @@ int32_t st_gapblock_pairs_sets(st_seqset queries, st_seqset refs, const int32_t*
         Context& ctx = context();
         std::lock_guard<std::mutex> lk(ctx.mu);
         gapblock_pairs_sets(*queries, *refs, query_idx, ref_idx, n, penalty, matrix_size, gap_open,
-                            gap_extend, prior, prior_len, prior_width, out_device,
+                            gap_extend, prior, prior_len, prior_width, out_device, nullptr,
+                            static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int32_t st_gapblock_pairs_pos_sets(st_seqset queries, st_seqset refs, const int32_t* query_idx,
+                                   const int32_t* ref_idx, int64_t n, const int32_t* penalty,
+                                   int32_t matrix_size, int32_t gap_open, int32_t gap_extend,
+                                   const int32_t* prior, int64_t prior_len, uint32_t prior_width,
+                                   int32_t* out_device, int32_t* pos_device, void* cuda_stream,
+                                   st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_set(queries);
+        check_set(refs);
+        if (!pos_device) fail(ST_EINVAL, "seqtree_b200: null position output");
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        gapblock_pairs_sets(*queries, *refs, query_idx, ref_idx, n, penalty, matrix_size, gap_open,
+                            gap_extend, prior, prior_len, prior_width, out_device, pos_device,
                             static_cast<cudaStream_t>(cuda_stream));
     });
 }

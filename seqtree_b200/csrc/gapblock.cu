@@ -485,10 +485,14 @@ struct GeneralArgs {
 
 // The gap-block score of one pair in int32 arithmetic with the reference's wrap
 // (src/gapblock.cpp:39-62, in the single-sweep form S + min_i(C_i + p_i)).
+// Score of one pair; with `pos`, also the block position of the minimum (the smallest such
+// position; 0 when the lengths are equal), counted in residues of the shorter sequence.
 __device__ __forceinline__ int32_t gapblock_cell(const uint8_t* q, int m, const uint8_t* r, int n,
                                                  const int32_t* s_pen, int A, int32_t go, int32_t ge,
-                                                 const int32_t* prior, int64_t pw1) {
+                                                 const int32_t* prior, int64_t pw1,
+                                                 int32_t* pos = nullptr) {
     const int L = min(m, n), d = abs(m - n);
+    if (pos) *pos = 0;
     if (d == 0) {
         uint32_t s = 0;
         for (int j = 0; j < L; ++j) s += uint32_t(s_pen[q[j] * A + r[j]]);
@@ -498,14 +502,19 @@ __device__ __forceinline__ int32_t gapblock_cell(const uint8_t* q, int m, const 
     const int32_t* prow = prior ? prior + (int64_t(max(m, n)) * pw1 + d) * pw1 : nullptr;
     int32_t S = 0, C = 0;
     int32_t best = prow ? prow[0] : 0;
+    int32_t at = 0;
     for (int j = 0; j < L; ++j) {
         const int32_t p0v = s_pen[q[j] * A + r[j]];
         const int32_t pdv = ql ? s_pen[q[j + d] * A + r[j]] : s_pen[q[j] * A + r[j + d]];
         S += pdv;
         C += p0v - pdv;
         const int32_t cand = C + (prow ? prow[j + 1] : 0);
-        best = cand < best ? cand : best;
+        if (cand < best) {
+            best = cand;
+            at = j + 1;
+        }
     }
+    if (pos) *pos = at;
     return int32_t(uint32_t(S) + uint32_t(best) + uint32_t(go) + uint32_t(d - 1) * uint32_t(ge));
 }
 
@@ -515,7 +524,8 @@ __global__ void __launch_bounds__(256) gapblock_pairs_kernel(
     const uint8_t* __restrict__ rcodes, const int64_t* __restrict__ roff,
     const int32_t* __restrict__ qi, const int32_t* __restrict__ ri, int64_t n,
     const int32_t* __restrict__ pen, int A, int32_t go, int32_t ge,
-    const int32_t* __restrict__ prior, int64_t pw1, int32_t* __restrict__ out) {
+    const int32_t* __restrict__ prior, int64_t pw1, int32_t* __restrict__ out,
+    int32_t* __restrict__ pos_out) {
     extern __shared__ int32_t s_pen[];
     for (int i = threadIdx.x; i < A * A; i += blockDim.x) s_pen[i] = pen[i];
     __syncthreads();
@@ -523,8 +533,10 @@ __global__ void __launch_bounds__(256) gapblock_pairs_kernel(
          p += int64_t(gridDim.x) * blockDim.x) {
         const int64_t i = qi[p], k = ri[p];
         const int m = int(qoff[i + 1] - qoff[i]), nn = int(roff[k + 1] - roff[k]);
+        int32_t at = 0;
         out[p] = gapblock_cell(qcodes + qoff[i], m, rcodes + roff[k], nn, s_pen, A, go, ge, prior,
-                               pw1);
+                               pw1, pos_out ? &at : nullptr);
+        if (pos_out) pos_out[p] = at;
     }
 }
 
@@ -919,7 +931,7 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
 void gapblock_pairs_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* qi_d, const int32_t* ri_d,
                          int64_t n, const int32_t* penalty, int32_t matrix_size, int32_t go,
                          int32_t ge, const int32_t* prior, int64_t prior_len, uint32_t prior_width,
-                         int32_t* out_d, cudaStream_t stream) {
+                         int32_t* out_d, int32_t* pos_d, cudaStream_t stream) {
     if (go < 0 || ge < 0) fail(ST_EINVAL, "gap_open and gap_extend must be >= 0");
     if (qs.alphabet < 0 || qs.alphabet != rs.alphabet)
         fail(ST_EINVAL, "seqtree_b200: gap-block sets must be encoded with one alphabet");
@@ -973,7 +985,7 @@ void gapblock_pairs_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* qi_d, 
     const int64_t blocks = std::min<int64_t>(ceil_div(n, 256), int64_t(ctx.num_sms) * 16);
     gapblock_pairs_kernel<<<unsigned(blocks), 256, size_t(A) * A * 4, stream>>>(
         qs.d_bytes, qs.d_off, rs.d_bytes, rs.d_off, qi_d, ri_d, n, d_pen, A, go, ge, d_prior, W1p,
-        out_d);
+        out_d, pos_d);
     STB_CUDA(cudaGetLastError());
     note_launch("gapblock_pairs_kernel");
 }

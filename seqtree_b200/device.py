@@ -144,3 +144,34 @@ def levenshtein_into(a: SeqSet, b: SeqSet, out_ptr: int, stream: int = 0) -> Non
     code = _lib.lib.st_levenshtein_matrix_sets(a.handle, b.handle, ctypes.c_void_p(out_ptr),
                                                ctypes.c_void_p(stream), ctypes.byref(err))
     _lib.check(code, err)
+
+
+class _DeviceArray:
+    """A borrowed device buffer exposed through ``__cuda_array_interface__`` (for torch views)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr,
+                                         "data": (ptr or 0, False), "version": 3, "strides": None}
+
+
+def hits_tensors(hits):
+    """(indptr int64, ref_ids int32, scores int32) torch copies of a device ``Hits``."""
+    import torch
+    info = hits.info()
+    rows, nnz = info["rows"], info["nnz"]
+
+    def view(ptr, n, ts, dt):
+        if n == 0:
+            return torch.zeros(0, dtype=dt, device="cuda")
+        return torch.as_tensor(_DeviceArray(ptr, n, ts), device="cuda").clone()
+
+    return (view(info["indptr"], rows + 1, "<i8", torch.int64),
+            view(info["ref_ids"], nnz, "<i4", torch.int32),
+            view(info["scores"], nnz, "<i4", torch.int32))
+
+
+def torch_rows(indptr):
+    """Row index of every CSR entry."""
+    import torch
+    n = indptr.numel() - 1
+    return torch.arange(n, device=indptr.device).repeat_interleave(indptr[1:] - indptr[:-1])

@@ -234,3 +234,109 @@ def score_sparse(queries: Sequence[str], refs: Sequence[str], max_penalty: int,
     indptr, ref_ids, scores = _gapblock_sparse(q, r, max_penalty, alphabet, matrix, gap_open,
                                               gap_extend, cube, width, threads)
     return SparseScores(indptr, ref_ids, scores, (len(q), len(r)), max_penalty)
+
+
+class GapBlockIndex:
+    """Thresholded single-gap-block search over a reference set, on the GPU.
+
+    The reference's ``GapBlockIndex`` (``python/seqtree/gapblock.py:567-673``) reaches refs of
+    length ``len(query) +- d`` for ``d <= d_max`` through Hamming searches over deletion
+    variants, and returns every ref within ``max_penalty`` with its best gap-block score.  That
+    score is the closed form of ``score_matrix`` (one block of ``|m - n|`` residues in the longer
+    sequence, prior only when ``d > 0``), so here a search is the exhaustive sparse kernel over
+    the batch (``score_sparse``), restricted to ``|m - n| <= d_max``, with the block position
+    taken from the exact pair kernel.  Build once, search many -- ``search_batch`` answers many
+    queries in one pass, which is where the GPU pays.
+
+    Results per query are ``(ref_id, score, block_length, block_position)`` sorted by ascending
+    score then ref id, as in the reference.  ``block_length`` is ``|len(query) - len(ref)|``;
+    ``block_position`` indexes the shorter sequence and, where several positions attain the
+    minimum, is the smallest (the reference reports the first position its traversal meets).
+    With ``max_penalty`` 0 only score-0 refs pass: identical sequences for matrices whose
+    penalties between different residues are positive (all the built-ins; the reference asks its
+    Hamming engine for zero substitutions in that case).
+    """
+
+    def __init__(self, refs: Iterable[str], alphabet: str = "aa", d_max: int = 1):
+        if d_max < 0:
+            raise ValueError("d_max must be >= 0")
+        from . import device
+        self.refs = list(refs)
+        self.d_max = d_max
+        self.alphabet = alphabet
+        self._set = device.SeqSet(self.refs, alphabet)
+        self._lens = np.fromiter(map(len, self.refs), np.int32, len(self.refs))
+
+    def __len__(self) -> int:
+        return len(self.refs)
+
+    def search(self, query: str, max_penalty: int, matrix: SubstitutionMatrix | None = None,
+               gap_open: int | None = None, gap_extend: int = 1,
+               gap_prior: GapPrior | None = None) -> list[tuple[int, int, int, int]]:
+        """All refs within ``max_penalty`` under the gap-block score (see the class docs)."""
+        return self.search_batch([query], max_penalty, matrix, gap_open, gap_extend, gap_prior)[0]
+
+    def search_batch(self, queries: Sequence[str], max_penalty: int,
+                     matrix: SubstitutionMatrix | None = None, gap_open: int | None = None,
+                     gap_extend: int = 1, gap_prior: GapPrior | None = None
+                     ) -> list[list[tuple[int, int, int, int]]]:
+        """``search`` for every query of the batch, in one GPU pass."""
+        import ctypes
+
+        import torch
+
+        from . import _lib, device
+        if gap_open is None:
+            gap_open = _default_gap_open(matrix)
+        if max_penalty < 0:
+            raise ValueError("max_penalty must be >= 0")
+        if gap_open < 0 or gap_extend < 0:
+            raise ValueError("gap_open and gap_extend must be >= 0")
+        q = list(queries)
+        if not q:
+            return []
+        if not self.refs:
+            return [[] for _ in q]
+        width = max(max(map(len, q)), int(self._lens.max()))
+        cube = np.asarray(prior_cube(gap_prior, width) if gap_prior is not None else [],
+                          dtype=np.int64).astype(np.int32).ravel()
+        qset = device.SeqSet(q, self.alphabet)
+        stream = torch.cuda.current_stream().cuda_stream
+        hits = device.Hits()
+        device.gapblock_sparse_into(qset, self._set, hits, stream, max_penalty=max_penalty,
+                                    matrix=matrix, gap_open=gap_open, gap_extend=gap_extend,
+                                    prior=cube, prior_width=width if cube.size else 0)
+        ip, rid, sc = device.hits_tensors(hits)
+        rows = device.torch_rows(ip)
+        qlen = torch.from_numpy(np.fromiter(map(len, q), np.int32, len(q))).cuda()
+        rlen = torch.from_numpy(self._lens).cuda()
+        d = (qlen[rows] - rlen[rid.long()]).abs()
+        keep = d <= self.d_max
+        rows, rid, sc, d = rows[keep], rid[keep], sc[keep], d[keep]
+        n = int(rows.numel())
+        pos = torch.empty(n, dtype=torch.int32, device="cuda")
+        if n:
+            qi = rows.to(torch.int32)
+            again = torch.empty(n, dtype=torch.int32, device="cuda")
+            pen = None if matrix is None else np.ascontiguousarray(matrix.penalty_grid, np.int32)
+            err = _lib.st_error()
+            _lib.check(_lib.lib.st_gapblock_pairs_pos_sets(
+                qset.handle, self._set.handle, ctypes.c_void_p(qi.data_ptr()),
+                ctypes.c_void_p(rid.data_ptr()), n, _lib.i32_ptr(pen),
+                0 if pen is None else pen.shape[0], gap_open, gap_extend,
+                _lib.i32_ptr(cube) if cube.size else None, int(cube.size),
+                width if cube.size else 0, ctypes.c_void_p(again.data_ptr()),
+                ctypes.c_void_p(pos.data_ptr()), ctypes.c_void_p(stream), ctypes.byref(err)), err)
+            if not torch.equal(again, sc):
+                raise RuntimeError("seqtree_b200: pair rescore disagrees with the sparse kernel")
+        # order: query, then score, then ref id (stable sorts, least significant key first)
+        order = torch.argsort(rid, stable=True)
+        order = order[torch.argsort(sc[order], stable=True)]
+        order = order[torch.argsort(rows[order], stable=True)]
+        rows, rid, sc, d, pos = (t[order].cpu().numpy() for t in (rows, rid, sc, d, pos))
+        bounds = np.searchsorted(rows, np.arange(len(q) + 1))
+        out = []
+        for a, b in zip(bounds[:-1], bounds[1:]):
+            out.append([(int(r), int(s), int(dd), int(p))
+                        for r, s, dd, p in zip(rid[a:b], sc[a:b], d[a:b], pos[a:b])])
+        return out

@@ -18,6 +18,7 @@ import ctypes
 import numpy as np
 
 from . import _lib
+from .device import hits_tensors as _hits_tensors, torch_rows
 from .matrix import SubstitutionMatrix
 
 AA24 = "ARNDCQEGHILKMFPSTWYVBZX*"
@@ -383,30 +384,6 @@ def train(enc: Encoder, n_pairs: int, *, seed: int, matrix, gap_open: int, gap_e
 
 
 # -------------------------------------------------------------------------- search ----------
-class _DeviceArray:
-    """A borrowed device buffer exposed through ``__cuda_array_interface__`` (for torch views)."""
-
-    def __init__(self, ptr: int, n: int, typestr: str):
-        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr,
-                                         "data": (ptr or 0, False), "version": 3, "strides": None}
-
-
-def _hits_tensors(hits):
-    """(indptr int64, ref_ids int32, scores int32) torch copies of a device ``Hits``."""
-    import torch
-    info = hits.info()
-    rows, nnz = info["rows"], info["nnz"]
-
-    def view(ptr, n, ts, dt):
-        if n == 0:
-            return torch.zeros(0, dtype=dt, device="cuda")
-        return torch.as_tensor(_DeviceArray(ptr, n, ts), device="cuda").clone()
-
-    return (view(info["indptr"], rows + 1, "<i8", torch.int64),
-            view(info["ref_ids"], nnz, "<i4", torch.int32),
-            view(info["scores"], nnz, "<i4", torch.int32))
-
-
 def _subset(codes, lens, rows):
     from .device import SeqSet
     return SeqSet(codes_to_packed(codes[rows], lens[rows]), "aa") if rows.size else None
@@ -662,10 +639,3 @@ class LearnedIndex:
                 "recall": r2["recall"], "found": r2["found"], "exact": r2["exact"],
                 "subset_of_exact": r2["subset_of_exact"], "exhaustive_share": share,
                 "cells_no_fallback": (r0["found_cells"], r0["exact_cells"])}
-
-
-def torch_rows(indptr):
-    """Row index of every CSR entry."""
-    import torch
-    n = indptr.numel() - 1
-    return torch.arange(n, device=indptr.device).repeat_interleave(indptr[1:] - indptr[:-1])
