@@ -248,6 +248,26 @@ int32_t st_propose_topk(const void *query_emb, int64_t nq, const void *ref_emb, 
                         int32_t k, int32_t *ids_device, float *scores_device, void *cuda_stream,
                         st_error *err);
 
+/* Per-row score cutoffs for a target E-value: thetas_from_scores of seqtree's
+ * python/seqtree/evalue.py:102-143 (with _theta, :86-99) over CSR rows of control hit scores in
+ * device memory (indptr_device rows + 1 int64, scores_device int32; row order within a row is
+ * free, e.g. the rows of st_gapblock_sparse_sets).  out_device[row] is the largest cutoff in
+ * [0, theta_max] whose control count stays <= floor(e_target * m_control / n_target), or -1
+ * (the reference's rules).  Errors as the reference: "n_target and m_control must be > 0",
+ * "e_target must be > 0", "theta_max must be >= 0" (ST_EINVAL). */
+int32_t st_thetas_csr(const int64_t *indptr_device, const int32_t *scores_device, int64_t rows,
+                      int64_t n_target, int64_t m_control, double e_target, int32_t theta_max,
+                      int32_t exclude_exact, int32_t *out_device, void *cuda_stream, st_error *err);
+
+/* IslandProfile.score_batch (seqtree python/seqtree/gapblock.py:365-377): the penalty of every
+ * sequence of a raw-byte device set (alphabet -1) in a profile's frame.  table is host
+ * int32 [width][256]: column j's penalty for each byte (the profile's cap for bytes it does not
+ * list); c is the frame column of the gap block and gap the gap byte.  A sequence longer than
+ * width, or shorter than c, scores `unreachable`.  out_device: int32 per sequence. */
+int32_t st_profile_scores_sets(const int32_t *table, int32_t width, int32_t c, uint8_t gap,
+                               int32_t unreachable, st_seqset set, int32_t *out_device,
+                               void *cuda_stream, st_error *err);
+
 /* Synchronises cuda_stream and reports (then clears) the device error words written by the
  * asynchronous *_sets and proposal calls since the last check: ST_ETIMEOUT when a bounded
  * device-side wait gave up. */

@@ -300,3 +300,47 @@ def ref_distance_matrix(a, b, levenshtein: bool, threads=0) -> np.ndarray:
     if st:
         _raise(st, err)
     return out
+
+
+# ----------------------------------------------------------------------------- E-value cutoffs
+def _theta(scores, k, c_max, theta_max):
+    """Port of seqtree python/seqtree/evalue.py:86-99 (_theta)."""
+    if k < 1:
+        return -1
+    theta = theta_max if len(scores) <= k else min(theta_max, scores[k] - 1)
+    if theta < 0:
+        return -1
+    n_control = sum(1 for s in scores if s <= theta)
+    if n_control == 0 and c_max < 3.0:
+        return -1
+    return theta
+
+
+def thetas_from_scores(control_scores, n_target, m_control, e_target, theta_max, *,
+                       exclude_exact=False):
+    """Port of seqtree python/seqtree/evalue.py:102-143 (thetas_from_scores)."""
+    if n_target <= 0 or m_control <= 0:
+        raise ValueError("n_target and m_control must be > 0")
+    if e_target <= 0.0:
+        raise ValueError("e_target must be > 0")
+    if theta_max < 0:
+        raise ValueError("theta_max must be >= 0")
+    c_max = e_target * m_control / n_target
+    k = int(c_max)
+    return [_theta(sorted(x for x in s if not (exclude_exact and x == 0)), k, c_max, theta_max)
+            for s in control_scores]
+
+
+# ----------------------------------------------------------------------------- island profiles
+PROFILE_UNREACHABLE = 1 << 20  # seqtree python/seqtree/gapblock.py:54
+
+
+def profile_score(penalties, width, c, seq, gap="-"):
+    """Port of IslandProfile.score (seqtree python/seqtree/gapblock.py:365-374) with
+    embed_in_frame (:186-205)."""
+    if len(seq) > width or c > len(seq):
+        return PROFILE_UNREACHABLE
+    d = width - len(seq)
+    emb = seq[:c] + gap * d + seq[c:]
+    cap = PROFILE_UNREACHABLE // (width + 1)
+    return sum(penalties[j].get(ch, cap) for j, ch in enumerate(emb))

@@ -19,12 +19,15 @@ from .matrix import ScoreMatrix, SubstitutionMatrix, alphabet_symbols, amino_aci
 
 __version__ = "0.1.0"
 
-_MODULES = {"distance", "gapblock", "pairwise", "device", "shard", "learned", "_core", "_lib"}
+_MODULES = {"distance", "gapblock", "pairwise", "device", "shard", "learned", "evalue", "_core",
+            "_lib"}
 _FROM_GAPBLOCK = {"score_matrix", "score_sparse", "central_prior", "frame_prior",
-                  "positions_prior", "profile_prior", "GapBlockIndex"}
+                  "positions_prior", "profile_prior", "GapBlockIndex", "IslandProfile",
+                  "embed_in_frame", "UNREACHABLE"}
 
 __all__ = ["distance", "gapblock", "pairwise", "score_matrix", "score_sparse", "central_prior",
-           "frame_prior", "positions_prior", "profile_prior", "GapBlockIndex", "ScoreMatrix",
+           "frame_prior", "positions_prior", "profile_prior", "GapBlockIndex", "IslandProfile",
+           "embed_in_frame", "UNREACHABLE", "evalue", "ScoreMatrix",
            "SubstitutionMatrix", "alphabet_symbols", "amino_acids"]
 
 

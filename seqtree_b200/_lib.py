@@ -95,6 +95,12 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
     ("st_stream_status", ctypes.c_int32, [ctypes.c_void_p, _ep]),
+    ("st_profile_scores_sets", ctypes.c_int32,
+     [_i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint8, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_thetas_csr", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+      ctypes.c_double, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, _ep]),
     ("st_seqset_create", ctypes.c_int32,
      [_sp, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p), _ep]),
     ("st_seqset_destroy", None, [ctypes.c_void_p]),

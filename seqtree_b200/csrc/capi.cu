@@ -4,6 +4,7 @@
 // fails with the same message: gap costs, alphabet, matrix size, empty shapes (no further
 // checks, as in the reference), symbol encoding (queries before refs), then per-family checks.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <memory>
 
@@ -38,6 +39,10 @@ float encoder_train_step(Encoder& m, const uint8_t* codes, const int32_t* lens, 
 void encoder_embed(Encoder& m, const st_seqset_s& set, void* out, int layout, cudaStream_t st);
 void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, int k, int32_t* ids,
                   float* scores, cudaStream_t stream);
+void profile_scores(const int32_t* table, int32_t width, int32_t c, uint8_t gap, int32_t unreachable,
+                    const st_seqset_s& set, int32_t* out_d, cudaStream_t stream);
+void thetas_csr(const int64_t* indptr_d, const int32_t* scores_d, int64_t rows, int32_t k, int rule3,
+                int32_t theta_max, int exclude_exact, int32_t* out_d, cudaStream_t stream);
 int last_launches();
 int64_t total_launches();
 std::string tuning_table();
@@ -656,6 +661,37 @@ int32_t st_propose_topk(const void* query_emb, int64_t nq, const void* ref_emb, 
         std::lock_guard<std::mutex> lk(ctx.mu);
         propose_topk(query_emb, nq, ref_emb, nr, k, ids_device, scores_device,
                      static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int32_t st_thetas_csr(const int64_t* indptr_device, const int32_t* scores_device, int64_t rows,
+                      int64_t n_target, int64_t m_control, double e_target, int32_t theta_max,
+                      int32_t exclude_exact, int32_t* out_device, void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        if (n_target <= 0 || m_control <= 0) fail(ST_EINVAL, "n_target and m_control must be > 0");
+        if (!(e_target > 0.0)) fail(ST_EINVAL, "e_target must be > 0");
+        if (theta_max < 0) fail(ST_EINVAL, "theta_max must be >= 0");
+        const double c_max = e_target * double(m_control) / double(n_target);
+        const double kd = std::floor(c_max);
+        const int32_t k = kd > 2147483647.0 ? 2147483647 : int32_t(kd);
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        thetas_csr(indptr_device, scores_device, rows, k, c_max < 3.0 ? 1 : 0, theta_max,
+                   exclude_exact, out_device, static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int32_t st_profile_scores_sets(const int32_t* table, int32_t width, int32_t c, uint8_t gap,
+                               int32_t unreachable, st_seqset set, int32_t* out_device,
+                               void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_set(set);
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        profile_scores(table, width, c, gap, unreachable, *set, out_device,
+                       static_cast<cudaStream_t>(cuda_stream));
     });
 }
 

@@ -340,3 +340,130 @@ class GapBlockIndex:
             out.append([(int(r), int(s), int(dd), int(p))
                         for r, s, dd, p in zip(rid[a:b], sc[a:b], d[a:b], pos[a:b])])
         return out
+
+
+# ------------------------------------------------------------------ island profiles --------
+UNREACHABLE = 1 << 20
+_AA = "ACDEFGHIKLMNPQRSTVWY"
+
+
+def embed_in_frame(seq: str, width: int, c: int, gap: str = "-") -> str:
+    """Place ``seq`` into a ``width``-column frame with its gap block at column ``c``: the first
+    ``c`` symbols, ``width - len(seq)`` gaps, then the rest (seqtree
+    ``python/seqtree/gapblock.py:186-205``; same errors)."""
+    d = width - len(seq)
+    if d < 0:
+        raise ValueError(f"sequence of length {len(seq)} does not fit a width-{width} frame")
+    if not 0 <= c <= len(seq):
+        raise ValueError(f"frame column {c} outside [0, {len(seq)}]")
+    return seq[:c] + gap * d + seq[c:]
+
+
+class IslandProfile:
+    """Column penalties over a frame -- seqtree's ``IslandProfile``
+    (``python/seqtree/gapblock.py:208-380``) with the same constructor, ``fit``, ``consensus``,
+    ``score`` and ``score_batch``.  Fitting is host statistics over an island's members (the
+    reference's arithmetic, so the integer penalties are identical); scoring runs on the GPU
+    (``st_profile_scores_sets``), one thread per sequence, and is meant for whole controls or
+    repertoires.  Penalties are ``round(lam * log(p_max_j / p_j(a)))``, zero on each column's
+    consensus symbol, capped so that a full-width score stays below :data:`UNREACHABLE`.
+    Sequences are taken as ASCII text (one byte per residue)."""
+
+    def __init__(self, penalties: list[dict[str, int]], width: int, c: int) -> None:
+        self.penalties = penalties
+        self.width = width
+        self.c = c
+
+    @classmethod
+    def fit(cls, members: Sequence[str], c: int | None = None, lam: int = 1000,
+            pseudocount: float = 0.5, gap: str = "-") -> "IslandProfile":
+        import collections
+        import math
+        members = list(members)
+        if not members:
+            raise ValueError("cannot fit a profile to an empty island")
+        if lam < 0:
+            raise ValueError("lam must be >= 0")
+        if pseudocount <= 0:
+            raise ValueError("pseudocount must be > 0")
+        width = max(len(s) for s in members)
+        shortest = min(len(s) for s in members)
+        if c is None:
+            c = min(range(shortest + 1), key=lambda k: cls._entropy(members, width, k, gap))
+        elif not 0 <= c <= shortest:
+            raise ValueError(f"frame column {c} outside [0, {shortest}]")
+        alpha = _AA + gap
+        cap = UNREACHABLE // (width + 1)
+        framed = [embed_in_frame(s, width, c, gap) for s in members]
+        penalties = []
+        for j in range(width):
+            counts = collections.Counter(f[j] for f in framed)
+            denom = sum(counts.values()) + pseudocount * len(alpha)
+            probs = {a: (counts.get(a, 0) + pseudocount) / denom for a in alpha}
+            p_max = max(probs.values())
+            penalties.append({a: min(cap, int(round(lam * math.log(p_max / p))))
+                              for a, p in probs.items()})
+        return cls(penalties, width, c)
+
+    @staticmethod
+    def _entropy(members: Sequence[str], width: int, c: int, gap: str) -> float:
+        import collections
+        import math
+        total = 0.0
+        framed = [embed_in_frame(s, width, c, gap) for s in members]
+        for j in range(width):
+            counts = collections.Counter(f[j] for f in framed)
+            n = sum(counts.values())
+            total -= sum((v / n) * math.log(v / n) for v in counts.values() if v)
+        return total
+
+    def consensus(self, gap: str = "-") -> str:
+        """The zero-penalty sequence: each column's cheapest symbol, gaps stripped."""
+        return "".join(min(col, key=col.get) for col in self.penalties).replace(gap, "")
+
+    def _table(self, gap: str) -> np.ndarray:
+        cap = UNREACHABLE // (self.width + 1)
+        t = np.full((max(self.width, 1), 256), cap, np.int32)
+        for j, col in enumerate(self.penalties):
+            for sym, v in col.items():
+                b = sym.encode()
+                if len(b) == 1:
+                    t[j, b[0]] = v
+        return t
+
+    def score(self, seq: str, gap: str = "-") -> int:
+        """Penalty of ``seq`` in this island's frame; :data:`UNREACHABLE` when it does not fit."""
+        return self.score_batch([seq], gap)[0]
+
+    def score_batch(self, seqs: Iterable[str], gap: str = "-") -> list[int]:
+        """:meth:`score` for many sequences, on the GPU."""
+        out = self.score_batch_np(seqs, gap)
+        return [int(x) for x in out]
+
+    def score_batch_np(self, seqs: Iterable[str], gap: str = "-") -> np.ndarray:
+        """:meth:`score_batch` as an int32 numpy array."""
+        import ctypes
+
+        import torch
+
+        from . import _lib, device
+        seqs = list(seqs)
+        g = gap.encode()
+        if len(g) != 1:
+            raise ValueError("gap must be a single ASCII symbol")
+        if not all(s.isascii() for s in seqs):
+            raise ValueError("profile scoring takes ASCII sequences")
+        if not seqs:
+            return np.zeros(0, np.int32)
+        table = np.ascontiguousarray(self._table(gap))
+        ss = device.SeqSet(seqs, None)
+        out = torch.empty(len(seqs), dtype=torch.int32, device="cuda")
+        err = _lib.st_error()
+        _lib.check(_lib.lib.st_profile_scores_sets(
+            _lib.i32_ptr(table), int(self.width), int(self.c), g[0], UNREACHABLE, ss.handle,
+            ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(torch.cuda.current_stream().cuda_stream),
+            ctypes.byref(err)), err)
+        return out.cpu().numpy()
+
+    def __repr__(self) -> str:
+        return f"IslandProfile(width={self.width}, c={self.c})"
