@@ -268,6 +268,23 @@ int32_t st_profile_scores_sets(const int32_t *table, int32_t width, int32_t c, u
                                int32_t unreachable, st_seqset set, int32_t *out_device,
                                void *cuda_stream, st_error *err);
 
+/* Alignments with traceback of listed pairs: seqtree::align_pair (include/seqtree/seqtree.hpp:
+ * 190-192, src/pairwise.cpp:141-267) for pair p = (queries[query_idx[p]], refs[ref_idx[p]]),
+ * e.g. the top hits of a sparse search.  All outputs are device memory: score_device[p] (int64;
+ * the reference refuses a score beyond int32 with std::overflow_error, which the caller
+ * reports), and in slot p of slot_bytes bytes (>= longest query + longest ref) of each of
+ * aligned_query_device / aligned_ref_device / ops_device the alignment, occupying
+ * [start_device[p], slot_bytes).  start_device[p] == -1 marks a pair with an empty side, whose
+ * strings are the raw inputs (global mode) or empty (local mode) as in the reference.  Ops:
+ * 'M' match, 'S' substitution, 'D' gap in the ref, 'I' gap in the query.  Exact for any gap
+ * cost (int64 cells); ties resolve as the reference. */
+int32_t st_align_pairs_sets(st_seqset queries, st_seqset refs, const int32_t *query_idx,
+                            const int32_t *ref_idx, int64_t n, const int32_t *similarity,
+                            int32_t matrix_size, int32_t mode, int32_t gap_open, int32_t gap_extend,
+                            int64_t *score_device, int32_t *start_device, char *aligned_query_device,
+                            char *aligned_ref_device, char *ops_device, int64_t slot_bytes,
+                            void *cuda_stream, st_error *err);
+
 /* Synchronises cuda_stream and reports (then clears) the device error words written by the
  * asynchronous *_sets and proposal calls since the last check: ST_ETIMEOUT when a bounded
  * device-side wait gave up. */

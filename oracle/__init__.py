@@ -193,6 +193,11 @@ def ref():
             ctypes.c_char_p, ctypes.c_int64, ctypes.c_char_p, ctypes.c_int64, ctypes.c_int,
             ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
             _i32p, ctypes.c_char_p, ctypes.c_int]
+        lib.ref_align_pair.argtypes = [
+            ctypes.c_char_p, ctypes.c_int64, ctypes.c_char_p, ctypes.c_int64, ctypes.c_int,
+            ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
+            _i32p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int64,
+            ctypes.c_char_p, ctypes.c_int]
         lib.ref_distance_matrix.argtypes = [
             ctypes.c_char_p, _i64p, ctypes.c_int64, ctypes.c_char_p, _i64p, ctypes.c_int64,
             ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_char_p, ctypes.c_int]
@@ -287,6 +292,23 @@ def ref_align_score(q, r, matrix="blosum62", mode="global", gap_open=11, gap_ext
     if st:
         _raise(st, err)
     return out.value
+
+
+def ref_align_pair(q, r, matrix="blosum62", mode="global", gap_open=11, gap_extend=1,
+                   alphabet="aa") -> tuple[int, str, str, str]:
+    """The reference's align_pair: (score, aligned_query, aligned_ref, ops)."""
+    mid, simp, size, _keep = _matrix_args(matrix)
+    cap = len(q) + len(r) + 2
+    out = ctypes.c_int32(0)
+    bufs = [ctypes.create_string_buffer(cap) for _ in range(3)]
+    err = ctypes.create_string_buffer(512)
+    qb, rb = q.encode("latin-1"), r.encode("latin-1")
+    st = ref().ref_align_pair(qb, len(qb), rb, len(rb), ALPHABETS[alphabet], mid, simp, size,
+                              int(mode == "local"), gap_open, gap_extend, ctypes.byref(out),
+                              bufs[0], bufs[1], bufs[2], cap, err, 512)
+    if st:
+        _raise(st, err)
+    return (out.value,) + tuple(b.value.decode("latin-1") for b in bufs)
 
 
 def ref_distance_matrix(a, b, levenshtein: bool, threads=0) -> np.ndarray:

@@ -11,7 +11,9 @@
 // and copies the exception text into `err`.
 #include "seqtree/seqtree.hpp"
 
+#include <algorithm>
 #include <cstdint>
+#include <utility>
 #include <cstring>
 #include <optional>
 #include <stdexcept>
@@ -134,6 +136,29 @@ int ref_align_score(const char* q, int64_t m, const char* r, int64_t n, int alph
         *out = align_score(std::string_view(q, size_t(m)), std::string_view(r, size_t(n)), *mat,
                            Alphabet(alphabet), local ? AlignMode::Local : AlignMode::Global,
                            gap_open, gap_extend);
+    });
+}
+
+// seqtree::align_pair (seqtree.hpp:190-192, src/pairwise.cpp:141-267): score plus the aligned
+// strings and ops, each written NUL-terminated into a caller buffer of `cap` bytes.
+int ref_align_pair(const char* q, int64_t m, const char* r, int64_t n, int alphabet, int matrix_id,
+                   const int32_t* sim, int size, int local, int32_t gap_open, int32_t gap_extend,
+                   int32_t* score, char* aq, char* ar, char* ops, int64_t cap, char* err,
+                   int errlen) {
+    return guard(err, errlen, [&] {
+        auto mat = make(matrix_id, sim, size);
+        if (!mat) throw std::invalid_argument("bad matrix id");
+        const Alignment al = align_pair(std::string_view(q, size_t(m)), std::string_view(r, size_t(n)),
+                                        *mat, Alphabet(alphabet),
+                                        local ? AlignMode::Local : AlignMode::Global, gap_open,
+                                        gap_extend);
+        *score = al.score;
+        for (auto [dst, src] : {std::pair<char*, const std::string*>{aq, &al.aligned_query},
+                                {ar, &al.aligned_ref}, {ops, &al.ops}}) {
+            const size_t len = std::min(src->size(), size_t(cap - 1));
+            std::memcpy(dst, src->data(), len);
+            dst[len] = 0;
+        }
     });
 }
 

@@ -95,6 +95,11 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
     ("st_stream_status", ctypes.c_int32, [ctypes.c_void_p, _ep]),
+    ("st_align_pairs_sets", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, _i32p,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+      ctypes.c_void_p, _ep]),
     ("st_profile_scores_sets", ctypes.c_int32,
      [_i32p, ctypes.c_int32, ctypes.c_int32, ctypes.c_uint8, ctypes.c_int32, ctypes.c_void_p,
       ctypes.c_void_p, ctypes.c_void_p, _ep]),

@@ -41,6 +41,10 @@ void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, in
                   float* scores, cudaStream_t stream);
 void profile_scores(const int32_t* table, int32_t width, int32_t c, uint8_t gap, int32_t unreachable,
                     const st_seqset_s& set, int32_t* out_d, cudaStream_t stream);
+void align_pairs_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* qi_d, const int32_t* ri_d,
+                      int64_t n, const int32_t* similarity, int32_t matrix_size, int32_t mode,
+                      int32_t go, int32_t ge, int64_t* score_d, int32_t* start_d, char* qa_d,
+                      char* ra_d, char* ops_d, int64_t out_cap, cudaStream_t stream);
 void thetas_csr(const int64_t* indptr_d, const int32_t* scores_d, int64_t rows, int32_t k, int rule3,
                 int32_t theta_max, int exclude_exact, int32_t* out_d, cudaStream_t stream);
 int last_launches();
@@ -692,6 +696,25 @@ int32_t st_profile_scores_sets(const int32_t* table, int32_t width, int32_t c, u
         std::lock_guard<std::mutex> lk(ctx.mu);
         profile_scores(table, width, c, gap, unreachable, *set, out_device,
                        static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int32_t st_align_pairs_sets(st_seqset queries, st_seqset refs, const int32_t* query_idx,
+                            const int32_t* ref_idx, int64_t n, const int32_t* similarity,
+                            int32_t matrix_size, int32_t mode, int32_t gap_open, int32_t gap_extend,
+                            int64_t* score_device, int32_t* start_device, char* aligned_query_device,
+                            char* aligned_ref_device, char* ops_device, int64_t slot_bytes,
+                            void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_set(queries);
+        check_set(refs);
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        align_pairs_sets(*queries, *refs, query_idx, ref_idx, n, similarity, matrix_size, mode,
+                         gap_open, gap_extend, score_device, start_device, aligned_query_device,
+                         aligned_ref_device, ops_device, slot_bytes,
+                         static_cast<cudaStream_t>(cuda_stream));
     });
 }
 

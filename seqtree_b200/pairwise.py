@@ -10,12 +10,19 @@ from __future__ import annotations
 
 from collections.abc import Sequence
 
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._core import _i32
 from ._core import align_dist_matrix as _dist_matrix
 from ._core import align_score as _align_score
 from ._core import align_score_matrix as _score_matrix
-from .matrix import ScoreMatrix, SubstitutionMatrix
+from .matrix import ScoreMatrix, SubstitutionMatrix, alphabet_symbols, parse_align_mode, parse_alphabet
 
-__all__ = ["score", "score_matrix", "dist_matrix"]
+__all__ = ["score", "align", "align_batch", "align_pairs", "Alignment", "score_matrix",
+           "dist_matrix"]
 
 
 def score(query: str, ref: str, matrix: SubstitutionMatrix, mode: str = "global",
@@ -39,3 +46,101 @@ def dist_matrix(queries: Sequence[str], refs: Sequence[str], matrix: Substitutio
     """Alignment distances ``d(a, b) = s(a,a) + s(b,b) - 2 s(a,b)``; zero on the diagonal."""
     return _dist_matrix(list(queries), list(refs), matrix, mode=mode, gap_open=gap_open,
                         gap_extend=gap_extend, alphabet=alphabet, threads=threads)
+
+
+class Alignment:
+    """An optimal alignment (seqtree's ``Alignment``, ``include/seqtree/types.hpp:67-72``):
+    ``aligned_query`` / ``aligned_ref`` with ``-`` for gaps, ``ops`` per column ('M' match,
+    'S' substitution, 'D' gap in the ref, 'I' gap in the query) and the similarity ``score``."""
+
+    __slots__ = ("aligned_query", "aligned_ref", "ops", "score")
+
+    def __init__(self, aligned_query: str, aligned_ref: str, ops: str, score: int):
+        self.aligned_query, self.aligned_ref, self.ops, self.score = aligned_query, aligned_ref, ops, score
+
+    def __repr__(self) -> str:
+        return f"Alignment(score={self.score}, ops='{self.ops}')"
+
+
+def align(query: str, ref: str, matrix: SubstitutionMatrix, mode: str = "global",
+          gap_open: int = 11, gap_extend: int = 1, alphabet: str = "aa") -> Alignment:
+    """As :func:`score`, but also returns the aligned strings and the edit ops (seqtree's
+    ``pairwise.align`` / ``align_pair``, ``src/pairwise.cpp:141-267``).  In local mode the aligned
+    strings are the matched sub-sequences only."""
+    return align_pairs([query], [ref], [0], [0], matrix, mode, gap_open, gap_extend, alphabet)[0]
+
+
+def align_batch(queries: Sequence[str], refs: Sequence[str], matrix: SubstitutionMatrix,
+                mode: str = "global", gap_open: int = 11, gap_extend: int = 1,
+                alphabet: str = "aa") -> list[Alignment]:
+    """``align(queries[p], refs[p])`` for every p, in one GPU launch."""
+    q, r = list(queries), list(refs)
+    if len(q) != len(r):
+        raise ValueError("queries and refs must pair up (equal lengths)")
+    idx = np.arange(len(q), dtype=np.int32)
+    return align_pairs(q, r, idx, idx, matrix, mode, gap_open, gap_extend, alphabet)
+
+
+def align_pairs(queries: Sequence[str], refs: Sequence[str], query_idx, ref_idx,
+                matrix: SubstitutionMatrix, mode: str = "global", gap_open: int = 11,
+                gap_extend: int = 1, alphabet: str = "aa") -> list[Alignment]:
+    """Alignments of the listed pairs ``(queries[query_idx[p]], refs[ref_idx[p]])`` -- e.g. the
+    hits of a sparse search -- one thread per pair on the GPU, exact for any gap cost."""
+    import torch
+
+    from .device import SeqSet
+    if not isinstance(matrix, SubstitutionMatrix):
+        raise TypeError("matrix must be a SubstitutionMatrix")
+    alph = parse_alphabet(alphabet)
+    md = parse_align_mode(mode)
+    go, ge = _i32("gap_open", gap_open), _i32("gap_extend", gap_extend)
+    if go < 0 or ge < 0:
+        raise ValueError("seqtree: gap_open and gap_extend must be >= 0 (they are magnitudes, and "
+                         "are subtracted)")
+    sim = np.ascontiguousarray(matrix.similarity_grid, np.int32)
+    if sim.shape[0] != len(alphabet_symbols(alphabet)):
+        raise ValueError("matrix size does not match the alphabet")
+    q, r = list(queries), list(refs)
+    qi = np.ascontiguousarray(query_idx, np.int32).ravel()
+    ri = np.ascontiguousarray(ref_idx, np.int32).ravel()
+    if qi.size != ri.size:
+        raise ValueError("query_idx and ref_idx must have the same length")
+    n = int(qi.size)
+    if n == 0:
+        return []
+    if qi.min() < 0 or qi.max() >= len(q) or ri.min() < 0 or ri.max() >= len(r):
+        raise IndexError("pair index out of range")
+    qs, rs = SeqSet(q, alphabet), SeqSet(r, alphabet)
+    slot = max(max(map(len, q)) + max(map(len, r)), 1)
+    dev = "cuda"
+    tq, tr = torch.from_numpy(qi).to(dev), torch.from_numpy(ri).to(dev)
+    score = torch.empty(n, dtype=torch.int64, device=dev)
+    start = torch.empty(n, dtype=torch.int32, device=dev)
+    bufs = [torch.empty(n * slot, dtype=torch.uint8, device=dev) for _ in range(3)]
+    err = _lib.st_error()
+    _lib.check(_lib.lib.st_align_pairs_sets(
+        qs.handle, rs.handle, ctypes.c_void_p(tq.data_ptr()), ctypes.c_void_p(tr.data_ptr()), n,
+        _lib.i32_ptr(sim), sim.shape[0], md, go, ge, ctypes.c_void_p(score.data_ptr()),
+        ctypes.c_void_p(start.data_ptr()), ctypes.c_void_p(bufs[0].data_ptr()),
+        ctypes.c_void_p(bufs[1].data_ptr()), ctypes.c_void_p(bufs[2].data_ptr()), slot,
+        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream), ctypes.byref(err)), err)
+    sc, st = score.cpu().numpy(), start.cpu().numpy()
+    if sc.size and (sc.max() > 2**31 - 1 or sc.min() < -2**31):
+        raise OverflowError("seqtree: the alignment score does not fit in 32 bits -- the gap costs "
+                            "are absurdly large for these sequences")
+    qa, ra, ops = (b.cpu().numpy().reshape(n, slot) for b in bufs)
+    local = md == 1
+    out = []
+    for p in range(n):
+        s = int(st[p])
+        if s < 0:  # an empty side: the reference writes the raw input (global) or nothing (local)
+            a, b = q[qi[p]], r[ri[p]]
+            if local:
+                out.append(Alignment("", "", "", int(sc[p])))
+            else:
+                out.append(Alignment(a + "-" * len(b), "-" * len(a) + b,
+                                     "D" * len(a) + "I" * len(b), int(sc[p])))
+            continue
+        out.append(Alignment(qa[p, s:].tobytes().decode(), ra[p, s:].tobytes().decode(),
+                             ops[p, s:].tobytes().decode(), int(sc[p])))
+    return out
