@@ -92,6 +92,19 @@ int32_t st_align_score_matrix(const st_strings *queries, const st_strings *refs,
                               int32_t threads, int32_t *out, st_error *err);
 
 /*
+ * Optimal alignment of one pair with its traceback.
+ * Replaces seqtree::align_pair (include/seqtree/seqtree.hpp:190-192, src/pairwise.cpp:141-267)
+ * and _core.align_pair (src/_bindings.cpp:515-525).  Host buffers: aligned_query, aligned_ref and
+ * ops receive NUL-terminated strings and must hold query_len + ref_len + 1 bytes; ops per
+ * column: 'M' match, 'S' substitution, 'D' gap in the ref, 'I' gap in the query.  Same checks,
+ * messages and tie order as the reference; ST_EOVERFLOW when the score does not fit int32.
+ */
+int32_t st_align_pair(const char *query, int64_t query_len, const char *ref, int64_t ref_len,
+                      const int32_t *similarity, int32_t matrix_size, int32_t alphabet, int32_t mode,
+                      int32_t gap_open, int32_t gap_extend, int32_t *score, char *aligned_query,
+                      char *aligned_ref, char *ops, int64_t capacity, st_error *err);
+
+/*
  * Dense sequence-level Gram distance d = s(a,a) + s(b,b) - 2 s(a,b) over Gotoh scores.
  * Replaces seqtree::align_dist_matrix (include/seqtree/seqtree.hpp:206-209,
  * src/pairwise.cpp:346-352) and _core.align_dist_matrix (src/_bindings.cpp:548-568).

@@ -182,6 +182,34 @@ inline int32_t align_score(std::string_view query, std::string_view ref,
                               gap_open, gap_extend)[0];
 }
 
+// An alignment with its traceback.  seqtree::Alignment (include/seqtree/types.hpp:67-72).
+struct Alignment {
+    std::string aligned_query;
+    std::string aligned_ref;
+    std::string ops;  // per column: 'M' match, 'S' substitution, 'I' insertion, 'D' deletion
+    int32_t score = 0;
+};
+
+// Optimal score plus the aligned strings and ops.  seqtree::align_pair
+// (include/seqtree/seqtree.hpp:190-192): one traceback launch on the GPU; for many pairs use
+// the batched st_align_pairs_sets.
+inline Alignment align_pair(std::string_view query, std::string_view ref, const SubstitutionMatrix& m,
+                            Alphabet alphabet, AlignMode mode, int32_t gap_open, int32_t gap_extend) {
+    const size_t cap = query.size() + ref.size() + 1;
+    std::string aq(cap, '\0'), ar(cap, '\0'), ops(cap, '\0');
+    Alignment al;
+    st_error err{};
+    detail::check(st_align_pair(query.data(), int64_t(query.size()), ref.data(),
+                                int64_t(ref.size()), m.similarity_data(), m.size(), int32_t(alphabet),
+                                int32_t(mode), gap_open, gap_extend, &al.score, aq.data(),
+                                ar.data(), ops.data(), int64_t(cap), &err),
+                  err);
+    al.aligned_query = aq.c_str();
+    al.aligned_ref = ar.c_str();
+    al.ops = ops.c_str();
+    return al;
+}
+
 // Dense N*K single-gap-block penalty matrix.  seqtree::gapblock_matrix
 // (include/seqtree/seqtree.hpp:215-222).  `matrix` null means unit cost; `prior` is the
 // [m][d][i] cube with stride prior_width + 1, or empty for none.

@@ -154,3 +154,40 @@ def hamming(a: str, b: str) -> int:
 def levenshtein(a: str, b: str) -> int:
     """Unit-cost edit distance; case-sensitive."""
     return levenshtein_matrix([a], [b])[0, 0]
+
+
+class Alignment:
+    """An optimal alignment (seqtree's ``Alignment``, ``include/seqtree/types.hpp:67-72``):
+    ``aligned_query`` / ``aligned_ref`` with ``-`` for gaps, ``ops`` per column ('M' match,
+    'S' substitution, 'D' gap in the ref, 'I' gap in the query) and the similarity ``score``."""
+
+    __slots__ = ("aligned_query", "aligned_ref", "ops", "score")
+
+    def __init__(self, aligned_query: str, aligned_ref: str, ops: str, score: int):
+        self.aligned_query, self.aligned_ref, self.ops, self.score = aligned_query, aligned_ref, ops, score
+
+    def __repr__(self) -> str:
+        return f"Alignment(score={self.score}, ops='{self.ops}')"
+
+
+def align_pair(query: str, ref: str, matrix: SubstitutionMatrix, mode: str = "global",
+               gap_open: int = 11, gap_extend: int = 1, alphabet: str = "aa") -> Alignment:
+    """Optimal alignment of one pair with its traceback (``_core.align_pair``,
+    src/_bindings.cpp:515-525), GIL released."""
+    if not isinstance(matrix, SubstitutionMatrix):
+        raise TypeError("matrix must be a SubstitutionMatrix")
+    alph = parse_alphabet(alphabet)
+    md = parse_align_mode(mode)
+    qb, rb = query.encode("utf-8"), ref.encode("utf-8")
+    sim = np.ascontiguousarray(matrix.similarity_grid, np.int32)
+    cap = len(qb) + len(rb) + 1
+    bufs = [ctypes.create_string_buffer(cap) for _ in range(3)]
+    score = ctypes.c_int32(0)
+    err = _lib.st_error()
+    code = _lib.lib.st_align_pair(qb, len(qb), rb, len(rb), _lib.i32_ptr(sim), sim.shape[0], alph,
+                                  md, _i32("gap_open", gap_open), _i32("gap_extend", gap_extend),
+                                  ctypes.byref(score), bufs[0], bufs[1], bufs[2], cap,
+                                  ctypes.byref(err))
+    _lib.check(code, err)
+    aq, ar, ops = (b.value.decode("utf-8") for b in bufs)
+    return Alignment(aq, ar, ops, int(score.value))

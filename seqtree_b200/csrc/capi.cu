@@ -4,9 +4,12 @@
 // fails with the same message: gap costs, alphabet, matrix size, empty shapes (no further
 // checks, as in the reference), symbol encoding (queries before refs), then per-family checks.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <string>
+#include <vector>
 
 #include "common.cuh"
 
@@ -346,6 +349,76 @@ static int32_t align_common(const st_strings* queries, const st_strings* refs,
             fail(ST_EOVERFLOW, std::string("seqtree: the alignment ") + (dist ? "distance" : "score") +
                                    " does not fit in 32 bits -- the gap costs are absurdly large "
                                    "for these sequences");
+    });
+}
+
+int32_t st_align_pair(const char* query, int64_t query_len, const char* ref, int64_t ref_len,
+                      const int32_t* similarity, int32_t matrix_size, int32_t alphabet, int32_t mode,
+                      int32_t gap_open, int32_t gap_extend, int32_t* score, char* aligned_query,
+                      char* aligned_ref, char* ops, int64_t capacity, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        // src/pairwise.cpp:141-146: check(), then encode the query, then the ref.
+        if (gap_open < 0 || gap_extend < 0)
+            fail(ST_EINVAL, "seqtree: gap_open and gap_extend must be >= 0 (they are magnitudes, "
+                            "and are subtracted)");
+        const int A = alphabet_size(alphabet);
+        if (A == 0) fail(ST_EINVAL, "unknown alphabet code " + std::to_string(alphabet));
+        if (!similarity || matrix_size != A) fail(ST_EINVAL, "matrix size does not match the alphabet");
+        if (mode != ST_MODE_GLOBAL && mode != ST_MODE_LOCAL)
+            fail(ST_EINVAL, "unknown mode (use 'global' or 'local')");
+        if (query_len < 0 || ref_len < 0 || (query_len && !query) || (ref_len && !ref))
+            fail(ST_EINVAL, "seqtree_b200: bad sequence buffer");
+        if (!score || !aligned_query || !aligned_ref || !ops || capacity < query_len + ref_len + 1)
+            fail(ST_EINVAL, "seqtree_b200: output buffers need query_len + ref_len + 1 bytes");
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        const int64_t qo[2] = {0, query_len}, ro[2] = {0, ref_len};
+        const st_strings qs{query, qo, 1}, rs{ref, ro, 1};
+        Transient t;
+        int64_t bad = -1;
+        char bc = 0;
+        t.q.reset(make_seqset(&qs, alphabet, ctx.stream, &bad, &bc, ctx.tq));
+        if (bad >= 0) fail(ST_EINVAL, std::string("invalid symbol '") + bc + "' in sequence");
+        t.r.reset(make_seqset(&rs, alphabet, ctx.stream, &bad, &bc, ctx.tr));
+        if (bad >= 0) fail(ST_EINVAL, std::string("invalid symbol '") + bc + "' in sequence");
+        const int64_t slot = std::max<int64_t>(query_len + ref_len, 1);
+        // device scratch: pair indices, score, start, three string slots
+        auto* base = static_cast<uint8_t*>(ctx.work_b.get(size_t(64 + 3 * slot)));
+        auto* idx = reinterpret_cast<int32_t*>(base);
+        auto* sc = reinterpret_cast<int64_t*>(base + 16);
+        auto* st = reinterpret_cast<int32_t*>(base + 24);
+        char* strs = reinterpret_cast<char*>(base + 64);
+        STB_CUDA(cudaMemsetAsync(idx, 0, 8, ctx.stream));
+        align_pairs_sets(*t.q, *t.r, idx, idx + 1, 1, similarity, matrix_size, mode, gap_open,
+                         gap_extend, sc, st, strs, strs + slot, strs + 2 * slot, slot, ctx.stream);
+        std::vector<uint8_t> host(size_t(64 + 3 * slot));
+        STB_CUDA(cudaMemcpyAsync(host.data(), base, host.size(), cudaMemcpyDeviceToHost, ctx.stream));
+        STB_CUDA(cudaStreamSynchronize(ctx.stream));
+        int64_t s64;
+        int32_t start;
+        std::memcpy(&s64, host.data() + 16, 8);
+        std::memcpy(&start, host.data() + 24, 4);
+        if (s64 > INT32_MAX || s64 < INT32_MIN)
+            fail(ST_EOVERFLOW, "seqtree: the alignment score does not fit in 32 bits -- the gap "
+                               "costs are absurdly large for these sequences");
+        *score = int32_t(s64);
+        std::string aq, ar, op;
+        if (start < 0) {  // an empty side: raw input in global mode, nothing in local mode
+            if (mode == ST_MODE_GLOBAL) {
+                aq = std::string(query ? query : "", size_t(query_len)) + std::string(size_t(ref_len), '-');
+                ar = std::string(size_t(query_len), '-') + std::string(ref ? ref : "", size_t(ref_len));
+                op = std::string(size_t(query_len), 'D') + std::string(size_t(ref_len), 'I');
+            }
+        } else {
+            const char* h = reinterpret_cast<const char*>(host.data() + 64);
+            aq.assign(h + start, size_t(slot - start));
+            ar.assign(h + slot + start, size_t(slot - start));
+            op.assign(h + 2 * slot + start, size_t(slot - start));
+        }
+        std::memcpy(aligned_query, aq.c_str(), aq.size() + 1);
+        std::memcpy(aligned_ref, ar.c_str(), ar.size() + 1);
+        std::memcpy(ops, op.c_str(), op.size() + 1);
     });
 }
 

@@ -15,7 +15,8 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._core import _i32
+from ._core import Alignment, _i32
+from ._core import align_pair as _align_pair
 from ._core import align_dist_matrix as _dist_matrix
 from ._core import align_score as _align_score
 from ._core import align_score_matrix as _score_matrix
@@ -48,26 +49,13 @@ def dist_matrix(queries: Sequence[str], refs: Sequence[str], matrix: Substitutio
                         gap_extend=gap_extend, alphabet=alphabet, threads=threads)
 
 
-class Alignment:
-    """An optimal alignment (seqtree's ``Alignment``, ``include/seqtree/types.hpp:67-72``):
-    ``aligned_query`` / ``aligned_ref`` with ``-`` for gaps, ``ops`` per column ('M' match,
-    'S' substitution, 'D' gap in the ref, 'I' gap in the query) and the similarity ``score``."""
-
-    __slots__ = ("aligned_query", "aligned_ref", "ops", "score")
-
-    def __init__(self, aligned_query: str, aligned_ref: str, ops: str, score: int):
-        self.aligned_query, self.aligned_ref, self.ops, self.score = aligned_query, aligned_ref, ops, score
-
-    def __repr__(self) -> str:
-        return f"Alignment(score={self.score}, ops='{self.ops}')"
-
-
 def align(query: str, ref: str, matrix: SubstitutionMatrix, mode: str = "global",
           gap_open: int = 11, gap_extend: int = 1, alphabet: str = "aa") -> Alignment:
     """As :func:`score`, but also returns the aligned strings and the edit ops (seqtree's
     ``pairwise.align`` / ``align_pair``, ``src/pairwise.cpp:141-267``).  In local mode the aligned
     strings are the matched sub-sequences only."""
-    return align_pairs([query], [ref], [0], [0], matrix, mode, gap_open, gap_extend, alphabet)[0]
+    return _align_pair(query, ref, matrix, mode=mode, gap_open=gap_open, gap_extend=gap_extend,
+                       alphabet=alphabet)
 
 
 def align_batch(queries: Sequence[str], refs: Sequence[str], matrix: SubstitutionMatrix,

@@ -8,6 +8,7 @@
 //                        H h / h lines     equal-length strings for the Hamming call
 //                        P width len / one line of len ints   the gap-prior cube
 //                      output lines are "<call> v0 v1 ..." or "<call> !<exception>: <what>".
+#include <algorithm>
 #include <iostream>
 #include <sstream>
 #include <string>
@@ -115,6 +116,26 @@ int main(int argc, char** argv) {
     call("align_overflow", [&] {
         return st::align_score_matrix({"AAAA"}, {"AAAAAAAA"}, b62, AA, st::AlignMode::Global,
                                       1500000000, 1500000000);
+    });
+    // align_pair: "alignpair <i> <mode> <score> <aligned_query> <aligned_ref> <ops>" (strings
+    // never hold spaces; an empty one prints as "~")
+    auto show = [](const std::string& s) { return s.empty() ? std::string("~") : s; };
+    for (size_t i = 0; i < std::min<size_t>(q.size(), r.size()); ++i)
+        for (int md = 0; md < 2; ++md) {
+            try {
+                const st::Alignment al = st::align_pair(q[i], r[i], b62, AA, md ? st::AlignMode::Local
+                                                                             : st::AlignMode::Global,
+                                                        11, 1);
+                std::cout << "alignpair " << i << ' ' << md << ' ' << al.score << ' '
+                          << show(al.aligned_query) << ' ' << show(al.aligned_ref) << ' '
+                          << show(al.ops) << '\n';
+            } catch (const std::exception& e) {
+                std::cout << "alignpair " << i << ' ' << md << " !" << e.what() << '\n';
+            }
+        }
+    call("align_pair_bad_symbol", [&] {
+        return std::vector<int32_t>{st::align_pair("CASJ", "CASS", b62, AA, st::AlignMode::Global,
+                                                   11, 1).score};
     });
     return 0;
 }

@@ -84,8 +84,9 @@ def test_cpp_api_matches_the_oracle(api_check, cuda_ready, seed):
     cube = np.asarray(prior_cube(central_prior(21), width), np.int32).ravel()
     stdin = "\n".join([f"Q {len(q)}", *q, f"R {len(r)}", *r, f"H {len(h)}", *h,
                        f"P {width} {cube.size}", " ".join(map(str, cube.tolist()))]) + "\n"
-    got = parse(subprocess.run([str(api_check), "run"], input=stdin, check=True,
-                               capture_output=True, text=True).stdout)
+    out = subprocess.run([str(api_check), "run"], input=stdin, check=True, capture_output=True,
+                         text=True).stdout
+    got = parse("\n".join(line for line in out.splitlines() if not line.startswith("alignpair ")))
     b62 = SubstitutionMatrix.blosum62()
     N, K = len(q), len(r)
 
@@ -115,3 +116,12 @@ def test_cpp_api_matches_the_oracle(api_check, cuda_ready, seed):
                                      "defined for equal-length sequences (got 3 and 4)")
     assert got["gapblock_bad_symbol"].startswith("invalid_argument: symbol 'J'")
     assert got["align_overflow"].startswith("overflow_error: seqtree: the alignment score")
+    assert got["align_pair_bad_symbol"] == "invalid_argument: invalid symbol 'J' in sequence"
+    pairs = [line.split(" ") for line in out.splitlines() if line.startswith("alignpair ")]
+    assert len(pairs) == 2 * min(N, K)
+    for _, i, md, score, aq, ar, ops in pairs:
+        un = lambda x: "" if x == "~" else x  # noqa: E731
+        i, mode = int(i), "local" if md == "1" else "global"
+        if oracle.ref_available():
+            want = oracle.ref_align_pair(q[i], r[i], "blosum62", mode=mode)
+            assert (int(score), un(aq), un(ar), un(ops)) == want
