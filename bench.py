@@ -582,6 +582,7 @@ def main_ours(args):
         "kernel": kernel_name,
         "cuda_graph": graph is not None,
         "clocks": sampler.summary(),
+        "tuning": [t for t in _lib.tuning_table().splitlines() if t],
     }
     if w["kind"] == "sparse":
         line["nnz"] = nnz_seen[-1]

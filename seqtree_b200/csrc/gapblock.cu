@@ -226,6 +226,13 @@ struct FastArgs {
     int32_t* out;            // dense output (unused by the sparse form)
     unsigned long long* err; // set when the bounded wait for the staging copies gives up
     SparseSink sink;         // sparse output (unused by the dense form)
+    // Persistent form: a grid of about one wave of CTAs takes tiles (chunk, pair group) from a
+    // global counter, longest query pairs first (the pairs are sorted by length), so the
+    // expensive tiles start early and the wave drains evenly.  0: one CTA per tile.
+    int persistent;
+    int nchunks;
+    int ntiles;
+    unsigned int* queue;     // zeroed before every launch
 };
 
 // One non-blocking probe of an mbarrier phase (callers bound the number of probes).
@@ -340,10 +347,28 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
     uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_len + ((a.rc + 15) & ~15));
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int chunk = blockIdx.x;
+    volatile int* s_next = reinterpret_cast<volatile int*>(s_bar + 1);  // in the barrier's 16 bytes
+    const uint32_t bar = uint32_t(__cvta_generic_to_shared(s_bar));
+    if (tid == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+    const int npg = int((a.P + kGP - 1) / kGP);
+    for (int iter = 0;; ++iter) {
+    int chunk, pg;
+    if (a.persistent) {
+        if (tid == 0) *s_next = int(atomicAdd(a.queue, 1u));
+        __syncthreads();
+        const int t = *s_next;
+        if (t >= a.ntiles) break;
+        pg = npg - 1 - t / a.nchunks;
+        chunk = t - (t / a.nchunks) * a.nchunks;
+    } else {
+        if (iter > 0) break;
+        chunk = blockIdx.x;
+        pg = blockIdx.y;
+    }
+    const uint32_t parity = uint32_t(iter & 1);
     const int64_t k0 = int64_t(chunk) * a.rc;
     const int kcount = int(a.K - k0 < a.rc ? a.K - k0 : a.rc);
-    const int p0 = blockIdx.y * kGP;
+    const int p0 = pg * kGP;
     const int np = int(a.P - p0 < kGP ? a.P - p0 : kGP);
     const int t0 = a.task_off[chunk], t1 = a.task_off[chunk + 1];
     const int tw0 = a.tasks[t0].w;
@@ -351,10 +376,11 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
 
     // Stage the CTA's profile slab and the chunk's code slab with two bulk (TMA) copies that
     // complete on one mbarrier, while the other threads load the (m, n) terms and lengths.
-    const uint32_t bar = uint32_t(__cvta_generic_to_shared(s_bar));
+    // (In the persistent form every tile is one phase of the barrier; the previous tile's
+    // generic-proxy writes to the same shared memory are ordered before these copies by the
+    // barrier that ended it and the proxy fence.)
     if (tid == 0) {
         const uint32_t prof_bytes = uint32_t(np) * LQ * kRow * 4;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
                      "r"(prof_bytes + uint32_t(slab_bytes))
@@ -373,10 +399,10 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
         // the failure, waits once more (bounded) for its copies in flight, and leaves as a
         // whole -- the host then reports ST_ETIMEOUT and no tile is stored.
         uint32_t done = 0;
-        for (int it = 0; it < (1 << 20) && !done; ++it) done = mbar_try_wait(bar, 0);
+        for (int it = 0; it < (1 << 20) && !done; ++it) done = mbar_try_wait(bar, parity);
         if (__syncthreads_or(!done)) {
             if (tid == 0) atomicExch(a.err, 1ull);
-            for (int it = 0; it < (1 << 20) && !done; ++it) done = mbar_try_wait(bar, 0);
+            for (int it = 0; it < (1 << 20) && !done; ++it) done = mbar_try_wait(bar, parity);
             __syncthreads();
             return;
         }
@@ -435,8 +461,7 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
                 key = sink_key(a.sink, b < 4 ? pr.x : pr.y, k0 + c + u);
             });
         }
-        return;
-    }
+    } else {
     const bool vec = (a.K & 3) == 0;
     for (int i = tid; i < np * cols4; i += kThreads) {
         const int pl = i / cols4;
@@ -463,6 +488,9 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
                 if (d2) d2[u] = int32_t((src[u] >> 16) + uint32_t(fc[u]));
             }
         }
+    }
+    }
+    __syncthreads();  // this tile's shared memory is free for the next one
     }
 }
 
@@ -695,7 +723,8 @@ namespace {
 // static choice; the autotuner (dense calls) measures all of them once per shape.
 constexpr int kRcCandidates[] = {1024, 768, 512, 384, 256};
 constexpr int kNumRc = int(sizeof(kRcCandidates) / sizeof(kRcCandidates[0]));
-thread_local int t_force_rc = 0;  // set while the autotuner times one chunk width
+thread_local int t_force_rc = 0;           // set while the autotuner times one chunk width
+thread_local int t_force_persistent = -1;  // and the launch form (-1: the tuned or static one)
 
 std::string gb_shape_key(const st_seqset_s& qs, const st_seqset_s& rs, bool has_prior) {
     return "gapblock|" + std::to_string(profile_height(qs.max_len)) + "|" +
@@ -744,12 +773,12 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
 
     const int W = longest, W1 = W + 1;
     const int lq = profile_height(qs.max_len);
+    const int tuned_choice = t_force_rc ? -1 : tuned_lookup(gb_shape_key(qs, rs, has_prior));
     RefPlan* rpp = nullptr;
     size_t smem = 0;
     if (fast) {
         RefPlan& rp = plan_slot<RefPlan>(rs.gb_ref_plan, ctx.tmp_ref_plan, rs.owns);
-        const int tuned = t_force_rc ? -1 : tuned_lookup(gb_shape_key(qs, rs, has_prior));
-        const int want_rc = t_force_rc ? t_force_rc : (tuned >= 0 ? kRcCandidates[tuned] : 0);
+        const int want_rc = t_force_rc ? t_force_rc : (tuned_choice >= 0 ? kRcCandidates[tuned_choice % kNumRc] : 0);
         if (rp.uid != rs.uid || (want_rc && rp.rc != want_rc)) {
             Phase ph("ref_plan");
             // Chunk width: the autotuner's measured choice when there is one; otherwise the
@@ -886,8 +915,25 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
     fa.err = err;
     if (sink) fa.sink = *sink;
 
-    const dim3 grid(unsigned(rp.nchunks), unsigned(ceil_div(qp.P, kGP)));
-    if (grid.y > 65535) fail(ST_EINVAL, "seqtree_b200: too many query pairs for one launch");
+    const int64_t npg = ceil_div(qp.P, kGP);
+    const int64_t ntiles = int64_t(rp.nchunks) * npg;
+    const int tuned_mode = t_force_persistent >= 0 ? t_force_persistent
+                           : (tuned_choice >= 0 ? tuned_choice / kNumRc : 0);
+    dim3 grid(unsigned(rp.nchunks), unsigned(npg));
+    if (tuned_mode == 1 && ntiles < (int64_t(1) << 31)) {
+        const void* kern = fast_kernel_ptr(lq, has_prior);
+        int per_sm = 0;
+        STB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        STB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
+        fa.persistent = 1;
+        fa.nchunks = rp.nchunks;
+        fa.ntiles = int(ntiles);
+        fa.queue = reinterpret_cast<unsigned int*>(ctx.flags_d + 13);
+        STB_CUDA(cudaMemsetAsync(fa.queue, 0, sizeof(unsigned int), stream));
+        grid = dim3(unsigned(std::min<int64_t>(ntiles, int64_t(std::max(per_sm, 1)) * ctx.num_sms)), 1);
+    } else if (grid.y > 65535) {
+        fail(ST_EINVAL, "seqtree_b200: too many query pairs for one launch");
+    }
     const char* name = dispatch_fast(lq, has_prior, fa, grid, smem, stream);
     note_launch(name);
     // The timeout flag is read by the caller after its synchronisation point.
@@ -914,15 +960,19 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
         return;
     }
     const bool has_prior = prior && prior_len > 0;
-    tuned_run(gb_shape_key(qs, rs, has_prior), kNumRc, -1, [&](int c) {
-        t_force_rc = c >= 0 ? kRcCandidates[c] : 0;  // -1: the static choice
+    // Candidates: every chunk width, each with one CTA per tile and in the persistent form.
+    tuned_run(gb_shape_key(qs, rs, has_prior), 2 * kNumRc, -1, [&](int c) {
+        t_force_rc = c >= 0 ? kRcCandidates[c % kNumRc] : 0;  // -1: the static choice
+        t_force_persistent = c >= 0 ? c / kNumRc : -1;
         try {
             run();
         } catch (...) {
             t_force_rc = 0;
+            t_force_persistent = -1;
             throw;
         }
         t_force_rc = 0;
+        t_force_persistent = -1;
     }, stream);
 }
 
