@@ -232,6 +232,10 @@ int64_t st_encoder_param_count(void);
 int32_t st_encoder_create(const float *params, st_encoder *out, st_error *err);
 void st_encoder_destroy(st_encoder enc);
 int32_t st_encoder_get_params(st_encoder enc, float *out, st_error *err);
+/* Precision of the training products (forward and backward of loss_grad / train_step):
+ * 1 (the default) bf16 tensor cores with fp32 accumulation, 0 fp32 on CUDA cores.  Weights,
+ * activations, gradients and the Adam state are fp32 either way. */
+int32_t st_encoder_set_precision(st_encoder enc, int32_t precision, st_error *err);
 /* A batch is S sequences (S even; pairs are (2i, 2i+1)) as host arrays: codes [S][32] (0..23,
  * zero beyond the length), lens [S] (1..32), scores [S/2] (exact gap-block scores).  loss_grad
  * returns the mean pair loss and, when grad is not NULL, its gradient; train_step also applies
@@ -249,6 +253,17 @@ int32_t st_encoder_train_step(st_encoder enc, const uint8_t *codes, const int32_
  *   layout 2: the fp32 forward stored in layout 1's format. */
 int32_t st_encoder_embed(st_encoder enc, st_seqset set, void *out_device, int32_t layout,
                          void *cuda_stream, st_error *err);
+
+/* The encoder's bf16 training GEMM (no counterpart in the reference), exported so it can be
+ * checked on its own: C = op(A) op(B) (C += when accumulate), op(A) [M x K] = A or, when trans_a,
+ * the transpose of A [K x M]; op(B) [K x N] = B or, when trans_b, the transpose of B [N x K]; all
+ * fp32 row-major device arrays with leading dimensions lda / ldb / ldc.  Operands are rounded to
+ * bf16 (nearest even) and the products accumulated in fp32 on the tensor cores.  Synchronous:
+ * returns when C is written. */
+int32_t st_train_gemm_bf16(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_t K,
+                           const float *A_device, int32_t lda, const float *B_device, int32_t ldb,
+                           float *C_device, int32_t ldc, int32_t accumulate, void *cuda_stream,
+                           st_error *err);
 
 /* Learned candidate proposal (no counterpart in the reference): for every query, the k refs with
  * the largest embedding dot product, computed on the tensor cores without materialising the

@@ -87,6 +87,7 @@ SIGNATURES = [
     ("st_encoder_create", ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), _ep]),
     ("st_encoder_destroy", None, [ctypes.c_void_p]),
     ("st_encoder_get_params", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_encoder_set_precision", ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32, _ep]),
     ("st_encoder_loss_grad", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
       ctypes.POINTER(ctypes.c_float), ctypes.c_void_p, _ep]),
@@ -95,6 +96,10 @@ SIGNATURES = [
       ctypes.c_float, ctypes.POINTER(ctypes.c_float), _ep]),
     ("st_encoder_embed", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, _ep]),
+    ("st_train_gemm_bf16", ctypes.c_int32,
+     [ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+      ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+      ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, _ep]),
     ("st_propose_topk", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),

@@ -35,6 +35,9 @@ int64_t encoder_param_count();
 Encoder* encoder_create(const float* params);
 void encoder_destroy(Encoder* m);
 void encoder_params(Encoder& m, float* out);
+void encoder_set_precision(Encoder& m, int precision);
+void gemm_bf16(bool ta, bool tb, int M, int N, int K, const float* A, int lda, const float* B,
+               int ldb, float* C, int ldc, bool accumulate, cudaStream_t st, int sms);
 float encoder_loss_grad(Encoder& m, const uint8_t* codes, const int32_t* lens, const int32_t* scores,
                         int S, float* grad_out);
 float encoder_train_step(Encoder& m, const uint8_t* codes, const int32_t* lens, const int32_t* scores,
@@ -690,6 +693,14 @@ int32_t st_encoder_get_params(st_encoder enc, float* out, st_error* err) {
     });
 }
 
+int32_t st_encoder_set_precision(st_encoder enc, int32_t precision, st_error* err) {
+    return guard(err, [&] {
+        Context& ctx = encoder_ctx(enc);
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        encoder_set_precision(*enc->impl, precision);
+    });
+}
+
 int32_t st_encoder_loss_grad(st_encoder enc, const uint8_t* codes, const int32_t* lens,
                              const int32_t* scores, int32_t S, float* loss, float* grad,
                              st_error* err) {
@@ -726,6 +737,32 @@ int32_t st_encoder_embed(st_encoder enc, st_seqset set, void* out_device, int32_
         if (layout < 0 || layout > 2) fail(ST_EINVAL, "seqtree_b200: embedding layout is 0, 1 or 2");
         std::lock_guard<std::mutex> lk(ctx.mu);
         encoder_embed(*enc->impl, *set, out_device, layout, static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int32_t st_train_gemm_bf16(int32_t trans_a, int32_t trans_b, int32_t M, int32_t N, int32_t K,
+                           const float* A_device, int32_t lda, const float* B_device, int32_t ldb,
+                           float* C_device, int32_t ldc, int32_t accumulate, void* cuda_stream,
+                           st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        Context& ctx = context();
+        if (M < 0 || N < 0 || K < 0) fail(ST_EINVAL, "seqtree_b200: negative GEMM size");
+        if (ldc < std::max(N, 1) || lda < std::max(trans_a ? M : K, 1) ||
+            ldb < std::max(trans_b ? K : N, 1))
+            fail(ST_EINVAL, "seqtree_b200: GEMM leading dimension too small");
+        if (M > 0 && N > 0 && (!C_device || (K > 0 && (!A_device || !B_device))))
+            fail(ST_EINVAL, "seqtree_b200: null GEMM operand");
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        const auto st = static_cast<cudaStream_t>(cuda_stream);
+        STB_CUDA(cudaMemsetAsync(ctx.flags_d + 8, 0, sizeof(int64_t), st));
+        gemm_bf16(trans_a != 0, trans_b != 0, M, N, K, A_device, lda, B_device, ldb, C_device, ldc,
+                  accumulate != 0, st, ctx.num_sms);
+        STB_CUDA(cudaMemcpyAsync(ctx.flags_h + 8, ctx.flags_d + 8, sizeof(int64_t),
+                                 cudaMemcpyDeviceToHost, st));
+        STB_CUDA(cudaStreamSynchronize(st));
+        if (ctx.flags_h[8] != 0)
+            fail(ST_ETIMEOUT, "seqtree_b200: a bounded device-side wait gave up (training GEMM)");
     });
 }
 

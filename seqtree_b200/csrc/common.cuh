@@ -84,6 +84,8 @@ struct Context {
     DevBuf sp_keys, sp_vals, sp_sorted, sp_temp;
     // candidate lists of the learned-proposal kernel
     DevBuf topk_cand;
+    // bf16 operands of the training GEMM, packed in the tensor-core layout
+    DevBuf gemm_a, gemm_b;
     // storage of the transient sets made by the host-buffer entry points
     DevBuf tq[3], tr[3];  // bytes, offsets, lengths
     // plans reused by transient sets (rebuilt in place for every call)

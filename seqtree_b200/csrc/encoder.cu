@@ -5,10 +5,12 @@
 // -> conv k=3 (128->128, ReLU, skip) -> 2 x single-head self-attention (d=128, residual) -> mean
 // over the valid positions -> linear 128->64 -> unit length.  Parameters are one flat fp32 array
 // in the order W1[3][24][128], b1, W2[384][128], b2, (Wqkv[128][384], bqkv, Wo[128][128], bo) x 2,
-// Wout[128][64], bout.  Training runs in fp32 on CUDA cores: a tiled SGEMM (128x128x8 tiles, 8x8
-// per thread, split-K for the weight gradients) carries the dense layers, and per-sequence
-// kernels carry the convolutions' gathers, attention, pooling and the pair loss.  The numbers
-// follow the float64 restatement used as the checker, to fp32 rounding.
+// Wout[128][64], bout.  Weights, activations, gradients and Adam state are fp32.  The dense
+// layers' products run by default on the bf16 tensor cores with fp32 accumulation (gemm_bf16);
+// the fp32 precision setting runs them in a tiled SGEMM on CUDA cores instead (128x128x8 tiles,
+// 8x8 per thread, split-K for the weight gradients), whose numbers follow the float64
+// restatement used as the checker to fp32 rounding.  Per-sequence kernels carry the
+// convolutions' gathers, attention, pooling and the pair loss in fp32 either way.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -18,6 +20,9 @@
 #include "encoder_layout.cuh"
 
 namespace stb {
+
+void gemm_bf16(bool ta, bool tb, int M, int N, int K, const float* A, int lda, const float* B,
+               int ldb, float* C, int ldc, bool accumulate, cudaStream_t st, int sms);
 
 namespace {
 
@@ -198,6 +203,15 @@ void sgemm(int M, int N, int K, const float* A, int lda, const float* B, int ldb
     sgemm_kernel<TA, TB><<<grid, 256, 0, stream>>>(M, N, K, A, lda, B, ldb, C, ldc, kslice, mode);
     STB_CUDA(cudaGetLastError());
     note_launch(nullptr);
+}
+
+// The training GEMM in the encoder's chosen precision: bf16 tensor cores (fp32 accumulation)
+// or the fp32 SIMT kernel above.
+template <bool TA, bool TB>
+void mm(bool bf16, int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C,
+        int ldc, bool accumulate, cudaStream_t stream, int num_sms) {
+    if (bf16) gemm_bf16(TA, TB, M, N, K, A, lda, B, ldb, C, ldc, accumulate, stream, num_sms);
+    else sgemm<TA, TB>(M, N, K, A, lda, B, ldb, C, ldc, accumulate, stream, num_sms);
 }
 
 // ------------------------------------------------------------------------- layer kernels ----
@@ -556,6 +570,7 @@ struct Encoder {
     int device = 0;
     DevBuf params, grads, adam_m, adam_v, loss;
     int64_t step = 0;            // Adam steps taken: also the version of the parameters
+    int precision = 1;           // training products: 1 bf16 tensor cores, 0 fp32 SIMT
     std::shared_ptr<void> bf16;  // weights and workspace of the bf16 inference path
     int S_cap = 0;  // sequences the workspace holds
     // forward activations (rows = 32 * S)
@@ -601,7 +616,7 @@ void set_attn_attrs() {
 }
 
 // Forward of S sequences whose padded codes and lengths are in m.codes / m.lens; z in m.z.
-void forward(Encoder& m, int S, cudaStream_t st, int sms) {
+void forward(Encoder& m, int S, cudaStream_t st, int sms, bool bf) {
     set_attn_attrs();
     const unsigned R = unsigned(S) * kP;
     const auto* codes = static_cast<const uint8_t*>(m.codes.ptr);
@@ -609,7 +624,7 @@ void forward(Encoder& m, int S, cudaStream_t st, int sms) {
     float* prm = P(m);
     conv1_fwd_kernel<<<R, kW, 0, st>>>(codes, lens, prm, F(m.pre1), F(m.h1));
     im2col_kernel<<<R, kW, 0, st>>>(F(m.h1), lens, F(m.x2));
-    sgemm<false, false>(int(R), kW, 3 * kW, F(m.x2), 3 * kW, prm + oW2, kW, F(m.pre2), kW, false, st, sms);
+    mm<false, false>(bf, int(R), kW, 3 * kW, F(m.x2), 3 * kW, prm + oW2, kW, F(m.pre2), kW, false, st, sms);
     conv2_out_kernel<<<R, kW, 0, st>>>(F(m.pre2), F(m.h1), lens, prm + ob2, F(m.hA));
     float* hin[2] = {F(m.hA), F(m.hB)};
     float* hout[2] = {F(m.hB), F(m.hC)};
@@ -618,21 +633,21 @@ void forward(Encoder& m, int S, cudaStream_t st, int sms) {
     float* ob[2] = {F(m.o0), F(m.o1)};
     for (int l = 0; l < 2; ++l) {
         const float* L = prm + oL0 + l * kLayer;
-        sgemm<false, false>(int(R), 3 * kW, kW, hin[l], kW, L + lWqkv, 3 * kW, qkv[l], 3 * kW, false, st, sms);
+        mm<false, false>(bf, int(R), 3 * kW, kW, hin[l], kW, L + lWqkv, 3 * kW, qkv[l], 3 * kW, false, st, sms);
         add_bias_kernel<<<R, 128, 0, st>>>(qkv[l], L + lbqkv, 3 * kW);
         attn_fwd_kernel<<<unsigned(S), 256, attn_fwd_smem(), st>>>(qkv[l], lens, att[l], ob[l]);
-        sgemm<false, false>(int(R), kW, kW, ob[l], kW, L + lWo, kW, F(m.y), kW, false, st, sms);
+        mm<false, false>(bf, int(R), kW, kW, ob[l], kW, L + lWo, kW, F(m.y), kW, false, st, sms);
         residual_kernel<<<R, kW, 0, st>>>(hin[l], F(m.y), L + lbo, lens, hout[l]);
     }
     pool_kernel<<<unsigned(S), kW, 0, st>>>(F(m.hC), lens, F(m.pool));
-    sgemm<false, false>(S, kE, kW, F(m.pool), kW, prm + oWout, kE, F(m.e), kE, false, st, sms);
+    mm<false, false>(bf, S, kE, kW, F(m.pool), kW, prm + oWout, kE, F(m.e), kE, false, st, sms);
     normalize_kernel<<<unsigned(ceil_div(S, 8)), 256, 0, st>>>(F(m.e), prm + obout, S, F(m.z), F(m.nrm));
     STB_CUDA(cudaGetLastError());
     note_launch(nullptr, 12);
 }
 
 // Loss and gradients (into m.grads) of S sequences = S/2 pairs with scores in m.scores.
-void loss_backward(Encoder& m, int S, cudaStream_t st, int sms) {
+void loss_backward(Encoder& m, int S, cudaStream_t st, int sms, bool bf) {
     const unsigned R = unsigned(S) * kP;
     const int pairs = S / 2;
     const auto* codes = static_cast<const uint8_t*>(m.codes.ptr);
@@ -645,9 +660,9 @@ void loss_backward(Encoder& m, int S, cudaStream_t st, int sms) {
         F(m.z), static_cast<const int32_t*>(m.scores.ptr), pairs, F(m.dz), F(m.loss));
     normalize_bwd_kernel<<<unsigned(ceil_div(S, 8)), 256, 0, st>>>(F(m.dz), F(m.e), F(m.nrm), S, F(m.de));
     // e = pool Wout + bout
-    sgemm<true, false>(kW, kE, S, F(m.pool), kW, F(m.de), kE, g + oWout, kE, true, st, sms);
+    mm<true, false>(bf, kW, kE, S, F(m.pool), kW, F(m.de), kE, g + oWout, kE, true, st, sms);
     colsum_kernel<<<unsigned(ceil_div(S, 256)), 64, 0, st>>>(F(m.de), S, kE, 256, g + obout);
-    sgemm<false, true>(S, kW, kE, F(m.de), kE, prm + oWout, kE, F(m.dpool), kW, false, st, sms);
+    mm<false, true>(bf, S, kW, kE, F(m.de), kE, prm + oWout, kE, F(m.dpool), kW, false, st, sms);
     pool_bwd_kernel<<<R, kW, 0, st>>>(F(m.dpool), lens, F(m.dh));
     float* hin[2] = {F(m.hA), F(m.hB)};
     float* qkv[2] = {F(m.qkv0), F(m.qkv1)};
@@ -657,26 +672,39 @@ void loss_backward(Encoder& m, int S, cudaStream_t st, int sms) {
         const float* L = prm + oL0 + l * kLayer;
         float* G = g + oL0 + l * kLayer;
         // h_next = (h + o Wo + bo) * mask; dh is already masked
-        sgemm<true, false>(kW, kW, int(R), ob[l], kW, F(m.dh), kW, G + lWo, kW, true, st, sms);
+        mm<true, false>(bf, kW, kW, int(R), ob[l], kW, F(m.dh), kW, G + lWo, kW, true, st, sms);
         colsum_kernel<<<unsigned(ceil_div(R, 1024)), 128, 0, st>>>(F(m.dh), R, kW, 1024, G + lbo);
-        sgemm<false, true>(int(R), kW, kW, F(m.dh), kW, L + lWo, kW, F(m.dO), kW, false, st, sms);
+        mm<false, true>(bf, int(R), kW, kW, F(m.dh), kW, L + lWo, kW, F(m.dO), kW, false, st, sms);
         attn_bwd_kernel<<<unsigned(S), 256, attn_bwd_smem(), st>>>(qkv[l], att[l], F(m.dO), lens, F(m.dqkv));
-        sgemm<true, false>(kW, 3 * kW, int(R), hin[l], kW, F(m.dqkv), 3 * kW, G + lWqkv, 3 * kW, true, st, sms);
+        mm<true, false>(bf, kW, 3 * kW, int(R), hin[l], kW, F(m.dqkv), 3 * kW, G + lWqkv, 3 * kW, true, st, sms);
         colsum_kernel<<<unsigned(ceil_div(R, 1024)), 128, 0, st>>>(F(m.dqkv), R, 3 * kW, 1024, G + lbqkv);
         // dh_prev = (dh + dqkv Wqkv^T) * mask
-        sgemm<false, true>(int(R), kW, 3 * kW, F(m.dqkv), 3 * kW, L + lWqkv, 3 * kW, F(m.dh), kW, true, st, sms);
+        mm<false, true>(bf, int(R), kW, 3 * kW, F(m.dqkv), 3 * kW, L + lWqkv, 3 * kW, F(m.dh), kW, true, st, sms);
         mask_kernel<<<R, kW, 0, st>>>(F(m.dh), lens);
     }
     // hA = (h1 + relu(pre2)) * mask
     relu_bwd_kernel<<<R, kW, 0, st>>>(F(m.dh), F(m.pre2), F(m.dpre));
-    sgemm<true, false>(3 * kW, kW, int(R), F(m.x2), 3 * kW, F(m.dpre), kW, g + oW2, kW, true, st, sms);
+    mm<true, false>(bf, 3 * kW, kW, int(R), F(m.x2), 3 * kW, F(m.dpre), kW, g + oW2, kW, true, st, sms);
     colsum_kernel<<<unsigned(ceil_div(R, 1024)), 128, 0, st>>>(F(m.dpre), R, kW, 1024, g + ob2);
-    sgemm<false, true>(int(R), 3 * kW, kW, F(m.dpre), kW, prm + oW2, kW, F(m.dx2), 3 * kW, false, st, sms);
+    mm<false, true>(bf, int(R), 3 * kW, kW, F(m.dpre), kW, prm + oW2, kW, F(m.dx2), 3 * kW, false, st, sms);
     col2im_bwd_kernel<<<R, kW, 0, st>>>(F(m.dh), F(m.dx2), F(m.pre1), lens, F(m.dpre));
     conv1_bwd_kernel<<<unsigned(ceil_div(R, 256)), 128, 0, st>>>(F(m.dpre), codes, lens, R, 256,
                                                                  g + oW1, g + ob1);
     STB_CUDA(cudaGetLastError());
     note_launch(nullptr, 16);
+}
+
+// The bounded waits of the tensor-core GEMM report through the context's error word 8.
+void clear_wait_flag(Context& ctx) {
+    STB_CUDA(cudaMemsetAsync(ctx.flags_d + 8, 0, sizeof(int64_t), ctx.stream));
+}
+// Synchronises the stream, then fails if a bounded wait gave up during the step.
+void check_wait_flag(Context& ctx) {
+    STB_CUDA(cudaMemcpyAsync(ctx.flags_h + 8, ctx.flags_d + 8, sizeof(int64_t),
+                             cudaMemcpyDeviceToHost, ctx.stream));
+    STB_CUDA(cudaStreamSynchronize(ctx.stream));
+    if (ctx.flags_h[8] != 0)
+        fail(ST_ETIMEOUT, "seqtree_b200: a bounded device-side wait gave up (training GEMM)");
 }
 
 void upload_batch(Encoder& m, const uint8_t* codes, const int32_t* lens, const int32_t* scores,
@@ -731,20 +759,28 @@ void encoder_params(Encoder& m, float* out) {
     STB_CUDA(cudaStreamSynchronize(ctx.stream));
 }
 
+// Precision of the training products: 1 bf16 tensor cores (fp32 accumulation), 0 fp32 SIMT.
+void encoder_set_precision(Encoder& m, int precision) {
+    if (precision != 0 && precision != 1)
+        fail(ST_EINVAL, "seqtree_b200: encoder precision is 0 (fp32) or 1 (bf16)");
+    m.precision = precision;
+}
+
 // Loss (and optionally the gradient, host) of one batch: S sequences = S/2 pairs.
 float encoder_loss_grad(Encoder& m, const uint8_t* codes, const int32_t* lens, const int32_t* scores,
                         int S, float* grad_out) {
     if (S < 2 || S % 2) fail(ST_EINVAL, "seqtree_b200: a batch is an even number of sequences (pairs)");
     Context& ctx = context();
     upload_batch(m, codes, lens, scores, S, ctx.stream);
-    forward(m, S, ctx.stream, ctx.num_sms);
-    loss_backward(m, S, ctx.stream, ctx.num_sms);
+    clear_wait_flag(ctx);
+    forward(m, S, ctx.stream, ctx.num_sms, m.precision == 1);
+    loss_backward(m, S, ctx.stream, ctx.num_sms, m.precision == 1);
     float loss = 0.f;
     STB_CUDA(cudaMemcpyAsync(&loss, m.loss.ptr, sizeof(float), cudaMemcpyDeviceToHost, ctx.stream));
     if (grad_out)
         STB_CUDA(cudaMemcpyAsync(grad_out, m.grads.ptr, sizeof(float) * kParams,
                                  cudaMemcpyDeviceToHost, ctx.stream));
-    STB_CUDA(cudaStreamSynchronize(ctx.stream));
+    check_wait_flag(ctx);
     return loss;
 }
 
@@ -754,8 +790,9 @@ float encoder_train_step(Encoder& m, const uint8_t* codes, const int32_t* lens, 
     if (S < 2 || S % 2) fail(ST_EINVAL, "seqtree_b200: a batch is an even number of sequences (pairs)");
     Context& ctx = context();
     upload_batch(m, codes, lens, scores, S, ctx.stream);
-    forward(m, S, ctx.stream, ctx.num_sms);
-    loss_backward(m, S, ctx.stream, ctx.num_sms);
+    clear_wait_flag(ctx);
+    forward(m, S, ctx.stream, ctx.num_sms, m.precision == 1);
+    loss_backward(m, S, ctx.stream, ctx.num_sms, m.precision == 1);
     ++m.step;
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.f - std::pow(b1, float(m.step)), c2 = 1.f - std::pow(b2, float(m.step));
@@ -765,7 +802,7 @@ float encoder_train_step(Encoder& m, const uint8_t* codes, const int32_t* lens, 
     note_launch(nullptr);
     float loss = 0.f;
     STB_CUDA(cudaMemcpyAsync(&loss, m.loss.ptr, sizeof(float), cudaMemcpyDeviceToHost, ctx.stream));
-    STB_CUDA(cudaStreamSynchronize(ctx.stream));
+    check_wait_flag(ctx);
     return loss;
 }
 
@@ -790,7 +827,7 @@ void encoder_embed(Encoder& m, const st_seqset_s& set, void* out, int layout, cu
         gather_codes_kernel<<<unsigned(S), kP, 0, st>>>(set.d_bytes, set.d_off, set.d_len, first, S,
                                                        static_cast<uint8_t*>(m.codes.ptr),
                                                        static_cast<int32_t*>(m.lens.ptr));
-        forward(m, S, st, ctx.num_sms);
+        forward(m, S, st, ctx.num_sms, false);  // layouts 0 and 2: the fp32 forward
         store_embed_kernel<<<unsigned(ceil_div(S, 8)), 256, 0, st>>>(F(m.z), S, first, layout ? 1 : 0,
                                                                     out);
         STB_CUDA(cudaGetLastError());

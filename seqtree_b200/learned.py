@@ -72,7 +72,10 @@ def pad_codes(seqs) -> tuple[np.ndarray, np.ndarray]:
 class Encoder:
     """The CUDA encoder (``st_encoder``): parameters, training steps and embeddings."""
 
-    def __init__(self, params: np.ndarray | None = None, seed: int = 0):
+    def __init__(self, params: np.ndarray | None = None, seed: int = 0, precision: str = "bf16"):
+        """``precision`` is that of the training products: "bf16" (tensor cores, fp32
+        accumulation) or "fp32" (CUDA cores, the numbers of the float64 checker to fp32
+        rounding).  Weights, gradients and optimizer state are fp32 either way."""
         p = init_params(seed) if params is None else np.ascontiguousarray(params, np.float32)
         if p.size != param_count():
             raise ValueError(f"expected {param_count()} parameters, got {p.size}")
@@ -81,6 +84,15 @@ class Encoder:
         err = _lib.st_error()
         _lib.check(_lib.lib.st_encoder_create(p.ctypes.data, ctypes.byref(self._h),
                                               ctypes.byref(err)), err)
+        self.set_precision(precision)
+
+    def set_precision(self, precision: str) -> None:
+        code = {"fp32": 0, "bf16": 1}.get(precision)
+        if code is None:
+            raise ValueError("precision is 'bf16' or 'fp32'")
+        err = _lib.st_error()
+        _lib.check(_lib.lib.st_encoder_set_precision(self._h, code, ctypes.byref(err)), err)
+        self.precision = precision
 
     def params(self) -> np.ndarray:
         out = np.empty(param_count(), np.float32)
@@ -183,6 +195,27 @@ def propose_topk(q_emb, r_emb, k: int = 256):
                       scores.data_ptr(), stream)
     stream_status(stream)
     return ids, scores
+
+
+def train_gemm_bf16(a, b, c, *, trans_a: bool = False, trans_b: bool = False,
+                    accumulate: bool = False) -> None:
+    """The encoder's training GEMM (``st_train_gemm_bf16``) on fp32 CUDA matrices:
+    ``c = op(a) @ op(b)`` (``+=`` when ``accumulate``), op the transpose when asked, products in
+    bf16 with fp32 accumulation.  Row-major operands with unit column stride."""
+    import torch
+    for t in (a, b, c):
+        if t.dtype != torch.float32 or t.dim() != 2 or not t.is_cuda or t.stride(1) != 1:
+            raise ValueError("train_gemm_bf16: 2-d fp32 CUDA matrices with unit column stride")
+    M, K = (a.shape[1], a.shape[0]) if trans_a else (a.shape[0], a.shape[1])
+    K2, N = (b.shape[1], b.shape[0]) if trans_b else (b.shape[0], b.shape[1])
+    if K2 != K or tuple(c.shape) != (M, N):
+        raise ValueError("train_gemm_bf16: shapes do not chain")
+    err = _lib.st_error()
+    _lib.check(_lib.lib.st_train_gemm_bf16(
+        int(trans_a), int(trans_b), M, N, K, ctypes.c_void_p(a.data_ptr()), max(a.stride(0), 1),
+        ctypes.c_void_p(b.data_ptr()), max(b.stride(0), 1), ctypes.c_void_p(c.data_ptr()),
+        max(c.stride(0), 1), int(accumulate),
+        ctypes.c_void_p(torch.cuda.current_stream(c.device).cuda_stream), ctypes.byref(err)), err)
 
 
 def stream_status(stream: int = 0) -> None:
