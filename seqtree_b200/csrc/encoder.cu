@@ -215,11 +215,13 @@ void mm(bool bf16, int M, int N, int K, const float* A, int lda, const float* B,
 }
 
 // ------------------------------------------------------------------------- layer kernels ----
-// Row r = s*32 + t; position t of sequence s is valid when t < len[s].
+// Row r = s*32 + t; position t of sequence s is valid when t < len[s].  The per-row kernels run
+// kRowsPerCta rows per CTA (threadIdx.y) of kW threads (threadIdx.x): R = 32 S is a multiple.
+constexpr int kRowsPerCta = 8;
 __global__ void conv1_fwd_kernel(const uint8_t* __restrict__ codes, const int32_t* __restrict__ lens,
                                  const float* __restrict__ prm, float* __restrict__ pre1,
                                  float* __restrict__ h1) {
-    const int64_t r = blockIdx.x;
+    const int64_t r = int64_t(blockIdx.x) * kRowsPerCta + threadIdx.y;
     const int s = int(r / kP), t = int(r % kP), j = threadIdx.x;
     const int L = lens[s];
     float v = 0.f, pre = 0.f;
@@ -238,7 +240,7 @@ __global__ void conv1_fwd_kernel(const uint8_t* __restrict__ codes, const int32_
 // x2[r] = [h1[r-1], h1[r], h1[r+1]] within the sequence (zero outside [0, L)).
 __global__ void im2col_kernel(const float* __restrict__ h1, const int32_t* __restrict__ lens,
                               float* __restrict__ x2) {
-    const int64_t r = blockIdx.x;
+    const int64_t r = int64_t(blockIdx.x) * kRowsPerCta + threadIdx.y;
     const int s = int(r / kP), t = int(r % kP), j = threadIdx.x;
     const int L = lens[s];
     const bool in = t < L;
@@ -251,7 +253,7 @@ __global__ void im2col_kernel(const float* __restrict__ h1, const int32_t* __res
 __global__ void conv2_out_kernel(float* __restrict__ pre2, const float* __restrict__ h1,
                                  const int32_t* __restrict__ lens, const float* __restrict__ b2,
                                  float* __restrict__ h) {
-    const int64_t r = blockIdx.x;
+    const int64_t r = int64_t(blockIdx.x) * kRowsPerCta + threadIdx.y;
     const int s = int(r / kP), t = int(r % kP), j = threadIdx.x;
     const float p = pre2[r * kW + j] + b2[j];
     pre2[r * kW + j] = p;
@@ -259,7 +261,7 @@ __global__ void conv2_out_kernel(float* __restrict__ pre2, const float* __restri
 }
 
 __global__ void add_bias_kernel(float* __restrict__ x, const float* __restrict__ b, int cols) {
-    const int64_t r = blockIdx.x;
+    const int64_t r = int64_t(blockIdx.x) * kRowsPerCta + threadIdx.y;
     for (int j = threadIdx.x; j < cols; j += blockDim.x) x[r * cols + j] += b[j];
 }
 
@@ -267,7 +269,7 @@ __global__ void add_bias_kernel(float* __restrict__ x, const float* __restrict__
 __global__ void residual_kernel(const float* __restrict__ h, const float* __restrict__ y,
                                 const float* __restrict__ bo, const int32_t* __restrict__ lens,
                                 float* __restrict__ out) {
-    const int64_t r = blockIdx.x;
+    const int64_t r = int64_t(blockIdx.x) * kRowsPerCta + threadIdx.y;
     const int s = int(r / kP), t = int(r % kP), j = threadIdx.x;
     out[r * kW + j] = t < lens[s] ? h[r * kW + j] + y[r * kW + j] + bo[j] : 0.f;
 }
@@ -294,26 +296,49 @@ __global__ void __launch_bounds__(256) attn_fwd_kernel(const float* __restrict__
     }
     __syncthreads();
     const float scale = rsqrtf(float(kW));
-    for (int t = warp; t < kP; t += 8) {
+    {
+        // warp w: rows w, w+8, w+16, w+24; lane u: key u.  Each k value feeds four rows.
         const int u = lane;
-        float sc = 0.f;
-        for (int d = 0; d < kW; ++d) sc = fmaf(q[t * kW + d], k[u * (kW + 1) + d], sc);
-        sc = u < L ? sc * scale : -INFINITY;
-        float mx = sc;
-        for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        float e = u < L ? expf(sc - mx) : 0.f;
-        float sum = e;
-        for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        const float av = t < L ? e / sum : 0.f;
-        a[t * (kP + 1) + u] = av;
-        a_out[(int64_t(s) * kP + t) * kP + u] = av;
+        float sc[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int d = 0; d < kW; ++d) {
+            const float kv = k[u * (kW + 1) + d];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) sc[i] = fmaf(q[(warp + 8 * i) * kW + d], kv, sc[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int t = warp + 8 * i;
+            const float x = u < L ? sc[i] * scale : -INFINITY;
+            float mx = x;
+            for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            const float e = u < L ? expf(x - mx) : 0.f;
+            float sum = e;
+            for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            const float av = t < L ? e / sum : 0.f;
+            a[t * (kP + 1) + u] = av;
+            a_out[(int64_t(s) * kP + t) * kP + u] = av;
+        }
     }
     __syncthreads();
-    for (int i = tid; i < kP * kW; i += 256) {
-        const int t = i / kW, j = i % kW;
-        float acc = 0.f;
-        for (int u = 0; u < L; ++u) acc = fmaf(a[t * (kP + 1) + u], v[u * kW + j], acc);
-        o_out[(int64_t(s) * kP + t) * kW + j] = acc;
+    {
+        // warp w: rows 4w..4w+3; lane: columns lane + 32c.  4 x 4 outputs per thread.
+        float acc[4][4] = {};
+        for (int u = 0; u < L; ++u) {
+            float av[4], vv[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) av[i] = a[(4 * warp + i) * (kP + 1) + u];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) vv[c] = v[u * kW + lane + 32 * c];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[i][c] = fmaf(av[i], vv[c], acc[i][c]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                o_out[(int64_t(s) * kP + 4 * warp + i) * kW + lane + 32 * c] = acc[i][c];
     }
 }
 
@@ -345,28 +370,62 @@ __global__ void __launch_bounds__(256) attn_bwd_kernel(const float* __restrict__
         a[(i / kP) * (kP + 1) + i % kP] = a_in[int64_t(s) * kP * kP + i];
     __syncthreads();
     const float scale = rsqrtf(float(kW));
-    for (int t = warp; t < kP; t += 8) {
+    {
+        // warp w: rows w, w+8, w+16, w+24; lane u: key u.
         const int u = lane;
-        float da = 0.f;
-        for (int d = 0; d < kW; ++d) da = fmaf(dO[t * R + d], v[u * R + d], da);
-        const float av = a[t * (kP + 1) + u];
-        float dot = da * av;
-        for (int o = 16; o; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
-        ds[t * (kP + 1) + u] = av * (da - dot) * scale;
+        float da[4] = {0.f, 0.f, 0.f, 0.f};
+        for (int d = 0; d < kW; ++d) {
+            const float vv = v[u * R + d];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) da[i] = fmaf(dO[(warp + 8 * i) * R + d], vv, da[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int t = warp + 8 * i;
+            const float av = a[t * (kP + 1) + u];
+            float dot = da[i] * av;
+            for (int o = 16; o; o >>= 1) dot += __shfl_xor_sync(0xffffffffu, dot, o);
+            ds[t * (kP + 1) + u] = av * (da[i] - dot) * scale;
+        }
     }
     __syncthreads();
-    for (int i = tid; i < kP * kW; i += 256) {
-        const int t = i / kW, j = i % kW;
-        float dq = 0.f, dk = 0.f, dv = 0.f;
+    {
+        // warp w: rows 4w..4w+3; lane: columns lane + 32c.  Every loaded value feeds four
+        // outputs of each of dq, dk, dv.
+        float dq[4][4] = {}, dk[4][4] = {}, dv[4][4] = {};
         for (int u = 0; u < kP; ++u) {
-            dq = fmaf(ds[t * (kP + 1) + u], k[u * R + j], dq);
-            dk = fmaf(ds[u * (kP + 1) + t], q[u * R + j], dk);
-            dv = fmaf(a[u * (kP + 1) + t], dO[u * R + j], dv);
+            float kv[4], qv[4], ov[4], dr[4], dc[4], ac[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                kv[c] = k[u * R + lane + 32 * c];
+                qv[c] = q[u * R + lane + 32 * c];
+                ov[c] = dO[u * R + lane + 32 * c];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                dr[i] = ds[(4 * warp + i) * (kP + 1) + u];
+                dc[i] = ds[u * (kP + 1) + 4 * warp + i];
+                ac[i] = a[u * (kP + 1) + 4 * warp + i];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    dq[i][c] = fmaf(dr[i], kv[c], dq[i][c]);
+                    dk[i][c] = fmaf(dc[i], qv[c], dk[i][c]);
+                    dv[i][c] = fmaf(ac[i], ov[c], dv[i][c]);
+                }
         }
-        float* out = dqkv + (int64_t(s) * kP + t) * 3 * kW;
-        out[j] = dq;
-        out[kW + j] = dk;
-        out[2 * kW + j] = dv;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            float* out = dqkv + (int64_t(s) * kP + 4 * warp + i) * 3 * kW;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                out[lane + 32 * c] = dq[i][c];
+                out[kW + lane + 32 * c] = dk[i][c];
+                out[2 * kW + lane + 32 * c] = dv[i][c];
+            }
+        }
     }
 }
 
@@ -433,14 +492,14 @@ __global__ void normalize_bwd_kernel(const float* __restrict__ dz, const float* 
 
 __global__ void pool_bwd_kernel(const float* __restrict__ dpool, const int32_t* __restrict__ lens,
                                 float* __restrict__ dh) {
-    const int64_t r = blockIdx.x;
+    const int64_t r = int64_t(blockIdx.x) * kRowsPerCta + threadIdx.y;
     const int s = int(r / kP), t = int(r % kP), j = threadIdx.x;
     const int L = lens[s];
     dh[r * kW + j] = t < L ? dpool[int64_t(s) * kW + j] / float(L) : 0.f;
 }
 
 __global__ void mask_kernel(float* __restrict__ x, const int32_t* __restrict__ lens) {
-    const int64_t r = blockIdx.x;
+    const int64_t r = int64_t(blockIdx.x) * kRowsPerCta + threadIdx.y;
     const int s = int(r / kP), t = int(r % kP), j = threadIdx.x;
     if (t >= lens[s]) x[r * kW + j] = 0.f;
 }
@@ -448,7 +507,7 @@ __global__ void mask_kernel(float* __restrict__ x, const int32_t* __restrict__ l
 // dpre2 = dh * (pre2 > 0)
 __global__ void relu_bwd_kernel(const float* __restrict__ dh, const float* __restrict__ pre,
                                 float* __restrict__ out) {
-    const int64_t i = int64_t(blockIdx.x) * kW + threadIdx.x;
+    const int64_t i = (int64_t(blockIdx.x) * kRowsPerCta + threadIdx.y) * kW + threadIdx.x;
     out[i] = pre[i] > 0.f ? dh[i] : 0.f;
 }
 
@@ -456,7 +515,7 @@ __global__ void relu_bwd_kernel(const float* __restrict__ dh, const float* __res
 __global__ void col2im_bwd_kernel(const float* __restrict__ dh, const float* __restrict__ dx2,
                                   const float* __restrict__ pre1, const int32_t* __restrict__ lens,
                                   float* __restrict__ dpre1) {
-    const int64_t r = blockIdx.x;
+    const int64_t r = int64_t(blockIdx.x) * kRowsPerCta + threadIdx.y;
     const int s = int(r / kP), t = int(r % kP), j = threadIdx.x;
     const int L = lens[s];
     float g = 0.f;
@@ -501,16 +560,50 @@ __global__ void __launch_bounds__(128) conv1_bwd_kernel(const float* __restrict_
     atomicAdd(db1 + j, bsum);
 }
 
-// out[c] += sum over rows of x[r][c], rows split over blocks.
+// out[c] += sum over rows [blockIdx.x * rows_per_block, ...) of x[r][c] (cols a multiple of 4,
+// at most 1024).  blockDim.x = (cols / 4) * G: thread t sums float4 column t % (cols / 4) over
+// every G-th row, the G partial sums meet in shared memory, one atomic per column per block.
 __global__ void colsum_kernel(const float* __restrict__ x, int64_t rows, int cols,
                               int rows_per_block, float* __restrict__ out) {
+    __shared__ float4 part[256];
+    const int cq = cols >> 2, G = blockDim.x / cq;
+    const int c4 = threadIdx.x % cq, g = threadIdx.x / cq;
     const int64_t r0 = int64_t(blockIdx.x) * rows_per_block;
     const int64_t r1 = min(rows, r0 + rows_per_block);
-    for (int c = threadIdx.x; c < cols; c += blockDim.x) {
-        float acc = 0.f;
-        for (int64_t r = r0; r < r1; ++r) acc += x[r * cols + c];
-        atomicAdd(out + c, acc);
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4* xv = reinterpret_cast<const float4*>(x);
+#pragma unroll 4
+    for (int64_t r = r0 + g; r < r1; r += G) {
+        const float4 v = xv[r * cq + c4];
+        acc.x += v.x;
+        acc.y += v.y;
+        acc.z += v.z;
+        acc.w += v.w;
     }
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    if (g == 0) {
+        for (int h = 1; h < G; ++h) {
+            const float4 v = part[h * cq + c4];
+            acc.x += v.x;
+            acc.y += v.y;
+            acc.z += v.z;
+            acc.w += v.w;
+        }
+        atomicAdd(out + 4 * c4, acc.x);
+        atomicAdd(out + 4 * c4 + 1, acc.y);
+        atomicAdd(out + 4 * c4 + 2, acc.z);
+        atomicAdd(out + 4 * c4 + 3, acc.w);
+    }
+}
+
+// Column sums of x [rows][cols] added into out (bias gradients).
+void colsum(const float* x, int64_t rows, int cols, float* out, cudaStream_t st) {
+    const int cq = cols / 4;
+    const int threads = cq * std::max(1, 256 / cq);
+    constexpr int kRowsPerBlock = 256;
+    colsum_kernel<<<unsigned(ceil_div(rows, kRowsPerBlock)), unsigned(threads), 0, st>>>(
+        x, rows, cols, kRowsPerBlock, out);
 }
 
 __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
@@ -622,10 +715,10 @@ void forward(Encoder& m, int S, cudaStream_t st, int sms, bool bf) {
     const auto* codes = static_cast<const uint8_t*>(m.codes.ptr);
     const auto* lens = static_cast<const int32_t*>(m.lens.ptr);
     float* prm = P(m);
-    conv1_fwd_kernel<<<R, kW, 0, st>>>(codes, lens, prm, F(m.pre1), F(m.h1));
-    im2col_kernel<<<R, kW, 0, st>>>(F(m.h1), lens, F(m.x2));
+    conv1_fwd_kernel<<<R / kRowsPerCta, dim3(kW, kRowsPerCta), 0, st>>>(codes, lens, prm, F(m.pre1), F(m.h1));
+    im2col_kernel<<<R / kRowsPerCta, dim3(kW, kRowsPerCta), 0, st>>>(F(m.h1), lens, F(m.x2));
     mm<false, false>(bf, int(R), kW, 3 * kW, F(m.x2), 3 * kW, prm + oW2, kW, F(m.pre2), kW, false, st, sms);
-    conv2_out_kernel<<<R, kW, 0, st>>>(F(m.pre2), F(m.h1), lens, prm + ob2, F(m.hA));
+    conv2_out_kernel<<<R / kRowsPerCta, dim3(kW, kRowsPerCta), 0, st>>>(F(m.pre2), F(m.h1), lens, prm + ob2, F(m.hA));
     float* hin[2] = {F(m.hA), F(m.hB)};
     float* hout[2] = {F(m.hB), F(m.hC)};
     float* qkv[2] = {F(m.qkv0), F(m.qkv1)};
@@ -634,10 +727,10 @@ void forward(Encoder& m, int S, cudaStream_t st, int sms, bool bf) {
     for (int l = 0; l < 2; ++l) {
         const float* L = prm + oL0 + l * kLayer;
         mm<false, false>(bf, int(R), 3 * kW, kW, hin[l], kW, L + lWqkv, 3 * kW, qkv[l], 3 * kW, false, st, sms);
-        add_bias_kernel<<<R, 128, 0, st>>>(qkv[l], L + lbqkv, 3 * kW);
+        add_bias_kernel<<<R / kRowsPerCta, dim3(128, kRowsPerCta), 0, st>>>(qkv[l], L + lbqkv, 3 * kW);
         attn_fwd_kernel<<<unsigned(S), 256, attn_fwd_smem(), st>>>(qkv[l], lens, att[l], ob[l]);
         mm<false, false>(bf, int(R), kW, kW, ob[l], kW, L + lWo, kW, F(m.y), kW, false, st, sms);
-        residual_kernel<<<R, kW, 0, st>>>(hin[l], F(m.y), L + lbo, lens, hout[l]);
+        residual_kernel<<<R / kRowsPerCta, dim3(kW, kRowsPerCta), 0, st>>>(hin[l], F(m.y), L + lbo, lens, hout[l]);
     }
     pool_kernel<<<unsigned(S), kW, 0, st>>>(F(m.hC), lens, F(m.pool));
     mm<false, false>(bf, S, kE, kW, F(m.pool), kW, prm + oWout, kE, F(m.e), kE, false, st, sms);
@@ -661,9 +754,9 @@ void loss_backward(Encoder& m, int S, cudaStream_t st, int sms, bool bf) {
     normalize_bwd_kernel<<<unsigned(ceil_div(S, 8)), 256, 0, st>>>(F(m.dz), F(m.e), F(m.nrm), S, F(m.de));
     // e = pool Wout + bout
     mm<true, false>(bf, kW, kE, S, F(m.pool), kW, F(m.de), kE, g + oWout, kE, true, st, sms);
-    colsum_kernel<<<unsigned(ceil_div(S, 256)), 64, 0, st>>>(F(m.de), S, kE, 256, g + obout);
+    colsum(F(m.de), S, kE, g + obout, st);
     mm<false, true>(bf, S, kW, kE, F(m.de), kE, prm + oWout, kE, F(m.dpool), kW, false, st, sms);
-    pool_bwd_kernel<<<R, kW, 0, st>>>(F(m.dpool), lens, F(m.dh));
+    pool_bwd_kernel<<<R / kRowsPerCta, dim3(kW, kRowsPerCta), 0, st>>>(F(m.dpool), lens, F(m.dh));
     float* hin[2] = {F(m.hA), F(m.hB)};
     float* qkv[2] = {F(m.qkv0), F(m.qkv1)};
     float* att[2] = {F(m.a0), F(m.a1)};
@@ -673,21 +766,21 @@ void loss_backward(Encoder& m, int S, cudaStream_t st, int sms, bool bf) {
         float* G = g + oL0 + l * kLayer;
         // h_next = (h + o Wo + bo) * mask; dh is already masked
         mm<true, false>(bf, kW, kW, int(R), ob[l], kW, F(m.dh), kW, G + lWo, kW, true, st, sms);
-        colsum_kernel<<<unsigned(ceil_div(R, 1024)), 128, 0, st>>>(F(m.dh), R, kW, 1024, G + lbo);
+        colsum(F(m.dh), R, kW, G + lbo, st);
         mm<false, true>(bf, int(R), kW, kW, F(m.dh), kW, L + lWo, kW, F(m.dO), kW, false, st, sms);
         attn_bwd_kernel<<<unsigned(S), 256, attn_bwd_smem(), st>>>(qkv[l], att[l], F(m.dO), lens, F(m.dqkv));
         mm<true, false>(bf, kW, 3 * kW, int(R), hin[l], kW, F(m.dqkv), 3 * kW, G + lWqkv, 3 * kW, true, st, sms);
-        colsum_kernel<<<unsigned(ceil_div(R, 1024)), 128, 0, st>>>(F(m.dqkv), R, 3 * kW, 1024, G + lbqkv);
+        colsum(F(m.dqkv), R, 3 * kW, G + lbqkv, st);
         // dh_prev = (dh + dqkv Wqkv^T) * mask
         mm<false, true>(bf, int(R), kW, 3 * kW, F(m.dqkv), 3 * kW, L + lWqkv, 3 * kW, F(m.dh), kW, true, st, sms);
-        mask_kernel<<<R, kW, 0, st>>>(F(m.dh), lens);
+        mask_kernel<<<R / kRowsPerCta, dim3(kW, kRowsPerCta), 0, st>>>(F(m.dh), lens);
     }
     // hA = (h1 + relu(pre2)) * mask
-    relu_bwd_kernel<<<R, kW, 0, st>>>(F(m.dh), F(m.pre2), F(m.dpre));
+    relu_bwd_kernel<<<R / kRowsPerCta, dim3(kW, kRowsPerCta), 0, st>>>(F(m.dh), F(m.pre2), F(m.dpre));
     mm<true, false>(bf, 3 * kW, kW, int(R), F(m.x2), 3 * kW, F(m.dpre), kW, g + oW2, kW, true, st, sms);
-    colsum_kernel<<<unsigned(ceil_div(R, 1024)), 128, 0, st>>>(F(m.dpre), R, kW, 1024, g + ob2);
+    colsum(F(m.dpre), R, kW, g + ob2, st);
     mm<false, true>(bf, int(R), 3 * kW, kW, F(m.dpre), kW, prm + oW2, kW, F(m.dx2), 3 * kW, false, st, sms);
-    col2im_bwd_kernel<<<R, kW, 0, st>>>(F(m.dh), F(m.dx2), F(m.pre1), lens, F(m.dpre));
+    col2im_bwd_kernel<<<R / kRowsPerCta, dim3(kW, kRowsPerCta), 0, st>>>(F(m.dh), F(m.dx2), F(m.pre1), lens, F(m.dpre));
     conv1_bwd_kernel<<<unsigned(ceil_div(R, 256)), 128, 0, st>>>(F(m.dpre), codes, lens, R, 256,
                                                                  g + oW1, g + ob1);
     STB_CUDA(cudaGetLastError());

@@ -9,7 +9,8 @@
 // one 128 x 128 output tile over a range of K chunks: warp 0 bulk-copies A and B chunks through a
 // 3-stage shared-memory ring, one thread of warp 1 issues M=128 N=128 K=16 tcgen05.mma into a
 // 128-column TMEM accumulator, and warps 2-5 (one TMEM lane quarter each) stage the tile in
-// shared memory and store, add or atomically add (split K) it into C with coalesced writes.
+// shared memory, from where all six warps store, add or atomically add (split K) it into C with
+// coalesced writes.
 // Every wait is bounded.
 #include <cuda_bf16.h>
 
@@ -168,9 +169,8 @@ __global__ void __launch_bounds__(kGThreads) gemm_bf16_kernel(GemmBf16Args g) {
         const int quarter = warp & 3;
         if (c1 > c0 && bar_wait_own(BAR(6), 0, g.err)) {
             tc_fence_after();
-            // The warp's 32 x 128 fp32 quarter goes through the (now idle) ring: TMEM lane r ->
-            // staged row r, its 16-byte unit u at u ^ (r & 7) (conflict-free both ways), then
-            // out row by row, a warp writing 128 consecutive columns per instruction.
+            // The warp's 32 x 128 fp32 quarter goes to the (now idle) ring: TMEM lane r -> tile
+            // row quarter * 32 + r, its 16-byte unit u at u ^ (r & 7) (conflict-free both ways).
             float* stage = reinterpret_cast<float*>(smem + quarter * (32 * kGT * 4));
             const uint32_t tl = tmem + (uint32_t(quarter * 32) << 16);
 #pragma unroll 1
@@ -183,23 +183,8 @@ __global__ void __launch_bounds__(kGThreads) gemm_bf16_kernel(GemmBf16Args g) {
                     *reinterpret_cast<uint4*>(stage + lane * kGT + (((grp * 8 + t) ^ (lane & 7)) << 2)) =
                         make_uint4(v[4 * t], v[4 * t + 1], v[4 * t + 2], v[4 * t + 3]);
             }
-            __syncwarp();
-#pragma unroll 1
-            for (int r = 0; r < 32; ++r) {
-                const int row = tm * kGT + quarter * 32 + r;
-                if (row >= g.M) break;
-                float* crow = g.C + int64_t(row) * g.ldc;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int c = lane + 32 * q, col = tn * kGT + c;
-                    if (col < g.N) {
-                        const float x = stage[r * kGT + (((c >> 2) ^ (r & 7)) << 2) + (c & 3)];
-                        if (g.mode == 0) crow[col] = x;
-                        else if (g.mode == 1) crow[col] += x;
-                        else atomicAdd(crow + col, x);
-                    }
-                }
-            }
+        } else {
+            *s_abort = 1;
         }
     }
 
@@ -209,6 +194,54 @@ __global__ void __launch_bounds__(kGThreads) gemm_bf16_kernel(GemmBf16Args g) {
         __syncwarp();
         tc_fence_after();
         tmem_free(tmem, 128);
+    }
+    if (c1 <= c0 || *s_abort) return;
+    // All six warps write the staged tile out, a warp per row at a time (128 consecutive
+    // columns per instruction), four rows per batch so that the loads of the add mode overlap.
+    const float* stage = reinterpret_cast<const float*>(smem);
+    constexpr int kWarps = kGThreads / 32;
+#pragma unroll 1
+    for (int r0 = warp; r0 < kGT; r0 += 4 * kWarps) {
+        float x[4][4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int r = r0 + b * kWarps;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int c = lane + 32 * q;
+                x[b][q] = r < kGT ? stage[r * kGT + (((c >> 2) ^ (r & 7)) << 2) + (c & 3)] : 0.f;
+            }
+        }
+        if (g.mode == 1) {
+            float y[4][4];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int r = r0 + b * kWarps, row = tm * kGT + r;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int col = tn * kGT + lane + 32 * q;
+                    y[b][q] = (r < kGT && row < g.M && col < g.N) ? g.C[int64_t(row) * g.ldc + col] : 0.f;
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) x[b][q] += y[b][q];
+        }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int r = r0 + b * kWarps, row = tm * kGT + r;
+            if (r >= kGT || row >= g.M) continue;
+            float* crow = g.C + int64_t(row) * g.ldc;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int col = tn * kGT + lane + 32 * q;
+                if (col < g.N) {
+                    if (g.mode == 2) atomicAdd(crow + col, x[b][q]);
+                    else crow[col] = x[b][q];
+                }
+            }
+        }
     }
 }
 
