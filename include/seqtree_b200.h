@@ -373,6 +373,14 @@ const char *st_last_kernel_name(void);
 void *st_host_alloc(uint64_t bytes);
 void st_host_free(void *ptr);
 
+/* Host helper for bindings that hold sequences as one buffer of `count` sequences joined by
+ * '\n' (no trailing separator): writes the sequences' bytes back to back into data_out
+ * (size - (count - 1) bytes) and their count + 1 offsets into offsets_out, the st_strings
+ * layout.  Returns the number of bytes written, or -1 when the buffer does not hold exactly
+ * count - 1 separators (a sequence containing '\n'). */
+int64_t st_split_joined(const uint8_t *joined, int64_t size, int64_t count, uint8_t *data_out,
+                        int64_t *offsets_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -42,7 +42,7 @@ def gapblock_matrix(queries, refs, alphabet: str = "aa", matrix: SubstitutionMat
     which builds it.
     """
     alph = parse_alphabet(alphabet)
-    q, r = _lib.Packed(queries), _lib.Packed(refs)
+    q, r = _lib.pack(queries), _lib.pack(refs)
     pen = None if matrix is None else np.ascontiguousarray(matrix.penalty_grid, np.int32)
     pr32 = _prior32(prior)
     out = _result(q.count, r.count)
@@ -57,6 +57,8 @@ def gapblock_matrix(queries, refs, alphabet: str = "aa", matrix: SubstitutionMat
 
 
 def _prior32(prior) -> np.ndarray:
+    if isinstance(prior, np.ndarray) and prior.dtype == np.int32:
+        return np.ascontiguousarray(prior).ravel()
     pr = np.ascontiguousarray(np.asarray(prior, dtype=np.int64), dtype=np.int64).ravel()
     if pr.size and (pr.min() < _INT32[0] or pr.max() > _INT32[1]):
         raise TypeError("prior entries must fit a 32-bit signed integer")
@@ -69,7 +71,7 @@ def gapblock_sparse(queries, refs, max_penalty: int, alphabet: str = "aa",
     """The cells of :func:`gapblock_matrix` with score <= ``max_penalty``, as CSR arrays
     ``(indptr int64[N+1], ref_ids int32[nnz], scores int32[nnz])``; refs ascend within a row."""
     alph = parse_alphabet(alphabet)
-    q, r = _lib.Packed(queries), _lib.Packed(refs)
+    q, r = _lib.pack(queries), _lib.pack(refs)
     pen = None if matrix is None else np.ascontiguousarray(matrix.penalty_grid, np.int32)
     pr32 = _prior32(prior)
     res = _lib.st_sparse()
@@ -94,7 +96,7 @@ def _align(queries, refs, matrix: SubstitutionMatrix, mode: str, gap_open: int, 
         raise TypeError("matrix must be a SubstitutionMatrix")
     alph = parse_alphabet(alphabet)
     md = parse_align_mode(mode)
-    q, r = _lib.Packed(queries), _lib.Packed(refs)
+    q, r = _lib.pack(queries), _lib.pack(refs)
     sim = np.ascontiguousarray(matrix.similarity_grid, np.int32)
     out = _result(q.count, r.count)
     err = _lib.st_error()
@@ -121,7 +123,7 @@ def align_dist_matrix(queries, refs, matrix: SubstitutionMatrix, mode: str = "gl
 
 
 def _distance(a, b, lev: bool) -> ScoreMatrix:
-    pa, pb = _lib.Packed(a), _lib.Packed(b)
+    pa, pb = _lib.pack(a), _lib.pack(b)
     out = _result(pa.count, pb.count)
     err = _lib.st_error()
     fn = _lib.lib.st_levenshtein_matrix if lev else _lib.lib.st_hamming_matrix

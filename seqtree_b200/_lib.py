@@ -129,6 +129,8 @@ SIGNATURES = [
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
     ("st_levenshtein_matrix_sets", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_split_joined", ctypes.c_int64,
+     [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]),
     ("st_levenshtein_matrix_noalloc", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
       ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, _ep]),
@@ -173,6 +175,25 @@ def check(code: int, err: st_error) -> None:
     raise RuntimeError(msg)
 
 
+def _pack_ascii(seqs: list):
+    """(bytes, offsets) of a list of ASCII strings without a per-string Python loop: the list is
+    joined with a newline separator, which the library splits (``st_split_joined``).  None when
+    that does not apply (non-str items, non-ASCII text, or a newline inside a string), so the
+    caller takes the general path."""
+    n = len(seqs)
+    if n == 0:
+        return None
+    try:
+        buf = "\n".join(seqs).encode("ascii")
+    except (TypeError, UnicodeError):
+        return None
+    data = np.empty(max(len(buf) - (n - 1), 1), dtype=np.uint8)
+    off = np.empty(n + 1, dtype=np.int64)
+    if lib.st_split_joined(buf, len(buf), n, data.ctypes.data, off.ctypes.data) < 0:
+        return None
+    return data, off
+
+
 class Packed:
     """A list of sequences as one byte buffer plus int64 offsets (keeps both alive)."""
 
@@ -180,6 +201,11 @@ class Packed:
 
     def __init__(self, seqs):
         seqs = seqs if isinstance(seqs, list) else list(seqs)
+        fast = _pack_ascii(seqs)
+        if fast is not None:
+            self.data, self.offsets = fast
+            self.struct = st_strings(self.data.ctypes.data, self.offsets.ctypes.data, len(seqs))
+            return
         try:
             data = "".join(seqs).encode("utf-8")
             lens = np.fromiter(map(len, seqs), dtype=np.int64, count=len(seqs))
@@ -216,6 +242,11 @@ class Packed:
     def count(self) -> int:
         return int(self.struct.count)
 
+    @property
+    def max_len(self) -> int:
+        """Length in bytes of the longest sequence (0 when there are none)."""
+        return int(np.diff(self.offsets).max()) if self.offsets.size > 1 else 0
+
     def ref(self):
         return ctypes.byref(self.struct)
 
@@ -233,6 +264,11 @@ class _PinnedOwner:
         if self.ptr:
             self._free(ctypes.c_void_p(self.ptr))
             self.ptr = 0
+
+
+def pack(seqs) -> "Packed":
+    """``seqs`` as a :class:`Packed` (returned as is when it already is one)."""
+    return seqs if isinstance(seqs, Packed) else Packed(seqs)
 
 
 def pinned_int32(rows: int, cols: int) -> np.ndarray:

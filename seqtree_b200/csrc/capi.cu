@@ -180,6 +180,26 @@ const char* st_last_kernel_name(void) { return last_kernel(); }
 void* st_host_alloc(uint64_t bytes) { return host_alloc(bytes); }
 void st_host_free(void* ptr) { host_free(ptr); }
 
+int64_t st_split_joined(const uint8_t* joined, int64_t size, int64_t count, uint8_t* data_out,
+                        int64_t* offsets_out) {
+    if (count <= 0 || size < count - 1 || !joined || !data_out || !offsets_out) return -1;
+    const uint8_t* p = joined;
+    const uint8_t* end = joined + size;
+    int64_t w = 0;
+    offsets_out[0] = 0;
+    for (int64_t i = 0; i < count; ++i) {
+        const uint8_t* nl =
+            static_cast<const uint8_t*>(std::memchr(p, '\n', size_t(end - p)));
+        const uint8_t* stop = nl ? nl : end;
+        if ((i + 1 < count) != (nl != nullptr)) return -1;  // separator count != count - 1
+        std::memcpy(data_out + w, p, size_t(stop - p));
+        w += stop - p;
+        offsets_out[i + 1] = w;
+        p = nl ? nl + 1 : end;
+    }
+    return w;
+}
+
 int32_t st_gapblock_matrix(const st_strings* queries, const st_strings* refs, int32_t alphabet,
                            const int32_t* penalty, int32_t matrix_size, int32_t gap_open,
                            int32_t gap_extend, const int32_t* prior, int64_t prior_len,

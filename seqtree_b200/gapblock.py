@@ -16,6 +16,7 @@ from collections.abc import Callable, Iterable, Sequence
 
 import numpy as np
 
+from . import _lib
 from ._core import gapblock_matrix as _gapblock_matrix
 from ._core import gapblock_sparse as _gapblock_sparse
 from .matrix import ScoreMatrix, SubstitutionMatrix
@@ -130,13 +131,23 @@ def prior_cube(prior: GapPrior, width: int):
     """
     fast = getattr(prior, "cube", None)
     if fast is not None:
+        # The built-in priors are pure functions of their parameters, so a cube is built and
+        # checked once per width and kept on the prior (read-only).
+        memo = prior.__dict__.setdefault("_cube_memo", {})
+        hit = memo.get(width)
+        if hit is not None:
+            return hit
         c = fast(width)
         if (c < 0).any():
             mm, dd, ii = (int(x[0]) for x in np.nonzero(c < 0))
             raise ValueError(f"gap_prior({ii}, {dd}, {mm}) = {int(c[mm, dd, ii])} is negative")
         if c.max(initial=0) >= 2 ** 31:
             raise TypeError("prior entries must fit a 32-bit signed integer")
-        return c.astype(np.int32).ravel()
+        out = c.astype(np.int32).ravel()
+        out.flags.writeable = False
+        if len(memo) < 16:
+            memo[width] = out
+        return out
     w1 = width + 1
     cube = [0] * (w1 * w1 * w1)
     for m in range(w1):
@@ -163,12 +174,12 @@ def score_matrix(queries: Sequence[str], refs: Sequence[str],
     materialised once into a lookup cube.  Returns a (len(queries), len(refs)) int32
     :class:`ScoreMatrix`; ``numpy.asarray`` wraps it without copying.
     """
-    q, r = list(queries), list(refs)
     if gap_open is None:
         gap_open = _default_gap_open(matrix)
     if gap_open < 0 or gap_extend < 0:
         raise ValueError("gap_open and gap_extend must be >= 0")
-    width = max(max(map(len, q), default=0), max(map(len, r), default=0))
+    q, r = _lib.pack(queries), _lib.pack(refs)
+    width = max(q.max_len, r.max_len)
     cube = prior_cube(gap_prior, width) if gap_prior is not None else []
     return _gapblock_matrix(q, r, alphabet, matrix, gap_open, gap_extend, cube, width, threads)
 
@@ -224,16 +235,16 @@ def score_sparse(queries: Sequence[str], refs: Sequence[str], max_penalty: int,
     """
     if max_penalty < 0:
         raise ValueError("max_penalty must be >= 0")
-    q, r = list(queries), list(refs)
     if gap_open is None:
         gap_open = _default_gap_open(matrix)
     if gap_open < 0 or gap_extend < 0:
         raise ValueError("gap_open and gap_extend must be >= 0")
-    width = max(max(map(len, q), default=0), max(map(len, r), default=0))
+    q, r = _lib.pack(queries), _lib.pack(refs)
+    width = max(q.max_len, r.max_len)
     cube = prior_cube(gap_prior, width) if gap_prior is not None else []
     indptr, ref_ids, scores = _gapblock_sparse(q, r, max_penalty, alphabet, matrix, gap_open,
                                               gap_extend, cube, width, threads)
-    return SparseScores(indptr, ref_ids, scores, (len(q), len(r)), max_penalty)
+    return SparseScores(indptr, ref_ids, scores, (q.count, r.count), max_penalty)
 
 
 class GapBlockIndex:

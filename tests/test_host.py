@@ -98,6 +98,34 @@ def test_packing_offsets_and_utf8():
         _lib.Packed([1, 2])
 
 
+@pytest.mark.parametrize("seqs", [["CASS", "", "AB"], [""], ["", ""], ["ACDEFGHIKLMNPQRSTVWY"] * 3,
+                                  ["A\nB", "C"], ["\n"], ["A", "B\n"], [b"AC", "D"], ["é", "a"]])
+def test_joined_packing_matches_the_general_path(seqs):
+    """The newline-joined fast path (``st_split_joined``, host code) and the per-string path give
+    the same bytes and offsets; strings with a newline, bytes items and non-ASCII text take the
+    general path."""
+    fast = _lib._pack_ascii(list(seqs))
+    enc = [s if isinstance(s, bytes) else s.encode() for s in seqs]
+    want_off = np.concatenate([[0], np.cumsum([len(e) for e in enc])])
+    if fast is None:
+        assert any(b"\n" in e for e in enc) or any(isinstance(s, bytes) for s in seqs) or \
+            any(not s.isascii() for s in seqs if isinstance(s, str))
+    else:
+        assert fast[1].tolist() == want_off.tolist()
+        assert bytes(fast[0][:want_off[-1]]) == b"".join(enc)
+    p = _lib.pack(seqs)
+    assert p.offsets.tolist() == want_off.tolist() and _lib.pack(p) is p
+    assert p.max_len == max(len(e) for e in enc)
+
+
+def test_builtin_prior_cubes_are_memoised_read_only():
+    cp = central_prior(7)
+    a, b = prior_cube(cp, 9), prior_cube(cp, 9)
+    assert a is b and not a.flags.writeable and a.dtype == np.int32
+    assert prior_cube(cp, 4) is not a and prior_cube(central_prior(7), 9) is not a
+    assert (a == prior_cube(central_prior(7), 9)).all()
+
+
 def test_pinned_results_are_plain_int32_arrays():
     a = _lib.pinned_int32(3, 4)
     assert a.shape == (3, 4) and a.dtype == np.int32 and a.flags.c_contiguous
