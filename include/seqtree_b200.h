@@ -105,6 +105,27 @@ int32_t st_align_pair(const char *query, int64_t query_len, const char *ref, int
                       char *aligned_ref, char *ops, int64_t capacity, st_error *err);
 
 /*
+ * Penalty-minimising global alignment with traceback for a list of (query, ref) pairs.
+ * Replaces seqtree::Index::align (src/index.cpp:105-179; Python Index.align,
+ * src/_bindings.cpp:197-201,454): pair p aligns queries[query_idx[p]] to refs[ref_idx[p]] with
+ * substitution cost penalty[a * matrix_size + b] (the matrix's penalty grid; NULL: unit cost
+ * on codec equality, case-insensitive) and affine gaps gap_open + (L-1) * gap_extend.  Same
+ * int32 arithmetic, tie order and messages as the reference: "invalid symbol 'c' in reference
+ * #k", "matrix size does not match the alphabet", "invalid symbol 'c' in query", "seqtree:
+ * gap_open and gap_extend must be >= 0" (checked in that order).  scores[p] and lengths[p]
+ * (alignment columns) are always written; aligned_query, aligned_ref and ops (all three or
+ * none) receive NUL-terminated strings at p * stride (stride >= longest query + longest ref + 1)
+ * made of the caller's own characters; ops per column 'M' match, 'S' substitution, 'D' query
+ * residue against a gap, 'I' ref residue against a gap.
+ */
+int32_t st_penalty_align_pairs(const st_strings *queries, const st_strings *refs,
+                               const int32_t *query_idx, const int32_t *ref_idx, int64_t n,
+                               int32_t alphabet, const int32_t *penalty, int32_t matrix_size,
+                               int32_t gap_open, int32_t gap_extend, int32_t *scores,
+                               char *aligned_query, char *aligned_ref, char *ops, int64_t stride,
+                               int32_t *lengths, st_error *err);
+
+/*
  * Dense sequence-level Gram distance d = s(a,a) + s(b,b) - 2 s(a,b) over Gotoh scores.
  * Replaces seqtree::align_dist_matrix (include/seqtree/seqtree.hpp:206-209,
  * src/pairwise.cpp:346-352) and _core.align_dist_matrix (src/_bindings.cpp:548-568).

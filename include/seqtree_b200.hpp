@@ -210,6 +210,52 @@ inline Alignment align_pair(std::string_view query, std::string_view ref, const 
     return al;
 }
 
+// Penalty-minimising global alignments of the pairs (queries[query_idx[p]], refs[ref_idx[p]]),
+// one GPU launch for the batch.  seqtree::Index::align (include/seqtree/seqtree.hpp, Index;
+// src/index.cpp:105-179) with `refs` as the index's references: `matrix` null means unit cost,
+// gaps cost gap_open + (L-1) * gap_extend, and the aligned strings keep the callers' characters.
+inline std::vector<Alignment> penalty_align_pairs(const std::vector<std::string>& queries,
+                                                  const std::vector<std::string>& refs,
+                                                  const std::vector<int32_t>& query_idx,
+                                                  const std::vector<int32_t>& ref_idx,
+                                                  Alphabet alphabet, const SubstitutionMatrix* matrix,
+                                                  int32_t gap_open, int32_t gap_extend) {
+    if (query_idx.size() != ref_idx.size())
+        throw std::invalid_argument("query_idx and ref_idx must have the same length");
+    detail::Packed q(queries), r(refs);
+    size_t mq = 0, mr = 0;
+    for (const auto& s : queries) mq = std::max(mq, s.size());
+    for (const auto& s : refs) mr = std::max(mr, s.size());
+    const size_t n = query_idx.size(), stride = mq + mr + 1;
+    std::vector<int32_t> scores(n), lengths(n);
+    std::string aq(std::max<size_t>(n * stride, 1), '\0'), ar(aq.size(), '\0'), ops(aq.size(), '\0');
+    st_error err{};
+    detail::check(st_penalty_align_pairs(&q.view, &r.view, query_idx.data(), ref_idx.data(),
+                                         int64_t(n), int32_t(alphabet),
+                                         matrix ? matrix->penalty_data() : nullptr,
+                                         matrix ? matrix->size() : 0, gap_open, gap_extend,
+                                         scores.data(), aq.data(), ar.data(), ops.data(),
+                                         int64_t(stride), lengths.data(), &err),
+                  err);
+    std::vector<Alignment> out(n);
+    for (size_t p = 0; p < n; ++p) {
+        const size_t at = p * stride, len = size_t(lengths[p]);
+        out[p].aligned_query.assign(aq, at, len);
+        out[p].aligned_ref.assign(ar, at, len);
+        out[p].ops.assign(ops, at, len);
+        out[p].score = scores[p];
+    }
+    return out;
+}
+
+// One pair of penalty_align_pairs: Index::align(query, ref_id, params) for ref = ref_seq(ref_id).
+inline Alignment penalty_align(std::string_view query, std::string_view ref,
+                               const SubstitutionMatrix* matrix, Alphabet alphabet,
+                               int32_t gap_open, int32_t gap_extend) {
+    return penalty_align_pairs({std::string(query)}, {std::string(ref)}, {0}, {0}, alphabet,
+                               matrix, gap_open, gap_extend)[0];
+}
+
 // Dense N*K single-gap-block penalty matrix.  seqtree::gapblock_matrix
 // (include/seqtree/seqtree.hpp:215-222).  `matrix` null means unit cost; `prior` is the
 // [m][d][i] cube with stride prior_width + 1, or empty for none.

@@ -198,6 +198,11 @@ def ref():
             ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
             _i32p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int64,
             ctypes.c_char_p, ctypes.c_int]
+        lib.ref_index_align.argtypes = [
+            ctypes.c_char_p, _i64p, ctypes.c_int64, ctypes.c_int, ctypes.c_int64,
+            ctypes.c_char_p, ctypes.c_int64, ctypes.c_int, _i32p, ctypes.c_int, ctypes.c_int32,
+            ctypes.c_int32, _i32p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+            ctypes.c_int64, ctypes.c_char_p, ctypes.c_int]
         lib.ref_distance_matrix.argtypes = [
             ctypes.c_char_p, _i64p, ctypes.c_int64, ctypes.c_char_p, _i64p, ctypes.c_int64,
             ctypes.c_int, ctypes.c_int, _i32p, ctypes.c_char_p, ctypes.c_int]
@@ -309,6 +314,102 @@ def ref_align_pair(q, r, matrix="blosum62", mode="global", gap_open=11, gap_exte
     if st:
         _raise(st, err)
     return (out.value,) + tuple(b.value.decode("latin-1") for b in bufs)
+
+
+def ref_index_align(refs, ref_id, query, matrix=None, gap_open=1, gap_extend=1,
+                    alphabet="aa") -> tuple[int, str, str, str]:
+    """The reference's Index.build(refs).align(ref_id, query, params):
+    (score, aligned_query, aligned_ref, ops).  ``matrix`` None is unit cost."""
+    mid, simp, size, _keep = _matrix_args(matrix)
+    rd, ro = pack(refs)
+    qb = query.encode("latin-1")
+    cap = len(qb) + max((len(r) for r in refs), default=0) + 2
+    out = ctypes.c_int32(0)
+    bufs = [ctypes.create_string_buffer(cap) for _ in range(3)]
+    err = ctypes.create_string_buffer(512)
+    st = ref().ref_index_align(rd.tobytes(), _p(ro, _i64p), len(refs), ALPHABETS[alphabet],
+                               int(ref_id), qb, len(qb), mid, simp, size, gap_open, gap_extend,
+                               ctypes.byref(out), bufs[0], bufs[1], bufs[2], cap, err, 512)
+    if st:
+        _raise(st, err)
+    return (out.value,) + tuple(b.value.decode("latin-1") for b in bufs)
+
+
+def _wrap32(x: int) -> int:
+    return (x + 2 ** 31) % 2 ** 32 - 2 ** 31
+
+
+def penalty_align(query, ref, pen=None, gap_open=1, gap_extend=1,
+                  alphabet="aa") -> tuple[int, str, str, str]:
+    """Port of seqtree src/index.cpp:105-179 (Index::align), pure Python for small cases:
+    min-cost global Gotoh in wrapping int32 with kInf = INT32_MAX // 4 borders (:127-137),
+    ties M, then X / Y only when strictly smaller (:140-145), the traceback of :157-178 with
+    the caller's own characters.  ``pen`` is the penalty grid (codes x codes) or None for unit
+    cost on codec equality.  Returns (score, aligned_query, aligned_ref, ops)."""
+    def codes(s):
+        c, o = encode([s], alphabet)
+        return [int(x) for x in c[:int(o[1])]]
+
+    qc, rc = codes(query), codes(ref)
+    if gap_open < 0 or gap_extend < 0:
+        raise ValueError("seqtree: gap_open and gap_extend must be >= 0")
+    go, ge = gap_open, gap_extend
+    inf = (2 ** 31 - 1) // 4
+    m, n = len(qc), len(rc)
+    M = [[inf] * (n + 1) for _ in range(m + 1)]
+    X = [[inf] * (n + 1) for _ in range(m + 1)]
+    Y = [[inf] * (n + 1) for _ in range(m + 1)]
+    bM = [[0] * (n + 1) for _ in range(m + 1)]
+    bX = [[0] * (n + 1) for _ in range(m + 1)]
+    bY = [[0] * (n + 1) for _ in range(m + 1)]
+    M[0][0] = 0
+    for i in range(1, m + 1):
+        X[i][0] = _wrap32(go + (i - 1) * ge)
+        bX[i][0] = 1 if i > 1 else 0
+    for j in range(1, n + 1):
+        Y[0][j] = _wrap32(go + (j - 1) * ge)
+        bY[0][j] = 2 if j > 1 else 0
+
+    def best3(mv, xv, yv):
+        v, w = mv, 0
+        if xv < v:
+            v, w = xv, 1
+        if yv < v:
+            v, w = yv, 2
+        return v, w
+
+    for i in range(1, m + 1):
+        for j in range(1, n + 1):
+            sp = (0 if qc[i - 1] == rc[j - 1] else 1) if pen is None else int(pen[qc[i - 1]][rc[j - 1]])
+            v, bM[i][j] = best3(M[i - 1][j - 1], X[i - 1][j - 1], Y[i - 1][j - 1])
+            M[i][j] = _wrap32(sp + v)
+            X[i][j], bX[i][j] = best3(_wrap32(M[i - 1][j] + go), _wrap32(X[i - 1][j] + ge),
+                                      _wrap32(Y[i - 1][j] + go))
+            Y[i][j], bY[i][j] = best3(_wrap32(M[i][j - 1] + go), _wrap32(X[i][j - 1] + go),
+                                      _wrap32(Y[i][j - 1] + ge))
+    score, st = best3(M[m][n], X[m][n], Y[m][n])
+    aq, ar, ops = [], [], []
+    i, j = m, n
+    while i > 0 or j > 0:
+        if st == 0:
+            aq.append(query[i - 1])
+            ar.append(ref[j - 1])
+            ops.append("M" if qc[i - 1] == rc[j - 1] else "S")
+            st = bM[i][j]
+            i, j = i - 1, j - 1
+        elif st == 1:
+            aq.append(query[i - 1])
+            ar.append("-")
+            ops.append("D")
+            st = bX[i][j]
+            i -= 1
+        else:
+            aq.append("-")
+            ar.append(ref[j - 1])
+            ops.append("I")
+            st = bY[i][j]
+            j -= 1
+    return score, "".join(reversed(aq)), "".join(reversed(ar)), "".join(reversed(ops))
 
 
 def ref_distance_matrix(a, b, levenshtein: bool, threads=0) -> np.ndarray:

@@ -2,7 +2,8 @@
 //
 // oracle/Makefile compiles this file together with the reference's own hot-path sources
 // (src/codec.cpp, src/substitution_matrix.cpp, src/gapblock.cpp, src/pairwise.cpp,
-// src/distance.cpp of seqtree 0.6.0) into oracle/_ref/libseqtree_ref.so.  The tests use it to
+// src/distance.cpp of seqtree 0.6.0, and the index sources Index::align needs) into
+// oracle/_ref/libseqtree_ref.so.  The tests use it to
 // generate and re-check golden vectors, and the benchmark's reference arm times it as the CPU
 // baseline.  Nothing here is part of the product.
 //
@@ -152,6 +153,35 @@ int ref_align_pair(const char* q, int64_t m, const char* r, int64_t n, int alpha
                                         *mat, Alphabet(alphabet),
                                         local ? AlignMode::Local : AlignMode::Global, gap_open,
                                         gap_extend);
+        *score = al.score;
+        for (auto [dst, src] : {std::pair<char*, const std::string*>{aq, &al.aligned_query},
+                                {ar, &al.aligned_ref}, {ops, &al.ops}}) {
+            const size_t len = std::min(src->size(), size_t(cap - 1));
+            std::memcpy(dst, src->data(), len);
+            dst[len] = 0;
+        }
+    });
+}
+
+// seqtree::Index::align (src/index.cpp:105-179): builds an Index over the packed refs, then
+// aligns `q` to reference `ref_id`.  matrix_id < 0 is unit cost (a null matrix); the strings go
+// NUL-terminated into caller buffers of `cap` bytes.
+int ref_index_align(const char* rb, const int64_t* ro, int64_t nr, int alphabet, int64_t ref_id,
+                    const char* q, int64_t m, int matrix_id, const int32_t* sim, int size,
+                    int32_t gap_open, int32_t gap_extend, int32_t* score, char* aq, char* ar,
+                    char* ops, int64_t cap, char* err, int errlen) {
+    return guard(err, errlen, [&] {
+        auto idx = Index::build(unpack(rb, ro, nr), Alphabet(alphabet));
+        std::optional<SubstitutionMatrix> mat;
+        if (matrix_id >= 0) {
+            mat = make(matrix_id, sim, size);
+            if (!mat) throw std::invalid_argument("bad matrix id");
+        }
+        SearchParams p;
+        p.gap_open = gap_open;
+        p.gap_extend = gap_extend;
+        p.matrix = mat ? &*mat : nullptr;
+        const Alignment al = idx->align(std::string_view(q, size_t(m)), uint32_t(ref_id), p);
         *score = al.score;
         for (auto [dst, src] : {std::pair<char*, const std::string*>{aq, &al.aligned_query},
                                 {ar, &al.aligned_ref}, {ops, &al.ops}}) {

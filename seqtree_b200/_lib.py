@@ -56,6 +56,10 @@ SIGNATURES = [
      [ctypes.c_char_p, ctypes.c_int64, ctypes.c_char_p, ctypes.c_int64, _i32p, ctypes.c_int32,
       ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_char_p,
       ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int64, _ep]),
+    ("st_penalty_align_pairs", ctypes.c_int32,
+     [_sp, _sp, _i32p, _i32p, ctypes.c_int64, ctypes.c_int32, _i32p, ctypes.c_int32,
+      ctypes.c_int32, ctypes.c_int32, _i32p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_int64, _i32p, _ep]),
     ("st_hamming_matrix", ctypes.c_int32, [_sp, _sp, ctypes.c_int32, ctypes.c_void_p, _ep]),
     ("st_levenshtein_matrix", ctypes.c_int32, [_sp, _sp, ctypes.c_int32, ctypes.c_void_p, _ep]),
     ("st_gapblock_sparse", ctypes.c_int32,

@@ -51,6 +51,10 @@ void align_pairs_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* qi_d, con
                       int64_t n, const int32_t* similarity, int32_t matrix_size, int32_t mode,
                       int32_t go, int32_t ge, int64_t* score_d, int32_t* start_d, char* qa_d,
                       char* ra_d, char* ops_d, int64_t out_cap, cudaStream_t stream);
+void penalty_align_pairs_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* qi_d,
+                              const int32_t* ri_d, int64_t n, const int32_t* penalty,
+                              int32_t matrix_size, int32_t go, int32_t ge, int32_t* score_d,
+                              int32_t* start_d, char* ops_d, int64_t out_cap, cudaStream_t stream);
 void thetas_csr(const int64_t* indptr_d, const int32_t* scores_d, int64_t rows, int32_t k, int rule3,
                 int32_t theta_max, int exclude_exact, int32_t* out_d, cudaStream_t stream);
 int last_launches();
@@ -442,6 +446,101 @@ int32_t st_align_pair(const char* query, int64_t query_len, const char* ref, int
         std::memcpy(aligned_query, aq.c_str(), aq.size() + 1);
         std::memcpy(aligned_ref, ar.c_str(), ar.size() + 1);
         std::memcpy(ops, op.c_str(), op.size() + 1);
+    });
+}
+
+int32_t st_penalty_align_pairs(const st_strings* queries, const st_strings* refs,
+                               const int32_t* query_idx, const int32_t* ref_idx, int64_t n,
+                               int32_t alphabet, const int32_t* penalty, int32_t matrix_size,
+                               int32_t gap_open, int32_t gap_extend, int32_t* scores,
+                               char* aligned_query, char* aligned_ref, char* ops, int64_t stride,
+                               int32_t* lengths, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        check_strings(queries);
+        check_strings(refs);
+        const int A = alphabet_size(alphabet);
+        if (A == 0) fail(ST_EINVAL, "unknown alphabet code " + std::to_string(alphabet));
+        if (n < 0) fail(ST_EINVAL, "seqtree_b200: negative pair count");
+        if (n > 0 && (!query_idx || !ref_idx || !scores || !lengths))
+            fail(ST_EINVAL, "seqtree_b200: null pair list or output");
+        const int64_t N = count_of(queries), K = count_of(refs);
+        int64_t mq = 0, mr = 0;
+        for (int64_t i = 0; i < N; ++i) mq = std::max(mq, queries->offsets[i + 1] - queries->offsets[i]);
+        for (int64_t i = 0; i < K; ++i) mr = std::max(mr, refs->offsets[i + 1] - refs->offsets[i]);
+        const bool strings = aligned_query || aligned_ref || ops;
+        if (strings && (!aligned_query || !aligned_ref || !ops))
+            fail(ST_EINVAL, "seqtree_b200: give all three string outputs or none");
+        if (strings && stride < mq + mr + 1)
+            fail(ST_EINVAL, "seqtree_b200: string stride shorter than the longest query + ref + 1");
+        for (int64_t p = 0; p < n; ++p)
+            if (query_idx[p] < 0 || query_idx[p] >= N || ref_idx[p] < 0 || ref_idx[p] >= K)
+                fail(ST_EINVAL, "seqtree_b200: pair index out of range");
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        clear_flags(ctx);
+        // Order of the reference's checks: the refs at Index::build (src/trie.cpp:62-66), the
+        // matrix against the alphabet (src/_bindings.cpp:90-95), then, in Index::align, the
+        // query's symbols and the gap costs (src/index.cpp:109-114).
+        Transient t;
+        int64_t bad = -1;
+        char bc = 0;
+        t.r.reset(make_seqset(refs, alphabet, ctx.stream, &bad, &bc, ctx.tr));
+        if (bad >= 0) {
+            const auto& off = t.r->h_off;
+            const int64_t id = int64_t(std::upper_bound(off.begin(), off.end(), bad) - off.begin()) - 1;
+            fail(ST_EINVAL, std::string("invalid symbol '") + bc + "' in reference #" +
+                                std::to_string(id));
+        }
+        if (penalty && matrix_size != A) fail(ST_EINVAL, "matrix size does not match the alphabet");
+        t.q.reset(make_seqset(queries, alphabet, ctx.stream, &bad, &bc, ctx.tq));
+        if (bad >= 0) fail(ST_EINVAL, std::string("invalid symbol '") + bc + "' in query");
+        if (gap_open < 0 || gap_extend < 0)
+            fail(ST_EINVAL, "seqtree: gap_open and gap_extend must be >= 0");
+        if (n == 0) return;
+        const int64_t slot = std::max<int64_t>(mq + mr, 1);
+        // device: pair indices, scores, starts, op slots
+        const size_t idx_b = size_t(n) * 8, sc_b = size_t(n) * 4, st_b = size_t(n) * 4;
+        auto* base = static_cast<uint8_t*>(ctx.work_b.get(idx_b + sc_b + st_b + size_t(n * slot) + 64));
+        auto* qi_d = reinterpret_cast<int32_t*>(base);
+        auto* ri_d = qi_d + n;
+        auto* sc_d = reinterpret_cast<int32_t*>(base + idx_b);
+        auto* st_d = reinterpret_cast<int32_t*>(base + idx_b + sc_b);
+        char* ops_d = reinterpret_cast<char*>(base + idx_b + sc_b + st_b);
+        h2d(qi_d, query_idx, size_t(n) * 4, ctx.stream);
+        h2d(ri_d, ref_idx, size_t(n) * 4, ctx.stream);
+        penalty_align_pairs_sets(*t.q, *t.r, qi_d, ri_d, n, penalty, matrix_size, gap_open,
+                                 gap_extend, sc_d, st_d, ops_d, slot, ctx.stream);
+        std::vector<int32_t> starts(static_cast<size_t>(n));
+        std::vector<char> opsh(strings ? static_cast<size_t>(n * slot) : 0);
+        STB_CUDA(cudaMemcpyAsync(scores, sc_d, sc_b, cudaMemcpyDeviceToHost, ctx.stream));
+        STB_CUDA(cudaMemcpyAsync(starts.data(), st_d, st_b, cudaMemcpyDeviceToHost, ctx.stream));
+        if (strings)
+            STB_CUDA(cudaMemcpyAsync(opsh.data(), ops_d, opsh.size(), cudaMemcpyDeviceToHost,
+                                     ctx.stream));
+        STB_CUDA(cudaStreamSynchronize(ctx.stream));
+        for (int64_t p = 0; p < n; ++p) {
+            if (starts[size_t(p)] < 0)
+                fail(ST_EOVERFLOW, "seqtree_b200: the traceback left the matrix -- gap costs near "
+                                   "2^29 overflow the reference's int32 recurrence");
+            const int64_t len = slot - starts[size_t(p)];
+            lengths[p] = int32_t(len);
+            if (!strings) continue;
+            // The aligned strings carry the caller's own characters (src/index.cpp:160-172).
+            const char* op = opsh.data() + p * slot + starts[size_t(p)];
+            const char* q = queries->bytes + queries->offsets[query_idx[p]];
+            const char* r = refs->bytes + refs->offsets[ref_idx[p]];
+            char* aq = aligned_query + p * stride;
+            char* ar = aligned_ref + p * stride;
+            char* oo = ops + p * stride;
+            for (int64_t c = 0; c < len; ++c) {
+                const char o = op[c];
+                aq[c] = o == 'I' ? '-' : *q++;
+                ar[c] = o == 'D' ? '-' : *r++;
+                oo[c] = o;
+            }
+            aq[len] = ar[len] = oo[len] = 0;
+        }
     });
 }
 

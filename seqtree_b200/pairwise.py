@@ -23,7 +23,7 @@ from ._core import align_score_matrix as _score_matrix
 from .matrix import ScoreMatrix, SubstitutionMatrix, alphabet_symbols, parse_align_mode, parse_alphabet
 
 __all__ = ["score", "align", "align_batch", "align_pairs", "Alignment", "score_matrix",
-           "dist_matrix"]
+           "dist_matrix", "penalty_align", "penalty_align_pairs"]
 
 
 def score(query: str, ref: str, matrix: SubstitutionMatrix, mode: str = "global",
@@ -132,3 +132,78 @@ def align_pairs(queries: Sequence[str], refs: Sequence[str], query_idx, ref_idx,
         out.append(Alignment(qa[p, s:].tobytes().decode(), ra[p, s:].tobytes().decode(),
                              ops[p, s:].tobytes().decode(), int(sc[p])))
     return out
+
+
+# ------------------------------------------------------------ penalty alignment (Index.align)
+_MATRIX_NAMES = ("identity", "blosum62", "blosum45", "blosum80", "pam250", "pam100", "structural")
+
+
+def _penalty_grid(matrix, alphabet: str) -> np.ndarray | None:
+    """The penalty grid of ``matrix`` as seqtree's SearchParams takes it (src/_bindings.cpp:
+    67-119): None or '' is unit cost, a name is a built-in matrix ('identity' is unit cost of the
+    alphabet's size; the others need amino acids), or a SubstitutionMatrix."""
+    if matrix is None:
+        return None
+    if isinstance(matrix, str):
+        name = matrix.lower()
+        if name and name not in _MATRIX_NAMES:
+            raise ValueError(f"unknown matrix '{matrix}' (use '', 'identity', 'BLOSUM62', "
+                             "'BLOSUM45', 'BLOSUM80', 'PAM250', 'PAM100', 'structural', or a "
+                             "SubstitutionMatrix)")
+        if not name:
+            return None
+        if name == "identity":
+            matrix = SubstitutionMatrix.unit(len(alphabet_symbols(alphabet)))
+        elif parse_alphabet(alphabet) != 0:
+            raise ValueError(f"{name} requires the amino-acid alphabet")
+        else:
+            matrix = SubstitutionMatrix._named(name)
+    if not isinstance(matrix, SubstitutionMatrix):
+        raise TypeError("matrix must be a name string or a SubstitutionMatrix")
+    return np.ascontiguousarray(matrix.penalty_grid, np.int32)
+
+
+def penalty_align_pairs(queries: Sequence[str], refs: Sequence[str], query_idx, ref_idx,
+                        matrix=None, gap_open: int = 1, gap_extend: int = 1,
+                        alphabet: str = "aa") -> list[Alignment]:
+    """Penalty-minimising global alignments of the listed pairs ``(queries[query_idx[p]],
+    refs[ref_idx[p]])`` on the GPU, one thread per pair: seqtree's ``Index.align(ref_id, query,
+    SearchParams(matrix=..., gap_open=..., gap_extend=...))`` (src/index.cpp:105-179) with
+    ``refs`` as the index's references.  ``score`` is the summed substitution penalty plus
+    ``gap_open + (L-1) * gap_extend`` per gap run (lower is closer); unit cost when ``matrix``
+    is None.  The aligned strings keep the caller's characters (case included)."""
+    alph = parse_alphabet(alphabet)
+    pen = _penalty_grid(matrix, alphabet)
+    go, ge = _i32("gap_open", gap_open), _i32("gap_extend", gap_extend)
+    qi = np.ascontiguousarray(query_idx, np.int32).ravel()
+    ri = np.ascontiguousarray(ref_idx, np.int32).ravel()
+    if qi.size != ri.size:
+        raise ValueError("query_idx and ref_idx must have the same length")
+    q, r = _lib.pack(queries), _lib.pack(refs)
+    n = int(qi.size)
+    if n and (qi.min() < 0 or qi.max() >= q.count or ri.min() < 0 or ri.max() >= r.count):
+        raise IndexError("pair index out of range")
+    stride = q.max_len + r.max_len + 1
+    scores = np.zeros(n, np.int32)
+    lengths = np.zeros(n, np.int32)
+    bufs = [ctypes.create_string_buffer(max(n * stride, 1)) for _ in range(3)]
+    err = _lib.st_error()
+    _lib.check(_lib.lib.st_penalty_align_pairs(
+        q.ref(), r.ref(), _lib.i32_ptr(qi), _lib.i32_ptr(ri), n, alph, _lib.i32_ptr(pen),
+        0 if pen is None else pen.shape[0], go, ge, _lib.i32_ptr(scores), bufs[0], bufs[1],
+        bufs[2], stride, _lib.i32_ptr(lengths), ctypes.byref(err)), err)
+    raw = [b.raw for b in bufs]
+    out = []
+    for p in range(n):
+        a, L = p * stride, int(lengths[p])
+        out.append(Alignment(raw[0][a:a + L].decode("latin-1"), raw[1][a:a + L].decode("latin-1"),
+                             raw[2][a:a + L].decode("latin-1"), int(scores[p])))
+    return out
+
+
+def penalty_align(query: str, ref: str, matrix=None, gap_open: int = 1, gap_extend: int = 1,
+                  alphabet: str = "aa") -> Alignment:
+    """One pair of :func:`penalty_align_pairs`: what ``Index.build(refs).align(k, query,
+    params)`` returns for ``ref = refs[k]``."""
+    return penalty_align_pairs([query], [ref], [0], [0], matrix, gap_open, gap_extend,
+                               alphabet)[0]

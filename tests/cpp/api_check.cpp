@@ -133,6 +133,17 @@ int main(int argc, char** argv) {
                 std::cout << "alignpair " << i << ' ' << md << " !" << e.what() << '\n';
             }
         }
+    // Index::align: "penalign <i> <score> <aligned_query> <aligned_ref> <ops>", BLOSUM62 for
+    // even i, unit cost for odd i
+    for (size_t i = 0; i < std::min<size_t>(q.size(), r.size()); ++i) {
+        const st::Alignment al = st::penalty_align_pairs(q, r, {int32_t(i)}, {int32_t(i)}, AA,
+                                                         (i & 1) ? nullptr : &b62, 11, 1)[0];
+        std::cout << "penalign " << i << ' ' << al.score << ' ' << show(al.aligned_query) << ' '
+                  << show(al.aligned_ref) << ' ' << show(al.ops) << '\n';
+    }
+    call("penalty_align_bad_symbol", [&] {
+        return std::vector<int32_t>{st::penalty_align("CASJ", "CASS", nullptr, AA, 1, 1).score};
+    });
     call("align_pair_bad_symbol", [&] {
         return std::vector<int32_t>{st::align_pair("CASJ", "CASS", b62, AA, st::AlignMode::Global,
                                                    11, 1).score};

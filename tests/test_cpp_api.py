@@ -86,7 +86,8 @@ def test_cpp_api_matches_the_oracle(api_check, cuda_ready, seed):
                        f"P {width} {cube.size}", " ".join(map(str, cube.tolist()))]) + "\n"
     out = subprocess.run([str(api_check), "run"], input=stdin, check=True, capture_output=True,
                          text=True).stdout
-    got = parse("\n".join(line for line in out.splitlines() if not line.startswith("alignpair ")))
+    got = parse("\n".join(line for line in out.splitlines()
+                          if not line.startswith(("alignpair ", "penalign "))))
     b62 = SubstitutionMatrix.blosum62()
     N, K = len(q), len(r)
 
@@ -117,6 +118,14 @@ def test_cpp_api_matches_the_oracle(api_check, cuda_ready, seed):
     assert got["gapblock_bad_symbol"].startswith("invalid_argument: symbol 'J'")
     assert got["align_overflow"].startswith("overflow_error: seqtree: the alignment score")
     assert got["align_pair_bad_symbol"] == "invalid_argument: invalid symbol 'J' in sequence"
+    assert got["penalty_align_bad_symbol"] == "invalid_argument: invalid symbol 'J' in query"
+    pen = [line.split(" ") for line in out.splitlines() if line.startswith("penalign ")]
+    assert len(pen) == min(N, K)
+    for _, i, score, aq, ar, ops in pen:
+        un = lambda x: "" if x == "~" else x  # noqa: E731
+        i = int(i)
+        want = oracle.penalty_align(q[i], r[i], None if i & 1 else b62.penalty_grid, 11, 1)
+        assert (int(score), un(aq), un(ar), un(ops)) == want
     pairs = [line.split(" ") for line in out.splitlines() if line.startswith("alignpair ")]
     assert len(pairs) == 2 * min(N, K)
     for _, i, md, score, aq, ar, ops in pairs:

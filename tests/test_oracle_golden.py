@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import prior_by_name
+from conftest import load_golden, prior_by_name
 from seqtree_b200.gapblock import prior_cube
 from seqtree_b200.matrix import SubstitutionMatrix
 
@@ -200,3 +200,52 @@ def test_port_matches_reference_build_on_fresh_inputs():
     for mode in ("global", "local"):
         assert (oracle.ref_align_matrix(q, r, "blosum62", mode=mode, dist=True) ==
                 oracle.align_matrix(q, r, sim, mode=mode, dist=True)).all()
+
+
+# --- penalty alignment (Index::align) ------------------------------------------------------
+
+def _index_pen(name):
+    if name is None:
+        return None
+    return getattr(SubstitutionMatrix, name)().penalty_grid
+
+
+def test_oracle_index_align_golden():
+    """The port of Index::align (src/index.cpp:105-179) against the reference's own output on
+    seeded pairs: unit cost and five matrices, gaps from free to 4e8, mixed case, empty sides."""
+    g = load_golden("index_align")
+    refs = g["refs"]
+    for case in g["cases"]:
+        pen = _index_pen(case["matrix"])
+        for q, k, score, aq, ar, ops in case["pairs"]:
+            got = oracle.penalty_align(q, refs[k], pen, case["gap_open"], case["gap_extend"])
+            assert got == (score, aq, ar, ops), (case["matrix"], case["gap_open"], q, refs[k])
+
+
+def test_oracle_index_align_known_answers():
+    """Known answers of the reference's tests: tests/python/test_engine_guards.py:53-79,
+    test_sanity.py:80-98 and test_matrix.py:27-40."""
+    b62 = _index_pen("blosum62")
+    ref = "CASSLGQAYEQYF"
+    two_gaps = "CASSLGYEQYF"
+    cheap = oracle.penalty_align(two_gaps, ref, b62, 11, 1)[0]
+    dear = oracle.penalty_align(two_gaps, ref, b62, 11, 9)[0]
+    assert dear - cheap == 8
+    s, _, _, ops = oracle.penalty_align(two_gaps, ref, None, 1, 1)
+    assert s == 2 and ops.count("I") + ops.count("D") == 2
+    assert "I" in oracle.penalty_align("CASSIRSSYEQYF", ref, b62, 1, 1)[3]
+    assert oracle.penalty_align("CASSIRSSYEQYF", ref, b62, 14, 1)[3] == "M" * 4 + "S" * 4 + "M" * 5
+    for pen in (b62, None):
+        assert oracle.penalty_align("casspgqayeqf", "CASSPGQAYEQF", pen, 1, 1)[0::3] == (0, "M" * 12)
+    assert oracle.penalty_align("CASSPGQAYEQY", "CASSPGQAYEQF", b62, 28, 1)[3] == "M" * 11 + "S"
+    with pytest.raises(ValueError, match=">= 0"):
+        oracle.penalty_align("CASS", "CASS", None, -1, 1)
+
+
+@pytest.mark.parametrize("name,expected", [("identity", 2), ("structural", 18), ("pam250", 24),
+                                           ("blosum62", 28), ("pam100", 30)])
+def test_oracle_index_align_matrix_scores(name, expected):
+    """tests/python/test_matrix.py:27-40: with gap_open 100 the global alignment is the
+    substitution-only score of the two junctions."""
+    pen = SubstitutionMatrix.unit(24).penalty_grid if name == "identity" else _index_pen(name)
+    assert oracle.penalty_align("CASSLAPGATNEKLFF", "CASSLELGATNEKLFF", pen, 100, 1)[0] == expected
