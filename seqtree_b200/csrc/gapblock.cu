@@ -313,10 +313,16 @@ __device__ __forceinline__ void run_unit(const FastArgs& a, const uint8_t* smem,
                 best[q] = __viaddmin_s16x2(Cb[q], pr, best[q]);
             }
         };
+        // The prior values of the next group of four positions are requested one group ahead,
+        // so their load latency hides behind the current group's lookups.
         int j = 0;
+        uint4 pnext = make_uint4(0u, 0u, 0u, 0u);
+        if constexpr (PRIOR)
+            if (L >= 4) pnext = __ldg(reinterpret_cast<const uint4*>(prow + 4));
         for (; j + 4 <= L; j += 4) {
-            uint4 pv = make_uint4(0u, 0u, 0u, 0u);
-            if constexpr (PRIOR) pv = __ldg(reinterpret_cast<const uint4*>(prow + j + 4));
+            const uint4 pv = pnext;
+            if constexpr (PRIOR)
+                if (j + 8 <= L) pnext = __ldg(reinterpret_cast<const uint4*>(prow + j + 8));
             step(j, pv.x);
             step(j + 1, pv.y);
             step(j + 2, pv.z);
