@@ -74,6 +74,7 @@ struct RefPlan {
     int64_t nchunks = 0;
     int64_t ntasks = 0;
     int64_t max_slab = 0;                // largest per-chunk code slab (bytes)
+    int max_tasks = 0;                   // most warp tasks in one chunk
     int64_t slab_bytes = 0;              // whole slab
     std::vector<int32_t> sorted;
     std::vector<int4> tasks;             // (n, start in sorted, count <= 32, slab byte offset)
@@ -129,6 +130,7 @@ void build_ref_plan(RefPlan& plan, const st_seqset_s& r, int rc, cudaStream_t st
     plan.tasks.clear();
     plan.task_off.assign(size_t(plan.nchunks + 1), 0);
     plan.max_slab = 0;
+    plan.max_tasks = 0;
     std::vector<int32_t> cnt(size_t(r.max_len) + 2);
     std::vector<int32_t> start(cnt.size());
     int64_t slab = 0;
@@ -149,6 +151,7 @@ void build_ref_plan(RefPlan& plan, const st_seqset_s& r, int rc, cudaStream_t st
             }
         }
         plan.max_slab = std::max(plan.max_slab, slab - slab0);
+        plan.max_tasks = std::max(plan.max_tasks, int(plan.tasks.size()) - plan.task_off[size_t(c)]);
         plan.task_off[size_t(c + 1)] = int32_t(plan.tasks.size());
     }
     if (slab > INT32_MAX) fail(ST_EINVAL, "seqtree_b200: reference set too large for one call");
@@ -218,6 +221,7 @@ struct FastArgs {
     const int4* tasks;
     const int32_t* task_off;
     int slab_cap;            // shared bytes reserved for a chunk's slab
+    int max_tasks;           // shared task slots (the most tasks of one chunk)
     const uint32_t* prior2;  // rows (M*W1 + d) of pstride words, value i at i + 3; or null
     int pstride;
     const int32_t* ftab;     // [m*W1 + n]: per-(m,n) additive term (prior minimum + gap cost)
@@ -262,13 +266,13 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
 // diagonal-d address by d rows; ref-longer pairs read the residue d positions further on.
 template <int LQ, bool PRIOR>
 __device__ __forceinline__ void run_unit(const FastArgs& a, const uint8_t* smem,
-                                         const uint8_t* s_codes, uint32_t* s_tile, int p0,
-                                         int slice, const int4 task, int tb, int64_t k0,
-                                         int lane) {
+                                         const uint8_t* s_codes, uint32_t* s_tile,
+                                         const int32_t* s_plen, const int16_t* s_col, int slice,
+                                         const int4 task, int tb, int64_t k0, int lane) {
     constexpr int kRowB = kRow * 4;
     constexpr int kPairB = LQ * kRowB;
     const int n = task.x;
-    const int m = a.plen[p0 + slice * kPairsPerSlice];
+    const int m = s_plen[slice * kPairsPerSlice];
     const int L = min(m, n);
     const int d = abs(m - n);
     const int dq = m > n ? d : 0;   // query longer: diagonal d is d profile rows further down
@@ -333,7 +337,7 @@ __device__ __forceinline__ void run_unit(const FastArgs& a, const uint8_t* smem,
         for (int q = 0; q < kPairsPerSlice; ++q) res[q] = S[q] + best[q] - a.bias2;
     }
     if (lane < task.z) {
-        const int col = int(a.ref_sorted[task.y + lane] - k0);
+        const int col = s_col[int(task.y - k0) + lane];
 #pragma unroll
         for (int q = 0; q < kPairsPerSlice; ++q)
             s_tile[(slice * kPairsPerSlice + q) * a.rc + col] = res[q];
@@ -350,7 +354,10 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
     uint32_t* s_tile = reinterpret_cast<uint32_t*>(s_codes + a.slab_cap);
     int32_t* s_ftab = reinterpret_cast<int32_t*>(s_tile + kGP * a.rc);
     uint8_t* s_len = reinterpret_cast<uint8_t*>(s_ftab + ((a.W1 * a.W1 + 3) & ~3));
-    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_len + ((a.rc + 15) & ~15));
+    int4* s_task = reinterpret_cast<int4*>(s_len + ((a.rc + 15) & ~15));
+    int16_t* s_col = reinterpret_cast<int16_t*>(s_task + a.max_tasks);
+    int32_t* s_plen = reinterpret_cast<int32_t*>(s_col + ((a.rc + 7) & ~7));
+    uint64_t* s_bar = reinterpret_cast<uint64_t*>(s_plen + kGP);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     volatile int* s_next = reinterpret_cast<volatile int*>(s_bar + 1);  // in the barrier's 16 bytes
@@ -397,8 +404,15 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
             bulk_g2s(uint32_t(__cvta_generic_to_shared(s_codes)), a.slab + tw0,
                      uint32_t(slab_bytes), bar);
     }
+    // Per-tile metadata in shared memory, so that a warp unit starts without a chain of global
+    // loads: the chunk's tasks, each sorted slot's column, the pairs' query lengths.
     for (int i = tid; i < a.W1 * a.W1; i += kThreads) s_ftab[i] = a.ftab[i];
-    for (int c = tid; c < kcount; c += kThreads) s_len[c] = uint8_t(a.rlen[k0 + c]);
+    for (int c = tid; c < kcount; c += kThreads) {
+        s_len[c] = uint8_t(a.rlen[k0 + c]);
+        s_col[c] = int16_t(a.ref_sorted[k0 + c] - k0);
+    }
+    for (int i = tid; i < t1 - t0; i += kThreads) s_task[i] = a.tasks[t0 + i];
+    if (tid < np) s_plen[tid] = a.plen[p0 + tid];
     __syncthreads();
     {
         // Bounded wait on phase 0 by every thread.  If any thread runs out, the CTA records
@@ -418,9 +432,10 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
     const int units = (t1 - t0) * nslices;
     for (int u = warp; u < units; u += kWarps) {
         const int ti = u / nslices;
-        const int4 task = a.tasks[t0 + ti];
+        const int4 task = s_task[ti];
         const int tb = task.w - tw0;
-        run_unit<LQ, PRIOR>(a, smem, s_codes, s_tile, p0, u - ti * nslices, task, tb, k0, lane);
+        run_unit<LQ, PRIOR>(a, smem, s_codes, s_tile, s_plen, s_col, u - ti * nslices, task, tb,
+                            k0, lane);
     }
     __syncthreads();
 
@@ -431,7 +446,7 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
     int32_t* s_fcol = reinterpret_cast<int32_t*>(smem);
     for (int i = tid; i < nslices * a.rc; i += kThreads) {
         const int sl = i / a.rc, c = i - sl * a.rc;
-        s_fcol[i] = c < kcount ? s_ftab[a.plen[p0 + sl * kPairsPerSlice] * a.W1 + s_len[c]] : 0;
+        s_fcol[i] = c < kcount ? s_ftab[s_plen[sl * kPairsPerSlice] * a.W1 + s_len[c]] : 0;
     }
     __syncthreads();
     const int cols4 = (kcount + 3) >> 2;
@@ -715,10 +730,11 @@ const void* fast_kernel_ptr(int lq, bool prior) {
 }
 
 // The profile area is reused for the per-slice column terms at write-out time.
-size_t fast_smem(int lq, int64_t slab_cap, int rc, int W1) {
+size_t fast_smem(int lq, int64_t slab_cap, int rc, int W1, int max_tasks) {
     const size_t prof = std::max(size_t(kGP) * lq * kRow * 4, size_t(kGP / kPairsPerSlice) * rc * 4);
     return prof + size_t(slab_cap) + size_t(kGP) * rc * 4 + size_t((W1 * W1 + 3) & ~3) * 4 +
-           size_t((rc + 15) & ~15) + 16;
+           size_t((rc + 15) & ~15) + size_t(max_tasks) * 16 + size_t((rc + 7) & ~7) * 2 +
+           size_t(kGP) * 4 + 16;
 }
 
 }  // namespace
@@ -795,7 +811,8 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
             for (int rc : {1024, 896, 768, 640, 512, 384, 256}) {
                 if (want_rc && rc != want_rc) continue;
                 build_ref_plan(rp, rs, rc, stream, /*upload=*/false);
-                const size_t sm = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rc, W1);
+                const size_t sm = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rc, W1,
+                                            rp.max_tasks);
                 if (sm > size_t(ctx.max_smem_optin)) continue;
                 int blocks = 0;
                 STB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -817,7 +834,7 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
                 note_launch(nullptr);
             }
         }
-        smem = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rp.rc, W1);
+        smem = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rp.rc, W1, rp.max_tasks);
         fast = smem <= size_t(ctx.max_smem_optin);
         rpp = &rp;
     }
@@ -912,6 +929,7 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
     fa.tasks = static_cast<int4*>(rp.d_tasks.ptr);
     fa.task_off = static_cast<int32_t*>(rp.d_task_off.ptr);
     fa.slab_cap = int((rp.max_slab + 15) & ~int64_t(15));
+    fa.max_tasks = rp.max_tasks;
     fa.prior2 = has_prior ? static_cast<uint32_t*>(tb.prior2.ptr) : nullptr;
     fa.ftab = static_cast<int32_t*>(tb.ftab.ptr);
     fa.W1 = W1;
