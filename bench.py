@@ -41,6 +41,7 @@ sys.path.insert(0, str(ROOT))
 AA20 = "ACDEFGHIKLMNPQRSTVWY"
 PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
 FALLBACK_HBM_GBS = 6650.0
+FALLBACK_BF16_TFLOPS = 1590.0
 # DRAM bytes (read + write) per launch of the dominant kernel on the named workload, from the ncu
 # captures summarised in profiles/ (None until captured).
 TRAFFIC: dict[str, float | None] = {
@@ -574,8 +575,9 @@ def main_ours(args):
         "gcups": cells * world * args.steps / (total_ms / 1e3) / 1e9,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": TRAFFIC.get(w["kind"]),
-                     "note": f"algorithmic bytes = 4 B/pair output + input residues; peak {src} "
-                             "(of measured); traffic = ncu dram read+write per launch (profiles/)"},
+                     "note": f"algorithmic bytes = 4 B/pair output + input residues; peak = "
+                             f"{'measured copy bandwidth' if src == 'measured' else 'fallback 6.65 TB/s'} "
+                             f"(of {src}); traffic = ncu dram read+write per launch (profiles/)"},
         "kernel_roofline": kernel_roofline(w, cells, per_launch_s, sampler.summary()),
         "e2e": e2e,
         "gpu_launches": launches * args.steps,
@@ -724,9 +726,9 @@ def main_learned(args):
     n_lq, n_lr = len(qb.learn_rows), idx.n_learn
     flops = 2.0 * 64 * n_lq * n_lr
     achieved = flops / prop_s / 1e12 if prop_s > 0 else None
-    peak = 1659.3
+    peak, peak_src = FALLBACK_BF16_TFLOPS, "fallback"
     try:
-        peak = float(json.loads(PEAKS_FILE.read_text())["bf16_tflops"])
+        peak, peak_src = float(json.loads(PEAKS_FILE.read_text())["bf16_tflops"]), "measured"
     except Exception:
         pass
     line = {
@@ -746,7 +748,7 @@ def main_learned(args):
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if achieved else None, "traffic": None,
                      "note": "propose_topk_kernel: 2*64 flops per (learned query, learned ref) "
-                             "pair / its phase time; peak = measured cuBLAS bf16 burst (of measured)"},
+                             f"pair / its phase time; peak = cuBLAS bf16 burst (of {peak_src})"},
         "e2e": {"value": nq * nr / e2e_s, "unit": "pairs/s",
                 "h2d_bytes_per_step": int(sum(map(len, w["queries"])) + 8 * nq),
                 "d2h_bytes_per_step": int(8 * (nq + 1) + 8 * e2e_nnz),
