@@ -166,3 +166,59 @@ def test_sparse_in_row_blocks(cuda_ready, monkeypatch, thresh):
         np.testing.assert_array_equal(scores, want[2])
     sp = score_sparse(q, r, thresh, m, gap_open=8, gap_prior=prior_by_name("central21"))
     assert_same(sp, dense, thresh)
+
+
+def _junctions_packed(rng, n):
+    """n CDR3-like junctions ('CASS' + uniform middle + 'F', lengths 8-25 with mode 14, wider on
+    the long side) as packed bytes + offsets, built with numpy (no per-string Python work)."""
+    from seqtree_b200 import _lib
+    z = rng.standard_normal(n)
+    lens = np.clip(np.rint(14 + np.where(z < 0, 2.5, 3.5) * z), 8, 25).astype(np.int64)
+    off = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=off[1:])
+    aa = np.frombuffer(b"ACDEFGHIKLMNPQRSTVWY", np.uint8)
+    data = aa[rng.integers(0, 20, int(off[-1]))]
+    pos = np.arange(int(off[-1])) - np.repeat(off[:-1], lens)
+    data[pos < 4] = np.frombuffer(b"CASS", np.uint8)[pos[pos < 4]]
+    data[pos == np.repeat(lens, lens) - 1] = ord("F")
+    return _lib.Packed.from_arrays(data, off)
+
+
+def _strings(p):
+    raw = p.data.tobytes()
+    return [raw[a:b].decode() for a, b in zip(p.offsets[:-1], p.offsets[1:])]
+
+
+@pytest.mark.gpu
+def test_full_size_sparse_configuration(cuda_ready):
+    """The 100,000 x 1,000,000 sparse configuration (BLOSUM62, gap 8/1, max_penalty 24) at full
+    size.  Every row is in ref order within the threshold; 24 sampled rows (rows are independent)
+    equal the oracle's thresholded rows; a 64-row block equals the GPU's dense matrix thresholded."""
+    import seqtree_b200 as stb
+    rng = np.random.default_rng(0)
+    refs = _junctions_packed(rng, 1_000_000)
+    queries = _junctions_packed(np.random.default_rng(1), 100_000)
+    m = SubstitutionMatrix.blosum62()
+    sp = score_sparse(queries, refs, 24, m, gap_open=8)
+    assert sp.shape == (100_000, 1_000_000) and sp.indptr[0] == 0
+    assert np.all(np.diff(sp.indptr) >= 0) and sp.indptr[-1] == sp.nnz > 0
+    assert sp.scores.min() >= 0 and sp.scores.max() <= 24
+    starts = np.zeros(sp.nnz, bool)
+    starts[sp.indptr[:-1][np.diff(sp.indptr) > 0]] = True
+    step = np.diff(sp.ref_ids.astype(np.int64), prepend=-1)
+    assert np.all((step > 0) | starts)
+    qs, rs = _strings(queries), _strings(refs)
+    rows = np.sort(rng.choice(100_000, 24, replace=False))
+    dense = oracle.gapblock_matrix([qs[i] for i in rows], rs, m.penalty_grid, gap_open=8,
+                                   gap_extend=1)
+    for k, i in enumerate(rows):
+        ids, sc = sp.row(int(i))
+        want = np.flatnonzero(dense[k] <= 24)
+        np.testing.assert_array_equal(ids, want)
+        np.testing.assert_array_equal(sc, dense[k, want])
+    block = np.asarray(stb.gapblock.score_matrix(qs[5000:5064], refs, m, gap_open=8))
+    for k in range(64):
+        ids, sc = sp.row(5000 + k)
+        want = np.flatnonzero(block[k] <= 24)
+        np.testing.assert_array_equal(ids, want)
+        np.testing.assert_array_equal(sc, block[k, want])
