@@ -169,3 +169,24 @@ def test_gapblock_chunk_width_is_tuned_and_exact(cuda_ready):
         got = np.asarray(stb.score_matrix(q, r, m, gap_open=8, gap_prior=prior))
         np.testing.assert_array_equal(got, want)
     assert "gapblock|" in _lib.tuning_table() or os.environ.get("SEQTREE_B200_TUNE") == "0"
+
+
+@pytest.mark.parametrize("mode", ["global", "local"])
+def test_full_size_protein_configuration(pw, B62, mode):
+    """The 4,096 x 4,096 protein configuration (log-normal lengths, median 180, clipped 50-500;
+    BLOSUM62, gap 11/1) at full size, distance form: six sampled rows (rows are independent)
+    against the oracle, a zero diagonal where a query meets itself, and d >= 0 everywhere."""
+    rng = np.random.default_rng(4096)
+    lens = np.clip(np.round(rng.lognormal(np.log(180), 0.5, size=8192)), 50, 500).astype(int)
+    aa = np.frombuffer(b"ACDEFGHIKLMNPQRSTVWY", np.uint8)
+    raw = aa[rng.integers(0, 20, int(lens.sum()))].tobytes().decode()
+    cut = np.concatenate([[0], np.cumsum(lens)])
+    seqs = [raw[a:b] for a, b in zip(cut[:-1], cut[1:])]
+    q, r = seqs[:4096], seqs[4096:]
+    r[17] = q[5]  # one self pair: distance 0
+    got = as_np(pw.dist_matrix(q, r, B62, mode=mode))
+    assert got.shape == (4096, 4096) and got.min() >= 0 and got[5, 17] == 0
+    rows = [0, 5, 1000, 2047, 3333, 4095]
+    exp = oracle.align_matrix([q[i] for i in rows], r, B62.similarity_grid, mode=mode, dist=True,
+                              threads=os.cpu_count() or 1)
+    assert np.array_equal(got[rows], exp)
