@@ -55,6 +55,8 @@ std::string dev_key(const std::string& key) {
 }
 }  // namespace
 
+bool tuning_enabled() { return tune_on(); }
+
 int tuned_lookup(const std::string& key) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(dev_key(key));

@@ -122,6 +122,8 @@ int tuned_run(const std::string& key, int n, int fallback, const std::function<v
               cudaStream_t stream);
 // The cached choice for `key` on the current device, or -1.
 int tuned_lookup(const std::string& key);
+// False when SEQTREE_B200_TUNE=0 switched measured tuning off.
+bool tuning_enabled();
 // log2 bucket of a size, for shape keys.
 inline int size_bucket(int64_t n) {
     int b = 0;

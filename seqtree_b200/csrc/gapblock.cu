@@ -795,7 +795,10 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
 
     const int W = longest, W1 = W + 1;
     const int lq = profile_height(qs.max_len);
-    const int tuned_choice = t_force_rc ? -1 : tuned_lookup(gb_shape_key(qs, rs, has_prior));
+    const int tuned_choice =
+        t_force_rc ? -1
+                   : tuned_lookup(sink ? "sparse|" + gb_shape_key(qs, rs, has_prior)
+                                       : gb_shape_key(qs, rs, has_prior));
     RefPlan* rpp = nullptr;
     size_t smem = 0;
     if (fast) {
@@ -1138,6 +1141,49 @@ void gapblock_sparse_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penal
     const int end_bit = shift + bits_for(N);
     const uint64_t kMaxBlockHits = max_block_hits();
     auto* count = reinterpret_cast<unsigned long long*>(ctx.flags_d + 10);
+
+    // The fast kernel's chunk width and launch form are tuned once per shape, as for the dense
+    // matrix, but on a slice of about 2e9 pairs of rows: every variant counts the slice's hits
+    // into the sink (what it stores is overwritten by the passes below).
+    {
+        const bool has_prior = prior && prior_len > 0;
+        const std::string skey = "sparse|" + gb_shape_key(qs, rs, has_prior);
+        bool nonneg = qs.alphabet >= 0 && qs.alphabet == rs.alphabet &&
+                      std::max(qs.max_len, rs.max_len) <= 64;
+        const int A = nonneg ? alphabet_size(qs.alphabet) : 0;
+        if (penalty && matrix_size != A) nonneg = false;
+        if (nonneg && penalty)
+            for (int i = 0; i < A * A; ++i) nonneg &= penalty[i] >= 0;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        STB_CUDA(cudaStreamIsCapturing(stream, &cs));
+        if (nonneg && tuning_enabled() && cs == cudaStreamCaptureStatusNone && tuned_lookup(skey) < 0) {
+            const int64_t tr1 = std::min<int64_t>(N, std::max<int64_t>(64, int64_t(2000000000) / K));
+            const uint64_t tcap = std::min<uint64_t>(std::max<uint64_t>(hits.cap_hint, uint64_t(1) << 20),
+                                                     kMaxBlockHits);
+            SparseSink ts{};
+            ts.keys = ctx.sp_keys.as<unsigned long long>(size_t(tcap));
+            ts.vals = ctx.sp_vals.as<int32_t>(size_t(tcap));
+            ts.count = count;
+            ts.cap = tcap;
+            ts.shift = shift;
+            ts.thresh = max_penalty;
+            tuned_run(skey, 2 * kNumRc, -1, [&](int c) {
+                t_force_rc = c >= 0 ? kRcCandidates[c % kNumRc] : 0;
+                t_force_persistent = c >= 0 ? c / kNumRc : -1;
+                try {
+                    STB_CUDA(cudaMemsetAsync(count, 0, sizeof(unsigned long long), stream));
+                    gapblock_run(qs, rs, penalty, matrix_size, go, ge, prior, prior_len,
+                                 prior_width, nullptr, &ts, stream, 0, tr1 == N ? -1 : tr1);
+                } catch (...) {
+                    t_force_rc = 0;
+                    t_force_persistent = -1;
+                    throw;
+                }
+                t_force_rc = 0;
+                t_force_persistent = -1;
+            }, stream);
+        }
+    }
 
     // One block of all rows when the hits fit one sort (the usual case: the set's cached plans
     // are used and nothing is copied); otherwise blocks sized from the hit density seen so far.
