@@ -743,7 +743,7 @@ namespace {
 
 // Chunk widths the fast kernel may use.  The widest that reaches the best CTA residency is the
 // static choice; the autotuner (dense calls) measures all of them once per shape.
-constexpr int kRcCandidates[] = {1024, 768, 512, 384, 256};
+constexpr int kRcCandidates[] = {1024, 896, 768, 640, 512, 384, 256};
 constexpr int kNumRc = int(sizeof(kRcCandidates) / sizeof(kRcCandidates[0]));
 thread_local int t_force_rc = 0;           // set while the autotuner times one chunk width
 thread_local int t_force_persistent = -1;  // and the launch form (-1: the tuned or static one)
