@@ -18,7 +18,7 @@
 //     by length into warp tasks of <= 32 refs, so d, L and the prior row are warp-uniform.  The
 //     refs' codes are laid out per task as [j][lane] bytes holding 4*code (a byte offset into a
 //     profile row), also once per call.
-//   * A CTA owns (chunk, 8 query pairs).  Two bulk (TMA) copies stage its 8-pair profile slab
+//   * A CTA owns (chunk, 4 query pairs).  Two bulk (TMA) copies stage its 4-pair profile slab
 //     and the chunk's code slab into shared memory, completing on one mbarrier.  A warp unit is
 //     (task, slice of 4 pairs of one length); the 4 pairs are swept together, and every lookup
 //     is LDS [lane register + compile-time immediate]: the register is the residue's byte offset
@@ -47,7 +47,7 @@ namespace stb {
 
 namespace {
 
-constexpr int kGP = 8;          // query pairs per CTA (tile rows = 16 queries)
+constexpr int kGP = 4;          // query pairs per CTA (tile rows = 8 queries; 8 pairs measured slower)
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRow = 32;        // words per profile row
@@ -376,7 +376,8 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
     } else {
         if (iter > 0) break;
         chunk = blockIdx.x;
-        pg = blockIdx.y;
+        pg = int(blockIdx.y + blockIdx.z * gridDim.y);  // pair groups past 65,535 use z
+        if (pg >= npg) break;
     }
     const uint32_t parity = uint32_t(iter & 1);
     const int64_t k0 = int64_t(chunk) * a.rc;
@@ -958,8 +959,11 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
         fa.queue = reinterpret_cast<unsigned int*>(ctx.flags_d + 13);
         STB_CUDA(cudaMemsetAsync(fa.queue, 0, sizeof(unsigned int), stream));
         grid = dim3(unsigned(std::min<int64_t>(ntiles, int64_t(std::max(per_sm, 1)) * ctx.num_sms)), 1);
-    } else if (grid.y > 65535) {
-        fail(ST_EINVAL, "seqtree_b200: too many query pairs for one launch");
+    } else if (npg > 65535) {
+        // pair groups split over y and z (the kernel skips the padding of the last z slice)
+        grid.y = 65535;
+        grid.z = unsigned(ceil_div(npg, 65535));
+        if (grid.z > 65535) fail(ST_EINVAL, "seqtree_b200: too many query pairs for one launch");
     }
     const char* name = dispatch_fast(lq, has_prior, fa, grid, smem, stream);
     note_launch(name);

@@ -104,6 +104,32 @@ def test_full_size_workload_against_the_oracle(st):
     assert np.array_equal(got, exp)
 
 
+def test_more_query_pairs_than_one_grid_dimension(st):
+    """600,000 queries are 300,000 length-sorted pairs, more pair groups than one grid dimension
+    holds (65,535): the dense and sparse forms stay exact on sampled rows, the last ones
+    included."""
+    from seqtree_b200 import _lib
+    rng = np.random.default_rng(65536)
+    lens = rng.integers(8, 26, 600_000)
+    off = np.zeros(lens.size + 1, np.int64)
+    np.cumsum(lens, out=off[1:])
+    data = np.frombuffer(b"ACDEFGHIKLMNPQRSTVWY", np.uint8)[rng.integers(0, 20, int(off[-1]))]
+    q = _lib.Packed.from_arrays(data, off)
+    raw = data.tobytes()
+    r = cdr3(np.random.default_rng(7), 40, 8, 25)
+    m = st.SubstitutionMatrix.blosum62()
+    got = as_np(st.score_matrix(q, r, m, gap_open=8))
+    sp = st.gapblock.score_sparse(q, r, 30, m, gap_open=8)
+    rows = np.r_[np.arange(5), rng.integers(0, 600_000, 200), np.arange(599_995, 600_000)]
+    qs = [raw[off[i]:off[i + 1]].decode() for i in rows]
+    exp = _oracle_gapblock(st, qs, r, m, 8, 1, None)
+    assert np.array_equal(got[rows], exp)
+    for k, i in enumerate(rows):
+        ids, sc = sp.row(int(i))
+        want = np.flatnonzero(exp[k] <= 30)
+        assert np.array_equal(ids, want) and np.array_equal(sc, exp[k, want])
+
+
 def test_threads_argument_is_ignored(st):
     rng = np.random.default_rng(13)
     q, r = rand_seqs(rng, 64, 6, 18), rand_seqs(rng, 40, 6, 18)
