@@ -45,7 +45,7 @@ FALLBACK_BF16_TFLOPS = 1590.0
 # DRAM bytes (read + write) per launch of the dominant kernel on the named workload, from the ncu
 # captures summarised in profiles/ (None until captured).
 TRAFFIC: dict[str, float | None] = {
-    "gapblock": 2.02e6,     # 1.89 MB read + 0.13 MB write (the result stays in L2)
+    "gapblock": 1.91e6,     # 1.89 MB read + 0.02 MB write (the result stays in L2)
     "hamming": 1.31e9,      # 262 MB per 4,000 rows, scaled to 20,000 rows
     "levenshtein": 1.03e9,  # 102.5 MB per 2,000 rows, scaled to 20,000 rows
     "align": 1.05e6,        # one row-bucket launch of the wavefront kernel
