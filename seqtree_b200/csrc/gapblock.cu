@@ -744,7 +744,7 @@ namespace {
 
 // Chunk widths the fast kernel may use.  The widest that reaches the best CTA residency is the
 // static choice; the autotuner (dense calls) measures all of them once per shape.
-constexpr int kRcCandidates[] = {1024, 896, 768, 640, 512, 384, 256};
+constexpr int kRcCandidates[] = {1536, 1280, 1024, 896, 768, 640, 512, 384, 256};
 constexpr int kNumRc = int(sizeof(kRcCandidates) / sizeof(kRcCandidates[0]));
 thread_local int t_force_rc = 0;           // set while the autotuner times one chunk width
 thread_local int t_force_persistent = -1;  // and the launch form (-1: the tuned or static one)
@@ -812,8 +812,9 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
             // kernel's registers allow, checked with the occupancy calculator.
             const void* kern = fast_kernel_ptr(lq, has_prior);
             int best_rc = 0, best_blocks = -1;
-            for (int rc : {1024, 896, 768, 640, 512, 384, 256}) {
-                if (want_rc && rc != want_rc) continue;
+            const std::vector<int> widths =
+                want_rc ? std::vector<int>{want_rc} : std::vector<int>{1024, 896, 768, 640, 512, 384, 256};
+            for (int rc : widths) {
                 build_ref_plan(rp, rs, rc, stream, /*upload=*/false);
                 const size_t sm = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rc, W1,
                                             rp.max_tasks);
@@ -828,7 +829,12 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
                 }
                 if (blocks >= kTargetBlocks) break;
             }
-            if (best_rc) build_ref_plan(rp, rs, best_rc, stream);
+            if (best_rc) {
+                build_ref_plan(rp, rs, best_rc, stream);
+            } else {
+                rp.uid = 0;  // no width fits shared memory: the plan is not used (general kernel)
+                rp.ntasks = 0;
+            }
             const unsigned blocks = unsigned(rp.ntasks);
             if (blocks) {
                 ref_slab_kernel<<<blocks, 128, 0, stream>>>(
@@ -839,7 +845,7 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
             }
         }
         smem = fast_smem(lq, (rp.max_slab + 15) & ~int64_t(15), rp.rc, W1, rp.max_tasks);
-        fast = smem <= size_t(ctx.max_smem_optin);
+        fast = rp.uid == rs.uid && smem <= size_t(ctx.max_smem_optin);
         rpp = &rp;
     }
 
