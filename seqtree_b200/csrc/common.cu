@@ -90,17 +90,23 @@ int tuned_run(const std::string& key, int n, int fallback, const std::function<v
     try {
         for (int c = 0; c < n; ++c) {
             run(c);  // untimed: first-use effects (plans, module loading, workspace growth)
-            // the median of three timed runs: one run's time varies by several percent, enough
-            // to reorder variants that are close
-            float t[3];
-            for (float& ti : t) {
+            // the median of several timed runs (one run's time varies by several percent,
+            // enough to reorder variants that are close): three, or up to nine while the runs
+            // so far took under 2 ms in all, so that short kernels get a steadier median
+            std::vector<float> t;
+            float spent = 0.f;
+            while (t.size() < 3 || (t.size() < 9 && spent < 2.0f)) {
+                float ti = 0.f;
                 STB_CUDA(cudaEventRecord(e0, stream));
                 run(c);
                 STB_CUDA(cudaEventRecord(e1, stream));
                 STB_CUDA(cudaEventSynchronize(e1));
                 STB_CUDA(cudaEventElapsedTime(&ti, e0, e1));
+                t.push_back(ti);
+                spent += ti;
             }
-            ms[size_t(c)] = std::max(std::min(t[0], t[1]), std::min(std::max(t[0], t[1]), t[2]));
+            std::nth_element(t.begin(), t.begin() + t.size() / 2, t.end());
+            ms[size_t(c)] = t[t.size() / 2];
             if (c == 0 || ms[size_t(c)] < best) {
                 best = ms[size_t(c)];
                 pick = c;

@@ -113,8 +113,8 @@ bool same_as_last(std::vector<uint8_t>& slot, const void* data, size_t bytes);
 // ----------------------------------------------------------------------------- tuning -------
 // Measured choice among `n` launch variants that produce identical results.  The first time `key`
 // is seen on a device (and tuning is on and `stream` is not being captured), every variant runs
-// once untimed and three times timed with CUDA events on `stream`, and the one with the fastest
-// median is cached; every
+// once untimed and then 3-9 times timed with CUDA events on `stream` (more while the runs are
+// short), and the one with the fastest median is cached; every
 // call ends with the chosen variant's results in place.  Later calls with the key run the cached
 // choice directly.  Tuning is off with SEQTREE_B200_TUNE=0; then, and while `stream` is being
 // captured before the key was tuned, `run(fallback)` runs (`fallback` may be -1, the caller's
