@@ -4,6 +4,8 @@
 #include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
+#include <set>
+#include <tuple>
 #include <atomic>
 #include <chrono>
 #include <cstdio>
@@ -56,6 +58,18 @@ std::string dev_key(const std::string& key) {
 }  // namespace
 
 bool tuning_enabled() { return tune_on(); }
+
+void ensure_smem_limit(const void* kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::set<std::tuple<int, const void*, size_t>> done;
+    int dev = 0;
+    STB_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(dev, kernel, bytes);
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count(key)) return;
+    STB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    done.insert(key);
+}
 
 int tuned_lookup(const std::string& key) {
     std::lock_guard<std::mutex> lk(g_tune_mu);

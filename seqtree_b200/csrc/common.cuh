@@ -100,6 +100,11 @@ struct Context {
 // device is usable.
 Context& context();
 
+// Raises `kernel`'s dynamic shared-memory limit to `bytes` on the current device, once per
+// (device, kernel, size).  The attribute belongs to a device, so a process that uses several
+// devices needs the call on each of them.
+void ensure_smem_limit(const void* kernel, size_t bytes);
+
 // Host -> device copy of per-call tables or plans.  Refuses to run while `stream` is being
 // captured into a CUDA graph: the captured copy would read host memory that is gone when the
 // graph is replayed.  Plans and tables are cached, so a call made once before capturing leaves

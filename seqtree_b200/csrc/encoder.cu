@@ -699,13 +699,8 @@ size_t attn_fwd_smem() { return sizeof(float) * (kP * kW + kP * (kW + 1) + kP * 
 size_t attn_bwd_smem() { return sizeof(float) * (4 * kP * (kW + 1) + 2 * kP * (kP + 1)); }
 
 void set_attn_attrs() {
-    static std::once_flag once;
-    std::call_once(once, [] {
-        STB_CUDA(cudaFuncSetAttribute(attn_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(attn_fwd_smem())));
-        STB_CUDA(cudaFuncSetAttribute(attn_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(attn_bwd_smem())));
-    });
+    ensure_smem_limit(reinterpret_cast<const void*>(attn_fwd_kernel), attn_fwd_smem());
+    ensure_smem_limit(reinterpret_cast<const void*>(attn_bwd_kernel), attn_bwd_smem());
 }
 
 // Forward of S sequences whose padded codes and lengths are in m.codes / m.lens; z in m.z.

@@ -665,22 +665,14 @@ struct Bf16State {
 };
 
 void launch_conv2(const GemmArgs& g, int sms, cudaStream_t st) {
-    static std::once_flag once;
-    std::call_once(once, [] {
-        STB_CUDA(cudaFuncSetAttribute(conv2_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(Conv2Shape::kSmem)));
-    });
+    ensure_smem_limit(reinterpret_cast<const void*>(conv2_gemm_kernel), Conv2Shape::kSmem);
     const int grid = int(std::min<int64_t>(g.tiles, sms));
     conv2_gemm_kernel<<<grid, kGemmThreads, Conv2Shape::kSmem, st>>>(g);
     STB_CUDA(cudaGetLastError());
 }
 
 void launch_layer(const LayerArgs& g, int sms, cudaStream_t st) {
-    static std::once_flag once;
-    std::call_once(once, [] {
-        STB_CUDA(cudaFuncSetAttribute(attn_layer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(kLySmem)));
-    });
+    ensure_smem_limit(reinterpret_cast<const void*>(attn_layer_kernel), kLySmem);
     const int grid = int(std::min<int64_t>(g.tiles, sms));
     attn_layer_kernel<<<grid, kGemmThreads, kLySmem, st>>>(g);
     STB_CUDA(cudaGetLastError());

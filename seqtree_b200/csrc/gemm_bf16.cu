@@ -275,11 +275,7 @@ void gemm_bf16(bool ta, bool tb, int M, int N, int K, const float* A, int lda, c
         return;
     }
     Context& ctx = context();
-    static std::once_flag once;
-    std::call_once(once, [] {
-        STB_CUDA(cudaFuncSetAttribute(gemm_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(kGSmem)));
-    });
+    ensure_smem_limit(reinterpret_cast<const void*>(gemm_bf16_kernel), kGSmem);
     int mtiles, ntiles, kchunks, kb;
     // op(A)[i][k] = ta ? A[k][i] : A[i][k];  op(B)^T[n][k] = tb ? B[n][k] : B[k][n]
     pack(A, lda, ta, M, K, ctx.gemm_a, st, mtiles, kchunks);

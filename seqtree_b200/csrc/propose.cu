@@ -472,11 +472,7 @@ void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, in
     if ((uintptr_t(qemb) | uintptr_t(remb)) & 15)
         fail(ST_EINVAL, "seqtree_b200: embeddings must be 16-byte aligned");
     Context& ctx = context();
-    static std::once_flag once;
-    std::call_once(once, [] {
-        STB_CUDA(cudaFuncSetAttribute(propose_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(kSmemBytes)));
-    });
+    ensure_smem_limit(reinterpret_cast<const void*>(propose_topk_kernel), kSmemBytes);
     const int64_t ntq = (nq + kQT - 1) / kQT;
     const int grid = int(std::min<int64_t>(ntq, ctx.num_sms));
     ProposeArgs a;
