@@ -133,3 +133,22 @@ def test_pinned_results_are_plain_int32_arrays():
     v = a[1:]
     del a
     assert int(v.sum()) == 7 * 8
+
+
+def test_penalty_alignment_matrix_argument_like_search_params():
+    """``penalty_align``'s matrix argument follows seqtree's SearchParams (src/_bindings.cpp:
+    67-119): None or '' is unit cost, built-in names are case-insensitive, 'identity' is the unit
+    grid of the alphabet, the others need amino acids, anything else is refused -- all checked
+    on the host before the library is called."""
+    from seqtree_b200.pairwise import _penalty_grid
+    assert _penalty_grid(None, "aa") is None and _penalty_grid("", "aa") is None
+    b62 = SubstitutionMatrix.blosum62().penalty_grid
+    assert np.array_equal(_penalty_grid("BLOSUM62", "aa"), b62)
+    assert np.array_equal(_penalty_grid(SubstitutionMatrix.blosum62(), "aa"), b62)
+    assert np.array_equal(_penalty_grid("identity", "nt"), 1 - np.eye(4, dtype=np.int32))
+    with pytest.raises(ValueError, match="unknown matrix 'BLOSUM99'"):
+        _penalty_grid("BLOSUM99", "aa")
+    with pytest.raises(ValueError, match="requires the amino-acid alphabet"):
+        _penalty_grid("pam250", "nt")
+    with pytest.raises(TypeError, match="name string or a SubstitutionMatrix"):
+        _penalty_grid(3, "aa")
