@@ -30,6 +30,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -222,11 +223,13 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        self._summary = None
+        fd, name = tempfile.mkstemp(prefix="seqtree_b200_clocks_", suffix=".csv")
+        os.close(fd)
+        self.path = Path(name)  # scratch: read by summary(), then removed
 
     def __enter__(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
@@ -234,6 +237,8 @@ class ClockSampler:
                 stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            if getattr(self, "fh", None) is not None:
+                self.fh.close()
         return self
 
     def __exit__(self, *exc):
@@ -246,8 +251,13 @@ class ClockSampler:
             self.fh.close()
 
     def summary(self):
-        if self.proc is None or not self.path.exists():
-            return None
+        if self._summary is None and self.path.exists():
+            if self.proc is not None:
+                self._summary = self._read()
+            self.path.unlink(missing_ok=True)
+        return self._summary
+
+    def _read(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.path.read_text().splitlines():
