@@ -11,6 +11,8 @@ read-only (rows, cols) int32 row-major block exported through the buffer protoco
 """
 from __future__ import annotations
 
+import operator
+
 import numpy as np
 
 from ._tables import SIMILARITY
@@ -154,6 +156,19 @@ class SubstitutionMatrix:
         return f"SubstitutionMatrix(size={self.size()})"
 
 
+def _unsigned_index(v) -> int:
+    """``v`` as a size_t index: an integer (or an object with ``__index__``) that is not
+    negative; a float, a string or a negative number is a TypeError, the way the reference's
+    binding rejects an argument it cannot convert to ``size_t``."""
+    try:
+        i = operator.index(v)
+    except TypeError:
+        raise TypeError(f"index must be a non-negative integer, not {type(v).__name__}") from None
+    if i < 0:
+        raise TypeError("index must be a non-negative integer")
+    return i
+
+
 class ScoreMatrix:
     """A read-only (n_queries, n_refs) int32 matrix, row-major, exported by buffer protocol."""
 
@@ -183,13 +198,18 @@ class ScoreMatrix:
         return int(self._a.shape[0])
 
     def row(self, i: int) -> list[int]:
-        if i < 0 or i >= self._a.shape[0]:
+        i = _unsigned_index(i)
+        if i >= self._a.shape[0]:
             raise IndexError("row out of range")
         return self._a[i].tolist()
 
     def __getitem__(self, ik):
-        i, k = ik
-        if i < 0 or k < 0 or i >= self._a.shape[0] or k >= self._a.shape[1]:
+        # a pair of unsigned indices, as the reference's std::pair<size_t, size_t> argument
+        # takes: anything else (a scalar, three indices, a float, a negative) is a TypeError
+        if isinstance(ik, (str, bytes)) or not hasattr(ik, "__len__") or len(ik) != 2:
+            raise TypeError("ScoreMatrix indices must be a pair (i, k) of non-negative integers")
+        i, k = (_unsigned_index(v) for v in ik)
+        if i >= self._a.shape[0] or k >= self._a.shape[1]:
             raise IndexError("index out of range")
         return int(self._a[i, k])
 

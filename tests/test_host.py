@@ -87,6 +87,14 @@ def test_score_matrix_buffer_protocol_and_indexing():
     with pytest.raises(IndexError):
         sm[0, 3]
     assert repr(sm) == "ScoreMatrix(2, 3)"
+    # the reference binds row(size_t) and __getitem__(pair<size_t, size_t>): pybind11 turns an
+    # argument it cannot convert (negative, float, not a pair) into TypeError, and accepts any
+    # integer-like value or a two-element list
+    assert sm.row(np.int64(1)) == [3, 4, 5] and sm[[1, 2]] == 5 and sm[np.int32(1), 2] == 5
+    for bad in (lambda: sm.row(-1), lambda: sm.row(1.0), lambda: sm[-1, 0], lambda: sm[0],
+                lambda: sm[0, 1, 2], lambda: sm[1.0, 0], lambda: sm["ab"]):
+        with pytest.raises(TypeError):
+            bad()
 
 
 def test_packing_offsets_and_utf8():
