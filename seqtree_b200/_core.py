@@ -9,6 +9,7 @@ calls on the same kernels.
 from __future__ import annotations
 
 import ctypes
+import operator
 
 import numpy as np
 
@@ -23,9 +24,26 @@ _INT32 = (-(2 ** 31), 2 ** 31 - 1)
 
 
 def _i32(name: str, v) -> int:
-    v = int(v)
+    """``v`` converted the way the reference binding's int32_t argument is: an integer or an
+    object with ``__index__`` in range, else TypeError (a float or a string is never truncated
+    or parsed)."""
+    try:
+        v = operator.index(v)
+    except TypeError:
+        raise TypeError(f"{name} must be an integer, not {type(v).__name__}") from None
     if not _INT32[0] <= v <= _INT32[1]:
         raise TypeError(f"{name} must fit a 32-bit signed integer")
+    return v
+
+
+def _u32(name: str, v) -> int:
+    """As :func:`_i32` for a uint32_t argument: a negative value is a TypeError."""
+    try:
+        v = operator.index(v)
+    except TypeError:
+        raise TypeError(f"{name} must be an integer, not {type(v).__name__}") from None
+    if not 0 <= v <= 0xFFFFFFFF:
+        raise TypeError(f"{name} must fit a 32-bit unsigned integer")
     return v
 
 
@@ -50,8 +68,8 @@ def gapblock_matrix(queries, refs, alphabet: str = "aa", matrix: SubstitutionMat
     code = _lib.lib.st_gapblock_matrix(
         q.ref(), r.ref(), alph, _lib.i32_ptr(pen), 0 if pen is None else pen.shape[0],
         _i32("gap_open", gap_open), _i32("gap_extend", gap_extend),
-        _lib.i32_ptr(pr32) if pr32.size else None, int(pr32.size), int(prior_width),
-        int(threads), out.ctypes.data, ctypes.byref(err))
+        _lib.i32_ptr(pr32) if pr32.size else None, int(pr32.size), _u32("prior_width", prior_width),
+        _i32("threads", threads), out.ctypes.data, ctypes.byref(err))
     _lib.check(code, err)
     return ScoreMatrix(out)
 
@@ -79,8 +97,8 @@ def gapblock_sparse(queries, refs, max_penalty: int, alphabet: str = "aa",
     code = _lib.lib.st_gapblock_sparse(
         q.ref(), r.ref(), alph, _lib.i32_ptr(pen), 0 if pen is None else pen.shape[0],
         _i32("gap_open", gap_open), _i32("gap_extend", gap_extend),
-        _lib.i32_ptr(pr32) if pr32.size else None, int(pr32.size), int(prior_width),
-        _i32("max_penalty", max_penalty), int(threads), ctypes.byref(res), ctypes.byref(err))
+        _lib.i32_ptr(pr32) if pr32.size else None, int(pr32.size), _u32("prior_width", prior_width),
+        _i32("max_penalty", max_penalty), _i32("threads", threads), ctypes.byref(res), ctypes.byref(err))
     _lib.check(code, err)
     # the arrays take over the library's pinned blocks (no copy of a possibly huge result)
     n, nnz = int(res.rows), int(res.nnz)
@@ -112,6 +130,7 @@ def align_score_matrix(queries, refs, matrix: SubstitutionMatrix, mode: str = "g
                        gap_open: int = 11, gap_extend: int = 1, alphabet: str = "aa",
                        threads: int = 0) -> ScoreMatrix:
     """Dense (n_queries, n_refs) similarity matrix, GIL released."""
+    _i32("threads", threads)
     return _align(queries, refs, matrix, mode, gap_open, gap_extend, alphabet, False)
 
 
@@ -119,6 +138,7 @@ def align_dist_matrix(queries, refs, matrix: SubstitutionMatrix, mode: str = "gl
                       gap_open: int = 11, gap_extend: int = 1, alphabet: str = "aa",
                       threads: int = 0) -> ScoreMatrix:
     """Dense distance matrix d = s(a,a) + s(b,b) - 2*s(a,b); non-negative, zero on identity."""
+    _i32("threads", threads)
     return _align(queries, refs, matrix, mode, gap_open, gap_extend, alphabet, True)
 
 
@@ -134,11 +154,13 @@ def _distance(a, b, lev: bool) -> ScoreMatrix:
 
 def hamming_matrix(a, b, threads: int = 0) -> ScoreMatrix:
     """Dense (len(a), len(b)) int32 Hamming matrix; ValueError if any pair differs in length."""
+    _i32("threads", threads)
     return _distance(a, b, False)
 
 
 def levenshtein_matrix(a, b, threads: int = 0) -> ScoreMatrix:
     """Dense (len(a), len(b)) int32 Levenshtein matrix."""
+    _i32("threads", threads)
     return _distance(a, b, True)
 
 

@@ -160,3 +160,23 @@ def test_penalty_alignment_matrix_argument_like_search_params():
         _penalty_grid("pam250", "nt")
     with pytest.raises(TypeError, match="name string or a SubstitutionMatrix"):
         _penalty_grid(3, "aa")
+
+
+def test_integer_arguments_convert_like_the_reference_binding():
+    """int32_t / uint32_t arguments of the reference binding reject floats, strings, None and
+    out-of-range values with TypeError (pybind11 never truncates or parses); the checks run on
+    the host before the library computes anything."""
+    from seqtree_b200 import _core
+    b62 = SubstitutionMatrix.blosum62()
+    calls = [lambda: _core.gapblock_matrix(["A"], ["A"], gap_open=1.5),
+             lambda: _core.gapblock_matrix(["A"], ["A"], gap_extend=2 ** 31),
+             lambda: _core.gapblock_matrix(["A"], ["A"], prior_width=-1),
+             lambda: _core.gapblock_matrix(["A"], ["A"], threads=0.5),
+             lambda: _core.align_score_matrix(["A"], ["A"], b62, gap_open="11"),
+             lambda: _core.align_dist_matrix(["A"], ["A"], b62, threads=None),
+             lambda: _core.hamming_matrix(["A"], ["A"], threads=1.0),
+             lambda: _core.levenshtein_matrix(["A"], ["A"], threads="0")]
+    for call in calls:
+        with pytest.raises(TypeError):
+            call()
+    assert _core._i32("gap_open", np.int64(8)) == 8 and _core._u32("w", np.uint8(25)) == 25
