@@ -287,6 +287,9 @@ def kernel_roofline(w, cells: float, seconds: float, clocks) -> dict | None:
     alignment: ALU pipe.  A DPX instruction updates one int16x2 cell pair, and the recurrence
     needs 6 of them per pair (M, X, Y, H and the two gap extends) -- 3 per cell -- against
     64 lanes/clk/SM.
+    levenshtein: ALU pipe.  The bit-vector step per text character is ten 64-bit logic, add and
+    shift operations (the whole pattern, <= 64 symbols, in one word): 20 32-bit ALU lane-ops
+    per (pair, query character) against 64 lanes/clk/SM.
     """
     mhz = (clocks or {}).get("sm_mhz") or 1965.0
     sms = 148
@@ -301,6 +304,14 @@ def kernel_roofline(w, cells: float, seconds: float, clocks) -> dict | None:
         peak = sms * 64 * mhz * 1e6 / 1e9
         return {"bound": "alu", "achieved": achieved, "peak": peak, "unit": "Glane-op/s",
                 "frac": achieved / peak, "work": "3 DPX lane-ops per cell (6 per int16x2 pair)",
+                "peak_basis": f"148 SMs x 64 ALU lanes/clk at {mhz:.0f} MHz"}
+    if w["kind"] == "levenshtein":
+        steps = float(sum(map(len, w["queries"]))) * len(w["refs"])
+        achieved = 20.0 * steps / seconds / 1e9
+        peak = sms * 64 * mhz * 1e6 / 1e9
+        return {"bound": "alu", "achieved": achieved, "peak": peak, "unit": "Glane-op/s",
+                "frac": achieved / peak,
+                "work": "20 ALU lane-ops per (pair, query character): one 64-bit bit-vector step",
                 "peak_basis": f"148 SMs x 64 ALU lanes/clk at {mhz:.0f} MHz"}
     return None
 
