@@ -311,6 +311,16 @@ void launch_thread(Context& ctx, ThreadArgs a, int nmax, bool local, int64_t wor
 // int16 safety: the host admits a call only when every finite cell lies within +-14000
 // (|s| * L + open + extend * (rows + cols) <= 14000, |s| <= 2000); then NEG = -16384 and every
 // NEG-derived candidate stays below every finite one without wrapping.
+//
+// Global mode with gap_extend <= gap_open (OFFSET) keeps every state of cell (i, j) raised by
+// (i + j) * extend: H~ = H + (i+j)e, and likewise M~, X~, Y~.  Then
+//   X~(i,j) = max(H~(i-1,j) + e - o, X~(i-1,j)),  Y~(i,j) = max(H~(i,j-1) + e - o, Y~(i,j-1)),
+//   M~(i,j) = H~(i-1,j-1) + s + 2e,               H~ = max(M~, X~, Y~),
+// so each gap state is one add-max instead of two (the 2e rides in the substitution table), and
+// every border H~ is the constant e - o (0 at the corner).  The score is H~(m,n) - (m+n)e.  The
+// offset is non-negative and at most extend * (rows + cols), which the admission bound above
+// already counts, so the raised states stay within +-14000; the gap states only take maxima, so
+// NEG never drifts downwards.
 constexpr int kWaveThreads = 256;
 constexpr uint32_t kNeg2 = 0xC000C000u;  // -16384 in both halves
 
@@ -352,6 +362,8 @@ __global__ void __launch_bounds__(kWaveThreads) gotoh_wave_kernel(const WaveArgs
     const int64_t nwarps = (int64_t(gridDim.x) * blockDim.x) >> 5;
     const int64_t ntasks = a.self ? a.nq : a.nq * a.nrp;
     const uint32_t mgo2 = dup2(-a.go), mge2 = dup2(-a.ge);
+    constexpr bool OFFSET = !LOCAL && !EXACT;
+    const uint32_t eo2 = dup2(a.ge - a.go);  // the raised border value, and the gap-open step
 
     for (int64_t task = gwarp; task < ntasks; task += nwarps) {
         const int64_t qi_idx = a.self ? task : task / a.nrp;
@@ -379,12 +391,13 @@ __global__ void __launch_bounds__(kWaveThreads) gotoh_wave_kernel(const WaveArgs
             const int row = lane * R + r;  // 0-indexed query position
             qb[r] = uint32_t((row < m ? q[row] : pad) * A1 * A1);
             const int gr = a.go + row * a.ge;  // gap_run(row + 1)
-            Hl[r] = LOCAL ? 0u : dup2(-gr);
+            Hl[r] = LOCAL ? 0u : (OFFSET ? eo2 : dup2(-gr));
             Yl[r] = kNeg2;
             if constexpr (EXACT) MXl[r] = Hl[r];
         }
         // H[lane*R][0]: the row above this lane's first row, at column 0.
-        uint32_t diag = (lane == 0 || LOCAL) ? 0u : dup2(-(a.go + (lane * R - 1) * a.ge));
+        uint32_t diag = (lane == 0 || LOCAL) ? 0u
+                        : (OFFSET ? eo2 : dup2(-(a.go + (lane * R - 1) * a.ge)));
         uint32_t best = 0u, cap = 0u;
         uint32_t outH = 0u, outX = kNeg2, outMY = 0u;
         int outRes = 0;
@@ -397,7 +410,7 @@ __global__ void __launch_bounds__(kWaveThreads) gotoh_wave_kernel(const WaveArgs
             int res = __shfl_up_sync(full, outRes, 1);
             const int j = s - lane + 1;
             if (lane == 0) {  // the virtual row 0 at column j
-                const uint32_t h0 = LOCAL ? 0u : dup2(-(a.go + (j - 1) * a.ge));
+                const uint32_t h0 = LOCAL ? 0u : (OFFSET ? eo2 : dup2(-(a.go + (j - 1) * a.ge)));
                 upH = h0;
                 upX = kNeg2;
                 upMY = h0;
@@ -416,6 +429,9 @@ __global__ void __launch_bounds__(kWaveThreads) gotoh_wave_kernel(const WaveArgs
                     if constexpr (EXACT) {
                         X = __viaddmax_s16x2(upMY, mgo2, __viaddmax_s16x2(upX, mge2, kNeg2));
                         Y = __viaddmax_s16x2(MXl[r], mgo2, __viaddmax_s16x2(Yl[r], mge2, kNeg2));
+                    } else if constexpr (OFFSET) {
+                        X = __viaddmax_s16x2(upH, eo2, upX);
+                        Y = __viaddmax_s16x2(Hl[r], eo2, Yl[r]);
                     } else {
                         X = __viaddmax_s16x2(upH, mgo2, __viaddmax_s16x2(upX, mge2, kNeg2));
                         Y = __viaddmax_s16x2(Hl[r], mgo2, __viaddmax_s16x2(Yl[r], mge2, kNeg2));
@@ -458,6 +474,10 @@ __global__ void __launch_bounds__(kWaveThreads) gotoh_wave_kernel(const WaveArgs
             cap = __shfl_sync(full, cap, cap_lane);
             v1 = lo16(cap);
             v2 = hi16(cap);
+            if constexpr (OFFSET) {
+                v1 -= (m + n1) * a.ge;
+                v2 -= (m + n2) * a.ge;
+            }
         }
         if (lane == 0) {
             if (a.self) {
@@ -609,13 +629,16 @@ void align_wave(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
     WaveState& ws = wave_state(ctx.device);
     const int A1 = A + 1;
     {
-        // T[(q*A1 + r1)*A1 + r2] = s(q,r1) | s(q,r2) << 16, the pad code scoring NEG.
-        std::vector<uint8_t> key(size_t(A) * A * 4);
-        std::memcpy(key.data(), similarity, key.size());
+        // T[(q*A1 + r1)*A1 + r2] = s(q,r1) | s(q,r2) << 16, the pad code scoring NEG; the
+        // offset form (global, gap_extend <= gap_open) adds 2 * gap_extend to every finite score.
+        const int32_t add = (mode != ST_MODE_LOCAL && ge <= go) ? 2 * ge : 0;
+        std::vector<uint8_t> key(size_t(A) * A * 4 + 4);
+        std::memcpy(key.data(), similarity, size_t(A) * A * 4);
+        std::memcpy(key.data() + size_t(A) * A * 4, &add, 4);
         if (!same_as_last(ws.key, key.data(), key.size())) {
             std::vector<uint32_t> tab(size_t(A1) * A1 * A1);
             auto sv = [&](int x, int y) -> int32_t {
-                return (x == A || y == A) ? -16384 : similarity[x * A + y];
+                return (x == A || y == A) ? -16384 : similarity[x * A + y] + add;
             };
             for (int x = 0; x < A1; ++x)
                 for (int y1 = 0; y1 < A1; ++y1)
