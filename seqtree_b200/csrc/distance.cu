@@ -227,21 +227,28 @@ const char* launch_hamming(const uint32_t* qp, const uint32_t* rp, int64_t N, in
 constexpr int kLevWarps = 8;
 constexpr int kLevRows = 16;  // query rows per CTA
 
-// Pattern = ref (lane), text = query (warp-uniform).  Peq in shared memory as [c][lane].
+// Pattern = ref (lane), text = query (warp-uniform).  Peq in shared memory as [c][word][lane].
+// W = 64-bit words per pattern: one word takes refs up to 64 symbols; longer refs (W = 2 or 4)
+// run the blocked form, where each word passes its bottom horizontal step (-1, 0 or +1) to the
+// next word as the carry into its first row (Myers 1999, "advance_block"): a -1 carry sets the
+// match bit of row 0 for the add and shifts a 1 into Mh, a +1 carry shifts a 1 into Ph.  Rows
+// past a lane's own ref length act as unmatched rows below the pattern and never reach rows above
+// them, so every lane runs all W words and masks its own length at the end.
+template <int W>
 __global__ void __launch_bounds__(kLevWarps * 32)
 levenshtein_kernel(const uint8_t* __restrict__ qc, const int64_t* __restrict__ qoff,
                    const uint8_t* __restrict__ rc, const int64_t* __restrict__ roff, int64_t N,
                    int64_t K, int sigma, int32_t* __restrict__ out) {
-    extern __shared__ unsigned long long s_peq[];  // [warp][sigma][32]
+    extern __shared__ unsigned long long s_peq[];  // [warp][sigma][W][32]
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned long long* peq = s_peq + size_t(warp) * sigma * 32;
+    unsigned long long* peq = s_peq + size_t(warp) * sigma * W * 32;
     const int64_t k = (int64_t(blockIdx.x) * kLevWarps + warp) * 32 + lane;
     const bool valid = k < K;
     const int64_t kk = valid ? k : (K - 1);
     const uint8_t* r = rc + roff[kk];
     const int n = int(roff[kk + 1] - roff[kk]);
-    for (int c = 0; c < sigma; ++c) peq[c * 32 + lane] = 0ull;
-    for (int j = 0; j < n; ++j) peq[r[j] * 32 + lane] |= 1ull << j;
+    for (int c = 0; c < sigma * W; ++c) peq[c * 32 + lane] = 0ull;
+    for (int j = 0; j < n; ++j) peq[(r[j] * W + (j >> 6)) * 32 + lane] |= 1ull << (j & 63);
     __syncwarp();
     const unsigned long long ones = n >= 64 ? ~0ull : ((1ull << n) - 1ull);
     const int64_t r0 = int64_t(blockIdx.y) * kLevRows;
@@ -253,6 +260,42 @@ levenshtein_kernel(const uint8_t* __restrict__ qc, const int64_t* __restrict__ q
         // read once from the last column, D[n][m] = D[0][m] + sum of its steps
         // = m + popc(Pv) - popc(Mv) over the n pattern bits, instead of following the bottom
         // cell through every column (which costs about a fifth of the loop's instructions).
+        if constexpr (W > 1) {
+            unsigned long long Pv[W], Mv[W];
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                Pv[w] = ~0ull;
+                Mv[w] = 0ull;
+            }
+            for (int t = 0; t < m; ++t) {
+                const unsigned long long* e = peq + q[t] * W * 32 + lane;
+                int h = 1;  // row 0 of the global distance: +1 per text character
+#pragma unroll
+                for (int w = 0; w < W; ++w) {
+                    unsigned long long Eq = e[w * 32];
+                    const unsigned long long Xv = Eq | Mv[w];
+                    Eq |= h < 0 ? 1ull : 0ull;
+                    const unsigned long long Xh = (((Eq & Pv[w]) + Pv[w]) ^ Pv[w]) | Eq;
+                    unsigned long long Ph = Mv[w] | ~(Xh | Pv[w]);
+                    unsigned long long Mh = Pv[w] & Xh;
+                    const int hout = int(Ph >> 63) - int(Mh >> 63);
+                    Ph = (Ph << 1) | (h > 0 ? 1ull : 0ull);
+                    Mh = (Mh << 1) | (h < 0 ? 1ull : 0ull);
+                    Pv[w] = Mh | ~(Xv | Ph);
+                    Mv[w] = Ph & Xv;
+                    h = hout;
+                }
+            }
+            int score = m;
+#pragma unroll
+            for (int w = 0; w < W; ++w) {
+                const int bits = min(64, max(0, n - 64 * w));
+                const unsigned long long mask = bits >= 64 ? ~0ull : ((1ull << bits) - 1ull);
+                score += __popcll(Pv[w] & mask) - __popcll(Mv[w] & mask);
+            }
+            if (valid) out[i * K + k] = score;
+            continue;
+        }
         unsigned long long Pv = ones, Mv = 0ull;
         for (int t = 0; t < m; ++t) {
             const unsigned long long Eq = peq[q[t] * 32 + lane];
@@ -376,12 +419,23 @@ void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream
     const uint8_t* ac = static_cast<uint8_t*>(dc.ac.ptr);
     const uint8_t* bc = static_cast<uint8_t*>(dc.bc.ptr);
     const dim3 grid(unsigned(ceil_div(K, kLevWarps * 32)), unsigned(ceil_div(N, kLevRows)));
-    if (b.max_len <= 64 && sigma <= 64 && grid.y <= 65535) {
-        const size_t smem = size_t(kLevWarps) * sigma * 32 * 8;
-        STB_CUDA(cudaFuncSetAttribute(levenshtein_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(smem)));
-        levenshtein_kernel<<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off, N, K,
-                                                                  sigma, out_d);
+    // Bit-vector path: refs up to 256 symbols (1, 2 or 4 words) while the Peq table fits.
+    const int words = b.max_len <= 64 ? 1 : b.max_len <= 128 ? 2 : b.max_len <= 256 ? 4 : 0;
+    const size_t smem = size_t(kLevWarps) * sigma * std::max(words, 1) * 32 * 8;
+    if (words && sigma <= 64 && smem <= size_t(200) * 1024 && grid.y <= 65535) {
+        const void* kern = words == 1 ? reinterpret_cast<const void*>(levenshtein_kernel<1>)
+                         : words == 2 ? reinterpret_cast<const void*>(levenshtein_kernel<2>)
+                                      : reinterpret_cast<const void*>(levenshtein_kernel<4>);
+        ensure_smem_limit(kern, smem);
+        if (words == 1)
+            levenshtein_kernel<1><<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off,
+                                                                         N, K, sigma, out_d);
+        else if (words == 2)
+            levenshtein_kernel<2><<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off,
+                                                                         N, K, sigma, out_d);
+        else
+            levenshtein_kernel<4><<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off,
+                                                                         N, K, sigma, out_d);
         STB_CUDA(cudaGetLastError());
         note_launch("levenshtein_kernel");
         return;

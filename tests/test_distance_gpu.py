@@ -68,6 +68,25 @@ def test_levenshtein_against_oracle(dist, alphabet, lo, hi):
                           oracle.levenshtein_matrix(a, b, threads=os.cpu_count() or 1))
 
 
+@pytest.mark.parametrize("alphabet,lo,hi,kernel", [
+    ("ACGT", 65, 128, "levenshtein_kernel"),     # two 64-bit words per ref
+    ("ACGT", 100, 256, "levenshtein_kernel"),    # four words, up to the last bit
+    (AA20, 129, 200, "levenshtein_kernel"),      # four words, 20 symbols
+    ("ACGT", 0, 140, "levenshtein_kernel"),      # empty and one-word refs beside four-word ones
+    ("ACGT", 200, 300, "levenshtein_dp_kernel"),  # past four words: the DP kernel
+])
+def test_long_refs_take_the_blocked_bit_vector(dist, alphabet, lo, hi, kernel):
+    """Refs longer than one 64-bit word run the blocked bit-vector form (each word hands its
+    bottom horizontal step to the next); results equal the reference's two-row DP."""
+    from seqtree_b200 import _lib
+    rng = np.random.default_rng(lo * 1000 + hi)
+    a = rand_seqs(rng, 23, lo, hi, alphabet)
+    b = rand_seqs(rng, 77, lo, hi, alphabet)
+    got = as_np(dist.levenshtein_matrix(a, b))
+    assert _lib.last_kernel_name() == kernel
+    assert np.array_equal(got, oracle.levenshtein_matrix(a, b, threads=os.cpu_count() or 1))
+
+
 def test_many_distinct_bytes_take_the_dp_path(dist):
     rng = np.random.default_rng(9)
     alpha = "".join(chr(c) for c in range(33, 127))  # 94 distinct symbols
