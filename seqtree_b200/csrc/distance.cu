@@ -228,7 +228,7 @@ constexpr int kLevWarps = 8;
 constexpr int kLevRows = 16;  // query rows per CTA
 
 // Pattern = ref (lane), text = query (warp-uniform).  Peq in shared memory as [c][word][lane].
-// W = 64-bit words per pattern: one word takes refs up to 64 symbols; longer refs (W = 2 or 4)
+// W = 64-bit words per pattern: one word takes refs up to 64 symbols; longer refs (W = 2, 4, 8)
 // run the blocked form, where each word passes its bottom horizontal step (-1, 0 or +1) to the
 // next word as the carry into its first row (Myers 1999, "advance_block"): a -1 carry sets the
 // match bit of row 0 for the add and shifts a 1 into Mh, a +1 carry shifts a 1 into Ph.  Rows
@@ -419,13 +419,18 @@ void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream
     const uint8_t* ac = static_cast<uint8_t*>(dc.ac.ptr);
     const uint8_t* bc = static_cast<uint8_t*>(dc.bc.ptr);
     const dim3 grid(unsigned(ceil_div(K, kLevWarps * 32)), unsigned(ceil_div(N, kLevRows)));
-    // Bit-vector path: refs up to 256 symbols (1, 2 or 4 words) while the Peq table fits.
-    const int words = b.max_len <= 64 ? 1 : b.max_len <= 128 ? 2 : b.max_len <= 256 ? 4 : 0;
+    // Bit-vector path: refs up to 512 symbols (1, 2, 4 or 8 words) while the Peq table fits.
+    const int words = b.max_len <= 64    ? 1
+                    : b.max_len <= 128 ? 2
+                    : b.max_len <= 256 ? 4
+                    : b.max_len <= 512 ? 8
+                                       : 0;
     const size_t smem = size_t(kLevWarps) * sigma * std::max(words, 1) * 32 * 8;
     if (words && sigma <= 64 && smem <= size_t(200) * 1024 && grid.y <= 65535) {
         const void* kern = words == 1 ? reinterpret_cast<const void*>(levenshtein_kernel<1>)
                          : words == 2 ? reinterpret_cast<const void*>(levenshtein_kernel<2>)
-                                      : reinterpret_cast<const void*>(levenshtein_kernel<4>);
+                         : words == 4 ? reinterpret_cast<const void*>(levenshtein_kernel<4>)
+                                      : reinterpret_cast<const void*>(levenshtein_kernel<8>);
         ensure_smem_limit(kern, smem);
         if (words == 1)
             levenshtein_kernel<1><<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off,
@@ -433,8 +438,11 @@ void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream
         else if (words == 2)
             levenshtein_kernel<2><<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off,
                                                                          N, K, sigma, out_d);
-        else
+        else if (words == 4)
             levenshtein_kernel<4><<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off,
+                                                                         N, K, sigma, out_d);
+        else
+            levenshtein_kernel<8><<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off,
                                                                          N, K, sigma, out_d);
         STB_CUDA(cudaGetLastError());
         note_launch("levenshtein_kernel");

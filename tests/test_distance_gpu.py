@@ -73,7 +73,9 @@ def test_levenshtein_against_oracle(dist, alphabet, lo, hi):
     ("ACGT", 100, 256, "levenshtein_kernel"),    # four words, up to the last bit
     (AA20, 129, 200, "levenshtein_kernel"),      # four words, 20 symbols
     ("ACGT", 0, 140, "levenshtein_kernel"),      # empty and one-word refs beside four-word ones
-    ("ACGT", 200, 300, "levenshtein_dp_kernel"),  # past four words: the DP kernel
+    ("ACGT", 257, 512, "levenshtein_kernel"),    # eight words (small alphabets only)
+    (AA20, 257, 300, "levenshtein_dp_kernel"),   # eight words of 20 symbols exceed the table
+    ("ACGT", 513, 560, "levenshtein_dp_kernel"),  # past eight words: the DP kernel
 ])
 def test_long_refs_take_the_blocked_bit_vector(dist, alphabet, lo, hi, kernel):
     """Refs longer than one 64-bit word run the blocked bit-vector form (each word hands its
