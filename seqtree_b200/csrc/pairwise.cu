@@ -195,6 +195,44 @@ __global__ void __launch_bounds__(128) gotoh_thread_kernel(const ThreadArgs a) {
         int32_t score;
         if (m == 0 || n == 0) {
             score = LOCAL ? 0 : -gap_run32(m ? m : n, a.go, a.ge);
+        } else if (!LOCAL && a.ge <= a.go) {
+            // Global with gap_extend <= gap_open: the single-H form with every state of (i, j)
+            // raised by (i+j) * extend, as in the wavefront kernel -- each gap state is one
+            // add-max, borders are the constant extend - open, score = H~(m,n) - (m+n) * extend.
+            int rcode[NMAX];
+            int32_t H[NMAX + 1], Xr[NMAX + 1];
+            const int32_t eo = a.ge - a.go, e2 = 2 * a.ge;
+            H[0] = 0;
+#pragma unroll
+            for (int j = 1; j <= NMAX; ++j) {
+                rcode[j - 1] = j <= n ? int(r[j - 1]) : 0;
+                H[j] = eo;
+                Xr[j] = kNeg32;
+            }
+            int32_t hn = 0;
+            for (int ii = 1; ii <= m; ++ii) {
+                int32_t hd = H[0];
+                int32_t hl = eo, yl = kNeg32;
+                H[0] = eo;
+                const int32_t* srow = s_sim + int(q[ii - 1]) * a.A;
+#pragma unroll
+                for (int j = 1; j <= NMAX; ++j) {
+                    if (j <= n) {
+                        const int32_t hu = H[j];
+                        const int32_t mv = hd + srow[rcode[j - 1]] + e2;
+                        const int32_t xv = __viaddmax_s32(hu, eo, Xr[j]);
+                        const int32_t yv = __viaddmax_s32(hl, eo, yl);
+                        const int32_t hv = __vimax3_s32(mv, xv, yv);
+                        hd = hu;
+                        H[j] = hv;
+                        Xr[j] = xv;
+                        hl = hv;
+                        yl = yv;
+                    }
+                }
+                hn = hl;
+            }
+            score = hn - (m + n) * a.ge;
         } else {
             int rcode[NMAX];
             int32_t M[NMAX + 1], X[NMAX + 1], Y[NMAX + 1];
