@@ -360,8 +360,10 @@ int32_t st_levenshtein_matrix_sets(st_seqset a, st_seqset b, int32_t *out_device
  * the library (held by every GPU that loads it); inputs whose DP row (shorter length + 1 words)
  * does not fit it for 256 threads are rejected with ST_EINVAL.  The first call on a device looks
  * up the array's address (make it before any stream capture).  The call synchronises
- * cuda_stream once (to size the launch) and returns with the matrix kernel enqueued on it.
- * Calls share the array: calls whose work overlaps on the GPU race.
+ * cuda_stream once (to size the launch, under a per-device host lock) and returns with the matrix
+ * kernel enqueued on it.  Calls share the array: calls whose kernels overlap on the GPU (several
+ * streams) race on its DP rows and may return wrong distances; the kernel never writes outside the
+ * array, and a pair whose row would not fit its launch's share of it gets -1.
  */
 int32_t st_levenshtein_matrix_noalloc(const char *a_bytes, const int64_t *a_offsets,
                                       int64_t a_count, const char *b_bytes,

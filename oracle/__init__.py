@@ -34,9 +34,12 @@ _i32p = ctypes.POINTER(ctypes.c_int32)
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 
 
-def build() -> None:
-    """Compile both checkers (the reference one only where its source tree exists)."""
-    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+def build(reference_tree: str | None = None) -> None:
+    """Compile both checkers; the reference one only when its source tree is given (argument or
+    the SEQTREE_REFERENCE environment variable) and present."""
+    tree = reference_tree or os.environ.get("SEQTREE_REFERENCE")
+    cmd = ["make", "-s", "-C", str(HERE)] + ([f"REF={tree}"] if tree else [])
+    subprocess.run(cmd, check=True)
 
 
 def pack(strings) -> tuple[np.ndarray, np.ndarray]:

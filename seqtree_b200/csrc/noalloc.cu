@@ -10,8 +10,12 @@
 // The array is kScratchBytes (32 MiB) per device; every GPU that loads the library holds it until
 // the process exits.  Its device address is looked up once per device, with that device current,
 // on the first call on that device (so make that first call before any stream capture).  All
-// calls share the array: the two header words are cleared at the start of every call, and calls
-// whose work overlaps on the GPU (for example, on two streams at once) race on it.
+// calls share the array.  The two header words that size the launch are cleared, filled and read
+// back under a per-device host lock, so concurrent host threads cannot size a launch from another
+// call's header.  The DP-row region after the header is not locked: calls whose kernels overlap
+// on the GPU (for example, on two streams at once) race on it and may return wrong distances.
+// Each kernel also checks that its row fits the capacity it was launched with and writes -1
+// (never a distance) for a pair whose row would not, touching no scratch for it.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -32,6 +36,7 @@ static __device__ __align__(256) int32_t g_noalloc_scratch[kScratchWords];
 
 int32_t* g_scratch_addr[kMaxDevices];  // device address of g_noalloc_scratch, per device
 std::mutex g_setup_mu;
+std::mutex g_call_mu[kMaxDevices];  // serialises the header's clear / fill / read per device
 
 int32_t set_error(st_error* err, int32_t code, const char* msg) {
     if (err) {
@@ -55,11 +60,13 @@ __global__ void longest_kernel(const int64_t* __restrict__ a_off, int64_t N,
 }
 
 // The single-row unit-cost DP of the reference (src/distance.cpp:78-95): the row runs over the
-// shorter string and lives in the fixed scratch, laid out [column][thread].
+// shorter string and lives in the fixed scratch, laid out [column][thread].  `row_cap` is the
+// number of row words each thread owns (room / threads); a pair whose row (shorter + 1 words)
+// exceeds it gets -1 and no scratch access.
 __global__ void __launch_bounds__(kThreads)
 levenshtein_rows_kernel(const uint8_t* __restrict__ a, const int64_t* __restrict__ ao, int64_t N,
                         const uint8_t* __restrict__ b, const int64_t* __restrict__ bo, int64_t K,
-                        int32_t* __restrict__ rows, int32_t* __restrict__ out) {
+                        int32_t* __restrict__ rows, int64_t row_cap, int32_t* __restrict__ out) {
     const int64_t T = int64_t(gridDim.x) * blockDim.x;
     const int64_t tid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
     for (int64_t idx = tid; idx < N * K; idx += T) {
@@ -74,6 +81,8 @@ levenshtein_rows_kernel(const uint8_t* __restrict__ a, const int64_t* __restrict
         int32_t v;
         if (n == 0) {
             v = m;
+        } else if (int64_t(n) + 1 > row_cap) {
+            v = -1;
         } else {
             for (int j = 0; j <= n; ++j) rows[j * T + tid] = j;
             for (int x = 1; x <= m; ++x) {
@@ -104,7 +113,7 @@ extern "C" int32_t st_levenshtein_matrix_noalloc(const char* a_bytes, const int6
     if (a_count < 0 || b_count < 0)
         return set_error(err, ST_EINVAL, "seqtree_b200: negative sequence count");
     if (a_count == 0 || b_count == 0) return set_error(err, ST_OK, "");
-    if (!a_offsets || !b_offsets || !out)
+    if (!a_offsets || !b_offsets || !out || !a_bytes || !b_bytes)
         return set_error(err, ST_EINVAL, "seqtree_b200: null device pointer");
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
@@ -135,7 +144,9 @@ extern "C" int32_t st_levenshtein_matrix_noalloc(const char* a_bytes, const int6
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (sms <= 0) sms = 1;
 
-    // Longest sequence on each side (the header starts at zero on every call).
+    // Longest sequence on each side.  The header is cleared, filled and read back under the
+    // device's lock, so another host thread's call cannot change it in between.
+    std::lock_guard<std::mutex> call_lock(g_call_mu[dev]);
     int32_t longest[2] = {0, 0};
     cudaError_t e = cudaMemsetAsync(scratch, 0, 2 * sizeof(int32_t), stream);
     if (e == cudaSuccess) {
@@ -152,16 +163,13 @@ extern "C" int32_t st_levenshtein_matrix_noalloc(const char* a_bytes, const int6
         return set_error(err, ST_ECUDA, msg);
     }
 
-    // One DP row of (shorter + 1) words per thread must fit the fixed scratch.
+    // One DP row of (shorter + 1) words per thread must fit the fixed scratch for at least one
+    // block of threads; the grid is the smaller of what fits, about 2,048 threads per SM, and
+    // the pair count rounded up to whole blocks.
     const int64_t row = int64_t(longest[0] < longest[1] ? longest[0] : longest[1]) + 1;
     const int64_t room = int64_t(kScratchWords - kHeaderWords);
-    int64_t threads = room / row;
-    const int64_t want = int64_t(sms) * 2048;
-    if (threads > want) threads = want;
-    const int64_t pairs = a_count * b_count;
-    if (threads > pairs) threads = pairs;
-    threads = (threads / kThreads) * kThreads;
-    if (threads < kThreads) {
+    const int64_t fit = (room / row / kThreads) * kThreads;
+    if (fit < kThreads) {
         char msg[220];
         std::snprintf(msg, sizeof msg,
                       "seqtree_b200: sequences too long for the fixed %zu MiB scratch (a DP row of "
@@ -169,9 +177,16 @@ extern "C" int32_t st_levenshtein_matrix_noalloc(const char* a_bytes, const int6
                       kScratchBytes >> 20, static_cast<long long>(row), kThreads);
         return set_error(err, ST_EINVAL, msg);
     }
+    const int64_t pairs = a_count * b_count;
+    int64_t threads = fit;
+    const int64_t want = int64_t(sms) * 2048;
+    if (threads > want) threads = want;
+    const int64_t need = (pairs + kThreads - 1) / kThreads * kThreads;
+    if (threads > need) threads = need;
     levenshtein_rows_kernel<<<unsigned(threads / kThreads), kThreads, 0, stream>>>(
         reinterpret_cast<const uint8_t*>(a_bytes), a_offsets, a_count,
-        reinterpret_cast<const uint8_t*>(b_bytes), b_offsets, b_count, scratch + kHeaderWords, out);
+        reinterpret_cast<const uint8_t*>(b_bytes), b_offsets, b_count, scratch + kHeaderWords,
+        room / threads, out);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
         char msg[200];

@@ -8,7 +8,7 @@ published NCBI/EMBOSS log-odds tables, the last one is generated by the referenc
 ``bench/gen_matrices.py``).  This script parses those files as text and writes the grids in
 this package's own layout.  It needs the reference tree and is run by hand:
 
-    python seqtree_b200/gen_tables.py /root/reference
+    python seqtree_b200/gen_tables.py <reference source tree>
 """
 import re
 import sys
@@ -67,4 +67,6 @@ def write_c_include(path: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: gen_tables.py <reference source tree>")
+    main(sys.argv[1])

@@ -21,7 +21,9 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+if len(sys.argv) != 2:
+    raise SystemExit("usage: gen_profiles.py <reference source tree>")
+REF = Path(sys.argv[1])
 OUT = Path(__file__).resolve().parent / "profiles.json"
 AA20 = "ACDEFGHIKLMNPQRSTVWY"
 
