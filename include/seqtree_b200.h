@@ -371,6 +371,35 @@ int32_t st_levenshtein_matrix_noalloc(const char *a_bytes, const int64_t *a_offs
                                       void *cuda_stream, st_error *err);
 
 /*
+ * Peak issue rate of one instruction on the current device, measured by a register-only (or, for
+ * ST_PEAK_LDS32, conflict-free shared-memory) probe: the denominators of the scoring kernels'
+ * rooflines (the gap-block sweep of src/gapblock.cpp:119-125 is LDS.32 + __viaddmin_s16x2 per
+ * cell pair; the Gotoh cell update of src/pairwise.cpp:106-117 is DPX add-max; the Levenshtein
+ * bit-vector step replacing src/distance.cpp:78-95 is LOP3/IADD3).  No counterpart in the
+ * reference.  all_sms = 0 runs one 1,024-thread block (one SM), otherwise two per SM.  Allocates
+ * and frees a few bytes of device memory; about 10 ms per call.
+ */
+enum {
+    ST_PEAK_LOP3 = 0,
+    ST_PEAK_IADD3 = 1,
+    ST_PEAK_IMAD = 2,
+    ST_PEAK_VIADDMIN_S16X2 = 3,
+    ST_PEAK_VIADDMAX_S32 = 4,
+    ST_PEAK_VIMAX3_S32 = 5,
+    ST_PEAK_LDS32 = 6
+};
+
+typedef struct st_peak {
+    double lane_ops_per_s;      /* lane operations (one thread's op, or one 4-byte load) per s */
+    double lane_ops_per_sm_clk; /* per SM per SM clock cycle (clock64 span of the longest block) */
+    double ms;                  /* duration of the fastest of three launches */
+    int32_t sms;                /* SMs the launch covered */
+    int32_t threads;            /* threads launched */
+} st_peak;
+
+int32_t st_measure_peak(int32_t op, int32_t all_sms, st_peak *out, st_error *err);
+
+/*
  * The raw similarity grid of a built-in amino-acid matrix ("blosum62", "blosum45", "blosum80",
  * "pam250", "pam100", "structural"), row-major 24*24 in the AminoAcid codec order, the numbers
  * behind seqtree::SubstitutionMatrix::blosum62() etc. (include/seqtree/seqtree.hpp:48-53,

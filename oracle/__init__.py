@@ -9,6 +9,10 @@ Two checkers live here, both loaded with ctypes:
   ``oracle/_ref/libseqtree_ref.so`` (present wherever the build ran; the file travels with
   the repository snapshot).
 
+Plus a pure-Python restatement of the reference's ``central_prior`` and ``_prior_cube``
+(``python/seqtree/gapblock.py:79-94, 492-509``), so that a process timing the reference needs
+nothing from ``seqtree_b200`` to build its prior cube.
+
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline leg may import this
 package, and only as the checker or the timed CPU baseline -- never on the product path.
 """
@@ -42,8 +46,19 @@ def build(reference_tree: str | None = None) -> None:
     subprocess.run(cmd, check=True)
 
 
+class Prepacked(list):
+    """A list of strings that keeps its packed form, so a timed call does not re-pack it (a C++
+    caller of the reference passes the same ``std::vector<std::string>`` to every call)."""
+
+    def __init__(self, strings):
+        super().__init__(strings)
+        self.packed = pack(list(strings))
+
+
 def pack(strings) -> tuple[np.ndarray, np.ndarray]:
     """list[str] -> (uint8 bytes, int64 offsets of len+1)."""
+    if isinstance(strings, Prepacked):
+        return strings.packed
     bs = [s.encode("latin-1") if isinstance(s, str) else bytes(s) for s in strings]
     lens = np.fromiter((len(b) for b in bs), dtype=np.int64, count=len(bs))
     off = np.zeros(len(bs) + 1, dtype=np.int64)
@@ -248,6 +263,35 @@ def ref_tables(matrix) -> tuple[np.ndarray, np.ndarray, int]:
         raise ValueError("bad matrix")
     a = A.value
     return sim[: a * a].reshape(a, a).copy(), pen[: a * a].reshape(a, a).copy(), scale.value
+
+
+def central_prior(lam: int):
+    """``python/seqtree/gapblock.py:79-94``: 0 at d == 0, else ``int(lam * |2i + d - m| // 2)``
+    (block [i, i + d) in a longer sequence of length m)."""
+    if lam < 0:
+        raise ValueError("lam must be >= 0")
+
+    def prior(i: int, d: int, m: int) -> int:
+        return 0 if d == 0 else int(lam * abs(2 * i + d - m) // 2)
+
+    return prior
+
+
+def prior_cube(prior, width: int) -> list[int]:
+    """``python/seqtree/gapblock.py:492-509``: ``prior`` flattened to ``[m][d][i]`` with stride
+    width + 1; only d >= 1 and i <= m - d are filled, the rest stay zero; a negative value
+    raises ``ValueError``."""
+    w1 = width + 1
+    cube = [0] * (w1 * w1 * w1)
+    for m in range(w1):
+        for d in range(1, m + 1):
+            base = (m * w1 + d) * w1
+            for i in range(m - d + 1):
+                v = int(prior(i, d, m))
+                if v < 0:
+                    raise ValueError(f"gap_prior({i}, {d}, {m}) = {v} is negative")
+                cube[base + i] = v
+    return cube
 
 
 def ref_gapblock_matrix(queries, refs, alphabet="aa", matrix=None, gap_open=1, gap_extend=1,

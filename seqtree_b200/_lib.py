@@ -28,6 +28,15 @@ class st_error(ctypes.Structure):
     _fields_ = [("code", ctypes.c_int32), ("message", ctypes.c_char * 256)]
 
 
+class st_peak(ctypes.Structure):
+    _fields_ = [("lane_ops_per_s", ctypes.c_double), ("lane_ops_per_sm_clk", ctypes.c_double),
+                ("ms", ctypes.c_double), ("sms", ctypes.c_int32), ("threads", ctypes.c_int32)]
+
+
+PEAK_OPS = {"lop3": 0, "iadd3": 1, "imad": 2, "viaddmin_s16x2": 3, "viaddmax_s32": 4,
+            "vimax3_s32": 5, "lds32": 6}
+
+
 class st_sparse(ctypes.Structure):
     _fields_ = [("rows", ctypes.c_int64), ("cols", ctypes.c_int64), ("nnz", ctypes.c_int64),
                 ("indptr", ctypes.POINTER(ctypes.c_int64)),
@@ -140,6 +149,8 @@ SIGNATURES = [
       ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, _ep]),
     ("st_builtin_similarity", ctypes.c_int32,
      [ctypes.c_char_p, _i32p, ctypes.c_int32, _i32p, _ep]),
+    ("st_measure_peak", ctypes.c_int32,
+     [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(st_peak), _ep]),
     ("st_last_launch_count", ctypes.c_int32, []),
     ("st_total_launch_count", ctypes.c_int64, []),
     ("st_tuning_table", ctypes.c_int64, [ctypes.c_char_p, ctypes.c_int64]),
@@ -332,3 +343,17 @@ def last_kernel_name() -> str:
 def device_count() -> int:
     return int(lib.st_device_count())
 
+
+def measure_peak(op: str, all_sms: bool) -> dict:
+    """Peak issue rate of one instruction on the current device (``st_measure_peak``)."""
+    out, err = st_peak(), st_error()
+    check(lib.st_measure_peak(PEAK_OPS[op], int(all_sms), ctypes.byref(out), ctypes.byref(err)),
+          err)
+    return {"lane_ops_per_s": out.lane_ops_per_s, "per_sm_clk": out.lane_ops_per_sm_clk,
+            "ms": out.ms, "sms": out.sms, "threads": out.threads}
+
+
+def measure_peaks() -> dict:
+    """Every probe of :func:`measure_peak`, on one SM and on all SMs."""
+    return {op: {"one_sm": measure_peak(op, False), "all_sms": measure_peak(op, True)}
+            for op in PEAK_OPS}

@@ -175,3 +175,28 @@ def torch_rows(indptr):
     import torch
     n = indptr.numel() - 1
     return torch.arange(n, device=indptr.device).repeat_interleave(indptr[1:] - indptr[:-1])
+
+
+def hits_rows(hits, rows) -> list:
+    """``[(ref_ids int32, scores int32), ...]`` numpy arrays of the listed CSR rows of a device
+    ``Hits``; only the row pointers and the listed rows cross to the host."""
+    import torch
+    info = hits.info()
+    rows = [int(i) for i in rows]
+    if info["rows"] == 0 or not rows:
+        return [(np.zeros(0, np.int32), np.zeros(0, np.int32)) for _ in rows]
+    ip = torch.as_tensor(_DeviceArray(info["indptr"], info["rows"] + 1, "<i8"),
+                         device="cuda").cpu().numpy()
+    out = []
+    nnz = info["nnz"]
+    ri = sc = None
+    if nnz:
+        ri = torch.as_tensor(_DeviceArray(info["ref_ids"], nnz, "<i4"), device="cuda")
+        sc = torch.as_tensor(_DeviceArray(info["scores"], nnz, "<i4"), device="cuda")
+    for i in rows:
+        a, b = int(ip[i]), int(ip[i + 1])
+        if b > a:
+            out.append((ri[a:b].cpu().numpy(), sc[a:b].cpu().numpy()))
+        else:
+            out.append((np.zeros(0, np.int32), np.zeros(0, np.int32)))
+    return out

@@ -20,14 +20,8 @@ import numpy as np
 from . import _lib
 from .device import hits_tensors as _hits_tensors, torch_rows
 from .matrix import SubstitutionMatrix
-
-AA24 = "ARNDCQEGHILKMFPSTWYVBZX*"
-AA20 = "ACDEFGHIKLMNPQRSTVWY"
-PAD = 32
-_CODE = np.full(256, 255, np.uint8)
-for _i, _c in enumerate(AA24):
-    _CODE[ord(_c)] = _i
-    _CODE[ord(_c.lower())] = _i
+from .workloads import AA20, AA20_CODES as _AA20_CODES, AA24, CODE as _CODE, PAD  # noqa: F401
+from .workloads import cdr3_codes, cdr3_lengths, codes_to_letters, codes_to_strings  # noqa: F401
 
 
 def param_count() -> int:
@@ -226,45 +220,13 @@ def stream_status(stream: int = 0) -> None:
 
 
 # ----------------------------------------------------------------------------- data ---------
-_LETTER = np.frombuffer(AA24.encode(), np.uint8)             # code -> ASCII
-_AA20_CODES = _CODE[np.frombuffer(AA20.encode(), np.uint8)]  # the 20 standard residues as codes
-_C, _A, _S, _F = (int(_CODE[ord(x)]) for x in "CASF")
-
-
-def cdr3_lengths(rng, n: int) -> np.ndarray:
-    """Junction lengths 8-25 with mode 14: P(L) is a Gaussian around 14 with sigma 2.5 below and
-    3.5 above (right-skewed, like TRB junctions)."""
-    L = np.arange(8, 26)
-    sig = np.where(L < 14, 2.5, 3.5)
-    p = np.exp(-0.5 * ((L - 14) / sig) ** 2)
-    return rng.choice(L, size=n, p=p / p.sum()).astype(np.int32)
-
-
-def cdr3_codes(seed: int, n: int) -> tuple[np.ndarray, np.ndarray]:
-    """n CDR3-like junctions 'CASS' + uniform middle + 'F' (lengths from :func:`cdr3_lengths`)
-    as amino-acid codes [n, 32] (zero past each length) and lengths [n]."""
-    rng = np.random.default_rng(seed)
-    lens = cdr3_lengths(rng, n)
-    codes = _AA20_CODES[rng.integers(0, 20, size=(n, PAD), dtype=np.uint8)]
-    codes[:, :4] = (_C, _A, _S, _S)
-    codes[np.arange(n), lens - 1] = _F
-    codes[np.arange(PAD)[None, :] >= lens[:, None]] = 0
-    return codes, lens
+# The CDR3-like generators (cdr3_lengths, cdr3_codes, codes_to_strings) live in
+# seqtree_b200.workloads, which loads no compiled code; they are re-exported here.
 
 
 def codes_to_packed(codes: np.ndarray, lens: np.ndarray) -> _lib.Packed:
     """Codes [n, 32] + lengths as one concatenated letter buffer (for ``device.SeqSet``)."""
-    lens = np.asarray(lens, np.int64)
-    data = _LETTER[codes[np.arange(PAD)[None, :] < lens[:, None]]]
-    off = np.zeros(lens.size + 1, np.int64)
-    np.cumsum(lens, out=off[1:])
-    return _lib.Packed.from_arrays(data, off)
-
-
-def codes_to_strings(codes: np.ndarray, lens: np.ndarray) -> list[str]:
-    p = codes_to_packed(codes, lens)
-    text = p.data.tobytes().decode() if p.offsets[-1] else ""
-    return [text[a:b] for a, b in zip(p.offsets[:-1].tolist(), p.offsets[1:].tolist())]
+    return _lib.Packed.from_arrays(*codes_to_letters(codes, lens))
 
 
 def cdr3_like(seed: int, n: int) -> list[str]:

@@ -1,19 +1,28 @@
 """Generate the golden vectors under tests/golden/ from the REFERENCE's own C++.
 
 Run in a checkout next to the reference tree (it needs oracle/_ref/libseqtree_ref.so, which
-oracle/Makefile builds from the reference sources):
+oracle/Makefile builds from the reference sources, and the reference's Python package for the
+gap-block priors):
 
-    make -C oracle && python tests/golden/gen_golden.py
+    make -C oracle REF=<reference tree> && python tests/golden/gen_golden.py <reference tree>
 
 Every expected matrix below is the output of seqtree 0.6.0's C++ (gapblock_matrix,
 align_score_matrix / align_dist_matrix, hamming_matrix / levenshtein_matrix) on seeded inputs;
 the inputs are stored beside it.  The tests compare both the CPU oracle and the CUDA library
 with these files, so neither needs the reference tree at test time.
+
+The prior cubes passed to the reference are built by the reference's own Python
+(``python/seqtree/gapblock.py``: ``central_prior``, ``frame_prior``, ``positions_prior``,
+``profile_prior`` and ``_prior_cube``), loaded from the reference tree with a stub in place of
+its compiled ``_core``; ``prior_cubes.json`` keeps their reachable cells so that the library's
+own ``prior_cube`` and the oracle's restatement are pinned against them.
 """
 from __future__ import annotations
 
+import importlib.util
 import json
 import sys
+import types
 from pathlib import Path
 
 import numpy as np
@@ -22,11 +31,34 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 import oracle  # noqa: E402
-from seqtree_b200.gapblock import (central_prior, frame_prior, positions_prior,  # noqa: E402
-                                   prior_cube, profile_prior)
 
+if len(sys.argv) != 2:
+    raise SystemExit("usage: gen_golden.py <reference source tree>")
+REF = Path(sys.argv[1])
 OUT = Path(__file__).resolve().parent
 AA20 = "ACDEFGHIKLMNPQRSTVWY"
+
+
+def load_reference_gapblock():
+    """The reference's python/seqtree/gapblock.py with a stub for its compiled ``_core`` (the
+    priors and ``_prior_cube`` use none of its names)."""
+    pkg = types.ModuleType("seqtree")
+    pkg.__path__ = [str(REF / "python" / "seqtree")]
+    core = types.ModuleType("seqtree._core")
+    for name in ("Index", "ScoreMatrix", "SearchParams", "SubstitutionMatrix", "gapblock_matrix"):
+        setattr(core, name, object)
+    sys.modules["seqtree"] = pkg
+    sys.modules["seqtree._core"] = core
+    spec = importlib.util.spec_from_file_location("seqtree.gapblock",
+                                                  REF / "python" / "seqtree" / "gapblock.py")
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["seqtree.gapblock"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+GB = load_reference_gapblock()
+prior_cube = GB._prior_cube
 
 
 def rand_seqs(rng, n, lo, hi, alphabet=AA20):
@@ -52,11 +84,33 @@ def tables():
 
 PRIORS = {
     "none": None,
-    "central21": central_prior(21),
-    "frame21_5": frame_prior(21, 5),
-    "positions": positions_prior((3, 4, -4, -3)),
-    "profile21": profile_prior(21, lambda j, m: 1.0 - abs(2 * j + 1 - m) / m),
+    "central21": GB.central_prior(21),
+    "frame21_5": GB.frame_prior(21, 5),
+    "positions": GB.positions_prior((3, 4, -4, -3)),
+    "profile21": GB.profile_prior(21, lambda j, m: 1.0 - abs(2 * j + 1 - m) / m),
 }
+
+
+def reachable(cube, width):
+    """The cells _prior_cube fills ([m][d][i], d >= 1, i <= m - d), in that order."""
+    w1 = width + 1
+    return [cube[(m * w1 + d) * w1 + i] for m in range(w1) for d in range(1, m + 1)
+            for i in range(m - d + 1)]
+
+
+def prior_cube_cases():
+    """The reference's cubes for every prior at the widths the gap-block cases use, plus the
+    CDR3 workloads' widths (20 and 25) and central_prior at lam 0, 1 and 33."""
+    cases = []
+    extra = {"central0": GB.central_prior(0), "central1": GB.central_prior(1),
+             "central33": GB.central_prior(33)}
+    for width in (7, 20, 25):
+        for name, prior in list(PRIORS.items()) + list(extra.items()):
+            if prior is None:
+                continue
+            cases.append({"prior": name, "width": width,
+                          "cells": reachable(prior_cube(prior, width), width)})
+    return cases
 
 
 def gapblock_cases():
@@ -112,7 +166,7 @@ def gapblock_cases():
     q = rand_seqs(rng, 10, 40, 120)
     r = rand_seqs(rng, 12, 30, 130)
     width = max(map(len, q + r))
-    cube = prior_cube(central_prior(21), width)
+    cube = prior_cube(PRIORS["central21"], width)
     exp = oracle.ref_gapblock_matrix(q, r, matrix="pam250", gap_open=30, gap_extend=2, prior=cube,
                                      prior_width=width)
     cases.append({"name": "long_pam250_central", "queries": q, "refs": r, "matrix": "pam250",
@@ -202,6 +256,7 @@ def main() -> None:
     (OUT / "gapblock.json").write_text(json.dumps(gapblock_cases()))
     (OUT / "align.json").write_text(json.dumps(align_cases()))
     (OUT / "distance.json").write_text(json.dumps(distance_cases()))
+    (OUT / "prior_cubes.json").write_text(json.dumps(prior_cube_cases()))
     for f in sorted(OUT.glob("*.json")):
         print(f.name, f.stat().st_size)
 

@@ -249,3 +249,38 @@ def test_oracle_index_align_matrix_scores(name, expected):
     substitution-only score of the two junctions."""
     pen = SubstitutionMatrix.unit(24).penalty_grid if name == "identity" else _index_pen(name)
     assert oracle.penalty_align("CASSLAPGATNEKLFF", "CASSLELGATNEKLFF", pen, 100, 1)[0] == expected
+
+
+# --- prior cubes (built by the reference's own Python) -------------------------------------
+
+def _reachable(cube, width):
+    w1 = width + 1
+    return [cube[(m * w1 + d) * w1 + i] for m in range(w1) for d in range(1, m + 1)
+            for i in range(m - d + 1)]
+
+
+def _unreachable_zero(cube, width):
+    w1 = width + 1
+    live = {(m * w1 + d) * w1 + i for m in range(w1) for d in range(1, m + 1)
+            for i in range(m - d + 1)}
+    return all(v == 0 for k, v in enumerate(cube) if k not in live)
+
+
+def test_prior_cubes_match_the_reference_python():
+    """The library's prior_cube (every prior) and the oracle's restatement (central_prior)
+    against cubes made by the reference's own central/frame/positions/profile priors and
+    _prior_cube (python/seqtree/gapblock.py:79-185, 492-509)."""
+    from seqtree_b200.gapblock import central_prior
+    lams = {"central0": 0, "central1": 1, "central21": 21, "central33": 33}
+    cases = load_golden("prior_cubes")
+    assert len(cases) == 3 * 7
+    for case in cases:
+        name, width = case["prior"], case["width"]
+        prior = central_prior(lams[name]) if name in lams else prior_by_name(name)
+        cube = prior_cube(prior, width)
+        assert len(cube) == (width + 1) ** 3
+        assert _reachable(cube, width) == case["cells"], (name, width)
+        assert _unreachable_zero(cube, width)
+        if name in lams:
+            ocube = oracle.prior_cube(oracle.central_prior(lams[name]), width)
+            assert list(ocube) == list(cube), (name, width)

@@ -152,6 +152,51 @@ def test_short_pairs_thread_and_wavefront_paths(pw, B62, mode, dist):
     assert "align|" in _lib.tuning_table() or os.environ.get("SEQTREE_B200_TUNE") == "0"
 
 
+_PER_THREAD_SCRIPT = r"""
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import oracle
+from seqtree_b200 import SubstitutionMatrix, _lib, pairwise
+AA20 = "ACDEFGHIKLMNPQRSTVWY"
+def rand_seqs(rng, n, lo, hi):
+    lens = rng.integers(lo, hi + 1, size=n)
+    return ["".join(rng.choice(list(AA20), size=int(L))) for L in lens]
+B62 = SubstitutionMatrix.blosum62()
+rng = np.random.default_rng(91)
+q = rand_seqs(rng, 120, 1, 32) + [""]
+r = rand_seqs(rng, 150, 1, 32) + ["", "W" * 32]
+checked = 0
+for mode in ("global", "local"):
+    for go, ge in ((5, 5), (1, 3), (11, 1), (0, 0)):
+        for dist in (False, True):
+            fn = pairwise.dist_matrix if dist else pairwise.score_matrix
+            got = np.asarray(fn(q, r, B62, mode=mode, gap_open=go, gap_extend=ge))
+            assert _lib.last_kernel_name() == "gotoh_thread_kernel", _lib.last_kernel_name()
+            want = oracle.align_matrix(q, r, B62.similarity_grid, mode=mode, gap_open=go,
+                                       gap_extend=ge, dist=dist)
+            assert np.array_equal(got, want), (mode, go, ge, dist)
+            checked += 1
+print("per-thread checked", checked)
+"""
+
+
+def test_per_thread_kernel_branches_against_oracle(cuda_ready):
+    """The one-thread-per-pair kernel on its own (tuning off, so its static choice runs for every
+    set of sequences of at most 32 residues): global mode's raised single-H branch
+    (gap_extend <= gap_open: 5/5, 11/1, 0/0), its three-state branch (gap_extend > gap_open:
+    1/3) and local mode, score and distance, against the oracle."""
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    env = dict(os.environ, SEQTREE_B200_TUNE="0")
+    res = subprocess.run([sys.executable, "-c", _PER_THREAD_SCRIPT, str(root)], env=env,
+                         capture_output=True, text=True, timeout=600, cwd=str(root))
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "per-thread checked 16" in res.stdout
+
+
 def test_gapblock_chunk_width_is_tuned_and_exact(cuda_ready):
     """The dense gap-block call times every chunk width once per shape and caches the fastest;
     every variant gives the same matrix (checked against the oracle on both calls)."""
