@@ -23,9 +23,10 @@ _MODULES = {"distance", "gapblock", "pairwise", "device", "shard", "learned", "e
             "_lib"}
 _FROM_GAPBLOCK = {"score_matrix", "score_sparse", "central_prior", "frame_prior",
                   "positions_prior", "profile_prior", "GapBlockIndex", "IslandProfile",
-                  "embed_in_frame", "UNREACHABLE"}
+                  "embed_in_frame", "gapblock_score", "UNREACHABLE"}
 
-__all__ = ["distance", "gapblock", "pairwise", "score_matrix", "score_sparse", "central_prior",
+__all__ = ["distance", "gapblock", "pairwise", "score_matrix", "score_sparse", "gapblock_score",
+           "central_prior",
            "frame_prior", "positions_prior", "profile_prior", "GapBlockIndex", "IslandProfile",
            "embed_in_frame", "UNREACHABLE", "evalue", "ScoreMatrix",
            "SubstitutionMatrix", "alphabet_symbols", "amino_acids"]

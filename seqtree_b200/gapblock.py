@@ -22,7 +22,8 @@ from ._core import gapblock_sparse as _gapblock_sparse
 from .matrix import ScoreMatrix, SubstitutionMatrix
 
 __all__ = ["score_matrix", "score_sparse", "SparseScores", "central_prior", "profile_prior",
-           "frame_prior", "positions_prior", "gap_cost", "ScoreMatrix", "UNREACHABLE"]
+           "frame_prior", "positions_prior", "gap_cost", "gapblock_score", "deletion_variants",
+           "ScoreMatrix", "UNREACHABLE"]
 
 #: A prior large enough that no layout carrying it wins, small enough not to overflow int32
 #: once a substitution cost is added (python/seqtree/gapblock.py:48-50).
@@ -162,6 +163,76 @@ def prior_cube(prior: GapPrior, width: int):
 
 
 _prior_cube = prior_cube
+
+
+def deletion_variants(q: str, d: int) -> list[tuple[int, str]]:
+    """``q`` with one contiguous run of ``d`` residues removed, for every start of the run, as
+    ``(block_position, variant)`` (python/seqtree/gapblock.py:383-400).  ``d == 0`` removes
+    nothing and gives the single pair ``(0, q)``; ``d`` outside ``[0, len(q)]`` raises
+    ValueError."""
+    if not 0 <= d <= len(q):
+        raise ValueError(f"cannot delete {d} residues from a length-{len(q)} sequence")
+    if d == 0:
+        return [(0, q)]
+    return [(start, q[:start] + q[start + d:]) for start in range(len(q) + 1 - d)]
+
+
+_PAIR_SYMBOLS = "ARNDCQEGHILKMFPSTWYVBZX*"  # the amino-acid codec's 24 symbols
+
+
+def gapblock_score(q: str, r: str, matrix: SubstitutionMatrix | None = None,
+                   gap_open: int | None = None, gap_extend: int = 1,
+                   gap_prior: GapPrior | None = None,
+                   _pen: dict | None = None) -> tuple[int, int]:
+    """``(score, block_position)`` of one pair (python/seqtree/gapblock.py:413-489), from the exact
+    pair kernel on the GPU.
+
+    Penalties are looked up on the characters themselves, as the reference's scalar scorer does:
+    ``_pen[(a, b)]`` when given, else ``matrix.penalty(a, b)``, else unit cost ``a != b``
+    (case-sensitive).  The pair's distinct characters (at most 24) are renamed to codec symbols
+    and scored with that table.  ``block_position`` indexes the shorter sequence (0 to
+    ``min(m, n)``) and is the first position that attains the minimum; it is 0 for equal
+    lengths.
+    """
+    import ctypes
+
+    import torch
+
+    from . import device
+    if gap_open is None:
+        gap_open = _default_gap_open(matrix)
+    if gap_open < 0 or gap_extend < 0:
+        raise ValueError("gap_open and gap_extend must be >= 0")
+    syms = sorted(set(q) | set(r))
+    if len(syms) > len(_PAIR_SYMBOLS):
+        raise ValueError("gapblock_score: more than 24 distinct symbols in one pair")
+    if _pen is not None:
+        pen = lambda a, b: _pen[a, b]  # noqa: E731
+    elif matrix is not None:
+        pen = matrix.penalty
+    else:
+        pen = lambda a, b: int(a != b)  # noqa: E731
+    grid = np.zeros((24, 24), np.int32)
+    for i, a in enumerate(syms):
+        for j, b in enumerate(syms):
+            grid[i, j] = pen(a, b)
+    rename = str.maketrans({c: _PAIR_SYMBOLS[i] for i, c in enumerate(syms)})
+    width = max(len(q), len(r))
+    cube = np.asarray(prior_cube(gap_prior, width) if gap_prior is not None else [],
+                      dtype=np.int64).astype(np.int32).ravel()
+    qs = device.SeqSet([q.translate(rename)], "aa")
+    rs = device.SeqSet([r.translate(rename)], "aa")
+    idx = torch.zeros(2, dtype=torch.int32, device="cuda")
+    res = torch.empty(2, dtype=torch.int32, device="cuda")
+    err = _lib.st_error()
+    _lib.check(_lib.lib.st_gapblock_pairs_pos_sets(
+        qs.handle, rs.handle, ctypes.c_void_p(idx.data_ptr()), ctypes.c_void_p(idx.data_ptr() + 4),
+        1, _lib.i32_ptr(grid), 24, gap_open, gap_extend,
+        _lib.i32_ptr(cube) if cube.size else None, int(cube.size), width if cube.size else 0,
+        ctypes.c_void_p(res.data_ptr()), ctypes.c_void_p(res.data_ptr() + 4),
+        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream), ctypes.byref(err)), err)
+    score, pos = res.tolist()
+    return int(score), int(pos)
 
 
 def score_matrix(queries: Sequence[str], refs: Sequence[str],
