@@ -255,7 +255,7 @@ def kernel_roofline(w, cells: float, seconds: float, clocks, int_peaks=None) -> 
     per cell.  The bound is the measured ``__viaddmin_s16x2`` rate.
     levenshtein: ALU pipe.  The bit-vector step per text character is ten 64-bit logic, add and
     shift operations (the whole pattern, <= 64 symbols, in one word): 20 32-bit ALU lane-ops per
-    (pair, query character), against the measured LOP3 rate.
+    (pair, query character), against the measured ALU-pipe rate (the IADD3 probe).
     """
     mhz = (clocks or {}).get("sm_mhz") or 1965.0
     sms = 148
@@ -292,9 +292,10 @@ def kernel_roofline(w, cells: float, seconds: float, clocks, int_peaks=None) -> 
     if w["kind"] == "levenshtein":
         steps = float(sum(map(len, w["queries"]))) * len(w["refs"])
         achieved = 20.0 * steps / seconds / 1e9
-        alu, alu_clk = _peak_rate(int_peaks, "lop3")
+        alu, alu_clk = _peak_rate(int_peaks, "iadd3")
         if alu:
-            peak, basis = alu / 1e9, f"measured LOP3 rate, all SMs ({alu_clk:.1f} lanes/SM/clk)"
+            peak, basis = alu / 1e9, (f"measured ALU-pipe rate (IADD3 probe), all SMs "
+                                      f"({alu_clk:.1f} lanes/SM/clk)")
         else:
             peak, basis = sms * 64 * mhz * 1e6 / 1e9, f"148 SMs x 64 ALU lanes/clk at {mhz:.0f} MHz"
         return {"bound": "alu", "achieved": achieved, "peak": peak, "unit": "Glane-op/s",
@@ -882,6 +883,13 @@ def measure_learned(args, world, rank, local):
     value = nq * nr * world * args.steps / (total_ms / 1e3)
     if rank != 0:
         return None
+    plans = None
+    if not args.no_plans:
+        plans = learned_plans(w, M, (cc, cl), rec_n=ne)
+        plans["trained_encoder"] = {
+            "ms_per_step": total_ms / args.steps, "effective_pairs_per_s": value / world,
+            "recall": rec["recall"], "exhaustive_share": cal["exhaustive_share"],
+            "query_fallback": cal["query_fallback"], "ref_fallback": cal["ref_fallback"]}
     e2e_s = statistics.median(e2e_times) if e2e_times else float("nan")
     prop_s = phase_ms.get("embed->propose", float("nan")) / 1e3
     n_lq, n_lr = len(qb.learn_rows), idx.n_learn
@@ -904,6 +912,7 @@ def measure_learned(args, world, rank, local):
         "calibration": {k: v for k, v in cal.items() if k != "cells_no_fallback"},
         "exhaustive_pairs_per_s": exh_rate, "speedup_vs_exhaustive": value / world / exh_rate,
         "phase_ms": phase_ms, "train_seconds": train_s,
+        "plans": plans,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if achieved else None, "traffic": None,
                      "note": "propose_topk_kernel: 2*64 flops per (learned query, learned ref) "
@@ -933,6 +942,46 @@ def measure_learned(args, world, rank, local):
     return line
 
 
+def learned_plans(w, M, cal, rec_n: int, steps: int = 3) -> dict:
+    """What the encoder earns: the same search, calibrated to the same recall bound (0.99 on the
+    same held-out batch), without the network (``k = 0``: the calibrated exhaustive fallback
+    alone) and with the network untrained (random weights, seed 0).  Each plan reports its step
+    time over all queries (refs re-embedded, as in the timed steps), the effective pairs/s, the
+    recall on the first ``rec_n`` workload queries and the share of pairs scored exhaustively."""
+    import torch
+
+    from seqtree_b200 import learned as Ln
+    out = {}
+    for name, enc, k in (("fallback_only", None, 0), ("untrained_encoder", Ln.Encoder(seed=0), 256)):
+        idx = Ln.LearnedIndex(enc, w["r_codes"], w["r_lens"], matrix=M, gap_open=8,
+                              max_penalty=24, k=k)
+        cal_res = idx.calibrate(*cal, bound=0.99)
+        qb = idx.queries(w["q_codes"], w["q_lens"])
+        idx.embed_refs()
+        res = idx.search(qb)
+        del res
+        times = []
+        for _ in range(steps):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            idx.embed_refs()
+            res = idx.search(qb)
+            b.record()
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b))
+            del res
+        rec = idx.recall(w["q_codes"][:rec_n], w["q_lens"][:rec_n])
+        ms = statistics.median(times)
+        out[name] = {"ms_per_step": ms, "effective_pairs_per_s": qb.count * idx.nr / (ms / 1e3),
+                     "recall": rec["recall"], "exhaustive_share": cal_res["exhaustive_share"],
+                     "query_fallback": cal_res["query_fallback"],
+                     "ref_fallback": cal_res["ref_fallback"]}
+        del idx, qb
+        torch.cuda.empty_cache()
+    return out
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -951,6 +1000,8 @@ def main(argv=None) -> int:
     ap.add_argument("--soak-seconds", type=float, default=1.5,
                     help="graph replays after the timed steps, for the clock record")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plans", action="store_true",
+                    help="learned workload: skip the without-network / untrained comparison")
     ap.add_argument("--no-graph", action="store_true", help="time eager launches instead")
     ap.add_argument("--queries", type=int, default=None,
                     help="use only the first N queries (smaller case for profiling captures)")

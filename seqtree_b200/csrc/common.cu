@@ -60,15 +60,18 @@ std::string dev_key(const std::string& key) {
 bool tuning_enabled() { return tune_on(); }
 
 void ensure_smem_limit(const void* kernel, size_t bytes) {
+    // The attribute is a limit: it only ever grows here, so a launch that needs less than an
+    // earlier one still fits (setting it to each call's own size would shrink it under a later,
+    // larger launch that the cache believed already allowed).
     static std::mutex mu;
-    static std::set<std::tuple<int, const void*, size_t>> done;
+    static std::map<std::pair<int, const void*>, size_t> limit;
     int dev = 0;
     STB_CUDA(cudaGetDevice(&dev));
-    const auto key = std::make_tuple(dev, kernel, bytes);
     std::lock_guard<std::mutex> lk(mu);
-    if (done.count(key)) return;
+    size_t& cur = limit[std::make_pair(dev, kernel)];
+    if (bytes <= cur) return;
     STB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
-    done.insert(key);
+    cur = bytes;
 }
 
 int tuned_lookup(const std::string& key) {

@@ -413,13 +413,18 @@ class LearnedIndex:
     against every ref, and the other queries against the fallback-length refs.  Every reported
     score is exact; rows are CSR with refs ascending, the format of ``score_sparse``.
     :meth:`calibrate` chooses the fallback lengths on a held-out batch.
+
+    ``k = 0`` turns the proposals off: the index is then the method without the network (the
+    calibrated exhaustive fallback alone), the baseline the encoder is measured against.
     """
 
-    def __init__(self, encoder: Encoder, ref_codes: np.ndarray, ref_lens: np.ndarray, *, matrix,
-                 gap_open: int, gap_extend: int = 1, max_penalty: int = 24, k: int = 256):
+    def __init__(self, encoder: Encoder | None, ref_codes: np.ndarray, ref_lens: np.ndarray, *,
+                 matrix, gap_open: int, gap_extend: int = 1, max_penalty: int = 24, k: int = 256):
         from .device import SeqSet
         if max_penalty < 0:
             raise ValueError("max_penalty must be >= 0")
+        if k < 0 or (k > 0 and encoder is None):
+            raise ValueError("k must be >= 0, and k > 0 needs an encoder")
         self.encoder, self.matrix = encoder, matrix
         self.gap_open, self.gap_extend, self.max_penalty, self.k = gap_open, gap_extend, max_penalty, k
         self.ref_codes = np.ascontiguousarray(ref_codes, np.uint8)
@@ -448,12 +453,13 @@ class LearnedIndex:
         self.learn_refs = _subset(self.ref_codes, self.ref_lens, learn)
         self.fb_refs = _subset(self.ref_codes, self.ref_lens, fbr)
         self.n_learn = int(learn.size)
-        self.r_emb = torch.empty((self.n_learn, 64), dtype=torch.bfloat16, device="cuda")
+        self.r_emb = torch.empty((self.n_learn if self.k else 0, 64), dtype=torch.bfloat16,
+                                 device="cuda")
         self.embed_refs()
 
     def embed_refs(self) -> None:
         import torch
-        if self.learn_refs is not None:
+        if self.learn_refs is not None and self.k:
             self.encoder.embed_into(self.learn_refs, self.r_emb.data_ptr(), 1,
                                     torch.cuda.current_stream().cuda_stream)
 
@@ -488,7 +494,7 @@ class LearnedIndex:
                 phases.setdefault(name, []).append(e)
 
         mark("start")
-        if qb.learn_set is not None and self.n_learn:
+        if qb.learn_set is not None and self.n_learn and self.k:
             n = len(qb.learn_set)
             q_emb = torch.empty((n, 64), dtype=torch.bfloat16, device="cuda")
             self.encoder.embed_into(qb.learn_set, q_emb.data_ptr(), 1, stream)

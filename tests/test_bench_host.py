@@ -72,7 +72,7 @@ def test_kernel_rooflines_use_measured_peaks(bench):
         return {"all_sms": {"lane_ops_per_s": rate, "per_sm_clk": per_clk},
                 "one_sm": {"lane_ops_per_s": rate / 148, "per_sm_clk": per_clk}}
     peaks = {"lds32": probe(8e12, 27.5), "viaddmin_s16x2": probe(9e12, 31.0),
-             "lop3": probe(1.8e13, 62.0)}
+             "iadd3": probe(1.8e13, 62.0)}
     r = bench.kernel_roofline({"kind": "gapblock"}, 1e12, 1.0, None, peaks)
     assert r["peak"] == pytest.approx(4 * 8e12 / 1e9) and "measured" in r["peak_basis"]
     assert r["achieved"] == pytest.approx(2e3) and r["dpx"]["frac"] == pytest.approx(0.5e12 / 9e12)

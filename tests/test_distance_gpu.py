@@ -123,3 +123,18 @@ def test_empty_inputs(dist):
     assert as_np(dist.hamming_matrix([], ["A"])).shape == (0, 1)
     assert as_np(dist.hamming_matrix(["A"], [])).shape == (1, 0)
     assert as_np(dist.levenshtein_matrix([], [])).shape == (0, 0)
+
+
+def test_shared_memory_limit_only_grows_across_calls(dist):
+    """The bit-vector kernel's shared memory grows with the alphabet.  A call on a large alphabet,
+    then a small one, then the large one again must all launch (the per-kernel limit is raised,
+    never lowered under a later, larger launch) -- the reference's own symmetric/bounds tests
+    hit this order with random amino-acid strings."""
+    rng = np.random.default_rng(44)
+    big = AA20 + AA20.lower() + "0123456789"
+    for alphabet in (big, "AC", big, "ACGT", big):
+        a, b = rand_seqs(rng, 9, 0, 40, alphabet), rand_seqs(rng, 11, 0, 40, alphabet)
+        assert np.array_equal(as_np(dist.levenshtein_matrix(a, b)), oracle.levenshtein_matrix(a, b))
+    for _ in range(50):
+        a, b = rand_seqs(rng, 1, 0, 15, AA20)[0], rand_seqs(rng, 1, 0, 15, AA20)[0]
+        assert dist.levenshtein(a, b) == dist.levenshtein(b, a)

@@ -185,8 +185,8 @@ def test_learned_search_is_exact_and_training_pays(cuda_ready):
     from seqtree_b200 import learned as L
     M = stb.SubstitutionMatrix.blosum62()
     rc, rl = L.cdr3_codes(40, 20000)
-    cc, cl = L.cdr3_codes(41, 1500)
-    ec, el = L.cdr3_codes(42, 800)
+    cc, cl = L.cdr3_codes(41, 3000)
+    ec, el = L.cdr3_codes(42, 1500)
 
     def long_recall(enc):
         idx = L.LearnedIndex(enc, rc, rl, matrix=M, gap_open=8, max_penalty=24, k=64)
@@ -205,4 +205,14 @@ def test_learned_search_is_exact_and_training_pays(cuda_ready):
     cal = idx.calibrate(cc, cl, bound=0.99)
     ev = idx.recall(ec, el)
     print("calibrated fallback", cal["query_fallback"], cal["ref_fallback"], "eval recall", ev["recall"])
-    assert ev["subset_of_exact"] and ev["recall"] >= 0.98
+    assert ev["subset_of_exact"] and ev["recall"] >= 0.99
+    # The method without the network (k = 0: the calibrated exhaustive fallback alone), held to
+    # the same bound on the same batch, has to score more pairs exhaustively.
+    base = L.LearnedIndex(None, rc, rl, matrix=M, gap_open=8, max_penalty=24, k=0)
+    bcal = base.calibrate(cc, cl, bound=0.99)
+    bev = base.recall(ec, el)
+    print("without the network:", bcal["query_fallback"], bcal["ref_fallback"],
+          f"share {bcal['exhaustive_share']:.3f} vs {cal['exhaustive_share']:.3f}",
+          "eval recall", bev["recall"])
+    assert bev["subset_of_exact"] and bev["recall"] >= 0.99
+    assert cal["exhaustive_share"] < bcal["exhaustive_share"]
