@@ -367,9 +367,31 @@ __global__ void lengths_kernel(const int64_t* __restrict__ off, int32_t* __restr
 
 }  // namespace
 
+namespace {
+std::atomic<uint64_t> g_next_uid{1};
+}  // namespace
+
+std::unique_ptr<st_seqset_s> row_view(const st_seqset_s& s, int64_t rows) {
+    auto v = std::make_unique<st_seqset_s>();
+    rows = std::max<int64_t>(0, std::min(rows, s.count));
+    v->device = s.device;
+    v->alphabet = s.alphabet;
+    v->count = rows;
+    v->h_off.assign(s.h_off.begin(), s.h_off.begin() + (rows + 1));
+    v->h_len.assign(s.h_len.begin(), s.h_len.begin() + rows);
+    v->total = v->h_off.back();
+    v->max_len = rows ? *std::max_element(v->h_len.begin(), v->h_len.end()) : 0;
+    v->d_bytes = s.d_bytes;
+    v->d_off = s.d_off;
+    v->d_len = s.d_len;
+    v->owns = false;
+    v->uid = g_next_uid.fetch_add(1);
+    return v;
+}
+
 st_seqset_s* make_seqset(const st_strings* s, int32_t alphabet, cudaStream_t stream,
                          int64_t* bad_index, char* bad_char, DevBuf* storage) {
-    static std::atomic<uint64_t> next_uid{1};
+    std::atomic<uint64_t>& next_uid = g_next_uid;
     if (!s || (s->count > 0 && !s->offsets)) fail(ST_EINVAL, "seqtree_b200: null sequence set");
     if (alphabet != -1 && alphabet_size(alphabet) == 0)
         fail(ST_EINVAL, "unknown alphabet code " + std::to_string(alphabet));

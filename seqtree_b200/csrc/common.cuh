@@ -191,6 +191,10 @@ st_seqset_s* make_seqset(const st_strings* s, int32_t alphabet, cudaStream_t str
 
 int32_t alphabet_size(int32_t alphabet);
 
+// The first `rows` sequences of `s` as a set that borrows its device storage (no copy, no
+// allocation; plans go to the context's transient slots).  Valid while `s` lives.
+std::unique_ptr<st_seqset_s> row_view(const st_seqset_s& s, int64_t rows);
+
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 }  // namespace stb

@@ -746,6 +746,8 @@ namespace {
 // static choice; the autotuner (dense calls) measures all of them once per shape.
 constexpr int kRcCandidates[] = {1536, 1280, 1024, 896, 768, 640, 512, 384, 256};
 constexpr int kNumRc = int(sizeof(kRcCandidates) / sizeof(kRcCandidates[0]));
+// Pairs a dense call's first-time tuning runs each variant on (its first query rows).
+constexpr int64_t kTuneSlicePairs = int64_t(100) * 1000 * 1000;
 thread_local int t_force_rc = 0;           // set while the autotuner times one chunk width
 thread_local int t_force_persistent = -1;  // and the launch form (-1: the tuned or static one)
 
@@ -757,7 +759,8 @@ std::string gb_shape_key(const st_seqset_s& qs, const st_seqset_s& rs, bool has_
 
 // Validated inputs -> the dense matrix in `out_d` (device, N*K int32), or, when `sink` is given,
 // the cells that pass its threshold appended to it.
-// `r0`, `r1` restrict the queries to rows [r0, r1) (sparse form only; r1 = -1: all rows).
+// `r0`, `r1` restrict the queries to rows [r0, r1) (r1 = -1: all rows): the sparse form's row
+// blocks, and the dense form's first-time tuning slice (which starts at row 0).
 void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int32_t matrix_size,
                   int32_t go, int32_t ge, const int32_t* prior, int64_t prior_len,
                   uint32_t prior_width, int32_t* out_d, const SparseSink* sink,
@@ -997,12 +1000,17 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
         return;
     }
     const bool has_prior = prior && prior_len > 0;
+    const std::string key = gb_shape_key(qs, rs, has_prior);
     // Candidates: every chunk width, each with one CTA per tile and in the persistent form.
-    tuned_run(gb_shape_key(qs, rs, has_prior), 2 * kNumRc, -1, [&](int c) {
+    auto variant = [&](int c, int64_t rows) {
         t_force_rc = c >= 0 ? kRcCandidates[c % kNumRc] : 0;  // -1: the static choice
         t_force_persistent = c >= 0 ? c / kNumRc : -1;
         try {
-            run();
+            if (rows < 0)
+                run();
+            else
+                gapblock_run(qs, rs, penalty, matrix_size, go, ge, prior, prior_len, prior_width,
+                             out_d, nullptr, stream, 0, rows);
         } catch (...) {
             t_force_rc = 0;
             t_force_persistent = -1;
@@ -1010,7 +1018,19 @@ void gapblock_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int
         }
         t_force_rc = 0;
         t_force_persistent = -1;
-    }, stream);
+    };
+    // A shape seen for the first time is tuned on its first query rows only (about
+    // kTuneSlicePairs pairs, written into their own rows of the result), so the first call costs
+    // the variants' runs on that slice rather than on the whole matrix; the chosen variant then
+    // computes the whole matrix.
+    const int64_t slice = std::min<int64_t>(
+        qs.count, std::max<int64_t>(4 * kGP * 2, kTuneSlicePairs / std::max<int64_t>(rs.count, 1)));
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    STB_CUDA(cudaStreamIsCapturing(stream, &cs));
+    if (slice < qs.count && tuning_enabled() && cs == cudaStreamCaptureStatusNone &&
+        tuned_lookup(key) < 0)
+        tuned_run(key, 2 * kNumRc, -1, [&](int c) { variant(c, slice); }, stream);
+    tuned_run(key, 2 * kNumRc, -1, [&](int c) { variant(c, -1); }, stream);
 }
 
 // Scores of listed pairs (device index arrays) into out_d; the general int32 kernel's

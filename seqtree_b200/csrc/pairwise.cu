@@ -24,6 +24,8 @@ namespace stb {
 namespace {
 
 constexpr int64_t kNegInf = INT64_MIN / 4;  // src/pairwise.cpp:37
+// Pairs a first-time tuning of per-thread against wavefront runs each variant on.
+constexpr int64_t kAlignTunePairs = int64_t(20) * 1000 * 1000;
 
 __device__ __forceinline__ int64_t gap_run(int64_t L, int32_t open, int32_t extend) {
     return L <= 0 ? 0 : int64_t(open) + (L - 1) * int64_t(extend);
@@ -535,6 +537,220 @@ __global__ void __launch_bounds__(kWaveThreads) gotoh_wave_kernel(const WaveArgs
     }
 }
 
+// Query-pair form of the wavefront, used for the N x K pass.  A CTA holds two queries of one row
+// bucket (neighbours in length order) and a chunk of refs taken in length order.  Its shared
+// memory holds the pair's substitution profile P[c][r][lane] = s(q1[lane*R + r], c) |
+// s(q2[lane*R + r], c) << 16 (NEG past a query's length; + 2 * gap_extend in the raised global
+// form), so a lane reads the scores of its R rows at column code c from the words
+// c*R*32 + r*32 + lane: one conflict-free 32-bit load per cell pair, at an immediate offset from
+// one per-column base.  A warp takes one ref at a time; the ref's codes, pre-multiplied into
+// profile offsets, are staged in the warp's slice of shared memory, so every lane reads its own
+// column's code without a shuffle.  The recurrence, the int16 safety argument and the raised
+// global form are those of gotoh_wave_kernel above.  Only the packing differs: the two halves
+// are two queries against one ref, so both end at the ref's last column, and the global score
+// of each query is read at its own last row.
+constexpr int kQpWarps = 8;
+constexpr int kQpMaxRef = 512;  // wave_eligible admits lengths up to 512
+
+struct QpArgs {
+    const uint8_t* qc;
+    const int64_t* qoff;
+    const uint8_t* rc;
+    const int64_t* roff;
+    const int2* qpairs;      // query pairs of this launch (one row bucket; x == y for a single)
+    int64_t nqp;
+    const int32_t* rorder;   // every ref, by length
+    int64_t K;
+    int64_t chunk;           // refs per CTA
+    const int32_t* simadd;   // A x A: s(a, b) + add
+    int A;
+    int32_t go, ge;
+    int dist;
+    const int64_t* q_self;
+    const int64_t* r_self;
+    int32_t* out;
+    unsigned int* overflow;
+};
+
+inline size_t qpair_smem(int A, int R) {
+    return size_t(A) * R * 32 * 4 + size_t(kQpWarps) * kQpMaxRef * 2;
+}
+
+template <int R, bool LOCAL, bool EXACT>
+__global__ void __launch_bounds__(kQpWarps * 32) gotoh_qpair_kernel(const QpArgs a) {
+    extern __shared__ uint32_t s_prof[];  // A * R * 32 words, then kQpWarps ref slices
+    uint16_t* my_ref = reinterpret_cast<uint16_t*>(s_prof + a.A * R * 32) +
+                       (threadIdx.x >> 5) * kQpMaxRef;
+    const unsigned full = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr bool OFFSET = !LOCAL && !EXACT;
+    const uint32_t mgo2 = dup2(-a.go), mge2 = dup2(-a.ge);
+    const uint32_t eo2 = dup2(a.ge - a.go);
+    const int64_t r_lo = int64_t(blockIdx.x) * a.chunk;
+    const int64_t r_hi = min(r_lo + a.chunk, a.K);
+    const int words = a.A * R * 32;
+
+    for (int64_t p = blockIdx.y; p < a.nqp; p += gridDim.y) {
+        const int2 qp = a.qpairs[p];
+        const uint8_t* q1 = a.qc + a.qoff[qp.x];
+        const uint8_t* q2 = a.qc + a.qoff[qp.y];
+        const int m1 = int(a.qoff[qp.x + 1] - a.qoff[qp.x]);
+        const int m2 = int(a.qoff[qp.y + 1] - a.qoff[qp.y]);
+        __syncthreads();  // every warp is done with the previous pair's profile
+        for (int w = threadIdx.x; w < words; w += blockDim.x) {
+            const int c = w / (R * 32), rr = (w >> 5) % R, row = (w & 31) * R + rr;
+            const int v1 = row < m1 ? a.simadd[int(q1[row]) * a.A + c] : -16384;
+            const int v2 = row < m2 ? a.simadd[int(q2[row]) * a.A + c] : -16384;
+            s_prof[w] = uint32_t(uint16_t(int16_t(v1))) | (uint32_t(uint16_t(int16_t(v2))) << 16);
+        }
+        __syncthreads();
+        // lane and register of each query's last row
+        const int cl1 = (m1 - 1) / R, cr1 = (m1 - 1) - cl1 * R;
+        const int cl2 = (m2 - 1) / R, cr2 = (m2 - 1) - cl2 * R;
+
+        for (int64_t t = r_lo + warp; t < r_hi; t += kQpWarps) {
+            const int k = a.rorder[t];
+            const uint8_t* rs = a.rc + a.roff[k];
+            const int n = int(a.roff[k + 1] - a.roff[k]);
+            __syncwarp();
+            for (int j = lane; j < n; j += 32) my_ref[j] = uint16_t(int(rs[j]) * R * 32);
+            __syncwarp();
+
+            uint32_t Hl[R], Yl[R], MXl[EXACT ? R : 1];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const int row = lane * R + r;
+                Hl[r] = LOCAL ? 0u : (OFFSET ? eo2 : dup2(-(a.go + row * a.ge)));
+                Yl[r] = kNeg2;
+                if constexpr (EXACT) MXl[r] = Hl[r];
+            }
+            uint32_t diag = (lane == 0 || LOCAL) ? 0u
+                            : (OFFSET ? eo2 : dup2(-(a.go + (lane * R - 1) * a.ge)));
+            uint32_t best = 0u, cap = 0u;
+            uint32_t outH = 0u, outX = kNeg2, outMY = 0u;
+            const int steps = n + 31;
+            for (int s = 0; s < steps; ++s) {
+                uint32_t upH = __shfl_up_sync(full, outH, 1);
+                uint32_t upX = __shfl_up_sync(full, outX, 1);
+                uint32_t upMY = EXACT ? __shfl_up_sync(full, outMY, 1) : 0u;
+                const int j = s - lane + 1;
+                if (lane == 0) {  // the virtual row 0 at column j
+                    const uint32_t h0 =
+                        LOCAL ? 0u : (OFFSET ? eo2 : dup2(-(a.go + (j - 1) * a.ge)));
+                    upH = h0;
+                    upX = kNeg2;
+                    upMY = h0;
+                }
+                if (j >= 1 && j <= n) {
+                    const uint32_t* pc = s_prof + my_ref[j - 1] + lane;
+                    const uint32_t top = upH;
+                    uint32_t d = diag;
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const uint32_t sc = pc[r * 32];
+                        const uint32_t M = LOCAL ? __viaddmax_s16x2_relu(d, sc, kNeg2)
+                                                 : __viaddmax_s16x2(d, sc, kNeg2);
+                        uint32_t X, Y;
+                        if constexpr (EXACT) {
+                            X = __viaddmax_s16x2(upMY, mgo2, __viaddmax_s16x2(upX, mge2, kNeg2));
+                            Y = __viaddmax_s16x2(MXl[r], mgo2,
+                                                 __viaddmax_s16x2(Yl[r], mge2, kNeg2));
+                        } else if constexpr (OFFSET) {
+                            X = __viaddmax_s16x2(upH, eo2, upX);
+                            Y = __viaddmax_s16x2(Hl[r], eo2, Yl[r]);
+                        } else {
+                            X = __viaddmax_s16x2(upH, mgo2, __viaddmax_s16x2(upX, mge2, kNeg2));
+                            Y = __viaddmax_s16x2(Hl[r], mgo2, __viaddmax_s16x2(Yl[r], mge2, kNeg2));
+                        }
+                        const uint32_t H = __vimax3_s16x2(M, X, Y);
+                        if constexpr (LOCAL) best = __vimax3_s16x2(best, M, kNeg2);
+                        d = Hl[r];
+                        Hl[r] = H;
+                        Yl[r] = Y;
+                        upH = H;
+                        upX = X;
+                        if constexpr (EXACT) {
+                            MXl[r] = __vimax3_s16x2(M, X, kNeg2);
+                            upMY = __vimax3_s16x2(M, Y, kNeg2);
+                        }
+                    }
+                    diag = top;
+                    outH = upH;
+                    outX = upX;
+                    outMY = upMY;
+                    if (!LOCAL && j == n) {
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            if (lane == cl1 && r == cr1) cap = (cap & 0xFFFF0000u) | (Hl[r] & 0xFFFFu);
+                            if (lane == cl2 && r == cr2) cap = (cap & 0xFFFFu) | (Hl[r] & 0xFFFF0000u);
+                        }
+                    }
+                }
+            }
+            int v1, v2;
+            if constexpr (LOCAL) {
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1)
+                    best = __vimax3_s16x2(best, __shfl_xor_sync(full, best, off), kNeg2);
+                v1 = lo16(best);
+                v2 = hi16(best);
+            } else {
+                v1 = lo16(__shfl_sync(full, cap, cl1));
+                v2 = hi16(__shfl_sync(full, cap, cl2));
+                if constexpr (OFFSET) {
+                    v1 -= (m1 + n) * a.ge;
+                    v2 -= (m2 + n) * a.ge;
+                }
+            }
+            if (lane == 0) {
+                for (int t2 = 0; t2 < (qp.y != qp.x ? 2 : 1); ++t2) {
+                    const int qi = t2 ? qp.y : qp.x;
+                    const int64_t sv = t2 ? v2 : v1;
+                    const int64_t v = a.dist ? a.q_self[qi] + a.r_self[k] - 2 * sv : sv;
+                    if (v < INT32_MIN || v > INT32_MAX)
+                        atomicOr(a.overflow, 1u);
+                    else
+                        a.out[int64_t(qi) * a.K + k] = int32_t(v);
+                }
+            }
+        }
+    }
+}
+
+template <int R>
+const void* qpair_kernel_ptr(bool local, bool exact) {
+    if (local)
+        return exact ? reinterpret_cast<const void*>(gotoh_qpair_kernel<R, true, true>)
+                     : reinterpret_cast<const void*>(gotoh_qpair_kernel<R, true, false>);
+    return exact ? reinterpret_cast<const void*>(gotoh_qpair_kernel<R, false, true>)
+                 : reinterpret_cast<const void*>(gotoh_qpair_kernel<R, false, false>);
+}
+
+const void* qpair_kernel(int R, bool local, bool exact) {
+    switch (R) {
+        case 1: return qpair_kernel_ptr<1>(local, exact);
+        case 2: return qpair_kernel_ptr<2>(local, exact);
+        case 3: return qpair_kernel_ptr<3>(local, exact);
+        case 4: return qpair_kernel_ptr<4>(local, exact);
+        case 5: return qpair_kernel_ptr<5>(local, exact);
+        case 6: return qpair_kernel_ptr<6>(local, exact);
+        case 7: return qpair_kernel_ptr<7>(local, exact);
+        case 8: return qpair_kernel_ptr<8>(local, exact);
+        case 9: return qpair_kernel_ptr<9>(local, exact);
+        case 10: return qpair_kernel_ptr<10>(local, exact);
+        case 11: return qpair_kernel_ptr<11>(local, exact);
+        case 12: return qpair_kernel_ptr<12>(local, exact);
+        case 13: return qpair_kernel_ptr<13>(local, exact);
+        case 14: return qpair_kernel_ptr<14>(local, exact);
+        case 15: return qpair_kernel_ptr<15>(local, exact);
+        default: return qpair_kernel_ptr<16>(local, exact);
+    }
+}
+
+// Rows per lane of the query-pair kernel: the smallest R with 32 * R >= m (32-row buckets, so a
+// query carries fewer than 32 padded rows).
+int qpair_rows_per_lane(int m) { return std::max(1, int((m + 31) / 32)); }
+
 constexpr int kRowBuckets[] = {2, 4, 6, 8, 10, 12, 14, 16};
 
 int rows_per_lane(int m) {
@@ -565,20 +781,35 @@ const void* wave_kernel(int R, bool local, bool exact) {
     }
 }
 
-// Substitution table of the wavefront path, per device, and the grid it was built from.
+// Substitution tables of the wavefront path, per device, and the grid they were built from:
+// the packed T[q][r1][r2] words of gotoh_wave_kernel and the A x A s(a, b) + add grid the
+// query-pair kernel builds its profiles from.
 struct WaveState {
     std::vector<uint8_t> key;
-    DevBuf table;
+    DevBuf table, simadd;
+    // Side streams and events that run the row buckets' launches concurrently (fork / join on
+    // the caller's stream), so that one bucket's tail of idle SMs is filled by the next bucket.
+    static constexpr int kSide = 4;
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t fork = nullptr, join[kSide] = {};
+    void ensure_streams() {
+        if (fork) return;
+        for (int i = 0; i < kSide; ++i) {
+            STB_CUDA(cudaStreamCreateWithFlags(&side[i], cudaStreamNonBlocking));
+            STB_CUDA(cudaEventCreateWithFlags(&join[i], cudaEventDisableTiming));
+        }
+        STB_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    }
 };
 
 // Per-set launch plan (depends only on the lengths): the set's indices grouped by rows per
-// lane, with the (R, offset, count) of each group, and the set's sequences sorted by length and
-// paired with their neighbour (used when the set is the ref side).
+// lane, with the (R, offset, count) of each group; inside each group the sequences sorted by
+// length and paired with their neighbour (the query side of the query-pair kernel), with the
+// (R, offset, count) of each group's pairs; and every index sorted by length (the ref side).
 struct WavePlan {
     uint64_t uid = 0;
-    std::vector<std::tuple<int, int64_t, int64_t>> groups;
-    int64_t npairs = 0;
-    DevBuf list, pairs;
+    std::vector<std::tuple<int, int64_t, int64_t>> groups, pair_groups;
+    DevBuf list, qpairs, sorted;
 };
 
 WavePlan& wave_plan(st_seqset_s& s, Context& ctx, int slot, cudaStream_t stream) {
@@ -597,21 +828,31 @@ WavePlan& wave_plan(st_seqset_s& s, Context& ctx, int slot, cudaStream_t stream)
             p.groups.emplace_back(R, int64_t(all.size()), int64_t(b[size_t(R)].size()));
             all.insert(all.end(), b[size_t(R)].begin(), b[size_t(R)].end());
         }
+    auto by_len = [&](int32_t x, int32_t y) { return s.h_len[size_t(x)] < s.h_len[size_t(y)]; };
     std::vector<int32_t> order(static_cast<size_t>(s.count));
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) {
-        return s.h_len[size_t(x)] < s.h_len[size_t(y)];
-    });
-    std::vector<int32_t> pairs;
-    pairs.reserve(order.size() + 1);
-    for (size_t i = 0; i < order.size(); i += 2) {
-        pairs.push_back(order[i]);
-        pairs.push_back(i + 1 < order.size() ? order[i + 1] : order[i]);
+    std::stable_sort(order.begin(), order.end(), by_len);
+    std::vector<int32_t> qpairs;
+    qpairs.reserve(size_t(s.count) + 2 * p.groups.size());
+    p.pair_groups.clear();
+    std::vector<std::vector<int32_t>> fine(17);
+    for (int64_t i = 0; i < s.count; ++i)
+        fine[size_t(qpair_rows_per_lane(s.h_len[size_t(i)]))].push_back(int32_t(i));
+    for (int R = 1; R <= 16; ++R) {
+        std::vector<int32_t>& g = fine[size_t(R)];
+        if (g.empty()) continue;
+        std::stable_sort(g.begin(), g.end(), by_len);
+        const int64_t first = int64_t(qpairs.size() / 2);
+        for (size_t i = 0; i < g.size(); i += 2) {
+            qpairs.push_back(g[i]);
+            qpairs.push_back(i + 1 < g.size() ? g[i + 1] : g[i]);
+        }
+        p.pair_groups.emplace_back(R, first, int64_t(qpairs.size() / 2) - first);
     }
-    p.npairs = int64_t(pairs.size() / 2);
     // (a pageable-source copy has consumed the host vectors by the time it returns)
     h2d(p.list.as<int32_t>(all.size()), all.data(), all.size() * 4, stream);
-    h2d(p.pairs.as<int32_t>(pairs.size()), pairs.data(), pairs.size() * 4, stream);
+    h2d(p.qpairs.as<int32_t>(qpairs.size()), qpairs.data(), qpairs.size() * 4, stream);
+    h2d(p.sorted.as<int32_t>(order.size()), order.data(), order.size() * 4, stream);
     p.uid = s.uid;
     return p;
 }
@@ -656,6 +897,20 @@ void launch_wave(Context& ctx, WaveArgs wa, int R, bool local, bool exact, cudaS
     note_launch("gotoh_wave_kernel");
 }
 
+// Launches one query-pair pass: the pairs of one row bucket against every ref, `chunk` refs per
+// CTA column.
+void launch_qpair(QpArgs qa, int R, bool local, bool exact, cudaStream_t stream) {
+    const void* kern = qpair_kernel(R, local, exact);
+    const size_t smem = qpair_smem(qa.A, R);
+    ensure_smem_limit(kern, smem);
+    const int64_t gx = ceil_div(qa.K, qa.chunk);
+    const int64_t gy = std::min<int64_t>(qa.nqp, 65535);
+    void* args[] = {&qa};
+    STB_CUDA(cudaLaunchKernel(kern, dim3(unsigned(gx), unsigned(gy)), dim3(kQpWarps * 32), args,
+                              smem, stream));
+    note_launch("gotoh_qpair_kernel");
+}
+
 }  // namespace
 
 // The warp-wavefront path for every pair (int16x2 cells; the caller checked wave_eligible).
@@ -684,8 +939,11 @@ void align_wave(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
                         tab[(size_t(x) * A1 + y1) * A1 + y2] =
                             uint32_t(uint16_t(int16_t(sv(x, y1)))) |
                             (uint32_t(uint16_t(int16_t(sv(x, y2)))) << 16);
+            std::vector<int32_t> sa(size_t(A) * A);
+            for (int x = 0; x < A * A; ++x) sa[size_t(x)] = similarity[x] + add;
             try {
                 h2d(ws.table.as<uint32_t>(tab.size()), tab.data(), tab.size() * 4, stream);
+                h2d(ws.simadd.as<int32_t>(sa.size()), sa.data(), sa.size() * 4, stream);
             } catch (...) {
                 ws.key.clear();  // not uploaded: the next call builds it again
                 throw;
@@ -723,21 +981,39 @@ void align_wave(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
             }
         }
     }
-    for (auto& [R, off, cnt] : qp.groups) {
-        WaveArgs ma = wa;
+    // The buckets' launches run on side streams forked from (and joined back into) the caller's
+    // stream; the longest rows first, so the short buckets fill the long ones' tails.
+    ws.ensure_streams();
+    const int nside = std::min<int>(WaveState::kSide, int(qp.pair_groups.size()));
+    STB_CUDA(cudaEventRecord(ws.fork, stream));
+    for (int i = 0; i < nside; ++i) STB_CUDA(cudaStreamWaitEvent(ws.side[i], ws.fork, 0));
+    int gi = 0;
+    for (auto it = qp.pair_groups.rbegin(); it != qp.pair_groups.rend(); ++it, ++gi) {
+        const auto& [R, off, cnt] = *it;
+        QpArgs ma{};
         ma.qc = qs.d_bytes;
         ma.qoff = qs.d_off;
         ma.rc = rs.d_bytes;
         ma.roff = rs.d_off;
-        ma.qlist = static_cast<int32_t*>(qp.list.ptr) + off;
-        ma.nq = cnt;
-        ma.rpairs = static_cast<int2*>(rp.pairs.ptr);
-        ma.nrp = rp.npairs;
+        ma.qpairs = static_cast<int2*>(qp.qpairs.ptr) + off;
+        ma.nqp = cnt;
+        ma.rorder = static_cast<int32_t*>(rp.sorted.ptr);
+        ma.K = K;
+        ma.chunk = 256;
+        ma.simadd = static_cast<int32_t*>(ws.simadd.ptr);
+        ma.A = A;
+        ma.go = go;
+        ma.ge = ge;
         ma.dist = dist;
         ma.q_self = q_self;
         ma.r_self = r_self;
         ma.out = out_d;
-        launch_wave(ctx, ma, R, local, exact, stream);
+        ma.overflow = ovf;
+        launch_qpair(ma, R, local, exact, ws.side[gi % nside]);
+    }
+    for (int i = 0; i < nside; ++i) {
+        STB_CUDA(cudaEventRecord(ws.join[i], ws.side[i]));
+        STB_CUDA(cudaStreamWaitEvent(stream, ws.join[i], 0));
     }
 }
 
@@ -788,7 +1064,8 @@ void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
                 throw;
             }
         }
-        auto run_thread = [&] {
+        auto run_thread = [&](st_seqset_s& q) {
+            const int64_t Nq = q.count;
             ThreadArgs t{};
             t.sim = d_sim;
             t.A = A;
@@ -798,10 +1075,10 @@ void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
             int64_t* q_self = nullptr;
             int64_t* r_self = nullptr;
             if (dist) {
-                q_self = ctx.work_b.as<int64_t>(size_t(N + K));
-                r_self = q_self + N;
+                q_self = ctx.work_b.as<int64_t>(size_t(Nq + K));
+                r_self = q_self + Nq;
                 for (int side = 0; side < 2; ++side) {
-                    const st_seqset_s& s = side == 0 ? qs : rs;
+                    const st_seqset_s& s = side == 0 ? q : rs;
                     ThreadArgs b = t;
                     b.qc = s.d_bytes;
                     b.qoff = s.d_off;
@@ -811,30 +1088,43 @@ void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
                     launch_thread(ctx, b, tn, mode == ST_MODE_LOCAL, s.count, stream);
                 }
             }
-            t.qc = qs.d_bytes;
-            t.qoff = qs.d_off;
+            t.qc = q.d_bytes;
+            t.qoff = q.d_off;
             t.rc = rs.d_bytes;
             t.roff = rs.d_off;
-            t.N = N;
+            t.N = Nq;
             t.K = K;
             t.dist = dist;
             t.q_self = q_self;
             t.r_self = r_self;
             t.out = out_d;
-            launch_thread(ctx, t, tn, mode == ST_MODE_LOCAL, N * K, stream);
+            launch_thread(ctx, t, tn, mode == ST_MODE_LOCAL, Nq * K, stream);
         };
         if (!wave_ok) {
-            run_thread();
+            run_thread(qs);
             return;
         }
         const std::string key = "align|" + std::to_string(mode) + "|" + std::to_string(dist) + "|" +
                                 std::to_string(A) + "|" + std::to_string(qs.max_len) + "|" +
                                 std::to_string(rs.max_len) + "|" + std::to_string(size_bucket(N)) +
                                 "|" + std::to_string(size_bucket(K));
-        tuned_run(key, 2, 0, [&](int c) {
-            if (c == 0) run_thread();
-            else align_wave(qs, rs, similarity, A, mode, go, ge, dist, out_d, ovf, stream);
-        }, stream);
+        auto variant = [&](int c, st_seqset_s& q) {
+            if (c == 0) run_thread(q);
+            else align_wave(q, rs, similarity, A, mode, go, ge, dist, out_d, ovf, stream);
+        };
+        // A shape seen for the first time is tuned on its first query rows only (about
+        // kAlignTunePairs pairs, written into their own rows of the result); the choice then
+        // computes the whole matrix.
+        const int64_t slice = std::min<int64_t>(
+            N, std::max<int64_t>(64, kAlignTunePairs / std::max<int64_t>(K, 1)));
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        STB_CUDA(cudaStreamIsCapturing(stream, &cs));
+        if (slice < N && tuning_enabled() && cs == cudaStreamCaptureStatusNone &&
+            tuned_lookup(key) < 0) {
+            std::unique_ptr<st_seqset_s> view = row_view(qs, slice);
+            tuned_run(key, 2, 0, [&](int c) { variant(c, *view); }, stream);
+        }
+        tuned_run(key, 2, 0, [&](int c) { variant(c, qs); }, stream);
         return;
     }
     if (wave_ok) {

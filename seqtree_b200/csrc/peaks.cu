@@ -39,7 +39,9 @@ int32_t peak_error(st_error* err, int32_t code, const char* msg) {
 template <int OP>
 __device__ __forceinline__ uint32_t step(uint32_t x, uint32_t y, uint32_t c) {
     if constexpr (OP == ST_PEAK_LOP3) {
-        return (x & y) ^ c;
+        uint32_t r;  // one three-input logic operation (x ^ y ^ c), written so it stays one
+        asm("lop3.b32 %0, %1, %2, %3, 0x96;" : "=r"(r) : "r"(x), "r"(y), "r"(c));
+        return r;
     } else if constexpr (OP == ST_PEAK_IADD3) {
         return x + y + c;
     } else if constexpr (OP == ST_PEAK_IMAD) {

@@ -14,6 +14,11 @@ the embedding, the proposal kernel and the exact scorer.
 from __future__ import annotations
 
 import ctypes
+import itertools
+import json
+import os
+import struct
+import zlib
 
 import numpy as np
 
@@ -22,6 +27,67 @@ from .device import hits_tensors as _hits_tensors, torch_rows
 from .matrix import SubstitutionMatrix
 from .workloads import AA20, AA20_CODES as _AA20_CODES, AA24, CODE as _CODE, PAD  # noqa: F401
 from .workloads import cdr3_codes, cdr3_lengths, codes_to_letters, codes_to_strings  # noqa: F401
+
+
+# ------------------------------------------------------------------------ model files -------
+# A trained encoder (and, from LearnedIndex, its calibrated fallback) is kept in one versioned
+# flat file, little-endian:
+#   magic "STBE" | version u32 | parameter count u64 | metadata length u32 | metadata (UTF-8 JSON)
+#   | parameters (fp32 x count) | CRC-32 of every preceding byte (u32)
+# It is written to a temporary beside the destination and renamed over it, so a concurrent reader
+# sees the old file or the new one, never half of one, and a failed write leaves no temporary
+# (the reference's src/atomic_write.hpp:47-75 does the same for its index files).
+MODEL_MAGIC = b"STBE"
+MODEL_VERSION = 1
+_tmp_seq = itertools.count()
+
+
+def encode_model(params: np.ndarray, meta: dict | None = None) -> bytes:
+    """The model-file bytes of ``params`` (fp32) and a JSON-serialisable ``meta``."""
+    p = np.ascontiguousarray(params, np.float32).ravel()
+    m = json.dumps(meta or {}, sort_keys=True).encode()
+    body = (MODEL_MAGIC + struct.pack("<IQI", MODEL_VERSION, p.size, len(m)) + m +
+            p.astype("<f4").tobytes())
+    return body + struct.pack("<I", zlib.crc32(body) & 0xFFFFFFFF)
+
+
+def decode_model(data: bytes, name: str = "model file") -> tuple[np.ndarray, dict]:
+    """(params, meta) of model-file bytes; ValueError when they are not a version-1 file, are
+    truncated, or fail the checksum."""
+    if len(data) < 20 or data[:4] != MODEL_MAGIC:
+        raise ValueError(f"seqtree_b200: '{name}' is not a seqtree_b200 encoder file")
+    version, count, mlen = struct.unpack_from("<IQI", data, 4)
+    if version != MODEL_VERSION:
+        raise ValueError(f"seqtree_b200: '{name}' is a version {version} encoder file; this "
+                         f"library reads version {MODEL_VERSION}")
+    end = 20 + mlen + 4 * count
+    if len(data) != end + 4:
+        raise ValueError(f"seqtree_b200: truncated or corrupt encoder file '{name}'")
+    (crc,) = struct.unpack_from("<I", data, end)
+    if zlib.crc32(data[:end]) & 0xFFFFFFFF != crc:
+        raise ValueError(f"seqtree_b200: truncated or corrupt encoder file '{name}' (checksum)")
+    meta = json.loads(data[20:20 + mlen].decode())
+    params = np.frombuffer(data, dtype="<f4", count=count, offset=20 + mlen).astype(np.float32)
+    return params, meta
+
+
+def atomic_write(path, data: bytes) -> None:
+    """Writes ``data`` to a temporary beside ``path`` and renames it over ``path``; on any failure
+    the temporary is removed and the error re-raised (``path`` is left as it was)."""
+    path = os.fspath(path)
+    tmp = f"{path}.tmp.{os.getpid()}.{next(_tmp_seq)}"
+    try:
+        with open(tmp, "wb") as f:
+            f.write(data)
+            f.flush()
+            os.fsync(f.fileno())
+        os.replace(tmp, path)
+    except BaseException:
+        try:
+            os.remove(tmp)
+        except FileNotFoundError:
+            pass
+        raise
 
 
 def param_count() -> int:
@@ -87,6 +153,23 @@ class Encoder:
         err = _lib.st_error()
         _lib.check(_lib.lib.st_encoder_set_precision(self._h, code, ctypes.byref(err)), err)
         self.precision = precision
+
+    def save(self, path, meta: dict | None = None) -> None:
+        """Writes the weights (and ``meta``) to a model file, atomically (see ``encode_model``)."""
+        atomic_write(path, encode_model(self.params(), meta))
+
+    @classmethod
+    def load(cls, path, precision: str = "bf16") -> "Encoder":
+        """An encoder with the weights of a model file; its metadata is in ``.meta``.  Raises
+        ValueError for a file that is not a version-1 encoder file or is truncated / corrupt."""
+        with open(path, "rb") as f:
+            params, meta = decode_model(f.read(), os.fspath(path))
+        if params.size != param_count():
+            raise ValueError(f"seqtree_b200: '{os.fspath(path)}' holds {params.size} parameters; "
+                             f"this encoder has {param_count()}")
+        enc = cls(params, precision=precision)
+        enc.meta = meta
+        return enc
 
     def params(self) -> np.ndarray:
         out = np.empty(param_count(), np.float32)
@@ -435,6 +518,31 @@ class LearnedIndex:
         self.ref_fallback = np.zeros(PAD + 1, bool)
         self._hits = None
         self._build()
+
+    def save_model(self, path) -> None:
+        """Writes the encoder and this index's search settings and calibrated fallback lengths to
+        one model file, so another process can answer searches without training or calibrating
+        (:meth:`from_model`)."""
+        if self.encoder is None:
+            raise ValueError("an index without an encoder has no model to save")
+        self.encoder.save(path, {
+            "k": self.k, "max_penalty": self.max_penalty, "gap_open": self.gap_open,
+            "gap_extend": self.gap_extend,
+            "query_fallback": np.flatnonzero(self.query_fallback).tolist(),
+            "ref_fallback": np.flatnonzero(self.ref_fallback).tolist()})
+
+    @classmethod
+    def from_model(cls, path, ref_codes: np.ndarray, ref_lens: np.ndarray, *, matrix,
+                   precision: str = "bf16") -> "LearnedIndex":
+        """An index over ``ref_codes`` with the encoder, settings and fallback lengths of a model
+        file written by :meth:`save_model` (the matrix is the caller's: it is not stored)."""
+        enc = Encoder.load(path, precision=precision)
+        m = enc.meta
+        idx = cls(enc, ref_codes, ref_lens, matrix=matrix, gap_open=int(m["gap_open"]),
+                  gap_extend=int(m["gap_extend"]), max_penalty=int(m["max_penalty"]),
+                  k=int(m["k"]))
+        idx.set_fallback(m["query_fallback"], m["ref_fallback"])
+        return idx
 
     def set_fallback(self, query_lengths=(), ref_lengths=()) -> None:
         self.query_fallback[:] = False

@@ -190,3 +190,18 @@ def test_device_sets_match_host_calls(st):
                              prior_width=width)
         torch.cuda.synchronize()
         assert np.array_equal(out.cpu().numpy(), host)
+
+
+def test_first_call_of_a_large_shape_tunes_on_a_slice(st):
+    """12,000 x 10,000 pairs is beyond the 1e8-pair tuning slice: the first call times its
+    variants on the first 10,000 query rows only, then computes the whole matrix with the choice.
+    Rows inside and past the slice are exact, and the second (cached) call agrees."""
+    q = cdr3(np.random.default_rng(71), 12000)
+    r = cdr3(np.random.default_rng(72), 10000)
+    m = st.SubstitutionMatrix.blosum62()
+    first = as_np(st.score_matrix(q, r, m, gap_open=8))
+    rows = [0, 9999, 10000, 11999]
+    exp = oracle.gapblock_matrix([q[i] for i in rows], r, m.penalty_grid, gap_open=8)
+    assert np.array_equal(first[rows], exp)
+    second = as_np(st.score_matrix(q, r, m, gap_open=8))
+    assert np.array_equal(first, second)

@@ -216,3 +216,33 @@ def test_learned_search_is_exact_and_training_pays(cuda_ready):
           "eval recall", bev["recall"])
     assert bev["subset_of_exact"] and bev["recall"] >= 0.99
     assert cal["exhaustive_share"] < bcal["exhaustive_share"]
+
+
+@pytest.mark.gpu
+def test_model_file_gives_the_same_encoder_and_search(cuda_ready, tmp_path):
+    """A trained encoder with its calibrated fallback, saved and loaded in a fresh index: the same
+    weights bit for bit, the same settings, and the same search results."""
+    import torch
+
+    import seqtree_b200 as stb
+    from seqtree_b200 import learned as L
+    M = stb.SubstitutionMatrix.blosum62()
+    enc = L.Encoder(seed=5)
+    L.train(enc, 20000, seed=9, matrix=M, gap_open=8)
+    rc, rl = L.cdr3_codes(50, 3000)
+    qc, ql = L.cdr3_codes(51, 300)
+    idx = L.LearnedIndex(enc, rc, rl, matrix=M, gap_open=8, max_penalty=24, k=64)
+    idx.set_fallback([8, 9], [8])
+    path = tmp_path / "model.stbe"
+    idx.save_model(path)
+    idx2 = L.LearnedIndex.from_model(path, rc, rl, matrix=M)
+    assert idx2.encoder.params().tobytes() == enc.params().tobytes()
+    assert (idx2.k, idx2.max_penalty, idx2.gap_open, idx2.gap_extend) == (64, 24, 8, 1)
+    assert np.array_equal(idx2.query_fallback, idx.query_fallback)
+    assert np.array_equal(idx2.ref_fallback, idx.ref_fallback)
+    a = idx.search(idx.queries(qc, ql))
+    b = idx2.search(idx2.queries(qc, ql))
+    assert all(torch.equal(x, y) for x, y in zip(a, b))
+    with pytest.raises(ValueError, match="not a seqtree_b200 encoder file"):
+        (tmp_path / "junk").write_bytes(b"not a model")
+        L.Encoder.load(tmp_path / "junk")

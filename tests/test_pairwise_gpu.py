@@ -235,3 +235,19 @@ def test_full_size_protein_configuration(pw, B62, mode):
     exp = oracle.align_matrix([q[i] for i in rows], r, B62.similarity_grid, mode=mode, dist=True,
                               threads=os.cpu_count() or 1)
     assert np.array_equal(got[rows], exp)
+
+
+def test_first_call_of_a_large_shape_tunes_on_a_slice(pw, B62):
+    """5,000 x 5,000 junctions (2.5e7 pairs) is beyond the 2e7-pair tuning slice of the
+    per-thread / wavefront choice: the first call tunes on the first 4,000 query rows, then runs
+    the choice on everything.  Rows inside and past the slice are exact in both modes."""
+    from conftest import cdr3
+    rng = np.random.default_rng(73)
+    q, r = cdr3(rng, 5000), cdr3(rng, 5000)
+    for mode in ("global", "local"):
+        first = as_np(pw.dist_matrix(q, r, B62, mode=mode))
+        rows = [0, 3999, 4000, 4999]
+        exp = oracle.align_matrix([q[i] for i in rows], r, B62.similarity_grid, mode=mode,
+                                  dist=True, threads=os.cpu_count() or 1)
+        assert np.array_equal(first[rows], exp)
+        assert np.array_equal(first, as_np(pw.dist_matrix(q, r, B62, mode=mode)))
