@@ -885,11 +885,14 @@ def measure_learned(args, world, rank, local):
         return None
     plans = None
     if not args.no_plans:
-        plans = learned_plans(w, M, (cc, cl), rec_n=ne)
-        plans["trained_encoder"] = {
+        plans = {"bound_0.99": learned_plans(w, M, (cc, cl), ne, 0.99, [
+            ("fallback_only", None, 0), ("untrained_encoder", Ln.Encoder(seed=0), 256)])}
+        plans["bound_0.99"]["trained_encoder"] = {
             "ms_per_step": total_ms / args.steps, "effective_pairs_per_s": value / world,
             "recall": rec["recall"], "exhaustive_share": cal["exhaustive_share"],
             "query_fallback": cal["query_fallback"], "ref_fallback": cal["ref_fallback"]}
+        plans["bound_0.999"] = learned_plans(w, M, (cc, cl), ne, 0.999, [
+            ("fallback_only", None, 0), ("trained_encoder", enc, 256)])
     e2e_s = statistics.median(e2e_times) if e2e_times else float("nan")
     prop_s = phase_ms.get("embed->propose", float("nan")) / 1e3
     n_lq, n_lr = len(qb.learn_rows), idx.n_learn
@@ -909,6 +912,7 @@ def measure_learned(args, world, rank, local):
         "config": dict(line_config(w, world), train_pairs=args.train_pairs),
         "recall": rec["recall"], "recall_found": rec["found"], "recall_exact": rec["exact"],
         "recall_hits_all_exact": rec["subset_of_exact"],
+        "recall_by_region": region_recall(rec["found_cells"], rec["exact_cells"]),
         "calibration": {k: v for k, v in cal.items() if k != "cells_no_fallback"},
         "exhaustive_pairs_per_s": exh_rate, "speedup_vs_exhaustive": value / world / exh_rate,
         "phase_ms": phase_ms, "train_seconds": train_s,
@@ -942,20 +946,35 @@ def measure_learned(args, world, rank, local):
     return line
 
 
-def learned_plans(w, M, cal, rec_n: int, steps: int = 3) -> dict:
-    """What the encoder earns: the same search, calibrated to the same recall bound (0.99 on the
-    same held-out batch), without the network (``k = 0``: the calibrated exhaustive fallback
-    alone) and with the network untrained (random weights, seed 0).  Each plan reports its step
+def region_recall(found_cells, exact_cells) -> dict:
+    """Recall by (query length, ref length) region: a short query (8-10), a short ref (8-10)
+    against a longer query, and both 11 or longer."""
+    f, e = np.asarray(found_cells, np.float64), np.asarray(exact_cells, np.float64)
+    regions = {"query_8_10": (slice(8, 11), slice(None)),
+               "query_11plus_ref_8_10": (slice(11, None), slice(8, 11)),
+               "both_11plus": (slice(11, None), slice(11, None))}
+    out = {}
+    for name, (a, b) in regions.items():
+        ex = float(e[a, b].sum())
+        out[name] = {"exact_hits": int(ex), "share_of_hits": ex / max(float(e.sum()), 1.0),
+                     "recall": float(f[a, b].sum()) / ex if ex else 1.0}
+    return out
+
+
+def learned_plans(w, M, cal, rec_n: int, bound: float, plans, steps: int = 3) -> dict:
+    """What the encoder earns: the same search, calibrated to the same recall ``bound`` on the
+    same held-out batch, for each ``(name, encoder, k)`` of ``plans`` -- ``k = 0`` is the method
+    without the network (the calibrated exhaustive fallback alone).  Each plan reports its step
     time over all queries (refs re-embedded, as in the timed steps), the effective pairs/s, the
     recall on the first ``rec_n`` workload queries and the share of pairs scored exhaustively."""
     import torch
 
     from seqtree_b200 import learned as Ln
     out = {}
-    for name, enc, k in (("fallback_only", None, 0), ("untrained_encoder", Ln.Encoder(seed=0), 256)):
+    for name, enc, k in plans:
         idx = Ln.LearnedIndex(enc, w["r_codes"], w["r_lens"], matrix=M, gap_open=8,
                               max_penalty=24, k=k)
-        cal_res = idx.calibrate(*cal, bound=0.99)
+        cal_res = idx.calibrate(*cal, bound=bound)
         qb = idx.queries(w["q_codes"], w["q_lens"])
         idx.embed_refs()
         res = idx.search(qb)

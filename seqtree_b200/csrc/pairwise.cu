@@ -616,6 +616,9 @@ __global__ void __launch_bounds__(kQpWarps * 32) gotoh_qpair_kernel(const QpArgs
             for (int j = lane; j < n; j += 32) my_ref[j] = uint16_t(int(rs[j]) * R * 32);
             __syncwarp();
 
+            // Lane state: H and Y of its R rows at the last column it computed (column 0 to
+            // start), the X (and, EXACT, max(M, Y)) of its last row for the lane below, and
+            // (EXACT) max(M, X) of each row.
             uint32_t Hl[R], Yl[R], MXl[EXACT ? R : 1];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -626,67 +629,72 @@ __global__ void __launch_bounds__(kQpWarps * 32) gotoh_qpair_kernel(const QpArgs
             }
             uint32_t diag = (lane == 0 || LOCAL) ? 0u
                             : (OFFSET ? eo2 : dup2(-(a.go + (lane * R - 1) * a.ge)));
-            uint32_t best = 0u, cap = 0u;
-            uint32_t outH = 0u, outX = kNeg2, outMY = 0u;
-            const int steps = n + 31;
-            for (int s = 0; s < steps; ++s) {
-                uint32_t upH = __shfl_up_sync(full, outH, 1);
-                uint32_t upX = __shfl_up_sync(full, outX, 1);
-                uint32_t upMY = EXACT ? __shfl_up_sync(full, outMY, 1) : 0u;
-                const int j = s - lane + 1;
-                if (lane == 0) {  // the virtual row 0 at column j
-                    const uint32_t h0 =
-                        LOCAL ? 0u : (OFFSET ? eo2 : dup2(-(a.go + (j - 1) * a.ge)));
+            uint32_t Xlast = kNeg2, MYlast = 0u, best = 0u;
+            const uint32_t* prof_lane = s_prof + lane;
+            const uint16_t* rcol = my_ref - lane;  // rcol[s]: this lane's column j - 1 = s - lane
+
+            // One column of this lane's rows at step s (the lane's column is j = s - lane + 1).
+            // Every lane shuffles; `active` lanes update.  The diagonal terms of all rows are
+            // formed first, so the old H of a row is dead once its own Y and H are formed.
+            auto step = [&](int s, bool active) {
+                uint32_t upH = __shfl_up_sync(full, Hl[R - 1], 1);
+                uint32_t upX = __shfl_up_sync(full, Xlast, 1);
+                uint32_t upMY = EXACT ? __shfl_up_sync(full, MYlast, 1) : 0u;
+                if (lane == 0) {  // the virtual row 0 at column j = s + 1
+                    const uint32_t h0 = LOCAL ? 0u : (OFFSET ? eo2 : dup2(-(a.go + s * a.ge)));
                     upH = h0;
                     upX = kNeg2;
                     upMY = h0;
                 }
-                if (j >= 1 && j <= n) {
-                    const uint32_t* pc = s_prof + my_ref[j - 1] + lane;
-                    const uint32_t top = upH;
-                    uint32_t d = diag;
+                if (!active) return;
+                const uint32_t* pc = prof_lane + rcol[s];
+                uint32_t M[R];
 #pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const uint32_t sc = pc[r * 32];
-                        const uint32_t M = LOCAL ? __viaddmax_s16x2_relu(d, sc, kNeg2)
-                                                 : __viaddmax_s16x2(d, sc, kNeg2);
-                        uint32_t X, Y;
-                        if constexpr (EXACT) {
-                            X = __viaddmax_s16x2(upMY, mgo2, __viaddmax_s16x2(upX, mge2, kNeg2));
-                            Y = __viaddmax_s16x2(MXl[r], mgo2,
-                                                 __viaddmax_s16x2(Yl[r], mge2, kNeg2));
-                        } else if constexpr (OFFSET) {
-                            X = __viaddmax_s16x2(upH, eo2, upX);
-                            Y = __viaddmax_s16x2(Hl[r], eo2, Yl[r]);
-                        } else {
-                            X = __viaddmax_s16x2(upH, mgo2, __viaddmax_s16x2(upX, mge2, kNeg2));
-                            Y = __viaddmax_s16x2(Hl[r], mgo2, __viaddmax_s16x2(Yl[r], mge2, kNeg2));
-                        }
-                        const uint32_t H = __vimax3_s16x2(M, X, Y);
-                        if constexpr (LOCAL) best = __vimax3_s16x2(best, M, kNeg2);
-                        d = Hl[r];
-                        Hl[r] = H;
-                        Yl[r] = Y;
-                        upH = H;
-                        upX = X;
-                        if constexpr (EXACT) {
-                            MXl[r] = __vimax3_s16x2(M, X, kNeg2);
-                            upMY = __vimax3_s16x2(M, Y, kNeg2);
-                        }
-                    }
-                    diag = top;
-                    outH = upH;
-                    outX = upX;
-                    outMY = upMY;
-                    if (!LOCAL && j == n) {
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            if (lane == cl1 && r == cr1) cap = (cap & 0xFFFF0000u) | (Hl[r] & 0xFFFFu);
-                            if (lane == cl2 && r == cr2) cap = (cap & 0xFFFFu) | (Hl[r] & 0xFFFF0000u);
-                        }
-                    }
+                for (int r = 0; r < R; ++r) {
+                    const uint32_t dg = r == 0 ? diag : Hl[r - 1];
+                    M[r] = LOCAL ? __viaddmax_s16x2_relu(dg, pc[r * 32], kNeg2)
+                                 : __viaddmax_s16x2(dg, pc[r * 32], kNeg2);
                 }
-            }
+                diag = upH;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    uint32_t X, Y;
+                    if constexpr (EXACT) {
+                        X = __viaddmax_s16x2(upMY, mgo2, __viaddmax_s16x2(upX, mge2, kNeg2));
+                        Y = __viaddmax_s16x2(MXl[r], mgo2, __viaddmax_s16x2(Yl[r], mge2, kNeg2));
+                    } else if constexpr (OFFSET) {
+                        X = __viaddmax_s16x2(upH, eo2, upX);
+                        Y = __viaddmax_s16x2(Hl[r], eo2, Yl[r]);
+                    } else {
+                        X = __viaddmax_s16x2(upH, mgo2, __viaddmax_s16x2(upX, mge2, kNeg2));
+                        Y = __viaddmax_s16x2(Hl[r], mgo2, __viaddmax_s16x2(Yl[r], mge2, kNeg2));
+                    }
+                    const uint32_t H = __vimax3_s16x2(M[r], X, Y);
+                    if constexpr (EXACT) {
+                        MXl[r] = __vimax3_s16x2(M[r], X, kNeg2);
+                        upMY = __vimax3_s16x2(M[r], Y, kNeg2);
+                    }
+                    Hl[r] = H;
+                    Yl[r] = Y;
+                    upH = H;
+                    upX = X;
+                }
+                if constexpr (LOCAL) {  // the running maximum of M, two rows per operation
+#pragma unroll
+                    for (int r = 0; r < R; r += 2)
+                        best = __vimax3_s16x2(best, M[r], r + 1 < R ? M[r + 1] : kNeg2);
+                }
+                Xlast = upX;
+                MYlast = upMY;
+            };
+            // Ramp in (lanes start one step apart), steady state (every lane on a column of
+            // 1..n: no range test), ramp out.
+            int s = 0;
+            for (; s < 31; ++s) step(s, s >= lane && s - lane < n);
+#pragma unroll 2
+            for (; s < n; ++s) step(s, true);
+            for (; s < n + 31; ++s) step(s, s - lane < n);
+
             int v1, v2;
             if constexpr (LOCAL) {
 #pragma unroll
@@ -695,8 +703,16 @@ __global__ void __launch_bounds__(kQpWarps * 32) gotoh_qpair_kernel(const QpArgs
                 v1 = lo16(best);
                 v2 = hi16(best);
             } else {
-                v1 = lo16(__shfl_sync(full, cap, cl1));
-                v2 = hi16(__shfl_sync(full, cap, cl2));
+                // A lane's H registers keep its last column (n) once it has passed it: each
+                // query's global score sits in the lane and register of its last row.
+                uint32_t c1 = 0u, c2 = 0u;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (r == cr1) c1 = Hl[r];
+                    if (r == cr2) c2 = Hl[r];
+                }
+                v1 = lo16(__shfl_sync(full, c1, cl1));
+                v2 = hi16(__shfl_sync(full, c2, cl2));
                 if constexpr (OFFSET) {
                     v1 -= (m1 + n) * a.ge;
                     v2 -= (m2 + n) * a.ge;

@@ -695,7 +695,7 @@ class LearnedIndex:
                 "exact_cells": exact, "subset_of_exact": ok}
 
     def calibrate(self, codes: np.ndarray, lens: np.ndarray, bound: float = 0.99,
-                  margin: float = 0.003) -> dict:
+                  margin: float | None = None) -> dict:
         """Chooses the fallback lengths on a held-out calibration batch.
 
         Without fallback, the proposals' found / exact hit counts are measured per (query
@@ -704,7 +704,9 @@ class LearnedIndex:
         length with the most recovered hits per exhaustively scored pair (pairs estimated from
         the calibration batch's query lengths and the refs' lengths) -- until the estimated
         recall reaches ``bound + margin``.  The recall with the chosen fallback is then measured
-        on the same batch."""
+        on the same batch.  ``margin`` defaults to min(0.003, (1 - bound) / 3)."""
+        if margin is None:
+            margin = min(0.003, (1.0 - bound) / 3.0)
         self.set_fallback()
         r0 = self.recall(codes, lens)
         f, e = r0["found_cells"].astype(np.float64), r0["exact_cells"].astype(np.float64)
