@@ -886,13 +886,15 @@ def measure_learned(args, world, rank, local):
     plans = None
     if not args.no_plans:
         plans = {"bound_0.99": learned_plans(w, M, (cc, cl), ne, 0.99, [
-            ("fallback_only", None, 0), ("untrained_encoder", Ln.Encoder(seed=0), 256)])}
+            ("fallback_only", None, 0, None), ("untrained_encoder", Ln.Encoder(seed=0), 256, None),
+            ("trained_encoder_band_1", enc, 256, 1), ("trained_encoder_band_2", enc, 256, 2)])}
         plans["bound_0.99"]["trained_encoder"] = {
             "ms_per_step": total_ms / args.steps, "effective_pairs_per_s": value / world,
             "recall": rec["recall"], "exhaustive_share": cal["exhaustive_share"],
             "query_fallback": cal["query_fallback"], "ref_fallback": cal["ref_fallback"]}
         plans["bound_0.999"] = learned_plans(w, M, (cc, cl), ne, 0.999, [
-            ("fallback_only", None, 0), ("trained_encoder", enc, 256)])
+            ("fallback_only", None, 0, None), ("trained_encoder", enc, 256, None),
+            ("trained_encoder_band_2", enc, 256, 2)])
     e2e_s = statistics.median(e2e_times) if e2e_times else float("nan")
     prop_s = phase_ms.get("embed->propose", float("nan")) / 1e3
     n_lq, n_lr = len(qb.learn_rows), idx.n_learn
@@ -963,17 +965,18 @@ def region_recall(found_cells, exact_cells) -> dict:
 
 def learned_plans(w, M, cal, rec_n: int, bound: float, plans, steps: int = 3) -> dict:
     """What the encoder earns: the same search, calibrated to the same recall ``bound`` on the
-    same held-out batch, for each ``(name, encoder, k)`` of ``plans`` -- ``k = 0`` is the method
-    without the network (the calibrated exhaustive fallback alone).  Each plan reports its step
+    same held-out batch, for each ``(name, encoder, k, band)`` of ``plans`` -- ``k = 0`` is the
+    method without the network (the calibrated exhaustive fallback alone); ``band`` limits each
+    query's proposals to refs within that many residues of its length.  Each plan reports its step
     time over all queries (refs re-embedded, as in the timed steps), the effective pairs/s, the
     recall on the first ``rec_n`` workload queries and the share of pairs scored exhaustively."""
     import torch
 
     from seqtree_b200 import learned as Ln
     out = {}
-    for name, enc, k in plans:
+    for name, enc, k, band in plans:
         idx = Ln.LearnedIndex(enc, w["r_codes"], w["r_lens"], matrix=M, gap_open=8,
-                              max_penalty=24, k=k)
+                              max_penalty=24, k=k, band=band)
         cal_res = idx.calibrate(*cal, bound=bound)
         qb = idx.queries(w["q_codes"], w["q_lens"])
         idx.embed_refs()
@@ -994,6 +997,7 @@ def learned_plans(w, M, cal, rec_n: int, bound: float, plans, steps: int = 3) ->
         ms = statistics.median(times)
         out[name] = {"ms_per_step": ms, "effective_pairs_per_s": qb.count * idx.nr / (ms / 1e3),
                      "recall": rec["recall"], "exhaustive_share": cal_res["exhaustive_share"],
+                     "recall_by_region": region_recall(rec["found_cells"], rec["exact_cells"]),
                      "query_fallback": cal_res["query_fallback"],
                      "ref_fallback": cal_res["ref_fallback"]}
         del idx, qb

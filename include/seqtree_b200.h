@@ -297,6 +297,15 @@ int32_t st_propose_topk(const void *query_emb, int64_t nq, const void *ref_emb, 
                         int32_t k, int32_t *ids_device, float *scores_device, void *cuda_stream,
                         st_error *err);
 
+/* st_propose_topk with each tile of 256 queries (rows 256t .. 256t+255) scanning only the ref
+ * tiles of 128 refs [tile_ranges_device[2t], tile_ranges_device[2t + 1]) (device int32, two per
+ * query tile; clamped into the ref tiles that exist).  With queries and refs sorted by length,
+ * this restricts each query's candidates to refs of nearby length.  The result is the exact
+ * top-k of the scanned refs.  No counterpart in the reference. */
+int32_t st_propose_topk_ranges(const void *query_emb, int64_t nq, const void *ref_emb, int64_t nr,
+                               int32_t k, const int32_t *tile_ranges_device, int32_t *ids_device,
+                               float *scores_device, void *cuda_stream, st_error *err);
+
 /* Per-row score cutoffs for a target E-value: thetas_from_scores of seqtree's
  * python/seqtree/evalue.py:102-143 (with _theta, :86-99) over CSR rows of control hit scores in
  * device memory (indptr_device rows + 1 int64, scores_device int32; row order within a row is

@@ -116,6 +116,9 @@ SIGNATURES = [
     ("st_propose_topk", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_propose_topk_ranges", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
     ("st_stream_status", ctypes.c_int32, [ctypes.c_void_p, _ep]),
     ("st_align_pairs_sets", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, _i32p,

@@ -44,7 +44,8 @@ float encoder_train_step(Encoder& m, const uint8_t* codes, const int32_t* lens, 
                          int S, float lr);
 void encoder_embed(Encoder& m, const st_seqset_s& set, void* out, int layout, cudaStream_t st);
 void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, int k, int32_t* ids,
-                  float* scores, cudaStream_t stream);
+                  float* scores, cudaStream_t stream,
+                  const int32_t* ranges = nullptr);
 void profile_scores(const int32_t* table, int32_t width, int32_t c, uint8_t gap, int32_t unreachable,
                     const st_seqset_s& set, int32_t* out_d, cudaStream_t stream);
 void align_pairs_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* qi_d, const int32_t* ri_d,
@@ -894,6 +895,19 @@ int32_t st_propose_topk(const void* query_emb, int64_t nq, const void* ref_emb, 
         std::lock_guard<std::mutex> lk(ctx.mu);
         propose_topk(query_emb, nq, ref_emb, nr, k, ids_device, scores_device,
                      static_cast<cudaStream_t>(cuda_stream));
+    });
+}
+
+int32_t st_propose_topk_ranges(const void* query_emb, int64_t nq, const void* ref_emb, int64_t nr,
+                               int32_t k, const int32_t* tile_ranges_device, int32_t* ids_device,
+                               float* scores_device, void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        if (!tile_ranges_device) fail(ST_EINVAL, "seqtree_b200: null tile ranges");
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        propose_topk(query_emb, nq, ref_emb, nr, k, ids_device, scores_device,
+                     static_cast<cudaStream_t>(cuda_stream), tile_ranges_device);
     });
 }
 

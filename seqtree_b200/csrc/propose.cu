@@ -74,11 +74,25 @@ struct ProposeArgs {
     const uint8_t* remb;
     int64_t nq, nr;
     int k;
+    const int32_t* ranges;     // null, or per query tile [first, last) ref tile (2 ints)
     unsigned long long* cand;  // [gridDim.x][kQT][kCap]
     int32_t* out_ids;          // [nq][k]
     float* out_scores;         // [nq][k] or null
     unsigned long long* err;
 };
+
+// The ref tiles a query tile scans: the caller's [first, last) clamped into [0, ntr), so every
+// copy stays inside the ref embeddings whatever the range array holds.
+__device__ __forceinline__ int64_t tile_first(const ProposeArgs& a, int64_t qt, int64_t ntr) {
+    if (!a.ranges) return 0;
+    const int64_t f = a.ranges[2 * qt];
+    return f < 0 ? 0 : (f > ntr ? ntr : f);
+}
+__device__ __forceinline__ int64_t tile_last(const ProposeArgs& a, int64_t qt, int64_t ntr) {
+    if (!a.ranges) return ntr;
+    const int64_t f = tile_first(a, qt, ntr), l = a.ranges[2 * qt + 1];
+    return l < f ? f : (l > ntr ? ntr : l);
+}
 
 __device__ __forceinline__ float fmax3(float a, float b, float c) {
     float m;
@@ -275,7 +289,8 @@ __global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a
             a_par = aphase;
             aphase ^= 1u;
             bool ok = true;
-            for (int64_t rt = 0; rt < ntr; ++rt) {
+            const int64_t rt0 = tile_first(a, qt, ntr), rt1 = tile_last(a, qt, ntr);
+            for (int64_t rt = rt0; rt < rt1; ++rt) {
                 if (!bar_wait(BAR(kStages + stage), sphase ^ 1u, s_abort, a.err)) {
                     ok = false;
                     break;
@@ -305,7 +320,8 @@ __global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a
             aphase ^= 1u;
             tc_fence_after();
             bool ok = true;
-            for (int64_t rt = 0; rt < ntr; ++rt) {
+            const int64_t rt0 = tile_first(a, qt, ntr), rt1 = tile_last(a, qt, ntr);
+            for (int64_t rt = rt0; rt < rt1; ++rt) {
                 if (!bar_wait(BAR(16 + acc), accphase ^ 1u, s_abort, a.err) ||
                     !bar_wait(BAR(stage), sphase, s_abort, a.err)) {
                     ok = false;
@@ -353,7 +369,8 @@ __global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a
             const int64_t q = qt * kQT + grp * 128 + row;
             float thr = q < a.nq ? -INFINITY : INFINITY;
             int count = 0;
-            for (int64_t rt = 0; rt < ntr; ++rt) {
+            const int64_t rt0 = tile_first(a, qt, ntr), rt1 = tile_last(a, qt, ntr);
+            for (int64_t rt = rt0; rt < rt1; ++rt) {
                 if (!bar_wait(BAR(14 + acc), accphase, s_abort, a.err)) {
                     ok = false;
                     break;
@@ -463,7 +480,7 @@ __global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a
 // aligned).  ids[q][i] / scores[q][i] hold the i-th best ref of query q (score descending, ties by
 // ascending ref id); entries past the number of refs are -1 / -inf.
 void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, int k, int32_t* ids,
-                  float* scores, cudaStream_t stream) {
+                  float* scores, cudaStream_t stream, const int32_t* ranges) {
     if (nq < 0 || nr < 0) fail(ST_EINVAL, "seqtree_b200: negative embedding count");
     if (k < 1 || k > kMaxK) fail(ST_EINVAL, "seqtree_b200: k must be in 1..256");
     if (nr >= (int64_t(1) << 31)) fail(ST_EINVAL, "seqtree_b200: at most 2^31 - 1 refs");
@@ -481,6 +498,7 @@ void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, in
     a.nq = nq;
     a.nr = nr;
     a.k = k;
+    a.ranges = ranges;
     a.cand = ctx.topk_cand.as<unsigned long long>(size_t(grid) * kQT * kCap);
     a.out_ids = ids;
     a.out_scores = scores;

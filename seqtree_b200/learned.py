@@ -251,13 +251,40 @@ def swizzle_rows(x):
 
 
 def propose_topk_into(q_ptr: int, nq: int, r_ptr: int, nr: int, k: int, ids_ptr: int,
-                      scores_ptr: int = 0, stream: int = 0) -> None:
-    """``st_propose_topk`` on device pointers (swizzled bf16 embeddings in, [nq][k] out)."""
+                      scores_ptr: int = 0, stream: int = 0, ranges_ptr: int = 0) -> None:
+    """``st_propose_topk`` on device pointers (swizzled bf16 embeddings in, [nq][k] out); with
+    ``ranges_ptr`` (device int32, two per 256-query tile) ``st_propose_topk_ranges``."""
     err = _lib.st_error()
-    _lib.check(_lib.lib.st_propose_topk(ctypes.c_void_p(q_ptr), int(nq), ctypes.c_void_p(r_ptr),
+    if ranges_ptr:
+        code = _lib.lib.st_propose_topk_ranges(
+            ctypes.c_void_p(q_ptr), int(nq), ctypes.c_void_p(r_ptr), int(nr), int(k),
+            ctypes.c_void_p(ranges_ptr), ctypes.c_void_p(ids_ptr),
+            ctypes.c_void_p(scores_ptr or None), ctypes.c_void_p(stream), ctypes.byref(err))
+    else:
+        code = _lib.lib.st_propose_topk(ctypes.c_void_p(q_ptr), int(nq), ctypes.c_void_p(r_ptr),
                                         int(nr), int(k), ctypes.c_void_p(ids_ptr),
                                         ctypes.c_void_p(scores_ptr or None),
-                                        ctypes.c_void_p(stream), ctypes.byref(err)), err)
+                                        ctypes.c_void_p(stream), ctypes.byref(err))
+    _lib.check(code, err)
+
+
+QUERY_TILE, REF_TILE = 256, 128  # the proposal kernel's tile heights
+
+
+def band_tile_ranges(q_lens_sorted: np.ndarray, r_lens_sorted: np.ndarray, band: int) -> np.ndarray:
+    """Per 256-query tile of length-sorted queries, the [first, last) 128-ref tiles of
+    length-sorted refs that hold every ref whose length is within ``band`` of a query of the
+    tile (int32 [tiles, 2])."""
+    q = np.asarray(q_lens_sorted, np.int64)
+    r = np.asarray(r_lens_sorted, np.int64)
+    nt = -(-q.size // QUERY_TILE)
+    out = np.zeros((nt, 2), np.int32)
+    for t in range(nt):
+        blk = q[t * QUERY_TILE:(t + 1) * QUERY_TILE]
+        lo = np.searchsorted(r, blk.min() - band, side="left")
+        hi = np.searchsorted(r, blk.max() + band, side="right")
+        out[t] = (lo // REF_TILE, -(-hi // REF_TILE)) if hi > lo else (0, 0)
+    return out
 
 
 def propose_topk(q_emb, r_emb, k: int = 256):
@@ -478,11 +505,18 @@ class QueryBatch:
         self.count = int(self.lens.size)
         fb = index.query_fallback[np.clip(self.lens, 0, PAD)]
         self.fb_rows = np.flatnonzero(fb).astype(np.int64)
-        self.learn_rows = np.flatnonzero(~fb).astype(np.int64)
+        learn = np.flatnonzero(~fb).astype(np.int64)
+        # learn rows in length order, so that a 256-query tile of the proposal kernel spans few
+        # lengths (its ref band is then narrow)
+        self.learn_rows = learn[np.argsort(self.lens[learn], kind="stable")]
         self.fb_set = _subset(codes, self.lens, self.fb_rows)
         self.learn_set = _subset(codes, self.lens, self.learn_rows)
         self.fb_rows_t = torch.from_numpy(self.fb_rows).cuda()
         self.learn_rows_t = torch.from_numpy(self.learn_rows).cuda()
+        self.ranges = None
+        if index.band is not None and self.learn_rows.size and index.n_learn:
+            r = band_tile_ranges(self.lens[self.learn_rows], index.learn_lens, index.band)
+            self.ranges = torch.from_numpy(r.ravel()).cuda()
 
 
 class LearnedIndex:
@@ -502,12 +536,19 @@ class LearnedIndex:
     """
 
     def __init__(self, encoder: Encoder | None, ref_codes: np.ndarray, ref_lens: np.ndarray, *,
-                 matrix, gap_open: int, gap_extend: int = 1, max_penalty: int = 24, k: int = 256):
+                 matrix, gap_open: int, gap_extend: int = 1, max_penalty: int = 24, k: int = 256,
+                 band: int | None = None):
+        """``band``: when set, a query's proposals come only from refs whose length differs from
+        the query tile's lengths by at most ``band`` (refs and queries sorted by length, each
+        256-query tile scanning its band of ref tiles); None scans every ref."""
         from .device import SeqSet
         if max_penalty < 0:
             raise ValueError("max_penalty must be >= 0")
         if k < 0 or (k > 0 and encoder is None):
             raise ValueError("k must be >= 0, and k > 0 needs an encoder")
+        if band is not None and band < 0:
+            raise ValueError("band must be >= 0 or None")
+        self.band = band
         self.encoder, self.matrix = encoder, matrix
         self.gap_open, self.gap_extend, self.max_penalty, self.k = gap_open, gap_extend, max_penalty, k
         self.ref_codes = np.ascontiguousarray(ref_codes, np.uint8)
@@ -526,7 +567,7 @@ class LearnedIndex:
         if self.encoder is None:
             raise ValueError("an index without an encoder has no model to save")
         self.encoder.save(path, {
-            "k": self.k, "max_penalty": self.max_penalty, "gap_open": self.gap_open,
+            "k": self.k, "band": self.band, "max_penalty": self.max_penalty, "gap_open": self.gap_open,
             "gap_extend": self.gap_extend,
             "query_fallback": np.flatnonzero(self.query_fallback).tolist(),
             "ref_fallback": np.flatnonzero(self.ref_fallback).tolist()})
@@ -540,7 +581,7 @@ class LearnedIndex:
         m = enc.meta
         idx = cls(enc, ref_codes, ref_lens, matrix=matrix, gap_open=int(m["gap_open"]),
                   gap_extend=int(m["gap_extend"]), max_penalty=int(m["max_penalty"]),
-                  k=int(m["k"]))
+                  k=int(m["k"]), band=m.get("band"))
         idx.set_fallback(m["query_fallback"], m["ref_fallback"])
         return idx
 
@@ -555,7 +596,9 @@ class LearnedIndex:
         import torch
         fb = self.ref_fallback[np.clip(self.ref_lens, 0, PAD)]
         learn = np.flatnonzero(~fb).astype(np.int64)
+        learn = learn[np.argsort(self.ref_lens[learn], kind="stable")]  # by length, then id
         fbr = np.flatnonzero(fb).astype(np.int64)
+        self.learn_lens = self.ref_lens[learn]
         self.learn_ids = torch.from_numpy(learn.astype(np.int32)).cuda()
         self.fb_ref_ids = torch.from_numpy(fbr.astype(np.int32)).cuda()
         self.learn_refs = _subset(self.ref_codes, self.ref_lens, learn)
@@ -609,7 +652,8 @@ class LearnedIndex:
             mark("embed")
             ids = torch.empty((n, self.k), dtype=torch.int32, device="cuda")
             propose_topk_into(q_emb.data_ptr(), n, self.r_emb.data_ptr(), self.n_learn, self.k,
-                              ids.data_ptr(), 0, stream)
+                              ids.data_ptr(), 0, stream,
+                              qb.ranges.data_ptr() if qb.ranges is not None else 0)
             mark("propose")
             qi = torch.arange(n, dtype=torch.int32, device="cuda").repeat_interleave(self.k)
             ri = ids.view(-1)

@@ -100,3 +100,53 @@ def test_topk_arguments(cuda_ready):
         propose_topk(buf[1:].view(8, 64), q, 4)
     ids, sc = propose_topk(q, q[:0], 3)  # no refs: every slot empty
     assert (ids.cpu().numpy() == -1).all() and np.isneginf(sc.cpu().numpy()).all()
+
+
+@pytest.mark.gpu
+def test_topk_over_per_tile_ref_ranges(cuda_ready):
+    """st_propose_topk_ranges: each 256-query tile ranks only the 128-ref tiles of its range
+    (an empty range yields no candidates; out-of-range values are clamped), exactly as the exact
+    top-k over those refs."""
+    import torch
+
+    from seqtree_b200.learned import propose_topk_into, swizzle_rows
+    rng = np.random.default_rng(17)
+    nq, nr, k = 700, 2000, 64
+    q, r = _emb(rng, nq), _emb(rng, nr, 40)
+    ranges = np.array([[2, 9], [0, 0], [10, 99]], np.int32)  # tile 3 asks past the end: clamped
+    qt, rt = swizzle_rows(torch.from_numpy(q).cuda()), swizzle_rows(torch.from_numpy(r).cuda())
+    ids = torch.empty((nq, k), dtype=torch.int32, device="cuda")
+    sc = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    rg = torch.from_numpy(ranges.ravel()).cuda()
+    propose_topk_into(qt.data_ptr(), nq, rt.data_ptr(), nr, k, ids.data_ptr(), sc.data_ptr(),
+                      torch.cuda.current_stream().cuda_stream, rg.data_ptr())
+    torch.cuda.synchronize()
+    ids, sc = ids.cpu().numpy(), sc.cpu().numpy()
+    ntr = -(-nr // 128)
+    for t in range(3):
+        rows = slice(256 * t, min(256 * (t + 1), nq))
+        lo, hi = max(0, min(ranges[t, 0], ntr)), max(0, min(ranges[t, 1], ntr))
+        lo_ref, hi_ref = lo * 128, min(max(hi, lo) * 128, nr)
+        want_ids, want_sc = _expected(q[rows], r[lo_ref:hi_ref], k)
+        want_ids = np.where(want_ids >= 0, want_ids + lo_ref, -1)
+        np.testing.assert_array_equal(sc[rows], want_sc.astype(np.float32))
+        np.testing.assert_array_equal(ids[rows], want_ids)
+
+
+@pytest.mark.gpu
+def test_banded_learned_search_is_exact(cuda_ready):
+    """A length band restricts the proposals; every reported hit is still an exhaustive hit with
+    its exact score, and with every length in the band's reach the recall is unchanged."""
+    import seqtree_b200 as stb
+    from seqtree_b200 import learned as L
+    M = stb.SubstitutionMatrix.blosum62()
+    enc = L.Encoder(seed=3)
+    rc, rl = L.cdr3_codes(60, 6000)
+    qc, ql = L.cdr3_codes(61, 400)
+    for band in (0, 2, 40):
+        idx = L.LearnedIndex(enc, rc, rl, matrix=M, gap_open=8, max_penalty=24, k=32, band=band)
+        rec = idx.recall(qc, ql)
+        assert rec["subset_of_exact"]
+    wide = L.LearnedIndex(enc, rc, rl, matrix=M, gap_open=8, max_penalty=24, k=32, band=40)
+    full = L.LearnedIndex(enc, rc, rl, matrix=M, gap_open=8, max_penalty=24, k=32)
+    assert wide.recall(qc, ql)["found"] == full.recall(qc, ql)["found"]
