@@ -887,14 +887,13 @@ def measure_learned(args, world, rank, local):
     if not args.no_plans:
         plans = {"bound_0.99": learned_plans(w, M, (cc, cl), ne, 0.99, [
             ("fallback_only", None, 0, None), ("untrained_encoder", Ln.Encoder(seed=0), 256, None),
-            ("trained_encoder_band_1", enc, 256, 1), ("trained_encoder_band_2", enc, 256, 2)])}
+            ("trained_encoder_band_1", enc, 256, 1)])}
         plans["bound_0.99"]["trained_encoder"] = {
             "ms_per_step": total_ms / args.steps, "effective_pairs_per_s": value / world,
             "recall": rec["recall"], "exhaustive_share": cal["exhaustive_share"],
             "query_fallback": cal["query_fallback"], "ref_fallback": cal["ref_fallback"]}
         plans["bound_0.999"] = learned_plans(w, M, (cc, cl), ne, 0.999, [
-            ("fallback_only", None, 0, None), ("trained_encoder", enc, 256, None),
-            ("trained_encoder_band_2", enc, 256, 2)])
+            ("fallback_only", None, 0, None), ("trained_encoder", enc, 256, None)])
     e2e_s = statistics.median(e2e_times) if e2e_times else float("nan")
     prop_s = phase_ms.get("embed->propose", float("nan")) / 1e3
     n_lq, n_lr = len(qb.learn_rows), idx.n_learn
