@@ -728,6 +728,9 @@ def measure(args, name, world, rank, local, int_peaks, soak_s: float = 0.0):
     }
     if soak is not None:
         line["soak"] = soak
+        if not clocks and soak.get("clocks"):  # a timed region of ~1 ms gets no 200 ms sample
+            line["clocks"] = dict(soak["clocks"], source="soak: back-to-back replays of the "
+                                                         "timed step, right after it")
     if w["kind"] == "sparse":
         line["nnz"] = nnz_seen[-1]
         line["roofline"]["note"] = ("algorithmic bytes = CSR output (8 B/hit + 8 B/row) + input "
