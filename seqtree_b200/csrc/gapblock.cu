@@ -39,6 +39,7 @@
 #include <numeric>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "common.cuh"
 #include "sparse.cuh"
@@ -52,6 +53,7 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRow = 32;        // words per profile row
 constexpr int kPairsPerSlice = 4;
+static_assert(kWarps == 2 * kGP, "the ordered sparse epilogue gives each tile row one warp");
 
 // ---------------------------------------------------------------------------- plans ---------
 // Plans depend only on the lengths (and codes) of a set, so a device-resident set builds them
@@ -451,7 +453,87 @@ __global__ void __launch_bounds__(kThreads, 3) gapblock_fast_kernel(const FastAr
     }
     __syncthreads();
     const int cols4 = (kcount + 3) >> 2;
-    if constexpr (SPARSE) {
+    if (SPARSE && a.sink.ordered) {
+        // Ordered form: warp w owns tile row (pair w / 2, half w % 2).  It counts its hits, the
+        // CTA reserves one segment for all of them, and the warp writes its row's hits there in
+        // ascending column order, recording the piece (row, chunk) it wrote.
+        __shared__ unsigned long long s_rowcnt[kWarps + 1];  // row counts, then the base
+        __shared__ int s_fits;
+        const unsigned full = 0xffffffffu;
+        const int pl = warp >> 1, hf = warp & 1;
+        int qrow = -1;
+        if (pl < np) {
+            const int2 pr = a.pairs[p0 + pl];
+            qrow = hf ? pr.y : pr.x;
+        }
+        const uint32_t* src = s_tile + pl * a.rc;
+        const int32_t* fc = s_fcol + (pl / kPairsPerSlice) * a.rc;
+        // Lane l takes columns 4l..4l+3 of each 128-column group (16-byte loads of the packed
+        // tile and of the column terms); bit u of the result marks a hit in column 4l + u.
+        auto group = [&](int g, int32_t (&v)[4]) {
+            const int c = g * 128 + lane * 4;
+            uint32_t hits = 0;
+            if (c < kcount) {
+                const uint4 t = *reinterpret_cast<const uint4*>(src + c);
+                const int4 f = *reinterpret_cast<const int4*>(fc + c);
+                const uint32_t tw[4] = {t.x, t.y, t.z, t.w};
+                const int32_t fw[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    v[u] = int32_t((hf ? (tw[u] >> 16) : (tw[u] & 0xFFFFu)) + uint32_t(fw[u]));
+                    if (c + u < kcount && v[u] <= a.sink.thresh) hits |= 1u << u;
+                }
+            }
+            return hits;
+        };
+        const int groups = (kcount + 127) >> 7;
+        int n = 0;
+        if (qrow >= 0)
+            for (int g = 0; g < groups; ++g) {
+                int32_t v[4];
+                n += __popc(group(g, v));
+            }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(full, n, o);
+        if (lane == 0) s_rowcnt[warp] = (unsigned long long)n;
+        __syncthreads();
+        if (tid == 0) {
+            unsigned long long tot = 0;
+            for (int w = 0; w < kWarps; ++w) tot += s_rowcnt[w];
+            const unsigned long long base = tot ? atomicAdd(a.sink.count, tot) : 0ull;
+            s_rowcnt[kWarps] = base;
+            s_fits = base + tot <= a.sink.cap ? 1 : 0;  // else counted only; the host re-runs
+        }
+        __syncthreads();
+        if (qrow >= 0) {
+            unsigned long long off = s_rowcnt[kWarps];
+            for (int w = 0; w < warp; ++w) off += s_rowcnt[w];
+            const int64_t piece = (int64_t(qrow) - a.sink.row0) * a.sink.nchunks + chunk;
+            if (lane == 0) {
+                a.sink.piece_off[piece] = int64_t(off);
+                a.sink.piece_cnt[piece] = n;
+            }
+            if (s_fits && n > 0) {
+                for (int g = 0; g < groups; ++g) {
+                    int32_t v[4];
+                    uint32_t hits = group(g, v);
+                    const int cnt = __popc(hits);
+                    int incl = cnt;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int t = __shfl_up_sync(full, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    unsigned long long pos = off + (unsigned long long)(incl - cnt);
+                    const int c = g * 128 + lane * 4;
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (hits & (1u << u)) a.sink.seg[pos++] = make_int2(int(k0 + c + u), v[u]);
+                    off += (unsigned long long)__shfl_sync(full, incl, 31);
+                }
+            }
+        }
+    } else if constexpr (SPARSE) {
         // Every lane runs the same number of rounds (sink_append is warp-collective).
         const int total = np * cols4;
         for (int i0 = 0; i0 < total; i0 += kThreads) {
@@ -623,12 +705,13 @@ __global__ void __launch_bounds__(256) gapblock_general_kernel(const GeneralArgs
 
 template <int LQ, bool PRIOR>
 const char* launch_fast(const FastArgs& args, dim3 grid, size_t smem, cudaStream_t stream) {
-    auto kern = args.sink.keys ? gapblock_fast_kernel<LQ, PRIOR, true>
-                               : gapblock_fast_kernel<LQ, PRIOR, false>;
+    const bool sparse = args.sink.keys != nullptr || args.sink.ordered;  // either sparse form
+    auto kern = sparse ? gapblock_fast_kernel<LQ, PRIOR, true>
+                       : gapblock_fast_kernel<LQ, PRIOR, false>;
     STB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     kern<<<grid, kThreads, smem, stream>>>(args);
     STB_CUDA(cudaGetLastError());
-    return args.sink.keys ? "gapblock_fast_kernel<sparse>" : "gapblock_fast_kernel";
+    return sparse ? "gapblock_fast_kernel<sparse>" : "gapblock_fast_kernel";
 }
 
 // Profile height LQ >= longest query: rows per pair in shared memory.
@@ -751,6 +834,24 @@ constexpr int64_t kTuneSlicePairs = int64_t(100) * 1000 * 1000;
 thread_local int t_force_rc = 0;           // set while the autotuner times one chunk width
 thread_local int t_force_persistent = -1;  // and the launch form (-1: the tuned or static one)
 
+// The conditions under which gapblock_run takes the fast kernel (non-negative penalties, every
+// length <= 64, halves that cannot carry), the form whose sparse output is ordered.
+bool fast_form_possible(const st_seqset_s& qs, const st_seqset_s& rs, const int32_t* penalty,
+                        int32_t matrix_size) {
+    if (qs.alphabet < 0 || qs.alphabet != rs.alphabet) return false;
+    const int A = alphabet_size(qs.alphabet);
+    if (penalty && matrix_size != A) return false;
+    int64_t maxpen = 0;
+    for (int x = 0; x < A; ++x)
+        for (int y = 0; y < A; ++y) {
+            const int64_t v = penalty ? penalty[x * A + y] : int64_t(x != y);
+            if (v < 0) return false;
+            maxpen = std::max(maxpen, v);
+        }
+    const int32_t longest = std::max(qs.max_len, rs.max_len);
+    return longest <= 64 && int64_t(std::min(qs.max_len, rs.max_len)) * maxpen <= 8191;
+}
+
 std::string gb_shape_key(const st_seqset_s& qs, const st_seqset_s& rs, bool has_prior) {
     return "gapblock|" + std::to_string(profile_height(qs.max_len)) + "|" +
            std::to_string(int(has_prior)) + "|" + std::to_string(std::max(qs.max_len, rs.max_len)) +
@@ -763,7 +864,7 @@ std::string gb_shape_key(const st_seqset_s& qs, const st_seqset_s& rs, bool has_
 // blocks, and the dense form's first-time tuning slice (which starts at row 0).
 void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int32_t matrix_size,
                   int32_t go, int32_t ge, const int32_t* prior, int64_t prior_len,
-                  uint32_t prior_width, int32_t* out_d, const SparseSink* sink,
+                  uint32_t prior_width, int32_t* out_d, SparseSink* sink,
                   cudaStream_t stream, int64_t r0 = 0, int64_t r1 = -1) {
     if (go < 0 || ge < 0) fail(ST_EINVAL, "gap_open and gap_extend must be >= 0");
     if (qs.alphabet < 0 || qs.alphabet != rs.alphabet)
@@ -852,6 +953,9 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
         rpp = &rp;
     }
 
+    if (!sink && !out_d) fail(ST_EINVAL, "seqtree_b200: null output buffer");
+    if (!fast && sink && sink->ordered)
+        fail(ST_ECUDA, "seqtree_b200: internal error: the ordered sparse form needs the fast kernel");
     if (!fast) {
         int32_t* d_pen = ctx.table_buf.as<int32_t>(pen.size());
         h2d(d_pen, pen.data(), pen.size() * 4, stream);
@@ -950,6 +1054,13 @@ void gapblock_run(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penalty, int3
     fa.bias2 = uint32_t(bias) * 0x10001u;
     fa.out = out_d;
     fa.err = err;
+    if (sink && sink->ordered) {
+        const int64_t rows = (r1 < 0 ? N : r1) - r0;
+        if (rows * int64_t(rp.nchunks) > sink->piece_cap)
+            fail(ST_ECUDA, "seqtree_b200: internal error: sparse piece table too small");
+        sink->nchunks = rp.nchunks;
+        sink->row0 = r0;
+    }
     if (sink) fa.sink = *sink;
 
     const int64_t npg = ceil_div(qp.P, kGP);
@@ -1134,6 +1245,68 @@ __global__ void csr_block_kernel(const unsigned long long* __restrict__ keys, in
     }
 }
 
+// Ordered form, step 1: hits of each row of the block (the sum of its pieces), one warp per row.
+__global__ void piece_rows_kernel(const int32_t* __restrict__ piece_cnt, int64_t rows, int nchunks,
+                                  int64_t* __restrict__ rowcnt) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < rows; r += nw) {
+        const int32_t* pc = piece_cnt + r * nchunks;
+        long long sum = 0;
+        for (int c = lane; c < nchunks; c += 32) sum += pc[c];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) rowcnt[r] = sum;
+    }
+}
+
+// Ordered form, step 2: the block's CSR rows.  start[r] is the exclusive prefix of the rows' hits
+// inside the block (start[rows] the block's total) and base the hits of earlier blocks.  A warp
+// walks its row's pieces in chunk order -- ascending columns -- and copies each (ref id, score)
+// run into place.
+__global__ void piece_copy_kernel(const int2* __restrict__ seg, const int64_t* __restrict__ piece_off,
+                                  const int32_t* __restrict__ piece_cnt,
+                                  const int64_t* __restrict__ start, int64_t rows, int nchunks,
+                                  int64_t row0, int64_t base, int64_t* __restrict__ indptr,
+                                  int32_t* __restrict__ ref_ids, int32_t* __restrict__ scores) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t r = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; r < rows; r += nw) {
+        long long pos = base + start[r];
+        if (lane == 0) {
+            indptr[row0 + r] = pos;
+            if (r == rows - 1) indptr[row0 + rows] = base + start[rows];
+        }
+        for (int c0 = 0; c0 < nchunks; c0 += 32) {
+            const int c = c0 + lane;
+            const int32_t cnt = c < nchunks ? piece_cnt[r * nchunks + c] : 0;
+            const long long src = cnt > 0 ? piece_off[r * nchunks + c] : 0;
+            long long incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const long long t = __shfl_up_sync(full, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const long long dst = pos + incl - cnt;
+            uint32_t m = __ballot_sync(full, cnt > 0);
+            while (m) {
+                const int L = __ffs(int(m)) - 1;
+                m &= m - 1;
+                const int32_t n = __shfl_sync(full, cnt, L);
+                const long long s0 = __shfl_sync(full, src, L);
+                const long long d0 = __shfl_sync(full, dst, L);
+                for (int i = lane; i < n; i += 32) {
+                    const int2 h = seg[s0 + i];
+                    ref_ids[d0 + i] = h.x;
+                    scores[d0 + i] = h.y;
+                }
+            }
+            pos += __shfl_sync(full, incl, 31);
+        }
+    }
+}
+
 // Hits one sort takes at most (2^28, about 10 GB of scratch); larger outputs are produced in
 // query-row blocks.  SEQTREE_B200_SPARSE_BLOCK_HITS lowers it (at least 1024), e.g. to bound the
 // scratch memory.
@@ -1144,6 +1317,13 @@ uint64_t max_block_hits() {
         if (x > 0) v = std::min<uint64_t>(v, std::max<uint64_t>(uint64_t(x), 1024));
     }
     return v;
+}
+
+// Hits one block of the ordered form holds (2^31: 16 GB of segments), or the same override as
+// the sort's cap, so that the row-block path can be exercised on small inputs.
+uint64_t max_segment_hits() {
+    const char* e = std::getenv("SEQTREE_B200_SPARSE_BLOCK_HITS");
+    return (e && std::atoll(e) > 0) ? max_block_hits() : (uint64_t(1) << 31);
 }
 
 }  // namespace
@@ -1171,6 +1351,7 @@ void gapblock_sparse_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penal
     const int end_bit = shift + bits_for(N);
     const uint64_t kMaxBlockHits = max_block_hits();
     auto* count = reinterpret_cast<unsigned long long*>(ctx.flags_d + 10);
+    const bool ordered = fast_form_possible(qs, rs, penalty, matrix_size);
 
     // The fast kernel's chunk width and launch form are tuned once per shape, as for the dense
     // matrix, but on a slice of about 2e9 pairs of rows: every variant counts the slice's hits
@@ -1191,12 +1372,24 @@ void gapblock_sparse_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penal
             const uint64_t tcap = std::min<uint64_t>(std::max<uint64_t>(hits.cap_hint, uint64_t(1) << 20),
                                                      kMaxBlockHits);
             SparseSink ts{};
-            ts.keys = ctx.sp_keys.as<unsigned long long>(size_t(tcap));
-            ts.vals = ctx.sp_vals.as<int32_t>(size_t(tcap));
             ts.count = count;
             ts.cap = tcap;
             ts.shift = shift;
             ts.thresh = max_penalty;
+            if (ordered) {
+                // room for hits at up to 1/8 density, so that the variants are timed with their
+                // hit writes (a tile whose hits do not fit only counts them)
+                ts.cap = std::min<uint64_t>(max_segment_hits(),
+                                            std::max<uint64_t>(tcap, uint64_t(tr1) * uint64_t(K) / 8));
+                ts.ordered = 1;
+                ts.seg = ctx.sp_keys.as<int2>(size_t(ts.cap));
+                ts.piece_cap = (tr1 == N ? N : tr1) * ceil_div(K, kRcCandidates[kNumRc - 1]);
+                ts.piece_off = ctx.sp_sorted.as<int64_t>(size_t(ts.piece_cap));
+                ts.piece_cnt = ctx.sp_vals.as<int32_t>(size_t(ts.piece_cap));
+            } else {
+                ts.keys = ctx.sp_keys.as<unsigned long long>(size_t(tcap));
+                ts.vals = ctx.sp_vals.as<int32_t>(size_t(tcap));
+            }
             tuned_run(skey, 2 * kNumRc, -1, [&](int c) {
                 t_force_rc = c >= 0 ? kRcCandidates[c % kNumRc] : 0;
                 t_force_persistent = c >= 0 ? c / kNumRc : -1;
@@ -1213,6 +1406,94 @@ void gapblock_sparse_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* penal
                 t_force_persistent = -1;
             }, stream);
         }
+    }
+
+    if (ordered) {
+        // Ordered form: no sort.  One block of all rows in the usual case; blocks of rows when
+        // the segments (max_segment_hits) or the piece table (2^28 entries) would not hold them.
+        const uint64_t seg_cap_max = max_segment_hits();
+        const int64_t most_chunks = ceil_div(K, kRcCandidates[kNumRc - 1]);
+        const int64_t piece_rows = std::max<int64_t>(1, (int64_t(1) << 28) / most_chunks);
+        int64_t r0 = 0, rows = std::min<int64_t>(
+            hits.block_rows_hint > 0 ? hits.block_rows_hint : N, piece_rows);
+        int64_t first_rows = 0, nblocks = 0, total = 0;
+        uint64_t cap = std::min<uint64_t>(std::max<uint64_t>(hits.cap_hint, uint64_t(1) << 20),
+                                          seg_cap_max);
+        bool exact_retry = false;
+        while (r0 < N) {
+            const int64_t r1 = std::min<int64_t>(N, r0 + rows);
+            SparseSink sink{};
+            sink.ordered = 1;
+            sink.count = count;
+            sink.cap = cap;
+            sink.shift = shift;
+            sink.thresh = max_penalty;
+            sink.seg = ctx.sp_keys.as<int2>(size_t(cap));
+            sink.piece_cap = (r1 - r0) * most_chunks;
+            sink.piece_off = ctx.sp_sorted.as<int64_t>(size_t(sink.piece_cap));
+            sink.piece_cnt = ctx.sp_vals.as<int32_t>(size_t(sink.piece_cap));
+            STB_CUDA(cudaMemsetAsync(ctx.flags_d + 8, 0, 8 * sizeof(int64_t), stream));
+            gapblock_run(qs, rs, penalty, matrix_size, go, ge, prior, prior_len, prior_width,
+                         nullptr, &sink, stream, r0, r1 == N && r0 == 0 ? -1 : r1);
+            STB_CUDA(cudaMemcpyAsync(ctx.flags_h + 8, ctx.flags_d + 8, 8 * sizeof(int64_t),
+                                     cudaMemcpyDeviceToHost, stream));
+            STB_CUDA(cudaStreamSynchronize(stream));
+            if (ctx.flags_h[8] != 0)
+                fail(ST_ETIMEOUT,
+                     "seqtree_b200: a bounded device-side wait gave up (shared-memory staging)");
+            const uint64_t H = static_cast<uint64_t>(ctx.flags_h[10]);
+            if (H > cap) {
+                if (exact_retry) fail(ST_ECUDA, "seqtree_b200: sparse hit count changed between passes");
+                const int64_t nrows = r1 - r0;
+                if (H <= seg_cap_max || nrows == 1) {
+                    cap = H;  // the same block at its exact size (one row holds < 2^31 hits)
+                    exact_retry = true;
+                } else {
+                    const double per_row = double(H) / double(nrows);
+                    rows = std::max<int64_t>(
+                        1, std::min<int64_t>(nrows - 1, int64_t(0.75 * double(seg_cap_max) / per_row)));
+                }
+                continue;
+            }
+            exact_retry = false;
+            const int64_t nrows = r1 - r0;
+            const size_t need = size_t(total + int64_t(H) + 1);
+            hits.ref_ids.grow_keep(need * sizeof(int32_t), size_t(total) * sizeof(int32_t), stream);
+            hits.scores.grow_keep(need * sizeof(int32_t), size_t(total) * sizeof(int32_t), stream);
+            int64_t* rowcnt = ctx.work_b.as<int64_t>(size_t(2 * (nrows + 1)));
+            int64_t* start = rowcnt + (nrows + 1);
+            const unsigned wblocks =
+                unsigned(std::min<int64_t>(ceil_div(nrows * 32, 256), int64_t(ctx.num_sms) * 16));
+            STB_CUDA(cudaMemsetAsync(rowcnt + nrows, 0, sizeof(int64_t), stream));
+            piece_rows_kernel<<<wblocks, 256, 0, stream>>>(sink.piece_cnt, nrows, sink.nchunks,
+                                                           rowcnt);
+            STB_CUDA(cudaGetLastError());
+            size_t temp = 0;
+            STB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, rowcnt, start, int(nrows + 1),
+                                                   stream));
+            void* d_temp = ctx.sp_temp.as<uint8_t>(temp + 16);
+            STB_CUDA(cub::DeviceScan::ExclusiveSum(d_temp, temp, rowcnt, start, int(nrows + 1),
+                                                   stream));
+            piece_copy_kernel<<<wblocks, 256, 0, stream>>>(
+                sink.seg, sink.piece_off, sink.piece_cnt, start, nrows, sink.nchunks, r0, total,
+                indptr, static_cast<int32_t*>(hits.ref_ids.ptr),
+                static_cast<int32_t*>(hits.scores.ptr));
+            STB_CUDA(cudaGetLastError());
+            note_launch(nullptr, 2);
+            total += int64_t(H);
+            if (nblocks++ == 0) first_rows = nrows;
+            const double per_row = double(std::max<uint64_t>(H, 1)) / double(nrows);
+            rows = std::min<int64_t>(piece_rows,
+                                     std::max<int64_t>(1, int64_t(0.75 * double(seg_cap_max) / per_row)));
+            cap = std::min<uint64_t>(
+                std::max<uint64_t>(cap, uint64_t(per_row * double(rows) * 1.25) + 1024), seg_cap_max);
+            r0 = r1;
+        }
+        hits.nnz = total;
+        hits.block_rows_hint = nblocks > 1 ? first_rows : 0;
+        hits.cap_hint = std::max<uint64_t>(
+            hits.cap_hint, std::min<uint64_t>(uint64_t(total) + uint64_t(total) / 8, seg_cap_max));
+        return;
     }
 
     // One block of all rows when the hits fit one sort (the usual case: the set's cached plans

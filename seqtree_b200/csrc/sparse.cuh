@@ -1,5 +1,12 @@
-// Thresholded sparse output of the all-vs-all kernels: the cells whose score passes a threshold,
-// appended as (row << shift | column, score) pairs to a device buffer and later sorted into CSR.
+// Thresholded sparse output of the all-vs-all kernels: the cells whose score passes a threshold.
+// Two forms:
+//   * append: (row << shift | column, score) pairs appended to a device buffer in any order and
+//     later radix-sorted into CSR (any kernel);
+//   * ordered (the fast gap-block kernel): a CTA owns whole (row, column chunk) pieces of the
+//     matrix, so it reserves one contiguous segment for its tile, writes each of its rows' hits
+//     there in ascending column order as (ref id, score), and records where each piece starts and
+//     how many hits it holds.  The CSR is then a prefix sum over the pieces and a segmented copy,
+//     with no sort.
 #pragma once
 
 #include <cstdint>
@@ -13,6 +20,14 @@ struct SparseSink {
     unsigned long long cap = 0;
     int shift = 0;                        // bits of the column index
     int32_t thresh = 0;                   // keep score <= thresh
+    // ordered form (cap counts hits of 8 bytes in seg)
+    int ordered = 0;
+    int2* seg = nullptr;                  // (ref id, score), one segment per tile
+    int64_t* piece_off = nullptr;         // [(row - row0) * nchunks + chunk]: start in seg
+    int32_t* piece_cnt = nullptr;         // [(row - row0) * nchunks + chunk]: hits of the piece
+    int64_t piece_cap = 0;                // entries of piece_off / piece_cnt
+    int64_t row0 = 0;                     // first row of the block
+    int nchunks = 0;                      // column chunks of the plan (set by the launcher)
 };
 
 __device__ __forceinline__ unsigned long long sink_key(const SparseSink& s, int64_t row,

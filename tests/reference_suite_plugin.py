@@ -1,7 +1,8 @@
 """pytest plugin that runs the reference's own hot-path test files against this library.
 
 Loaded with ``-p reference_suite_plugin`` before collection, it installs ``seqtree``,
-``seqtree.gapblock``, ``seqtree.pairwise`` and ``seqtree.distance`` as this library's modules, so a
+``seqtree.gapblock``, ``seqtree.pairwise``, ``seqtree.distance`` and ``seqtree.evalue`` as this
+library's modules, so a
 reference test's ``import seqtree`` / ``from seqtree.gapblock import ...`` binds the drop-in's
 names, defaults, exceptions and buffers unchanged.  The test files themselves are not part of this
 repository: ``tests/test_reference_suite_gpu.py`` points pytest at a copy of the reference's
@@ -29,12 +30,15 @@ SKIP = {
     "test_matrix.py::test_custom_matrix_matches_builtin": OUT_OF_SCOPE,
     "test_matrix.py::test_matrix_size_mismatch_raises": OUT_OF_SCOPE,
     "test_matrix.py::test_collisions_only_with_indels": OUT_OF_SCOPE,
+    "test_gapblock.py::test_index_handles_an_empty_auxiliary_level":
+        "inspects the reference index's private per-deletion-level trie indexes (_var); the "
+        "search it then checks is covered by the other GapBlockIndex tests",
 }
 
 
 def _install() -> None:
     import seqtree_b200 as lib
-    from seqtree_b200 import distance, gapblock, matrix, pairwise
+    from seqtree_b200 import distance, evalue, gapblock, matrix, pairwise
     pkg = types.ModuleType("seqtree")
     pkg.__path__ = []  # a package: submodules come from sys.modules below
     for name in ("SubstitutionMatrix", "ScoreMatrix", "alphabet_symbols", "amino_acids"):
@@ -43,12 +47,16 @@ def _install() -> None:
                  "frame_prior", "gapblock_score", "positions_prior", "profile_prior",
                  "score_matrix"):
         setattr(pkg, name, getattr(gapblock, name))
-    pkg.gapblock, pkg.pairwise, pkg.distance = gapblock, pairwise, distance
+    pkg.gapblock, pkg.pairwise, pkg.distance, pkg.evalue = gapblock, pairwise, distance, evalue
+    for name in ("thetas_from_scores", "evalues", "threshold_for_evalue"):
+        if hasattr(evalue, name):
+            setattr(pkg, name, getattr(evalue, name))
     pkg.__version__ = lib.__version__
     sys.modules["seqtree"] = pkg
     sys.modules["seqtree.gapblock"] = gapblock
     sys.modules["seqtree.pairwise"] = pairwise
     sys.modules["seqtree.distance"] = distance
+    sys.modules["seqtree.evalue"] = evalue
 
 
 _install()
