@@ -24,8 +24,13 @@ namespace stb {
 namespace {
 
 constexpr int64_t kNegInf = INT64_MIN / 4;  // src/pairwise.cpp:37
-// Pairs a first-time tuning of per-thread against wavefront runs each variant on.
+// Pairs a first-time tuning of per-thread against the wavefront (32- or 64-row buckets) runs
+// each variant on.
 constexpr int64_t kAlignTunePairs = int64_t(20) * 1000 * 1000;
+// Pairs a first-time tuning of the wavefront's row-bucket width runs each variant on.
+// A slice much smaller than this holds too few rows per bucket to fill the GPU, and so favours
+// the wider buckets (fewer launches) where the whole matrix favours the narrower ones.
+constexpr int64_t kWaveTunePairs = int64_t(20) * 1000 * 1000;
 
 __device__ __forceinline__ int64_t gap_run(int64_t L, int32_t open, int32_t extend) {
     return L <= 0 ? 0 : int64_t(open) + (L - 1) * int64_t(extend);
@@ -763,9 +768,13 @@ const void* qpair_kernel(int R, bool local, bool exact) {
     }
 }
 
-// Rows per lane of the query-pair kernel: the smallest R with 32 * R >= m (32-row buckets, so a
-// query carries fewer than 32 padded rows).
-int qpair_rows_per_lane(int m) { return std::max(1, int((m + 31) / 32)); }
+// Rows per lane of the query-pair kernel: the smallest R with 32 * R >= m, rounded up to a
+// multiple of `step` (step 1: 32-row buckets, a query carries fewer than 32 padded rows; step 2:
+// 64-row buckets, fewer and larger launches).
+int qpair_rows_per_lane(int m, int step = 1) {
+    const int r = std::max(1, int((m + 31) / 32));
+    return std::min(16, (r + step - 1) / step * step);
+}
 
 constexpr int kRowBuckets[] = {2, 4, 6, 8, 10, 12, 14, 16};
 
@@ -824,8 +833,8 @@ struct WaveState {
 // (R, offset, count) of each group's pairs; and every index sorted by length (the ref side).
 struct WavePlan {
     uint64_t uid = 0;
-    std::vector<std::tuple<int, int64_t, int64_t>> groups, pair_groups;
-    DevBuf list, qpairs, sorted;
+    std::vector<std::tuple<int, int64_t, int64_t>> groups, pair_groups[2];
+    DevBuf list, qpairs[2], sorted;
 };
 
 WavePlan& wave_plan(st_seqset_s& s, Context& ctx, int slot, cudaStream_t stream) {
@@ -848,26 +857,31 @@ WavePlan& wave_plan(st_seqset_s& s, Context& ctx, int slot, cudaStream_t stream)
     std::vector<int32_t> order(static_cast<size_t>(s.count));
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), by_len);
-    std::vector<int32_t> qpairs;
-    qpairs.reserve(size_t(s.count) + 2 * p.groups.size());
-    p.pair_groups.clear();
-    std::vector<std::vector<int32_t>> fine(17);
-    for (int64_t i = 0; i < s.count; ++i)
-        fine[size_t(qpair_rows_per_lane(s.h_len[size_t(i)]))].push_back(int32_t(i));
-    for (int R = 1; R <= 16; ++R) {
-        std::vector<int32_t>& g = fine[size_t(R)];
-        if (g.empty()) continue;
-        std::stable_sort(g.begin(), g.end(), by_len);
-        const int64_t first = int64_t(qpairs.size() / 2);
-        for (size_t i = 0; i < g.size(); i += 2) {
-            qpairs.push_back(g[i]);
-            qpairs.push_back(i + 1 < g.size() ? g[i + 1] : g[i]);
+    // Query pairs per bucket, for both bucket widths (32 and 64 rows; the tuner picks one).
+    std::vector<int32_t> qpairs[2];
+    for (int w = 0; w < 2; ++w) {
+        qpairs[w].reserve(size_t(s.count) + 34);
+        p.pair_groups[w].clear();
+        std::vector<std::vector<int32_t>> fine(17);
+        for (int64_t i = 0; i < s.count; ++i)
+            fine[size_t(qpair_rows_per_lane(s.h_len[size_t(i)], w + 1))].push_back(int32_t(i));
+        for (int R = 1; R <= 16; ++R) {
+            std::vector<int32_t>& g = fine[size_t(R)];
+            if (g.empty()) continue;
+            std::stable_sort(g.begin(), g.end(), by_len);
+            const int64_t first = int64_t(qpairs[w].size() / 2);
+            for (size_t i = 0; i < g.size(); i += 2) {
+                qpairs[w].push_back(g[i]);
+                qpairs[w].push_back(i + 1 < g.size() ? g[i + 1] : g[i]);
+            }
+            p.pair_groups[w].emplace_back(R, first, int64_t(qpairs[w].size() / 2) - first);
         }
-        p.pair_groups.emplace_back(R, first, int64_t(qpairs.size() / 2) - first);
     }
     // (a pageable-source copy has consumed the host vectors by the time it returns)
     h2d(p.list.as<int32_t>(all.size()), all.data(), all.size() * 4, stream);
-    h2d(p.qpairs.as<int32_t>(qpairs.size()), qpairs.data(), qpairs.size() * 4, stream);
+    for (int w = 0; w < 2; ++w)
+        h2d(p.qpairs[w].as<int32_t>(qpairs[w].size()), qpairs[w].data(), qpairs[w].size() * 4,
+            stream);
     h2d(p.sorted.as<int32_t>(order.size()), order.data(), order.size() * 4, stream);
     p.uid = s.uid;
     return p;
@@ -932,7 +946,7 @@ void launch_qpair(QpArgs qa, int R, bool local, bool exact, cudaStream_t stream)
 // The warp-wavefront path for every pair (int16x2 cells; the caller checked wave_eligible).
 void align_wave(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int A, int32_t mode,
                 int32_t go, int32_t ge, int32_t dist, int32_t* out_d, unsigned int* ovf,
-                cudaStream_t stream) {
+                cudaStream_t stream, int bucket = 0) {
     Context& ctx = context();
     const int64_t N = qs.count, K = rs.count;
     WaveState& ws = wave_state(ctx.device);
@@ -1000,18 +1014,19 @@ void align_wave(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
     // The buckets' launches run on side streams forked from (and joined back into) the caller's
     // stream; the longest rows first, so the short buckets fill the long ones' tails.
     ws.ensure_streams();
-    const int nside = std::min<int>(WaveState::kSide, int(qp.pair_groups.size()));
+    const auto& pgroups = qp.pair_groups[bucket];
+    const int nside = std::min<int>(WaveState::kSide, int(pgroups.size()));
     STB_CUDA(cudaEventRecord(ws.fork, stream));
     for (int i = 0; i < nside; ++i) STB_CUDA(cudaStreamWaitEvent(ws.side[i], ws.fork, 0));
     int gi = 0;
-    for (auto it = qp.pair_groups.rbegin(); it != qp.pair_groups.rend(); ++it, ++gi) {
+    for (auto it = pgroups.rbegin(); it != pgroups.rend(); ++it, ++gi) {
         const auto& [R, off, cnt] = *it;
         QpArgs ma{};
         ma.qc = qs.d_bytes;
         ma.qoff = qs.d_off;
         ma.rc = rs.d_bytes;
         ma.roff = rs.d_off;
-        ma.qpairs = static_cast<int2*>(qp.qpairs.ptr) + off;
+        ma.qpairs = static_cast<int2*>(qp.qpairs[bucket].ptr) + off;
         ma.nqp = cnt;
         ma.rorder = static_cast<int32_t*>(rp.sorted.ptr);
         ma.K = K;
@@ -1126,7 +1141,7 @@ void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
                                 "|" + std::to_string(size_bucket(K));
         auto variant = [&](int c, st_seqset_s& q) {
             if (c == 0) run_thread(q);
-            else align_wave(q, rs, similarity, A, mode, go, ge, dist, out_d, ovf, stream);
+            else align_wave(q, rs, similarity, A, mode, go, ge, dist, out_d, ovf, stream, c - 1);
         };
         // A shape seen for the first time is tuned on its first query rows only (about
         // kAlignTunePairs pairs, written into their own rows of the result); the choice then
@@ -1138,13 +1153,31 @@ void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
         if (slice < N && tuning_enabled() && cs == cudaStreamCaptureStatusNone &&
             tuned_lookup(key) < 0) {
             std::unique_ptr<st_seqset_s> view = row_view(qs, slice);
-            tuned_run(key, 2, 0, [&](int c) { variant(c, *view); }, stream);
+            tuned_run(key, 3, 0, [&](int c) { variant(c, *view); }, stream);
         }
-        tuned_run(key, 2, 0, [&](int c) { variant(c, qs); }, stream);
+        tuned_run(key, 3, 0, [&](int c) { variant(c, qs); }, stream);
         return;
     }
     if (wave_ok) {
-        align_wave(qs, rs, similarity, A, mode, go, ge, dist, out_d, ovf, stream);
+        // The row-bucket width (32 or 64 rows) is tuned once per shape, on the first query rows
+        // (about kWaveTunePairs pairs, written into their own rows of the result).
+        const std::string key = "wave|" + std::to_string(mode) + "|" + std::to_string(dist) + "|" +
+                                std::to_string(A) + "|" + std::to_string(qs.max_len) + "|" +
+                                std::to_string(rs.max_len) + "|" + std::to_string(size_bucket(N)) +
+                                "|" + std::to_string(size_bucket(K));
+        auto bucketed = [&](int c, st_seqset_s& q) {
+            align_wave(q, rs, similarity, A, mode, go, ge, dist, out_d, ovf, stream, c);
+        };
+        const int64_t slice = std::min<int64_t>(
+            N, std::max<int64_t>(64, kWaveTunePairs / std::max<int64_t>(K, 1)));
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        STB_CUDA(cudaStreamIsCapturing(stream, &cs));
+        if (slice < N && tuning_enabled() && cs == cudaStreamCaptureStatusNone &&
+            tuned_lookup(key) < 0) {
+            std::unique_ptr<st_seqset_s> view = row_view(qs, slice);
+            tuned_run(key, 2, 0, [&](int c) { bucketed(c, *view); }, stream);
+        }
+        tuned_run(key, 2, 0, [&](int c) { bucketed(c, qs); }, stream);
         return;
     }
 

@@ -251,3 +251,21 @@ def test_first_call_of_a_large_shape_tunes_on_a_slice(pw, B62):
                                   dist=True, threads=os.cpu_count() or 1)
         assert np.array_equal(first[rows], exp)
         assert np.array_equal(first, as_np(pw.dist_matrix(q, r, B62, mode=mode)))
+
+
+def test_first_call_of_a_long_shape_tunes_the_bucket_width_on_a_slice(pw, B62):
+    """2,500 x 10,000 strings of 40-200 residues (2.5e7 pairs) is beyond the 2e7-pair slice on
+    which the wavefront's row-bucket width (32 or 64 rows) is tuned: the first call tunes on the
+    first 2,000 query rows, then runs the chosen width on everything.  Rows inside and past the
+    slice are exact, and the second call (cached width) repeats the first."""
+    rng = np.random.default_rng(79)
+    q, r = rand_seqs(rng, 2500, 40, 200), rand_seqs(rng, 10000, 40, 200)
+    for mode in ("global", "local"):
+        first = as_np(pw.score_matrix(q, r, B62, mode=mode))
+        rows = [0, 1999, 2000, 2499]
+        exp = oracle.align_matrix([q[i] for i in rows], r, B62.similarity_grid, mode=mode,
+                                  threads=os.cpu_count() or 1)
+        assert np.array_equal(first[rows], exp)
+        assert np.array_equal(first, as_np(pw.score_matrix(q, r, B62, mode=mode)))
+    from seqtree_b200 import _lib
+    assert "wave|" in _lib.tuning_table() or os.environ.get("SEQTREE_B200_TUNE") == "0"
