@@ -780,10 +780,11 @@ def measure_learned(args, world, rank, local):
     """Learned proposal + exact rescore on 1M x 1M CDR3-like junctions.
 
     Setup (untimed): train the encoder on ``--train-pairs`` seeded pairs labelled by the exact
-    kernel, embed the refs, calibrate the fallback lengths on 4,000 held-out queries (seed 2).
-    A timed step re-embeds the refs and answers all queries: embed, propose top-256, exact
-    rescore, exhaustive fallback parts, CSR merge.  ``value`` = nq * nr / step time (effective
-    pairs/s).  Recall is measured on the first 2,000 workload queries against the exhaustive
+    kernel, embed the refs, calibrate on 4,000 held-out queries (seed 2): the threshold form's
+    per-cell thresholds and fallback lengths (``--proposal range``, the default) or the top-256
+    form's fallback lengths (``--proposal topk``).  A timed step re-embeds the refs and answers
+    all queries: embed, propose, exact rescore, exhaustive fallback parts, CSR merge.  ``value``
+    = nq * nr / step time (effective pairs/s).  Recall is measured on the first 2,000 workload queries against the exhaustive
     kernel; the exhaustive kernel's own pairs/s on 20,000 queries x all refs is reported beside.
     """
     import torch
@@ -806,7 +807,7 @@ def measure_learned(args, world, rank, local):
         enc = Ln.Encoder(params)
     train_s = time.perf_counter() - t0
     idx = Ln.LearnedIndex(enc, w["r_codes"], w["r_lens"], matrix=M, gap_open=8, max_penalty=24,
-                          k=256)
+                          k=256, proposal=args.proposal)
     cc, cl = W.cdr3_codes(2, 4000)
     cal = idx.calibrate(cc, cl, bound=0.99)
     qb = idx.queries(w["q_codes"], w["q_lens"])
@@ -888,25 +889,37 @@ def measure_learned(args, world, rank, local):
         return None
     plans = None
     if not args.no_plans:
+        other = "topk" if args.proposal == "range" else "range"
         plans = {"bound_0.99": learned_plans(w, M, (cc, cl), ne, 0.99, [
-            ("fallback_only", None, 0, None), ("untrained_encoder", Ln.Encoder(seed=0), 256, None),
-            ("trained_encoder_band_1", enc, 256, 1)])}
-        plans["bound_0.99"]["trained_encoder"] = {
+            ("fallback_only", None, 0, None, "topk"),
+            ("untrained_encoder", Ln.Encoder(seed=0), 256, None, args.proposal),
+            (f"trained_encoder_{other}", enc, 256, 1 if other == "topk" else None, other)])}
+        plans["bound_0.99"][f"trained_encoder_{args.proposal}"] = {
             "ms_per_step": total_ms / args.steps, "effective_pairs_per_s": value / world,
             "recall": rec["recall"], "exhaustive_share": cal["exhaustive_share"],
-            "query_fallback": cal["query_fallback"], "ref_fallback": cal["ref_fallback"]}
+            "query_fallback": cal["query_fallback"], "ref_fallback": cal["ref_fallback"],
+            "the_timed_line": True}
         plans["bound_0.999"] = learned_plans(w, M, (cc, cl), ne, 0.999, [
-            ("fallback_only", None, 0, None), ("trained_encoder", enc, 256, None)])
+            ("fallback_only", None, 0, None, "topk"),
+            (f"trained_encoder_{args.proposal}", enc, 256, None, args.proposal)])
     e2e_s = statistics.median(e2e_times) if e2e_times else float("nan")
     prop_s = phase_ms.get("embed->propose", float("nan")) / 1e3
     n_lq, n_lr = len(qb.learn_rows), idx.n_learn
-    flops = 2.0 * 64 * n_lq * n_lr
+    if args.proposal == "range":  # the pairs the threshold form's tile ranges scan
+        rg = qb.range_tiles(idx).view(-1, 2).cpu().numpy().astype(np.int64)
+        rows = np.minimum(Ln.QUERY_TILE, n_lq - Ln.QUERY_TILE * np.arange(len(rg)))
+        cols = np.minimum(rg[:, 1] * Ln.REF_TILE, n_lr) - np.minimum(rg[:, 0] * Ln.REF_TILE, n_lr)
+        scanned = float((rows * np.maximum(cols, 0)).sum())
+    else:
+        scanned = float(n_lq) * n_lr
+    flops = 2.0 * 64 * scanned
     achieved = flops / prop_s / 1e12 if prop_s > 0 else None
     peak, peak_src = FALLBACK_BF16_TFLOPS, "fallback"
     try:
         peak, peak_src = float(json.loads(PEAKS_FILE.read_text())["bf16_tflops"]), "measured"
     except Exception:
         pass
+    kernel = "propose_range_kernel" if args.proposal == "range" else "propose_topk_kernel"
     line = {
         "metric": w["metric"], "value": value, "unit": "pairs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -917,20 +930,23 @@ def measure_learned(args, world, rank, local):
         "recall": rec["recall"], "recall_found": rec["found"], "recall_exact": rec["exact"],
         "recall_hits_all_exact": rec["subset_of_exact"],
         "recall_by_region": region_recall(rec["found_cells"], rec["exact_cells"]),
-        "calibration": {k: v for k, v in cal.items() if k != "cells_no_fallback"},
+        "calibration": {k: v for k, v in cal.items()
+                        if k not in ("cells_no_fallback", "candidate_cells", "levels")},
         "exhaustive_pairs_per_s": exh_rate, "speedup_vs_exhaustive": value / world / exh_rate,
         "phase_ms": phase_ms, "train_seconds": train_s,
         "plans": plans,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if achieved else None, "traffic": None,
-                     "note": "propose_topk_kernel: 2*64 flops per (learned query, learned ref) "
-                             f"pair / its phase time; peak = cuBLAS bf16 burst (of {peak_src})"},
+                     "note": f"{kernel}: 2*64 flops per scanned (learned query, learned ref) "
+                             f"pair / its phase time; peak = cuBLAS bf16 burst (of {peak_src})",
+                     "scanned_pairs": scanned},
         "e2e": {"value": nq * nr / e2e_s, "unit": "pairs/s",
                 "h2d_bytes_per_step": int(sum(map(len, w["queries"])) + 8 * nq),
                 "d2h_bytes_per_step": int(8 * (nq + 1) + 8 * e2e_nnz),
                 "seconds_per_step": e2e_s},
         "gpu_launches": int(launches * args.steps),
-        "kernel": "propose_topk_kernel",
+        "kernel": kernel,
+        "proposal": args.proposal,
         "cuda_graph": False,
         "clocks": sampler.summary(),
     }
@@ -967,18 +983,19 @@ def region_recall(found_cells, exact_cells) -> dict:
 
 def learned_plans(w, M, cal, rec_n: int, bound: float, plans, steps: int = 3) -> dict:
     """What the encoder earns: the same search, calibrated to the same recall ``bound`` on the
-    same held-out batch, for each ``(name, encoder, k, band)`` of ``plans`` -- ``k = 0`` is the
-    method without the network (the calibrated exhaustive fallback alone); ``band`` limits each
-    query's proposals to refs within that many residues of its length.  Each plan reports its step
+    same held-out batch, for each ``(name, encoder, k, band, proposal)`` of ``plans`` -- ``k = 0``
+    is the method without the network (the calibrated exhaustive fallback alone); ``band`` limits
+    each top-k query's proposals to refs within that many residues of its length; ``proposal`` is
+    the top-k or the threshold form.  Each plan reports its step
     time over all queries (refs re-embedded, as in the timed steps), the effective pairs/s, the
     recall on the first ``rec_n`` workload queries and the share of pairs scored exhaustively."""
     import torch
 
     from seqtree_b200 import learned as Ln
     out = {}
-    for name, enc, k, band in plans:
+    for name, enc, k, band, proposal in plans:
         idx = Ln.LearnedIndex(enc, w["r_codes"], w["r_lens"], matrix=M, gap_open=8,
-                              max_penalty=24, k=k, band=band)
+                              max_penalty=24, k=k, band=band, proposal=proposal)
         cal_res = idx.calibrate(*cal, bound=bound)
         qb = idx.queries(w["q_codes"], w["q_lens"])
         idx.embed_refs()
@@ -1001,7 +1018,8 @@ def learned_plans(w, M, cal, rec_n: int, bound: float, plans, steps: int = 3) ->
                      "recall": rec["recall"], "exhaustive_share": cal_res["exhaustive_share"],
                      "recall_by_region": region_recall(rec["found_cells"], rec["exact_cells"]),
                      "query_fallback": cal_res["query_fallback"],
-                     "ref_fallback": cal_res["ref_fallback"]}
+                     "ref_fallback": cal_res["ref_fallback"],
+                     "candidates_per_query": cal_res.get("candidates_per_query")}
         del idx, qb
         torch.cuda.empty_cache()
     return out
@@ -1025,6 +1043,8 @@ def main(argv=None) -> int:
     ap.add_argument("--soak-seconds", type=float, default=1.5,
                     help="graph replays after the timed steps, for the clock record")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--proposal", choices=["range", "topk"], default="range",
+                    help="learned workload: threshold (range) or top-256 proposals")
     ap.add_argument("--no-plans", action="store_true",
                     help="learned workload: skip the without-network / untrained comparison")
     ap.add_argument("--no-graph", action="store_true", help="time eager launches instead")

@@ -306,6 +306,31 @@ int32_t st_propose_topk_ranges(const void *query_emb, int64_t nq, const void *re
                                int32_t k, const int32_t *tile_ranges_device, int32_t *ids_device,
                                float *scores_device, void *cuda_stream, st_error *err);
 
+/* Learned candidate proposal by threshold (no counterpart in the reference): every (query, ref)
+ * pair whose embedding dot product is >= thresholds[query_len * 33 + ref_len], where the lengths
+ * come from query_lens_device[q] / ref_lens_device[r] (device uint8; lengths above 32 use row or
+ * column 32) and thresholds is a host float [33][33] table (+inf switches a length cell off).
+ * Embeddings as for st_propose_topk.  tile_ranges_device may be NULL (every ref tile) or limit
+ * each tile of 256 queries to ref tiles of 128 refs as st_propose_topk_ranges does.  The pairs
+ * found first (in no particular order) are written to pair_query_device / pair_ref_device (device
+ * int32, capacity entries each); *count receives how many pairs pass in all, so a count above
+ * capacity means the call should be repeated with room for that many.  Synchronous: returns when
+ * the pairs are written.  The candidate pairs are meant to be rescored by the exact gap-block
+ * kernel (st_gapblock_pairs_sets). */
+int32_t st_propose_range(const void *query_emb, int64_t nq, const uint8_t *query_lens_device,
+                         const void *ref_emb, int64_t nr, const uint8_t *ref_lens_device,
+                         const float *thresholds, const int32_t *tile_ranges_device,
+                         int32_t *pair_query_device, int32_t *pair_ref_device, int64_t capacity,
+                         int64_t *count, void *cuda_stream, st_error *err);
+
+/* Dot products of listed pairs of layout-1 embeddings (no counterpart in the reference):
+ * out_device[i] = <query_emb[query_idx_device[i]], ref_emb[ref_idx_device[i]]> in fp32, NaN for
+ * an index outside [0, nq) / [0, nr).  Used to calibrate st_propose_range's thresholds on known
+ * hits.  Asynchronous on cuda_stream. */
+int32_t st_embed_dots(const void *query_emb, int64_t nq, const void *ref_emb, int64_t nr,
+                      const int32_t *query_idx_device, const int32_t *ref_idx_device, int64_t n,
+                      float *out_device, void *cuda_stream, st_error *err);
+
 /* Per-row score cutoffs for a target E-value: thetas_from_scores of seqtree's
  * python/seqtree/evalue.py:102-143 (with _theta, :86-99) over CSR rows of control hit scores in
  * device memory (indptr_device rows + 1 int64, scores_device int32; row order within a row is

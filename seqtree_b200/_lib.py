@@ -119,6 +119,13 @@ SIGNATURES = [
     ("st_propose_topk_ranges", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _ep]),
+    ("st_propose_range", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+      ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p, _ep]),
+    ("st_embed_dots", ctypes.c_int32,
+     [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+      ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, _ep]),
     ("st_stream_status", ctypes.c_int32, [ctypes.c_void_p, _ep]),
     ("st_align_pairs_sets", ctypes.c_int32,
      [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, _i32p,

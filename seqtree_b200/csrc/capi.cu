@@ -46,6 +46,11 @@ void encoder_embed(Encoder& m, const st_seqset_s& set, void* out, int layout, cu
 void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, int k, int32_t* ids,
                   float* scores, cudaStream_t stream,
                   const int32_t* ranges = nullptr);
+int64_t propose_range(const void* qemb, int64_t nq, const uint8_t* qlens, const void* remb,
+                      int64_t nr, const uint8_t* rlens, const float* thr, int32_t* pq, int32_t* pr,
+                      int64_t cap, cudaStream_t stream, const int32_t* ranges);
+void embed_dots(const void* qemb, int64_t nq, const void* remb, int64_t nr, const int32_t* qi,
+                const int32_t* ri, int64_t n, float* out, cudaStream_t stream);
 void profile_scores(const int32_t* table, int32_t width, int32_t c, uint8_t gap, int32_t unreachable,
                     const st_seqset_s& set, int32_t* out_d, cudaStream_t stream);
 void align_pairs_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* qi_d, const int32_t* ri_d,
@@ -908,6 +913,34 @@ int32_t st_propose_topk_ranges(const void* query_emb, int64_t nq, const void* re
         std::lock_guard<std::mutex> lk(ctx.mu);
         propose_topk(query_emb, nq, ref_emb, nr, k, ids_device, scores_device,
                      static_cast<cudaStream_t>(cuda_stream), tile_ranges_device);
+    });
+}
+
+int32_t st_propose_range(const void* query_emb, int64_t nq, const uint8_t* query_lens_device,
+                         const void* ref_emb, int64_t nr, const uint8_t* ref_lens_device,
+                         const float* thresholds, const int32_t* tile_ranges_device,
+                         int32_t* pair_query_device, int32_t* pair_ref_device, int64_t capacity,
+                         int64_t* count, void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        if (!count) fail(ST_EINVAL, "seqtree_b200: null count");
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        *count = propose_range(query_emb, nq, query_lens_device, ref_emb, nr, ref_lens_device,
+                               thresholds, pair_query_device, pair_ref_device, capacity,
+                               static_cast<cudaStream_t>(cuda_stream), tile_ranges_device);
+    });
+}
+
+int32_t st_embed_dots(const void* query_emb, int64_t nq, const void* ref_emb, int64_t nr,
+                      const int32_t* query_idx_device, const int32_t* ref_idx_device, int64_t n,
+                      float* out_device, void* cuda_stream, st_error* err) {
+    return guard(err, [&] {
+        reset_launches();
+        Context& ctx = context();
+        std::lock_guard<std::mutex> lk(ctx.mu);
+        embed_dots(query_emb, nq, ref_emb, nr, query_idx_device, ref_idx_device, n, out_device,
+                   static_cast<cudaStream_t>(cuda_stream));
     });
 }
 

@@ -82,8 +82,9 @@ struct Context {
     DevBuf out_buf, q_codes, r_codes, table_buf, prior_buf, ftab_buf, work_a, work_b, work_c;
     // sparse output: unsorted hit keys and scores, sorted keys, radix-sort scratch
     DevBuf sp_keys, sp_vals, sp_sorted, sp_temp;
-    // candidate lists of the learned-proposal kernel
-    DevBuf topk_cand;
+    // candidate lists of the learned-proposal kernel; the threshold form's table
+    DevBuf topk_cand, prop_thr;
+    std::vector<uint8_t> prop_thr_key;
     // bf16 operands of the training GEMM, packed in the tensor-core layout
     DevBuf gemm_a, gemm_b;
     // storage of the transient sets made by the host-buffer entry points

@@ -31,6 +31,12 @@
 // top-k under that order.  Every wait is bounded (a few seconds of %globaltimer); on time-out
 // the CTA records the failure, drains its copies and MMAs with bounded waits, frees TMEM and
 // returns.
+//
+// The threshold form (propose_range_kernel) keeps the producer and MMA warps and replaces the
+// selection: a pair is proposed when its score reaches the threshold of its (query length, ref
+// length) cell, read from a 33 x 33 table staged in shared memory.  Nothing is kept per query, so
+// a group without a survivor costs one TMEM load, one max tree and one vote, and survivors are
+// appended with one atomicAdd per warp.
 #include <cuda_bf16.h>
 
 #include <cfloat>
@@ -69,6 +75,8 @@ constexpr size_t kSmemBytes = size_t(kSmTotal) + 1024;    // + alignment slack
 constexpr uint32_t kIdesc = idesc_bf16(128, kRT);
 
 
+constexpr int kLenSlots = 33;                  // lengths 0..32 of the threshold table
+
 struct ProposeArgs {
     const uint8_t* qemb;
     const uint8_t* remb;
@@ -79,6 +87,14 @@ struct ProposeArgs {
     int32_t* out_ids;          // [nq][k]
     float* out_scores;         // [nq][k] or null
     unsigned long long* err;
+    // threshold form
+    const uint8_t* qlens;      // [nq] query lengths
+    const uint8_t* rlens;      // [nr] ref lengths
+    const float* thr;          // [kLenSlots][kLenSlots] dot-product threshold per length cell
+    int32_t* pair_q;           // [cap] proposed pairs: query index
+    int32_t* pair_r;           // [cap] proposed pairs: ref index
+    unsigned long long cap;
+    unsigned long long* count; // every proposed pair counted, the first cap written
 };
 
 // The ref tiles a query tile scans: the caller's [first, last) clamped into [0, ntr), so every
@@ -233,7 +249,11 @@ __device__ void warp_sort256_desc(unsigned long long* s, int lane) {
 }
 
 // ------------------------------------------------------------------------ kernel ------------
-__global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a) {
+// The body of both proposal kernels: the producer and MMA warps are shared; the selection warps
+// keep a running top-k (RANGE false) or append every pair at or above its length cell's
+// threshold (RANGE true).
+template <bool RANGE>
+__device__ __forceinline__ void propose_body(const ProposeArgs& a) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((uintptr_t(smem_raw) + 1023) & ~uintptr_t(1023));
     unsigned long long* bars = reinterpret_cast<unsigned long long*>(smem + kSmBar);
@@ -267,6 +287,11 @@ __global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a
                          smem_u32(s_tmem)),
                      "r"(kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if constexpr (RANGE) {
+        // the threshold table, in the selection warps' scratch (unused by this form)
+        float* thr_s = reinterpret_cast<float*>(smem + kSmWarp);
+        for (int i = threadIdx.x; i < kLenSlots * kLenSlots; i += kThreads) thr_s[i] = a.thr[i];
     }
     tc_fence_before();
     __syncthreads();
@@ -352,7 +377,127 @@ __global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a
         }
         tc_commit(BAR(18));
         bar_drain(BAR(18), 0);
-    } else if (warp >= 2) {
+    } else if (RANGE && warp >= 2) {
+        // ------------------------------------------------------ threshold selection -------
+        // Lane = query row, as below.  Each lane also loads one column's ref length and a warp
+        // vote tells whether the 32-column group has a single length (nearly every group when
+        // the refs are sorted by length; any order is correct).  Such a group is rejected by one
+        // 3-input max tree against the row's threshold for that length; otherwise each column's
+        // threshold is looked up with its length taken by shuffle.  Survivors are appended
+        // warp-aggregated: one atomicAdd per warp and group with any survivor, then each lane
+        // writes its pairs.
+        const int ew = warp - 2, grp = ew >> 2, quarter = warp & 3;
+        const int row = quarter * 32 + lane;
+        const float* thr_s = reinterpret_cast<const float*>(smem + kSmWarp);
+        const uint32_t tlane = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(grp) * 128u;
+        uint32_t acc = 0, accphase = 0;
+        bool ok = true;
+        for (int64_t qt = blockIdx.x; qt < ntq && ok; qt += gridDim.x) {
+            const int64_t q = qt * kQT + grp * 128 + row;
+            const bool qvalid = q < a.nq;
+            const int ql = qvalid ? min(int(a.qlens[q]), kLenSlots - 1) : 0;
+            const float* trow = thr_s + ql * kLenSlots;
+            const int64_t rt0 = tile_first(a, qt, ntr), rt1 = tile_last(a, qt, ntr);
+            // One 32-column group: survivor mask against the row's thresholds, then the
+            // warp-aggregated append.  `lcol` is this lane's column length (-1 past the refs).
+            auto group = [&](const uint32_t (&v)[32], int lcol, int64_t cb, int nv) {
+                const uint32_t vmask = nv >= 32 ? 0xFFFFFFFFu : ((1u << nv) - 1u);
+                const int l0 = __shfl_sync(0xFFFFFFFFu, lcol, 0);
+                uint32_t mask = 0;
+                if (__all_sync(0xFFFFFFFFu, lcol == l0 || lcol < 0)) {
+                    const float t = trow[l0];
+                    float m[11];
+#pragma unroll
+                    for (int j = 0; j < 10; ++j)
+                        m[j] = fmax3(__uint_as_float(v[3 * j]), __uint_as_float(v[3 * j + 1]),
+                                     __uint_as_float(v[3 * j + 2]));
+                    m[10] = fmaxf(__uint_as_float(v[30]), __uint_as_float(v[31]));
+                    const float mx = fmaxf(fmax3(fmax3(m[0], m[1], m[2]), fmax3(m[3], m[4], m[5]),
+                                                 fmax3(m[6], m[7], m[8])),
+                                           fmax3(m[9], m[10], -INFINITY));
+                    if (mx >= t) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            mask |= (__uint_as_float(v[j]) >= t) ? (1u << j) : 0u;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int lj = __shfl_sync(0xFFFFFFFFu, lcol, j);
+                        if (lj >= 0) mask |= (__uint_as_float(v[j]) >= trow[lj]) ? (1u << j) : 0u;
+                    }
+                }
+                mask = qvalid ? (mask & vmask) : 0u;
+                if (__any_sync(0xFFFFFFFFu, mask != 0u)) {
+                    const uint32_t n = __popc(mask);
+                    uint32_t incl = n;
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                        if (lane >= o) incl += t;
+                    }
+                    const uint32_t tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+                    unsigned long long base = 0;
+                    if (lane == 31) base = atomicAdd(a.count, (unsigned long long)tot);
+                    base = __shfl_sync(0xFFFFFFFFu, base, 31);
+                    unsigned long long pos = base + (incl - n);
+                    while (mask) {
+                        const int j = __ffs(mask) - 1;
+                        mask &= mask - 1;
+                        if (pos < a.cap) {
+                            a.pair_q[pos] = int32_t(q);
+                            a.pair_r[pos] = int32_t(cb + j);
+                        }
+                        ++pos;
+                    }
+                }
+            };
+            for (int64_t rt = rt0; rt < rt1; ++rt) {
+                const int64_t r0 = rt * kRT;
+                const int nvalid = int((a.nr - r0 < kRT ? a.nr - r0 : kRT));
+                // the tile's column lengths (lane l: columns l, l+32, l+64, l+96), requested
+                // before the accumulator wait so that their latency hides behind it
+                int lc[kRT / 32];
+#pragma unroll
+                for (int g = 0; g < kRT / 32; ++g) {
+                    const int col = g * 32 + lane;
+                    lc[g] = col < nvalid ? min(int(a.rlens[r0 + col]), kLenSlots - 1) : -1;
+                }
+                if (!bar_wait(BAR(14 + acc), accphase, s_abort, a.err)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                // groups c = 0..3, the TMEM load of group c + 1 in flight while c is examined
+                uint32_t va[32], vb[32];
+                const uint32_t tbase = tlane + acc * 256u;
+                __syncwarp();
+                tmem_ld32_issue(tbase, va);
+                tmem_ld32_wait(va);
+                if (nvalid > 32) tmem_ld32_issue(tbase + 32u, vb);
+                group(va, lc[0], r0, nvalid);
+                if (nvalid > 32) {
+                    tmem_ld32_wait(vb);
+                    if (nvalid > 64) tmem_ld32_issue(tbase + 64u, va);
+                    group(vb, lc[1], r0 + 32, nvalid - 32);
+                }
+                if (nvalid > 64) {
+                    tmem_ld32_wait(va);
+                    if (nvalid > 96) tmem_ld32_issue(tbase + 96u, vb);
+                    group(va, lc[2], r0 + 64, nvalid - 64);
+                }
+                if (nvalid > 96) {
+                    tmem_ld32_wait(vb);
+                    group(vb, lc[3], r0 + 96, nvalid - 96);
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) bar_arrive(BAR(16 + acc));
+                acc ^= 1u;
+                if (acc == 0) accphase ^= 1u;
+            }
+        }
+    } else if (!RANGE && warp >= 2) {
         // --------------------------------------------------------------- selection --------
         const int ew = warp - 2, grp = ew >> 2, quarter = warp & 3;
         const int row = quarter * 32 + lane;
@@ -474,6 +619,44 @@ __global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a
     }
 }
 
+__global__ void __launch_bounds__(kThreads, 1) propose_topk_kernel(ProposeArgs a) {
+    propose_body<false>(a);
+}
+
+__global__ void __launch_bounds__(kThreads, 1) propose_range_kernel(ProposeArgs a) {
+    propose_body<true>(a);
+}
+
+// Dot products of listed (query, ref) pairs of swizzled bf16 embeddings, one thread per pair,
+// fp32 accumulation in chunk order.  An index outside its embedding set gives NaN.
+__global__ void embed_dots_kernel(const uint4* __restrict__ qemb, int64_t nq,
+                                  const uint4* __restrict__ remb, int64_t nr,
+                                  const int32_t* __restrict__ qi, const int32_t* __restrict__ ri,
+                                  int64_t n, float* __restrict__ out) {
+    const int64_t p = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const int64_t a = qi[p], b = ri[p];
+    if (a < 0 || a >= nq || b < 0 || b >= nr) {
+        out[p] = __int_as_float(0x7FC00000);
+        return;
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const uint4 x = qemb[a * 8 + (c ^ int(a & 7))];
+        const uint4 y = remb[b * 8 + (c ^ int(b & 7))];
+        const uint32_t xs[4] = {x.x, x.y, x.z, x.w}, ys[4] = {y.x, y.y, y.z, y.w};
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+            const float2 fx = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&xs[w]));
+            const float2 fy = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&ys[w]));
+            s = fmaf(fx.x, fy.x, s);
+            s = fmaf(fx.y, fy.y, s);
+        }
+    }
+    out[p] = s;
+}
+
 }  // namespace
 
 // Top-k refs of every query by dot product of the swizzled bf16 embeddings (device memory, 16-byte
@@ -492,7 +675,7 @@ void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, in
     ensure_smem_limit(reinterpret_cast<const void*>(propose_topk_kernel), kSmemBytes);
     const int64_t ntq = (nq + kQT - 1) / kQT;
     const int grid = int(std::min<int64_t>(ntq, ctx.num_sms));
-    ProposeArgs a;
+    ProposeArgs a{};
     a.qemb = static_cast<const uint8_t*>(qemb);
     a.remb = static_cast<const uint8_t*>(remb);
     a.nq = nq;
@@ -506,6 +689,74 @@ void propose_topk(const void* qemb, int64_t nq, const void* remb, int64_t nr, in
     propose_topk_kernel<<<grid, kThreads, kSmemBytes, stream>>>(a);
     STB_CUDA(cudaGetLastError());
     note_launch("propose_topk_kernel");
+}
+
+// Every (query, ref) pair whose embedding dot product is >= thr[qlen][rlen] (host float
+// [33][33]; lengths above 32 use row / column 32).  Writes the first `cap` pairs found (in no
+// particular order) to pq / pr and returns how many pairs pass in all.  Synchronous on `stream`.
+int64_t propose_range(const void* qemb, int64_t nq, const uint8_t* qlens, const void* remb,
+                      int64_t nr, const uint8_t* rlens, const float* thr, int32_t* pq, int32_t* pr,
+                      int64_t cap, cudaStream_t stream, const int32_t* ranges) {
+    if (nq < 0 || nr < 0) fail(ST_EINVAL, "seqtree_b200: negative embedding count");
+    if (cap < 0) fail(ST_EINVAL, "seqtree_b200: negative pair capacity");
+    if (nq >= (int64_t(1) << 31) || nr >= (int64_t(1) << 31))
+        fail(ST_EINVAL, "seqtree_b200: at most 2^31 - 1 queries and refs");
+    if (!thr) fail(ST_EINVAL, "seqtree_b200: null threshold table");
+    if (nq == 0 || nr == 0) return 0;
+    if (!qemb || !remb || !qlens || !rlens || (cap > 0 && (!pq || !pr)))
+        fail(ST_EINVAL, "seqtree_b200: null embedding, length or output");
+    if ((uintptr_t(qemb) | uintptr_t(remb)) & 15)
+        fail(ST_EINVAL, "seqtree_b200: embeddings must be 16-byte aligned");
+    Context& ctx = context();
+    constexpr size_t kThrBytes = sizeof(float) * kLenSlots * kLenSlots;
+    float* d_thr = ctx.prop_thr.as<float>(kLenSlots * kLenSlots);
+    if (!same_as_last(ctx.prop_thr_key, thr, kThrBytes)) h2d(d_thr, thr, kThrBytes, stream);
+    ensure_smem_limit(reinterpret_cast<const void*>(propose_range_kernel), kSmemBytes);
+    const int64_t ntq = (nq + kQT - 1) / kQT;
+    const int grid = int(std::min<int64_t>(ntq, ctx.num_sms));
+    ProposeArgs a{};
+    a.qemb = static_cast<const uint8_t*>(qemb);
+    a.remb = static_cast<const uint8_t*>(remb);
+    a.nq = nq;
+    a.nr = nr;
+    a.ranges = ranges;
+    a.err = reinterpret_cast<unsigned long long*>(ctx.flags_d + 8);
+    a.qlens = qlens;
+    a.rlens = rlens;
+    a.thr = d_thr;
+    a.pair_q = pq;
+    a.pair_r = pr;
+    a.cap = static_cast<unsigned long long>(cap);
+    a.count = reinterpret_cast<unsigned long long*>(ctx.flags_d + 11);
+    STB_CUDA(cudaMemsetAsync(ctx.flags_d + 8, 0, 8 * sizeof(int64_t), stream));
+    propose_range_kernel<<<grid, kThreads, kSmemBytes, stream>>>(a);
+    STB_CUDA(cudaGetLastError());
+    note_launch("propose_range_kernel");
+    STB_CUDA(cudaMemcpyAsync(ctx.flags_h + 8, ctx.flags_d + 8, 8 * sizeof(int64_t),
+                             cudaMemcpyDeviceToHost, stream));
+    STB_CUDA(cudaStreamSynchronize(stream));
+    if (ctx.flags_h[8] != 0)
+        fail(ST_ETIMEOUT, "seqtree_b200: a bounded device-side wait gave up (proposal)");
+    return ctx.flags_h[11];
+}
+
+// Dot products of listed pairs of swizzled bf16 embeddings (asynchronous on `stream`).
+void embed_dots(const void* qemb, int64_t nq, const void* remb, int64_t nr, const int32_t* qi,
+                const int32_t* ri, int64_t n, float* out, cudaStream_t stream) {
+    if (nq < 0 || nr < 0 || n < 0) fail(ST_EINVAL, "seqtree_b200: negative count");
+    if (n == 0) return;
+    if (!qemb || !remb || !qi || !ri || !out)
+        fail(ST_EINVAL, "seqtree_b200: null embedding, index or output");
+    if ((uintptr_t(qemb) | uintptr_t(remb)) & 15)
+        fail(ST_EINVAL, "seqtree_b200: embeddings must be 16-byte aligned");
+    context();
+    const int threads = 256;
+    const int64_t blocks = (n + threads - 1) / threads;
+    if (blocks > 0x7FFFFFFF) fail(ST_EINVAL, "seqtree_b200: too many pairs for one call");
+    embed_dots_kernel<<<unsigned(blocks), threads, 0, stream>>>(
+        static_cast<const uint4*>(qemb), nq, static_cast<const uint4*>(remb), nr, qi, ri, n, out);
+    STB_CUDA(cudaGetLastError());
+    note_launch("embed_dots_kernel");
 }
 
 }  // namespace stb

@@ -271,6 +271,88 @@ def propose_topk_into(q_ptr: int, nq: int, r_ptr: int, nr: int, k: int, ids_ptr:
 QUERY_TILE, REF_TILE = 256, 128  # the proposal kernel's tile heights
 
 
+def propose_range_into(q_ptr: int, nq: int, qlens_ptr: int, r_ptr: int, nr: int, rlens_ptr: int,
+                       thresholds: np.ndarray, pq_ptr: int, pr_ptr: int, capacity: int,
+                       stream: int = 0, ranges_ptr: int = 0) -> int:
+    """``st_propose_range`` on device pointers: writes up to ``capacity`` (query, ref) pairs whose
+    dot product reaches ``thresholds[qlen, rlen]`` (float32 [33, 33]) and returns how many pass in
+    all (synchronous)."""
+    thr = np.ascontiguousarray(thresholds, np.float32)
+    if thr.shape != (PAD + 1, PAD + 1):
+        raise ValueError("thresholds must be float32 [33, 33]")
+    count = ctypes.c_int64()
+    err = _lib.st_error()
+    _lib.check(_lib.lib.st_propose_range(
+        ctypes.c_void_p(q_ptr), int(nq), ctypes.c_void_p(qlens_ptr), ctypes.c_void_p(r_ptr),
+        int(nr), ctypes.c_void_p(rlens_ptr), thr.ctypes.data, ctypes.c_void_p(ranges_ptr or None),
+        ctypes.c_void_p(pq_ptr or None), ctypes.c_void_p(pr_ptr or None), int(capacity),
+        ctypes.byref(count), ctypes.c_void_p(stream), ctypes.byref(err)), err)
+    return int(count.value)
+
+
+def embed_dots_into(q_ptr: int, nq: int, r_ptr: int, nr: int, qi_ptr: int, ri_ptr: int, n: int,
+                    out_ptr: int, stream: int = 0) -> None:
+    """``st_embed_dots``: fp32 dot products of listed pairs of swizzled bf16 embeddings."""
+    err = _lib.st_error()
+    _lib.check(_lib.lib.st_embed_dots(
+        ctypes.c_void_p(q_ptr), int(nq), ctypes.c_void_p(r_ptr), int(nr), ctypes.c_void_p(qi_ptr),
+        ctypes.c_void_p(ri_ptr), int(n), ctypes.c_void_p(out_ptr), ctypes.c_void_p(stream),
+        ctypes.byref(err)), err)
+
+
+def propose_range(q_emb, q_lens, r_emb, r_lens, thresholds, capacity: int | None = None,
+                  ranges=None):
+    """Every (query, ref) pair of swizzled bf16 embeddings (torch CUDA [n][64]) whose dot product
+    is >= ``thresholds[len q, len r]``; lengths are uint8 CUDA tensors.  Returns (query idx,
+    ref idx) int32 tensors in no particular order (the call is repeated at the exact size when
+    the first ``capacity`` did not hold every pair)."""
+    import torch
+    nq, nr = q_emb.shape[0], r_emb.shape[0]
+    cap = max(1, nq * 16) if capacity is None else max(1, int(capacity))
+    stream = torch.cuda.current_stream(q_emb.device).cuda_stream
+    while True:
+        pq = torch.empty(cap, dtype=torch.int32, device=q_emb.device)
+        pr = torch.empty(cap, dtype=torch.int32, device=q_emb.device)
+        n = propose_range_into(q_emb.data_ptr(), nq, q_lens.data_ptr(), r_emb.data_ptr(), nr,
+                               r_lens.data_ptr(), thresholds, pq.data_ptr(), pr.data_ptr(), cap,
+                               stream, 0 if ranges is None else ranges.data_ptr())
+        if n <= cap:
+            return pq[:n], pr[:n]
+        cap = n
+
+
+def range_tile_ranges(q_lens_sorted: np.ndarray, r_lens_sorted: np.ndarray,
+                      thresholds: np.ndarray) -> np.ndarray:
+    """Per 256-query tile of length-sorted queries, the [first, last) 128-ref tiles of
+    length-sorted refs spanning every ref length that has a finite threshold for some query length
+    of the tile (int32 [tiles, 2]); tiles without one get an empty range."""
+    q = np.asarray(q_lens_sorted, np.int64)
+    r = np.asarray(r_lens_sorted, np.int64)
+    finite = np.isfinite(np.asarray(thresholds, np.float32))
+    nt = -(-q.size // QUERY_TILE)
+    out = np.zeros((nt, 2), np.int32)
+    for t in range(nt):
+        blk = q[t * QUERY_TILE:(t + 1) * QUERY_TILE]
+        on = finite[np.clip(blk.min(), 0, PAD):np.clip(blk.max(), 0, PAD) + 1].any(axis=0)
+        ls = np.flatnonzero(on)
+        if ls.size == 0:
+            continue
+        lo = np.searchsorted(r, ls[0], side="left")
+        hi = np.searchsorted(r, ls[-1], side="right")
+        out[t] = (lo // REF_TILE, -(-hi // REF_TILE)) if hi > lo else (0, 0)
+    return out
+
+
+# Cost weights of the threshold form's fallback choice, seconds per unit on one B200: an
+# exhaustively scored pair (sparse gap-block kernel), a scanned (query, ref) pair of the threshold
+# proposal kernel, and a rescored candidate pair (pair kernel and its filtering).  Calibration
+# measures the exhaustive and candidate costs on its batch when the batch is large enough to
+# fill the GPU and keeps these otherwise; only the ratios matter to the choice.
+RANGE_COSTS = {"exhaustive": 1 / 3.0e11, "scan": 1 / 4.0e12, "candidate": 1 / 1.0e10}
+# Recall levels a cell's threshold can take (fraction of the cell's calibration hits kept).
+RANGE_LEVELS = (0.5, 0.75, 0.9, 0.95, 0.98, 0.99, 0.995, 1.0)
+
+
 def band_tile_ranges(q_lens_sorted: np.ndarray, r_lens_sorted: np.ndarray, band: int) -> np.ndarray:
     """Per 256-query tile of length-sorted queries, the [first, last) 128-ref tiles of
     length-sorted refs that hold every ref whose length is within ``band`` of a query of the
@@ -488,6 +570,78 @@ def train(enc: Encoder, n_pairs: int, *, seed: int, matrix, gap_open: int, gap_e
     return losses
 
 
+def allocate_recall(E, FL, CL, wq, wr, costs: dict, target: float):
+    """The threshold form's plan: per (query length, ref length) cell a recall level (index into
+    the last axis of ``FL`` / ``CL``, -1 = no proposals) and the query / ref lengths scored
+    exhaustively, chosen greedily until the estimated recall reaches ``target``.
+
+    ``E`` [S, S] holds the calibration batch's exact hits per cell, ``FL`` / ``CL`` [S, S, LV] the
+    hits found and the candidates proposed at each level (non-decreasing along the level axis),
+    ``wq`` / ``wr`` the query and ref counts per length; ``costs`` gives seconds per exhaustively
+    scored pair ("exhaustive"), per scanned pair of a cell with proposals ("scan") and per
+    candidate ("candidate").  Every step takes the move with the most recovered hits per added
+    second: raising one cell by one level, or scoring one query or ref length exhaustively (its
+    cells are then exact and cost their pairs).  Returns (level, query lengths, ref lengths,
+    estimated recall, estimated seconds)."""
+    E = np.asarray(E, np.float64)
+    S, LV = E.shape[0], FL.shape[2]
+    pairs = np.outer(np.asarray(wq, np.float64), np.asarray(wr, np.float64))
+    exh = costs["exhaustive"] * pairs
+    level = np.full((S, S), -1, np.int64)
+    covered = np.zeros((S, S), bool)
+    q_fb, r_fb = [], []
+
+    def at(arr, lv):
+        v = np.take_along_axis(arr, np.clip(lv, 0, LV - 1)[:, :, None], 2)[:, :, 0]
+        return np.where(lv >= 0, v, 0.0)
+
+    def prop_cost(lv):
+        return np.where(lv >= 0, costs["scan"] * pairs + costs["candidate"] * at(CL, lv), 0.0)
+
+    te = E.sum()
+    while te:
+        pc, fnd = prop_cost(level), at(FL, level)
+        if (E[covered].sum() + fnd[~covered].sum()) / te >= target:
+            break
+        best, move = 0.0, None
+        for a, b in zip(*np.where(~covered & (E > 0) & (level < LV - 1))):
+            nl = level[a, b] + 1
+            gain = FL[a, b, nl] - fnd[a, b]
+            dt = costs["candidate"] * (CL[a, b, nl] - (CL[a, b, nl - 1] if nl > 0 else 0.0))
+            if nl == 0:
+                dt += costs["scan"] * pairs[a, b]
+            if gain > 0 and gain / max(dt, 1e-15) > best:
+                best, move = gain / max(dt, 1e-15), ("cell", a, b)
+        for side, w, taken in (("q", wq, q_fb), ("r", wr, r_fb)):
+            for x in range(S):
+                if w[x] == 0 or x in taken:
+                    continue
+                new = np.zeros((S, S), bool)
+                if side == "q":
+                    new[x, :] = True
+                else:
+                    new[:, x] = True
+                new &= ~covered
+                gain = (E - fnd)[new].sum()
+                dt = (exh - pc)[new].sum()
+                if gain > 0 and gain / max(dt, 1e-15) > best:
+                    best, move = gain / max(dt, 1e-15), (side, x)
+        if move is None:
+            break
+        if move[0] == "cell":
+            level[move[1], move[2]] += 1
+        elif move[0] == "q":
+            q_fb.append(move[1])
+            covered[move[1], :] = True
+        else:
+            r_fb.append(move[1])
+            covered[:, move[1]] = True
+    level[covered] = -1
+    rec = (E[covered].sum() + at(FL, level)[~covered].sum()) / te if te else 1.0
+    est = float(np.where(covered, exh, prop_cost(level)).sum())
+    return level, sorted(q_fb), sorted(r_fb), float(rec), est
+
+
 # -------------------------------------------------------------------------- search ----------
 def _subset(codes, lens, rows):
     from .device import SeqSet
@@ -513,10 +667,23 @@ class QueryBatch:
         self.learn_set = _subset(codes, self.lens, self.learn_rows)
         self.fb_rows_t = torch.from_numpy(self.fb_rows).cuda()
         self.learn_rows_t = torch.from_numpy(self.learn_rows).cuda()
+        self.learn_lens_t = torch.from_numpy(
+            np.clip(self.lens[self.learn_rows], 0, PAD).astype(np.uint8)).cuda()
         self.ranges = None
         if index.band is not None and self.learn_rows.size and index.n_learn:
             r = band_tile_ranges(self.lens[self.learn_rows], index.learn_lens, index.band)
             self.ranges = torch.from_numpy(r.ravel()).cuda()
+        self._range_key = None
+
+    def range_tiles(self, index: "LearnedIndex"):
+        """The threshold form's per-tile ref ranges for the index's current thresholds."""
+        import torch
+        key = (index._thr_version, index.n_learn)
+        if self._range_key != key:
+            r = range_tile_ranges(self.lens[self.learn_rows], index.learn_lens, index.thresholds)
+            self.ranges_thr = torch.from_numpy(r.ravel()).cuda()
+            self._range_key = key
+        return self.ranges_thr
 
 
 class LearnedIndex:
@@ -533,14 +700,22 @@ class LearnedIndex:
 
     ``k = 0`` turns the proposals off: the index is then the method without the network (the
     calibrated exhaustive fallback alone), the baseline the encoder is measured against.
+
+    ``proposal="range"`` replaces the top-k by thresholds: every (query, ref) pair whose
+    embedding dot product reaches the threshold of its (query length, ref length) cell is
+    proposed (``st_propose_range``), so no per-query selection is kept and a query proposes as
+    many refs as its cells let through.  :meth:`calibrate` then sets each cell's threshold from
+    the embeddings of the cell's exact hits on the held-out batch and chooses the fallback
+    lengths by estimated cost (``k`` only switches the network on, ``k = 0`` off).
     """
 
     def __init__(self, encoder: Encoder | None, ref_codes: np.ndarray, ref_lens: np.ndarray, *,
                  matrix, gap_open: int, gap_extend: int = 1, max_penalty: int = 24, k: int = 256,
-                 band: int | None = None):
+                 band: int | None = None, proposal: str = "topk"):
         """``band``: when set, a query's proposals come only from refs whose length differs from
         the query tile's lengths by at most ``band`` (refs and queries sorted by length, each
-        256-query tile scanning its band of ref tiles); None scans every ref."""
+        256-query tile scanning its band of ref tiles); None scans every ref (top-k form only;
+        the threshold form scans the ref lengths its thresholds leave on)."""
         from .device import SeqSet
         if max_penalty < 0:
             raise ValueError("max_penalty must be >= 0")
@@ -548,6 +723,12 @@ class LearnedIndex:
             raise ValueError("k must be >= 0, and k > 0 needs an encoder")
         if band is not None and band < 0:
             raise ValueError("band must be >= 0 or None")
+        if proposal not in ("topk", "range"):
+            raise ValueError("proposal is 'topk' or 'range'")
+        self.proposal = proposal
+        self.thresholds = np.full((PAD + 1, PAD + 1), np.inf, np.float32)
+        self._thr_version = 0
+        self._range_cap = 0
         self.band = band
         self.encoder, self.matrix = encoder, matrix
         self.gap_open, self.gap_extend, self.max_penalty, self.k = gap_open, gap_extend, max_penalty, k
@@ -570,7 +751,10 @@ class LearnedIndex:
             "k": self.k, "band": self.band, "max_penalty": self.max_penalty, "gap_open": self.gap_open,
             "gap_extend": self.gap_extend,
             "query_fallback": np.flatnonzero(self.query_fallback).tolist(),
-            "ref_fallback": np.flatnonzero(self.ref_fallback).tolist()})
+            "ref_fallback": np.flatnonzero(self.ref_fallback).tolist(),
+            "proposal": self.proposal,
+            "thresholds": [[float(x) if np.isfinite(x) else None for x in row]
+                           for row in self.thresholds]})
 
     @classmethod
     def from_model(cls, path, ref_codes: np.ndarray, ref_lens: np.ndarray, *, matrix,
@@ -581,9 +765,21 @@ class LearnedIndex:
         m = enc.meta
         idx = cls(enc, ref_codes, ref_lens, matrix=matrix, gap_open=int(m["gap_open"]),
                   gap_extend=int(m["gap_extend"]), max_penalty=int(m["max_penalty"]),
-                  k=int(m["k"]), band=m.get("band"))
+                  k=int(m["k"]), band=m.get("band"), proposal=m.get("proposal", "topk"))
         idx.set_fallback(m["query_fallback"], m["ref_fallback"])
+        if m.get("thresholds") is not None:
+            idx.set_thresholds(np.array([[np.inf if x is None else x for x in row]
+                                         for row in m["thresholds"]], np.float32))
         return idx
+
+    def set_thresholds(self, thresholds) -> None:
+        """The threshold form's dot-product threshold per (query length, ref length) cell
+        (float32 [33, 33]; +inf leaves a cell without proposals)."""
+        t = np.array(thresholds, np.float32)
+        if t.shape != (PAD + 1, PAD + 1) or np.isnan(t).any():
+            raise ValueError("thresholds must be a float [33, 33] table without NaN")
+        self.thresholds = t
+        self._thr_version += 1
 
     def set_fallback(self, query_lengths=(), ref_lengths=()) -> None:
         self.query_fallback[:] = False
@@ -599,6 +795,8 @@ class LearnedIndex:
         learn = learn[np.argsort(self.ref_lens[learn], kind="stable")]  # by length, then id
         fbr = np.flatnonzero(fb).astype(np.int64)
         self.learn_lens = self.ref_lens[learn]
+        self.learn_lens_t = torch.from_numpy(
+            np.clip(self.learn_lens, 0, PAD).astype(np.uint8)).cuda()
         self.learn_ids = torch.from_numpy(learn.astype(np.int32)).cuda()
         self.fb_ref_ids = torch.from_numpy(fbr.astype(np.int32)).cuda()
         self.learn_refs = _subset(self.ref_codes, self.ref_lens, learn)
@@ -650,15 +848,18 @@ class LearnedIndex:
             q_emb = torch.empty((n, 64), dtype=torch.bfloat16, device="cuda")
             self.encoder.embed_into(qb.learn_set, q_emb.data_ptr(), 1, stream)
             mark("embed")
-            ids = torch.empty((n, self.k), dtype=torch.int32, device="cuda")
-            propose_topk_into(q_emb.data_ptr(), n, self.r_emb.data_ptr(), self.n_learn, self.k,
-                              ids.data_ptr(), 0, stream,
-                              qb.ranges.data_ptr() if qb.ranges is not None else 0)
+            if self.proposal == "range":
+                qi, ri = self._range_pairs(qb, q_emb)
+            else:
+                ids = torch.empty((n, self.k), dtype=torch.int32, device="cuda")
+                propose_topk_into(q_emb.data_ptr(), n, self.r_emb.data_ptr(), self.n_learn,
+                                  self.k, ids.data_ptr(), 0, stream,
+                                  qb.ranges.data_ptr() if qb.ranges is not None else 0)
+                qi = torch.arange(n, dtype=torch.int32, device="cuda").repeat_interleave(self.k)
+                ri = ids.view(-1)
+                keep = ri >= 0
+                qi, ri = qi[keep], ri[keep]
             mark("propose")
-            qi = torch.arange(n, dtype=torch.int32, device="cuda").repeat_interleave(self.k)
-            ri = ids.view(-1)
-            keep = ri >= 0
-            qi, ri = qi[keep], ri[keep]
             sc = torch.empty(qi.numel(), dtype=torch.int32, device="cuda")
             if qi.numel():
                 pair_scores(qb.learn_set, self.learn_refs, qi.data_ptr(), ri.data_ptr(), qi.numel(),
@@ -689,6 +890,17 @@ class LearnedIndex:
         out = indptr, ri[order], sc[order]
         mark("merge")
         return out
+
+    def _range_pairs(self, qb: QueryBatch, q_emb):
+        """The threshold form's proposals of the batch's learned rows (local query and learned-ref
+        indices); the candidate buffers keep the largest size seen, so a repeated search is sized
+        right the first time."""
+        n = len(qb.learn_set)
+        cap = max(self._range_cap, 16 * n)
+        qi, ri = propose_range(q_emb, qb.learn_lens_t, self.r_emb, self.learn_lens_t,
+                               self.thresholds, cap, qb.range_tiles(self))
+        self._range_cap = max(self._range_cap, int(qi.numel() * 1.1) + 1)
+        return qi, ri
 
     def search_strings(self, queries) -> "SparseScores":
         """The public call: thresholded hits of host query strings against the index's refs, as
@@ -749,6 +961,8 @@ class LearnedIndex:
         the calibration batch's query lengths and the refs' lengths) -- until the estimated
         recall reaches ``bound + margin``.  The recall with the chosen fallback is then measured
         on the same batch.  ``margin`` defaults to min(0.003, (1 - bound) / 3)."""
+        if self.proposal == "range" and self.k:
+            return self.calibrate_range(codes, lens, bound, margin)
         if margin is None:
             margin = min(0.003, (1.0 - bound) / 3.0)
         self.set_fallback()
@@ -794,3 +1008,126 @@ class LearnedIndex:
                 "recall": r2["recall"], "found": r2["found"], "exact": r2["exact"],
                 "subset_of_exact": r2["subset_of_exact"], "exhaustive_share": share,
                 "cells_no_fallback": (r0["found_cells"], r0["exact_cells"])}
+
+    def calibrate_range(self, codes: np.ndarray, lens: np.ndarray, bound: float = 0.99,
+                        margin: float | None = None, slack: float = 0.02,
+                        costs: dict | None = None, levels=RANGE_LEVELS,
+                        chunk_queries: int = 1024) -> dict:
+        """The threshold form's calibration on a held-out batch: a per-cell recall budget.
+
+        1. The batch's exact hits against every ref come from the exhaustive sparse kernel and
+           their embedding dot products from ``st_embed_dots``.  For each (query length, ref
+           length) cell and each recall level q of ``levels``, the candidate threshold is the dot
+           product that keeps a fraction q of the cell's hits (the floor((1 - q) n)-th smallest),
+           lowered by ``slack``.
+        2. The proposals at every cell's most inclusive threshold are made on the batch in
+           chunks of ``chunk_queries`` queries (bounded memory) and counted per cell and level.
+        3. A greedy allocation then minimises the estimated time (``costs``: seconds per
+           exhaustively scored pair -- measured on the batch when it is large enough -- per
+           scanned pair and per candidate; defaults ``RANGE_COSTS``) until the recall estimate
+           reaches ``bound + margin``: every step takes the move with the most recovered hits
+           per added second, a move being either raising one cell to its next level (a cell
+           may also stay off: its hits count as lost) or scoring one query or ref length
+           exhaustively (the fallback).
+        The recall with the chosen thresholds and fallback is then measured on the same batch."""
+        import torch
+        if margin is None:
+            margin = min(0.003, (1.0 - bound) / 3.0)
+        c = dict(RANGE_COSTS, **(costs or {}))
+        target = bound + margin
+        S, LV = PAD + 1, len(levels)
+        self.set_fallback()
+        self.set_thresholds(np.full((S, S), np.inf, np.float32))
+        qb = self.queries(codes, lens)
+        stream = torch.cuda.current_stream().cuda_stream
+        n = len(qb.learn_set) if qb.learn_set is not None else 0
+        ql_sorted = np.clip(qb.lens[qb.learn_rows], 0, PAD)
+        wq = np.bincount(ql_sorted, minlength=S)[:S].astype(np.float64)
+        wr = np.bincount(np.clip(self.ref_lens, 0, PAD), minlength=S)[:S].astype(np.float64)
+        E = np.zeros((S, S))
+        tau = np.full((S, S, LV), np.inf, np.float32)   # threshold per cell and level
+        FL = np.zeros((S, S, LV))                       # hits found per cell and level
+        CL = np.zeros((S, S, LV))                       # candidates per cell and level
+        measured = {}
+        if n and self.n_learn:
+            q_emb = torch.empty((n, 64), dtype=torch.bfloat16, device="cuda")
+            self.encoder.embed_into(qb.learn_set, q_emb.data_ptr(), 1, stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            rows, rr, _ = self._sparse(qb.learn_set, self.learn_refs)
+            e1.record()
+            e1.synchronize()
+            if n * self.n_learn >= 1e9:
+                measured["exhaustive"] = e0.elapsed_time(e1) / 1e3 / (n * self.n_learn)
+            dots = torch.empty(rows.numel(), dtype=torch.float32, device="cuda")
+            rows32 = rows.to(torch.int32)
+            embed_dots_into(q_emb.data_ptr(), n, self.r_emb.data_ptr(), self.n_learn,
+                            rows32.data_ptr(), rr.data_ptr(), rows.numel(), dots.data_ptr(), stream)
+            cell = ql_sorted[rows.cpu().numpy()].astype(np.int64) * S + \
+                np.clip(self.learn_lens[rr.cpu().numpy()], 0, PAD)
+            d = dots.cpu().numpy()
+            E = np.bincount(cell, minlength=S * S).reshape(S, S).astype(np.float64)
+            order = np.lexsort((d, cell))
+            cs, ds = cell[order], d[order]
+            start = np.searchsorted(cs, np.arange(S * S))
+            cnt = E.ravel().astype(np.int64)
+            tf, ff = tau.reshape(S * S, LV), FL.reshape(S * S, LV)
+            for ce in np.flatnonzero(cnt):
+                seg = ds[start[ce]:start[ce] + cnt[ce]]
+                for li, q in enumerate(levels):
+                    t = seg[min(int(np.floor((1.0 - q) * cnt[ce])), cnt[ce] - 1)] - slack
+                    tf[ce, li] = t
+                    ff[ce, li] = cnt[ce] - np.searchsorted(seg, t, side="left")
+            # candidates per cell and level, from the most inclusive thresholds, in chunks
+            self.set_thresholds(tau[:, :, LV - 1])
+            ql_t = torch.from_numpy(ql_sorted.astype(np.int64)).cuda()
+            rl_t = self.learn_lens_t.long()
+            tau_t = torch.from_numpy(tau.reshape(S * S, LV)).cuda()
+            cl_t = torch.zeros((LV, S * S), dtype=torch.float64, device="cuda")
+            thr_last = self.thresholds
+            for c0 in range(0, n, chunk_queries):
+                c1 = min(n, c0 + chunk_queries)
+                qe = q_emb[c0:c1]
+                rg = range_tile_ranges(ql_sorted[c0:c1], self.learn_lens, thr_last)
+                pq, pr = propose_range(qe, qb.learn_lens_t[c0:c1], self.r_emb, self.learn_lens_t,
+                                       thr_last, None, torch.from_numpy(rg.ravel()).cuda())
+                if pq.numel() == 0:
+                    continue
+                dd = torch.empty(pq.numel(), dtype=torch.float32, device="cuda")
+                embed_dots_into(qe.data_ptr(), c1 - c0, self.r_emb.data_ptr(), self.n_learn,
+                                pq.data_ptr(), pr.data_ptr(), pq.numel(), dd.data_ptr(), stream)
+                ce_t = ql_t[c0 + pq.long()] * S + rl_t[pr.long()]
+                for li in range(LV):
+                    ge = (dd >= tau_t[:, li][ce_t]).to(torch.float64)
+                    cl_t[li].index_add_(0, ce_t, ge)
+                    del ge
+                del pq, pr, dd, ce_t
+            CL = cl_t.T.reshape(S, S, LV).cpu().numpy()
+        c.update(measured)
+        level, q_fb, r_fb, est_rec, est = allocate_recall(E, FL, CL, wq, wr, c, target)
+        covered = np.zeros((S, S), bool)
+        covered[q_fb, :] = True
+        covered[:, r_fb] = True
+        idx = np.clip(level, 0, LV - 1)
+        thr = np.where((level >= 0) & ~covered,
+                       np.take_along_axis(tau, idx[:, :, None], 2)[:, :, 0], np.inf)
+        q_fb, r_fb = sorted(q_fb), sorted(r_fb)
+        self.set_fallback(q_fb, r_fb)
+        self.set_thresholds(thr.astype(np.float32))
+        cand = np.take_along_axis(CL, idx[:, :, None], 2)[:, :, 0]
+        cand_q = float(np.where((level >= 0) & ~covered, cand, 0.0).sum() / max(n, 1))
+        te = E.sum()
+        r2 = self.recall(codes, lens)
+        wq1, wr1 = wq / max(wq.sum(), 1.0), wr / max(wr.sum(), 1.0)
+        share = float(wq1[q_fb].sum() + (1.0 - wq1[q_fb].sum()) * wr1[r_fb].sum())
+        return {"ref_fallback": r_fb, "query_fallback": q_fb,
+                "recall_no_fallback": float(FL[:, :, LV - 1].sum() / te) if te else 1.0,
+                "recall_estimate": float(est_rec),
+                "recall": r2["recall"], "found": r2["found"], "exact": r2["exact"],
+                "subset_of_exact": r2["subset_of_exact"], "exhaustive_share": share,
+                "cells_with_proposals": int(((level >= 0) & ~covered).sum()),
+                "candidates_per_query": cand_q,
+                "estimated_seconds_per_query": est / max(n, 1),
+                "costs": {k: float(v) for k, v in c.items()}, "costs_measured": sorted(measured),
+                "cells_no_fallback": (FL[:, :, LV - 1], E), "candidate_cells": CL[:, :, LV - 1],
+                "levels": level}

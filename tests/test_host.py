@@ -180,3 +180,54 @@ def test_integer_arguments_convert_like_the_reference_binding():
         with pytest.raises(TypeError):
             call()
     assert _core._i32("gap_open", np.int64(8)) == 8 and _core._u32("w", np.uint8(25)) == 25
+
+
+def test_threshold_tile_ranges_cover_every_cell_that_is_on():
+    """range_tile_ranges: a 256-query tile scans the 128-ref tiles holding every ref length with a
+    finite threshold for one of the tile's query lengths, and nothing for a tile without one."""
+    from seqtree_b200.learned import range_tile_ranges
+    rng = np.random.default_rng(3)
+    q = np.sort(rng.integers(8, 26, size=1000))
+    r = np.sort(rng.integers(8, 26, size=5000))
+    thr = np.full((33, 33), np.inf, np.float32)
+    for a in range(33):
+        thr[a, max(0, a - 1):a + 2] = 0.5  # lengths within one residue
+    thr[8:11, :] = np.inf                  # short queries: no proposals
+    out = range_tile_ranges(q, r, thr)
+    assert out.shape == (4, 2) and out.dtype == np.int32
+    for t in range(4):
+        blk = q[256 * t:256 * (t + 1)]
+        on = np.isfinite(thr[blk.min():blk.max() + 1]).any(axis=0)
+        need = np.flatnonzero(on[r])
+        if need.size == 0:
+            assert out[t, 0] == out[t, 1]
+            continue
+        assert out[t, 0] * 128 <= need.min() and need.max() < out[t, 1] * 128
+        assert out[t, 1] * 128 - need.max() <= 128 and need.min() - out[t, 0] * 128 < 128
+    assert (range_tile_ranges(q, r, np.full((33, 33), np.inf)) == 0).all()
+
+
+def test_recall_allocation_prefers_cheap_proposals_and_falls_back_where_they_are_dear():
+    """allocate_recall: a cell whose proposals recover hits cheaply gets them, a query length
+    whose cells would need more candidates than exhaustive scoring costs falls back, and the
+    estimated recall reaches the target."""
+    from seqtree_b200.learned import allocate_recall
+    S, LV = 4, 3
+    wq = np.array([0, 100, 100, 0], float)
+    wr = np.array([0, 1000, 1000, 0], float)
+    E = np.zeros((S, S))
+    E[1, 1], E[1, 2], E[2, 2] = 500, 400, 50      # short queries (length 1) carry most hits
+    FL = np.zeros((S, S, LV))
+    CL = np.zeros((S, S, LV))
+    FL[1, 1], CL[1, 1] = [250, 400, 490], [5e4, 8e4, 1e5]   # dear: half of all pairs
+    FL[1, 2], CL[1, 2] = [200, 300, 390], [5e4, 8e4, 1e5]
+    FL[2, 2], CL[2, 2] = [40, 48, 50], [10, 30, 100]        # cheap
+    costs = {"exhaustive": 1e-9, "scan": 1e-11, "candidate": 1e-8}
+    level, qf, rf, rec, est = allocate_recall(E, FL, CL, wq, wr, costs, 0.99)
+    assert qf == [1] and rf == []
+    assert level[2, 2] >= 1 and (level[1] == -1).all()
+    assert rec >= 0.99 and est > 0
+    # with free candidates nothing falls back and every cell with hits gets proposals
+    cheap = dict(costs, candidate=0.0)
+    level, qf, rf, rec, _ = allocate_recall(E, FL, CL, wq, wr, cheap, 0.95)
+    assert qf == [] and rf == [] and rec >= 0.95 and (level[E > 0] >= 0).all()

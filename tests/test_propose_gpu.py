@@ -150,3 +150,138 @@ def test_banded_learned_search_is_exact(cuda_ready):
     wide = L.LearnedIndex(enc, rc, rl, matrix=M, gap_open=8, max_penalty=24, k=32, band=40)
     full = L.LearnedIndex(enc, rc, rl, matrix=M, gap_open=8, max_penalty=24, k=32)
     assert wide.recall(qc, ql)["found"] == full.recall(qc, ql)["found"]
+
+
+# ------------------------------------------------------------------ threshold form ----------
+def _range_expected(q, r, ql, rl, thr):
+    s = q.astype(np.float64) @ r.astype(np.float64).T  # exact
+    t = thr.astype(np.float64)[np.minimum(ql, 32)[:, None], np.minimum(rl, 32)[None, :]]
+    qi, ri = np.nonzero(s >= t)
+    return np.stack([qi, ri], 1)
+
+
+def _range_run(q, r, ql, rl, thr, capacity=None, ranges=None):
+    import torch
+
+    from seqtree_b200.learned import propose_range, swizzle_rows
+    qt = swizzle_rows(torch.from_numpy(q).cuda())
+    rt = swizzle_rows(torch.from_numpy(r).cuda())
+    qlt = torch.from_numpy(ql.astype(np.uint8)).cuda()
+    rlt = torch.from_numpy(rl.astype(np.uint8)).cuda()
+    rg = None if ranges is None else torch.from_numpy(np.asarray(ranges, np.int32).ravel()).cuda()
+    pq, pr = propose_range(qt, qlt, rt, rlt, thr, capacity, rg)
+    got = np.stack([pq.cpu().numpy(), pr.cpu().numpy()], 1).astype(np.int64)
+    return got[np.lexsort((got[:, 1], got[:, 0]))]
+
+
+def _thr_table(rng, off=0.3):
+    """Thresholds on the 2^-8 grid (ties with exact scores happen), a few cells switched off."""
+    thr = (np.round(rng.uniform(-0.5, 1.5, size=(33, 33)) * 256) / 256 + off).astype(np.float32)
+    thr[rng.random((33, 33)) < 0.1] = np.inf
+    return thr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nq,nr,sort_refs,distinct", [
+    (300, 1000, True, None),       # partial query and ref tiles
+    (600, 50_000, True, 40),       # many tiles, exact ties between refs
+    (257, 4099, False, None),      # unsorted ref lengths: every group straddles lengths
+    (1, 1, True, None),            # one pair
+])
+def test_range_matches_exact_threshold(cuda_ready, nq, nr, sort_refs, distinct):
+    """st_propose_range returns exactly the pairs whose exact dot product reaches the threshold
+    of their (query length, ref length) cell, each once."""
+    rng = np.random.default_rng(nq * 13 + nr)
+    q, r = _emb(rng, nq), _emb(rng, nr, distinct)
+    ql = rng.integers(8, 26, size=nq)
+    rl = rng.integers(8, 26, size=nr)
+    if sort_refs:
+        rl = np.sort(rl)
+    thr = _thr_table(rng)
+    got = _range_run(q, r, ql, rl, thr)
+    want = _range_expected(q, r, ql, rl, thr)
+    np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_range_capacity_ranges_and_lengths_past_32(cuda_ready):
+    """A capacity below the count still returns the full count and then the exact set (the
+    wrapper repeats the call); per-tile ranges limit the scanned refs; lengths above 32 use the
+    table's last row and column; a table of +inf proposes nothing."""
+    import torch
+
+    from seqtree_b200.learned import propose_range_into, swizzle_rows
+    rng = np.random.default_rng(23)
+    nq, nr = 520, 3000
+    q, r = _emb(rng, nq), _emb(rng, nr)
+    ql = rng.integers(20, 40, size=nq)
+    rl = np.sort(rng.integers(20, 40, size=nr))
+    thr = np.full((33, 33), 0.25, np.float32)
+    thr[32, 32] = 0.0
+    want = _range_expected(q, r, ql, rl, thr)
+    assert want.shape[0] > 200
+    got = _range_run(q, r, ql, rl, thr, capacity=7)
+    np.testing.assert_array_equal(got, want)
+    # a raw call with room for 7 pairs: the full count, seven distinct expected pairs written
+    qt, rt = swizzle_rows(torch.from_numpy(q).cuda()), swizzle_rows(torch.from_numpy(r).cuda())
+    qlt = torch.from_numpy(ql.astype(np.uint8)).cuda()
+    rlt = torch.from_numpy(rl.astype(np.uint8)).cuda()
+    pq = torch.full((7,), -1, dtype=torch.int32, device="cuda")
+    pr = torch.full((7,), -1, dtype=torch.int32, device="cuda")
+    n = propose_range_into(qt.data_ptr(), nq, qlt.data_ptr(), rt.data_ptr(), nr, rlt.data_ptr(),
+                           thr, pq.data_ptr(), pr.data_ptr(), 7,
+                           torch.cuda.current_stream().cuda_stream)
+    assert n == want.shape[0]
+    part = set(zip(pq.cpu().tolist(), pr.cpu().tolist()))
+    assert len(part) == 7 and part <= set(map(tuple, want.tolist()))
+    # per-tile ranges: tile 0 scans ref tiles [3, 9), tile 1 none, tile 2 past the end (clamped)
+    ranges = np.array([[3, 9], [0, 0], [20, 99]], np.int32)
+    got = _range_run(q, r, ql, rl, thr, ranges=ranges)
+    keep = np.zeros(len(want), bool)
+    for t, (lo, hi) in enumerate(ranges):
+        lo_ref, hi_ref = min(lo, 24) * 128, min(max(hi, lo), 24) * 128
+        keep |= (want[:, 0] // 256 == t) & (want[:, 1] >= lo_ref) & (want[:, 1] < hi_ref)
+    np.testing.assert_array_equal(got, want[keep])
+    off = np.full((33, 33), np.inf, np.float32)
+    assert _range_run(q, r, ql, rl, off).shape[0] == 0
+
+
+@pytest.mark.gpu
+def test_embed_dots_are_the_exact_dot_products(cuda_ready):
+    import torch
+
+    from seqtree_b200.learned import embed_dots_into, swizzle_rows
+    rng = np.random.default_rng(29)
+    q, r = _emb(rng, 77), _emb(rng, 301)
+    qi = rng.integers(0, 77, size=5000).astype(np.int32)
+    ri = rng.integers(0, 301, size=5000).astype(np.int32)
+    qi[:3] = [77, -1, 0]  # out of range: NaN
+    ri[:3] = [0, 0, 301]
+    qt, rt = swizzle_rows(torch.from_numpy(q).cuda()), swizzle_rows(torch.from_numpy(r).cuda())
+    qit, rit = torch.from_numpy(qi).cuda(), torch.from_numpy(ri).cuda()
+    out = torch.empty(5000, dtype=torch.float32, device="cuda")
+    embed_dots_into(qt.data_ptr(), 77, rt.data_ptr(), 301, qit.data_ptr(), rit.data_ptr(), 5000,
+                    out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    got = out.cpu().numpy()
+    assert np.isnan(got[:3]).all()
+    want = (q[qi[3:]].astype(np.float64) * r[ri[3:]].astype(np.float64)).sum(1)
+    np.testing.assert_array_equal(got[3:], want.astype(np.float32))
+
+
+@pytest.mark.gpu
+def test_range_learned_search_is_exact_and_calibrated(cuda_ready):
+    """The threshold form of LearnedIndex: every reported hit is an exhaustive hit with its exact
+    score, calibration reaches the bound on its batch, and a model file keeps the thresholds."""
+    import seqtree_b200 as stb
+    from seqtree_b200 import learned as L
+    M = stb.SubstitutionMatrix.blosum62()
+    enc = L.Encoder(seed=3)
+    rc, rl = L.cdr3_codes(70, 8000)
+    cc, cl = L.cdr3_codes(71, 600)
+    idx = L.LearnedIndex(enc, rc, rl, matrix=M, gap_open=8, max_penalty=24, proposal="range")
+    cal = idx.calibrate(cc, cl, bound=0.99)
+    assert cal["subset_of_exact"] and cal["recall"] >= 0.99
+    qc, ql = L.cdr3_codes(72, 500)
+    rec = idx.recall(qc, ql)
+    assert rec["subset_of_exact"]
+    assert rec["recall"] >= 0.9
