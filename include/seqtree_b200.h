@@ -72,7 +72,8 @@ int32_t st_device_count(void);
  *                when `penalty` is NULL.
  *   prior        the [m][d][i] gap-prior cube of (prior_width+1)^3 entries, or NULL /
  *                prior_len == 0 for no prior.
- *   out          N*K int32, host memory (pinned or pageable).
+ *   out          N*K int32, host memory (pinned or pageable); its contents are unspecified
+ *                after a call that fails (the symbol check runs beside the kernel).
  */
 int32_t st_gapblock_matrix(const st_strings *queries, const st_strings *refs, int32_t alphabet,
                            const int32_t *penalty, int32_t matrix_size, int32_t gap_open,

@@ -230,23 +230,52 @@ int32_t st_gapblock_matrix(const st_strings* queries, const st_strings* refs, in
         Context& ctx = context();
         std::lock_guard<std::mutex> lk(ctx.mu);
         clear_flags(ctx);
-        // src/gapblock.cpp:85-94: queries are encoded before refs.
+        // src/gapblock.cpp:85-94: queries are encoded before refs.  The symbol check is
+        // deferred to the call's one synchronisation (words 0 and 1 of the flag area: the first
+        // invalid byte of the queries, of the refs); invalid symbols compute as code 0 meanwhile
+        // and the call then fails with the reference's message, queries first, as the reference
+        // does.  `out` is unspecified after a failed call.
         Transient t;
         {
             Phase ph("upload+encode");
-            t.q.reset(make_seqset(queries, alphabet, ctx.stream, nullptr, nullptr, ctx.tq));
-            t.r.reset(make_seqset(refs, alphabet, ctx.stream, nullptr, nullptr, ctx.tr));
+            STB_CUDA(cudaMemsetAsync(ctx.flags_d, 0xFF, 2 * sizeof(int64_t), ctx.stream));
+            t.q.reset(make_seqset(queries, alphabet, ctx.stream, nullptr, nullptr, ctx.tq, 0));
+            t.r.reset(make_seqset(refs, alphabet, ctx.stream, nullptr, nullptr, ctx.tr, 1));
         }
+        auto check_symbols = [&] {
+            for (int w = 0; w < 2; ++w) {
+                const uint64_t bad = static_cast<uint64_t>(ctx.flags_h[w]);
+                if (bad != ~uint64_t(0)) {
+                    const st_strings* s = w == 0 ? queries : refs;
+                    const char c =
+                        reinterpret_cast<const char*>(s->bytes)[s->offsets[0] + int64_t(bad)];
+                    fail(ST_EINVAL, std::string("symbol '") + c + "' is not in the alphabet");
+                }
+            }
+        };
         int32_t* out_d = ctx.out_buf.as<int32_t>(size_t(N) * size_t(K));
         {
             Phase ph("plan+launch");
-            gapblock_sets(*t.q, *t.r, penalty, matrix_size, gap_open, gap_extend, prior, prior_len,
-                          prior_width, out_d, ctx.stream);
+            try {
+                gapblock_sets(*t.q, *t.r, penalty, matrix_size, gap_open, gap_extend, prior,
+                              prior_len, prior_width, out_d, ctx.stream);
+            } catch (...) {
+                // the reference reports an invalid symbol before the prior-table errors that
+                // planning finds (src/gapblock.cpp:85-102)
+                STB_CUDA(cudaMemcpyAsync(ctx.flags_h, ctx.flags_d, 2 * sizeof(int64_t),
+                                         cudaMemcpyDeviceToHost, ctx.stream));
+                STB_CUDA(cudaStreamSynchronize(ctx.stream));
+                check_symbols();
+                throw;
+            }
         }
         {
             Phase ph("kernel+d2h");
+            STB_CUDA(cudaMemcpyAsync(ctx.flags_h, ctx.flags_d, 2 * sizeof(int64_t),
+                                     cudaMemcpyDeviceToHost, ctx.stream));
             finish(ctx, out, N, K, out_d);
         }
+        check_symbols();
         check_timeout(ctx);
         trace_report("st_gapblock_matrix");
     });

@@ -328,7 +328,7 @@ Lut make_lut(int32_t alphabet) {
 // recorded with atomicMin so the error names the same symbol the reference's sequential
 // encoder stops at.
 __global__ void encode_kernel(const uint8_t* __restrict__ in, uint8_t* __restrict__ out,
-                              int64_t n, Lut lut, unsigned long long* first_bad) {
+                              int64_t n, Lut lut, unsigned long long* first_bad, uint8_t bad_code) {
     __shared__ uint8_t s_lut[256];
     for (int i = threadIdx.x; i < 256; i += blockDim.x) s_lut[i] = lut.v[i];
     __syncthreads();
@@ -342,9 +342,10 @@ __global__ void encode_kernel(const uint8_t* __restrict__ in, uint8_t* __restric
 #pragma unroll
             for (int b = 0; b < 4; ++b) {
                 uint8_t c = s_lut[(w >> (8 * b)) & 0xFF];
-                if (c == 0xFF && !bad) {
-                    atomicMin(first_bad, (unsigned long long)(base + b));
+                if (c == 0xFF) {
+                    if (!bad) atomicMin(first_bad, (unsigned long long)(base + b));
                     bad = true;
+                    c = bad_code;
                 }
                 o |= uint32_t(c) << (8 * b);
             }
@@ -352,7 +353,10 @@ __global__ void encode_kernel(const uint8_t* __restrict__ in, uint8_t* __restric
         } else {
             for (int64_t i = base; i < n; ++i) {
                 uint8_t c = s_lut[in[i]];
-                if (c == 0xFF) atomicMin(first_bad, (unsigned long long)i);
+                if (c == 0xFF) {
+                    atomicMin(first_bad, (unsigned long long)i);
+                    c = bad_code;
+                }
                 out[i] = c;
             }
         }
@@ -390,7 +394,7 @@ std::unique_ptr<st_seqset_s> row_view(const st_seqset_s& s, int64_t rows) {
 }
 
 st_seqset_s* make_seqset(const st_strings* s, int32_t alphabet, cudaStream_t stream,
-                         int64_t* bad_index, char* bad_char, DevBuf* storage) {
+                         int64_t* bad_index, char* bad_char, DevBuf* storage, int defer_word) {
     std::atomic<uint64_t>& next_uid = g_next_uid;
     if (!s || (s->count > 0 && !s->offsets)) fail(ST_EINVAL, "seqtree_b200: null sequence set");
     if (alphabet != -1 && alphabet_size(alphabet) == 0)
@@ -445,15 +449,17 @@ st_seqset_s* make_seqset(const st_strings* s, int32_t alphabet, cudaStream_t str
             uint8_t* d_raw = raw.as<uint8_t>(padded);
             STB_CUDA(cudaMemsetAsync(d_raw + set->total, 0, 64, stream));
             STB_CUDA(cudaMemcpyAsync(d_raw, src, size_t(set->total), cudaMemcpyHostToDevice, stream));
-            auto* flag = reinterpret_cast<unsigned long long*>(ctx.flags_d);
-            const unsigned long long none = ~0ull;
-            STB_CUDA(cudaMemcpyAsync(flag, &none, sizeof none, cudaMemcpyHostToDevice, stream));
+            auto* flag = reinterpret_cast<unsigned long long*>(ctx.flags_d + (defer_word > 0 ? defer_word : 0));
+            STB_CUDA(cudaMemsetAsync(flag, 0xFF, sizeof(unsigned long long), stream));
             const Lut lut = make_lut(alphabet);
             const int64_t words = ceil_div(set->total, 4);
             const unsigned grid = unsigned(std::min<int64_t>(ceil_div(words, 256), ctx.num_sms * 8));
-            encode_kernel<<<grid, 256, 0, stream>>>(d_raw, set->d_bytes, set->total, lut, flag);
+            encode_kernel<<<grid, 256, 0, stream>>>(d_raw, set->d_bytes, set->total, lut, flag,
+                                                    uint8_t(defer_word >= 0 ? 0 : 0xFF));
             STB_CUDA(cudaGetLastError());
             note_launch(nullptr);
+            if (defer_word >= 0) return set.release();
+            const unsigned long long none = ~0ull;
             STB_CUDA(cudaMemcpyAsync(ctx.flags_h, flag, sizeof none, cudaMemcpyDeviceToHost, stream));
             STB_CUDA(cudaStreamSynchronize(stream));
             const unsigned long long bad = static_cast<unsigned long long>(ctx.flags_h[0]);

@@ -187,8 +187,13 @@ namespace stb {
 // order errors across two sets exactly as the reference does.
 // `storage` (three buffers: bytes, offsets, lengths) makes a transient set that borrows
 // context memory instead of allocating.
+// `defer_word` >= 0 defers the symbol check: nothing waits for the encode, an invalid symbol is
+// stored as code 0 (so every later kernel indexes its tables in range) and the first invalid
+// byte index is left in device word `defer_word` of the context's flag area (all ones when
+// there is none) for the caller to read after its own final synchronisation.
 st_seqset_s* make_seqset(const st_strings* s, int32_t alphabet, cudaStream_t stream,
-                         int64_t* bad_index, char* bad_char, DevBuf* storage = nullptr);
+                         int64_t* bad_index, char* bad_char, DevBuf* storage = nullptr,
+                         int defer_word = -1);
 
 int32_t alphabet_size(int32_t alphabet);
 

@@ -35,8 +35,8 @@
 // The threshold form (propose_range_kernel) keeps the producer and MMA warps and replaces the
 // selection: a pair is proposed when its score reaches the threshold of its (query length, ref
 // length) cell, read from a 33 x 33 table staged in shared memory.  Nothing is kept per query, so
-// a group without a survivor costs one TMEM load, one max tree and one vote, and survivors are
-// appended with one atomicAdd per warp.
+// a group without a survivor costs one TMEM load and one max tree, and survivors are staged per
+// warp in shared memory and flushed to global memory 512 pairs at a time (one atomicAdd each).
 #include <cuda_bf16.h>
 
 #include <cfloat>
@@ -76,6 +76,8 @@ constexpr uint32_t kIdesc = idesc_bf16(128, kRT);
 
 
 constexpr int kLenSlots = 33;                  // lengths 0..32 of the threshold table
+constexpr int kStageBytes = 32 * 128;          // threshold form: a warp's staging buffer (park row)
+constexpr int kStage = kStageBytes / 8;        // pairs it holds
 
 struct ProposeArgs {
     const uint8_t* qemb;
@@ -383,13 +385,34 @@ __device__ __forceinline__ void propose_body(const ProposeArgs& a) {
         // vote tells whether the 32-column group has a single length (nearly every group when
         // the refs are sorted by length; any order is correct).  Such a group is rejected by one
         // 3-input max tree against the row's threshold for that length; otherwise each column's
-        // threshold is looked up with its length taken by shuffle.  Survivors are appended
-        // warp-aggregated: one atomicAdd per warp and group with any survivor, then each lane
-        // writes its pairs.
+        // threshold is looked up with its length taken by shuffle.  Survivors are staged per
+        // warp in shared memory and flushed to global memory with one atomicAdd per flush.
         const int ew = warp - 2, grp = ew >> 2, quarter = warp & 3;
         const int row = quarter * 32 + lane;
         const float* thr_s = reinterpret_cast<const float*>(smem + kSmWarp);
         const uint32_t tlane = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(grp) * 128u;
+        // Survivors go to a warp-private staging buffer in shared memory (the park area,
+        // unused by this form) and reach global memory in flushes of up to kStage pairs, one
+        // atomicAdd each, so no tile waits for an atomic's round trip.  A tile with more
+        // survivors than the buffer holds appends them to global memory directly.
+        int2* wbuf = reinterpret_cast<int2*>(smem + kSmPark + ew * kStageBytes);
+        int wcnt = 0;  // warp-uniform
+        auto flush = [&] {
+            __syncwarp();
+            unsigned long long base = 0;
+            if (lane == 0 && wcnt) base = atomicAdd(a.count, (unsigned long long)wcnt);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            for (int i = lane; i < wcnt; i += 32) {
+                const unsigned long long pos = base + unsigned(i);
+                if (pos < a.cap) {
+                    const int2 e = wbuf[i];
+                    a.pair_q[pos] = e.x;
+                    a.pair_r[pos] = e.y;
+                }
+            }
+            __syncwarp();
+            wcnt = 0;
+        };
         uint32_t acc = 0, accphase = 0;
         bool ok = true;
         for (int64_t qt = blockIdx.x; qt < ntq && ok; qt += gridDim.x) {
@@ -398,14 +421,12 @@ __device__ __forceinline__ void propose_body(const ProposeArgs& a) {
             const int ql = qvalid ? min(int(a.qlens[q]), kLenSlots - 1) : 0;
             const float* trow = thr_s + ql * kLenSlots;
             const int64_t rt0 = tile_first(a, qt, ntr), rt1 = tile_last(a, qt, ntr);
-            // One 32-column group: survivor mask against the row's thresholds, then the
-            // warp-aggregated append.  `lcol` is this lane's column length (-1 past the refs).
-            auto group = [&](const uint32_t (&v)[32], int lcol, int64_t cb, int nv) {
-                const uint32_t vmask = nv >= 32 ? 0xFFFFFFFFu : ((1u << nv) - 1u);
-                const int l0 = __shfl_sync(0xFFFFFFFFu, lcol, 0);
+            // Survivor mask of one 32-column group.  `uni` / `t`: the group has one ref length
+            // and its threshold; otherwise each column's threshold is looked up with its length
+            // (`lcol`, -1 past the refs) taken by shuffle.
+            auto group_mask = [&](const uint32_t (&v)[32], int lcol, bool uni, float t, int nv) {
                 uint32_t mask = 0;
-                if (__all_sync(0xFFFFFFFFu, lcol == l0 || lcol < 0)) {
-                    const float t = trow[l0];
+                if (uni) {
                     float m[11];
 #pragma unroll
                     for (int j = 0; j < 10; ++j)
@@ -427,76 +448,117 @@ __device__ __forceinline__ void propose_body(const ProposeArgs& a) {
                         if (lj >= 0) mask |= (__uint_as_float(v[j]) >= trow[lj]) ? (1u << j) : 0u;
                     }
                 }
-                mask = qvalid ? (mask & vmask) : 0u;
-                if (__any_sync(0xFFFFFFFFu, mask != 0u)) {
-                    const uint32_t n = __popc(mask);
-                    uint32_t incl = n;
+                const uint32_t vmask = nv >= 32 ? 0xFFFFFFFFu : (nv > 0 ? (1u << nv) - 1u : 0u);
+                return qvalid ? (mask & vmask) : 0u;
+            };
+            auto append = [&](const uint32_t (&mk)[kRT / 32], int64_t r0) {
+                uint32_t n = 0;
 #pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-                        if (lane >= o) incl += t;
+                for (int g = 0; g < kRT / 32; ++g) n += __popc(mk[g]);
+                uint32_t incl = n;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const int tot = int(__shfl_sync(0xFFFFFFFFu, incl, 31));
+                if (wcnt + tot > kStage) flush();
+                if (tot <= kStage) {
+                    int at = wcnt + int(incl - n);
+#pragma unroll
+                    for (int g = 0; g < kRT / 32; ++g) {
+                        uint32_t mask = mk[g];
+                        while (mask) {
+                            const int j = __ffs(mask) - 1;
+                            mask &= mask - 1;
+                            wbuf[at++] = make_int2(int32_t(q), int32_t(r0 + g * 32 + j));
+                        }
                     }
-                    const uint32_t tot = __shfl_sync(0xFFFFFFFFu, incl, 31);
-                    unsigned long long base = 0;
-                    if (lane == 31) base = atomicAdd(a.count, (unsigned long long)tot);
-                    base = __shfl_sync(0xFFFFFFFFu, base, 31);
-                    unsigned long long pos = base + (incl - n);
+                    wcnt += tot;
+                    return;
+                }
+                unsigned long long base = 0;
+                if (lane == 31) base = atomicAdd(a.count, (unsigned long long)tot);
+                base = __shfl_sync(0xFFFFFFFFu, base, 31);
+                unsigned long long pos = base + (incl - n);
+#pragma unroll
+                for (int g = 0; g < kRT / 32; ++g) {
+                    uint32_t mask = mk[g];
                     while (mask) {
                         const int j = __ffs(mask) - 1;
                         mask &= mask - 1;
                         if (pos < a.cap) {
                             a.pair_q[pos] = int32_t(q);
-                            a.pair_r[pos] = int32_t(cb + j);
+                            a.pair_r[pos] = int32_t(r0 + g * 32 + j);
                         }
                         ++pos;
                     }
                 }
             };
-            for (int64_t rt = rt0; rt < rt1; ++rt) {
+            // Column lengths of a ref tile (lane l: columns l, l+32, l+64, l+96; -1 past the
+            // refs), loaded one tile ahead so that their latency hides behind a whole tile.
+            auto load_lens = [&](int64_t rt, int (&lc)[kRT / 32]) {
                 const int64_t r0 = rt * kRT;
                 const int nvalid = int((a.nr - r0 < kRT ? a.nr - r0 : kRT));
-                // the tile's column lengths (lane l: columns l, l+32, l+64, l+96), requested
-                // before the accumulator wait so that their latency hides behind it
-                int lc[kRT / 32];
 #pragma unroll
                 for (int g = 0; g < kRT / 32; ++g) {
                     const int col = g * 32 + lane;
-                    lc[g] = col < nvalid ? min(int(a.rlens[r0 + col]), kLenSlots - 1) : -1;
+                    lc[g] = col < nvalid ? int(a.rlens[r0 + col]) : -1;
+                }
+            };
+            int lnext[kRT / 32];
+            if (rt0 < rt1) load_lens(rt0, lnext);
+            for (int64_t rt = rt0; rt < rt1; ++rt) {
+                const int64_t r0 = rt * kRT;
+                const int nvalid = int((a.nr - r0 < kRT ? a.nr - r0 : kRT));
+                // Before the accumulator wait: whether each group has a single length, and that
+                // length's threshold for this row.
+                int lc[kRT / 32];
+                bool uni[kRT / 32];
+                float tg[kRT / 32];
+#pragma unroll
+                for (int g = 0; g < kRT / 32; ++g) lc[g] = min(lnext[g], kLenSlots - 1);
+                if (rt + 1 < rt1) load_lens(rt + 1, lnext);
+#pragma unroll
+                for (int g = 0; g < kRT / 32; ++g) {
+                    const int l0 = __shfl_sync(0xFFFFFFFFu, lc[g], 0);
+                    uni[g] = __all_sync(0xFFFFFFFFu, lc[g] == l0 || lc[g] < 0);
+                    tg[g] = l0 >= 0 ? trow[l0] : INFINITY;
                 }
                 if (!bar_wait(BAR(14 + acc), accphase, s_abort, a.err)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                // groups c = 0..3, the TMEM load of group c + 1 in flight while c is examined
-                uint32_t va[32], vb[32];
+                // two groups per round: both TMEM loads in flight, then both masks
+                uint32_t va[32], vb[32], mk[kRT / 32];
                 const uint32_t tbase = tlane + acc * 256u;
                 __syncwarp();
-                tmem_ld32_issue(tbase, va);
-                tmem_ld32_wait(va);
-                if (nvalid > 32) tmem_ld32_issue(tbase + 32u, vb);
-                group(va, lc[0], r0, nvalid);
-                if (nvalid > 32) {
-                    tmem_ld32_wait(vb);
-                    if (nvalid > 64) tmem_ld32_issue(tbase + 64u, va);
-                    group(vb, lc[1], r0 + 32, nvalid - 32);
+#pragma unroll
+                for (int h = 0; h < kRT / 64; ++h) {
+                    const int g0 = 2 * h, g1 = 2 * h + 1;
+                    mk[g0] = mk[g1] = 0u;
+                    if (nvalid > g0 * 32) {  // warp-uniform
+                        tmem_ld32_issue(tbase + uint32_t(g0 * 32), va);
+                        if (nvalid > g1 * 32) tmem_ld32_issue(tbase + uint32_t(g1 * 32), vb);
+                        tmem_ld32_wait(va);
+                        mk[g0] = group_mask(va, lc[g0], uni[g0], tg[g0], nvalid - g0 * 32);
+                        if (nvalid > g1 * 32) {
+                            tmem_ld32_wait(vb);
+                            mk[g1] = group_mask(vb, lc[g1], uni[g1], tg[g1], nvalid - g1 * 32);
+                        }
+                    }
                 }
-                if (nvalid > 64) {
-                    tmem_ld32_wait(va);
-                    if (nvalid > 96) tmem_ld32_issue(tbase + 96u, vb);
-                    group(va, lc[2], r0 + 64, nvalid - 64);
-                }
-                if (nvalid > 96) {
-                    tmem_ld32_wait(vb);
-                    group(vb, lc[3], r0 + 96, nvalid - 96);
-                }
+                // the accumulator is free as soon as it has been read
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0) bar_arrive(BAR(16 + acc));
                 acc ^= 1u;
                 if (acc == 0) accphase ^= 1u;
+                if (__any_sync(0xFFFFFFFFu, (mk[0] | mk[1] | mk[2] | mk[3]) != 0u)) append(mk, r0);
             }
         }
+        flush();
     } else if (!RANGE && warp >= 2) {
         // --------------------------------------------------------------- selection --------
         const int ew = warp - 2, grp = ew >> 2, quarter = warp & 3;

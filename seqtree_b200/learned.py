@@ -3,10 +3,13 @@ kernel's 10^12 pairs are the cost (1e6 x 1e6 CDR3-like junctions).
 
 A small encoder (:class:`Encoder`; 2 conv + 2 attention layers, width 128, 64-d unit-length
 output) is trained on pairs scored by the exact gap-block kernel so that squared embedding
-distance tracks the score.  Its embeddings feed a BF16 tensor-core product that proposes the
-top-k refs of every query.  Every proposal is rescored by the exact kernel, so reported scores are
-always exact.  Recall against exhaustive search is measured on a held-out calibration slice, and
-query lengths whose recall falls below the bound are routed to the exhaustive kernel.
+distance tracks the score.  Its embeddings feed a BF16 tensor-core product that proposes
+candidate refs for every query: the top-k by dot product (``st_propose_topk``), or every ref whose
+dot product reaches a threshold chosen per (query length, ref length) cell
+(``st_propose_range``).  Every proposal is rescored by the exact kernel, so reported scores are
+always exact.  A held-out calibration batch sets the thresholds and routes the query and ref
+lengths where proposals cost more than exhaustive scoring to the exhaustive kernel, so that the
+estimated recall reaches the bound.
 
 Everything runs through ``libseqtree_b200.so``: the training kernels (forward, backward, Adam),
 the embedding, the proposal kernel and the exact scorer.
@@ -348,7 +351,9 @@ def range_tile_ranges(q_lens_sorted: np.ndarray, r_lens_sorted: np.ndarray,
 # proposal kernel, and a rescored candidate pair (pair kernel and its filtering).  Calibration
 # measures the exhaustive and candidate costs on its batch when the batch is large enough to
 # fill the GPU and keeps these otherwise; only the ratios matter to the choice.
-RANGE_COSTS = {"exhaustive": 1 / 3.0e11, "scan": 1 / 4.0e12, "candidate": 1 / 1.0e10}
+RANGE_COSTS = {"exhaustive": 1 / 3.0e11, "scan": 1 / 2.5e12, "candidate": 1 / 6.0e9}
+# Candidate pairs one proposal block may hold (the search splits its queries into blocks).
+RANGE_BLOCK_PAIRS = 1 << 27
 # Recall levels a cell's threshold can take (fraction of the cell's calibration hits kept).
 RANGE_LEVELS = (0.5, 0.75, 0.9, 0.95, 0.98, 0.99, 0.995, 1.0)
 
@@ -578,15 +583,19 @@ def allocate_recall(E, FL, CL, wq, wr, costs: dict, target: float):
     ``E`` [S, S] holds the calibration batch's exact hits per cell, ``FL`` / ``CL`` [S, S, LV] the
     hits found and the candidates proposed at each level (non-decreasing along the level axis),
     ``wq`` / ``wr`` the query and ref counts per length; ``costs`` gives seconds per exhaustively
-    scored pair ("exhaustive"), per scanned pair of a cell with proposals ("scan") and per
-    candidate ("candidate").  Every step takes the move with the most recovered hits per added
-    second: raising one cell by one level, or scoring one query or ref length exhaustively (its
-    cells are then exact and cost their pairs).  Returns (level, query lengths, ref lengths,
-    estimated recall, estimated seconds)."""
+    scored pair ("exhaustive"), per scanned pair ("scan") and per candidate ("candidate").  A query
+    length's proposals scan every ref whose length lies between the shortest and the longest
+    ref length it has a cell on for (refs are sorted by length), so switching a cell on may widen
+    that span.  Every step takes the move with the most recovered hits per added second:
+    raising one cell by one level, or scoring one query or ref length exhaustively (its cells
+    are then exact and cost their pairs).  Returns (level, query lengths, ref lengths, estimated
+    recall, estimated seconds)."""
     E = np.asarray(E, np.float64)
     S, LV = E.shape[0], FL.shape[2]
-    pairs = np.outer(np.asarray(wq, np.float64), np.asarray(wr, np.float64))
+    wq, wr = np.asarray(wq, np.float64), np.asarray(wr, np.float64)
+    pairs = np.outer(wq, wr)
     exh = costs["exhaustive"] * pairs
+    cum_r = np.concatenate([[0.0], np.cumsum(wr)])
     level = np.full((S, S), -1, np.int64)
     covered = np.zeros((S, S), bool)
     q_fb, r_fb = [], []
@@ -595,35 +604,46 @@ def allocate_recall(E, FL, CL, wq, wr, costs: dict, target: float):
         v = np.take_along_axis(arr, np.clip(lv, 0, LV - 1)[:, :, None], 2)[:, :, 0]
         return np.where(lv >= 0, v, 0.0)
 
-    def prop_cost(lv):
-        return np.where(lv >= 0, costs["scan"] * pairs + costs["candidate"] * at(CL, lv), 0.0)
+    def row_scan(a, on_row):
+        on = np.flatnonzero(on_row)
+        if on.size == 0:
+            return 0.0
+        return costs["scan"] * wq[a] * (cum_r[on[-1] + 1] - cum_r[on[0]])
+
+    def total(lv, cov):
+        on = (lv >= 0) & ~cov
+        t = exh[cov].sum() + costs["candidate"] * at(CL, lv)[on].sum()
+        return t + sum(row_scan(a, on[a]) for a in range(S))
 
     te = E.sum()
+    now = total(level, covered)
     while te:
-        pc, fnd = prop_cost(level), at(FL, level)
+        fnd = at(FL, level)
         if (E[covered].sum() + fnd[~covered].sum()) / te >= target:
             break
         best, move = 0.0, None
+        on = (level >= 0) & ~covered
         for a, b in zip(*np.where(~covered & (E > 0) & (level < LV - 1))):
             nl = level[a, b] + 1
             gain = FL[a, b, nl] - fnd[a, b]
             dt = costs["candidate"] * (CL[a, b, nl] - (CL[a, b, nl - 1] if nl > 0 else 0.0))
             if nl == 0:
-                dt += costs["scan"] * pairs[a, b]
+                row = on[a].copy()
+                row[b] = True
+                dt += row_scan(a, row) - row_scan(a, on[a])
             if gain > 0 and gain / max(dt, 1e-15) > best:
                 best, move = gain / max(dt, 1e-15), ("cell", a, b)
         for side, w, taken in (("q", wq, q_fb), ("r", wr, r_fb)):
             for x in range(S):
                 if w[x] == 0 or x in taken:
                     continue
-                new = np.zeros((S, S), bool)
+                cov = covered.copy()
                 if side == "q":
-                    new[x, :] = True
+                    cov[x, :] = True
                 else:
-                    new[:, x] = True
-                new &= ~covered
-                gain = (E - fnd)[new].sum()
-                dt = (exh - pc)[new].sum()
+                    cov[:, x] = True
+                gain = (E - fnd)[cov & ~covered].sum()
+                dt = total(level, cov) - now
                 if gain > 0 and gain / max(dt, 1e-15) > best:
                     best, move = gain / max(dt, 1e-15), (side, x)
         if move is None:
@@ -636,10 +656,10 @@ def allocate_recall(E, FL, CL, wq, wr, costs: dict, target: float):
         else:
             r_fb.append(move[1])
             covered[:, move[1]] = True
+        now = total(level, covered)
     level[covered] = -1
     rec = (E[covered].sum() + at(FL, level)[~covered].sum()) / te if te else 1.0
-    est = float(np.where(covered, exh, prop_cost(level)).sum())
-    return level, sorted(q_fb), sorted(r_fb), float(rec), est
+    return level, sorted(q_fb), sorted(r_fb), float(rec), float(total(level, covered))
 
 
 # -------------------------------------------------------------------------- search ----------
@@ -728,7 +748,7 @@ class LearnedIndex:
         self.proposal = proposal
         self.thresholds = np.full((PAD + 1, PAD + 1), np.inf, np.float32)
         self._thr_version = 0
-        self._range_cap = 0
+        self._range_per_query = 16.0
         self.band = band
         self.encoder, self.matrix = encoder, matrix
         self.gap_open, self.gap_extend, self.max_penalty, self.k = gap_open, gap_extend, max_penalty, k
@@ -849,7 +869,11 @@ class LearnedIndex:
             self.encoder.embed_into(qb.learn_set, q_emb.data_ptr(), 1, stream)
             mark("embed")
             if self.proposal == "range":
-                qi, ri = self._range_pairs(qb, q_emb)
+                # proposals and their rescore run block by block (bounded memory)
+                qi, ri, sc = self._range_hits(qb, q_emb)
+                parts.append((qb.learn_rows_t[qi.long()], self.learn_ids[ri.long()], sc))
+                mark("propose")
+                mark("rescore")
             else:
                 ids = torch.empty((n, self.k), dtype=torch.int32, device="cuda")
                 propose_topk_into(q_emb.data_ptr(), n, self.r_emb.data_ptr(), self.n_learn,
@@ -859,15 +883,16 @@ class LearnedIndex:
                 ri = ids.view(-1)
                 keep = ri >= 0
                 qi, ri = qi[keep], ri[keep]
-            mark("propose")
-            sc = torch.empty(qi.numel(), dtype=torch.int32, device="cuda")
-            if qi.numel():
-                pair_scores(qb.learn_set, self.learn_refs, qi.data_ptr(), ri.data_ptr(), qi.numel(),
-                            sc.data_ptr(), stream, matrix=self.matrix, gap_open=self.gap_open,
-                            gap_extend=self.gap_extend)
-            hit = sc <= self.max_penalty
-            parts.append((qb.learn_rows_t[qi[hit].long()], self.learn_ids[ri[hit].long()], sc[hit]))
-            mark("rescore")
+                mark("propose")
+                sc = torch.empty(qi.numel(), dtype=torch.int32, device="cuda")
+                if qi.numel():
+                    pair_scores(qb.learn_set, self.learn_refs, qi.data_ptr(), ri.data_ptr(),
+                                qi.numel(), sc.data_ptr(), stream, matrix=self.matrix,
+                                gap_open=self.gap_open, gap_extend=self.gap_extend)
+                hit = sc <= self.max_penalty
+                parts.append((qb.learn_rows_t[qi[hit].long()], self.learn_ids[ri[hit].long()],
+                              sc[hit]))
+                mark("rescore")
         if qb.learn_set is not None and self.fb_refs is not None:
             rows, rr, sc = self._sparse(qb.learn_set, self.fb_refs)
             parts.append((qb.learn_rows_t[rows], self.fb_ref_ids[rr.long()], sc))
@@ -891,16 +916,69 @@ class LearnedIndex:
         mark("merge")
         return out
 
-    def _range_pairs(self, qb: QueryBatch, q_emb):
-        """The threshold form's proposals of the batch's learned rows (local query and learned-ref
-        indices); the candidate buffers keep the largest size seen, so a repeated search is sized
-        right the first time."""
+    def _range_hits(self, qb: QueryBatch, q_emb):
+        """The threshold form's hits of the batch's learned rows: proposals, exact rescore and
+        the threshold, as (local query, learned-ref index, score).  The queries go in blocks of
+        whole 256-query tiles sized so that one block's candidates fit ``RANGE_BLOCK_PAIRS``
+        (the candidate count per query of the previous search sizes the blocks; a block that
+        overflows is split), so memory stays bounded whatever the thresholds let through."""
+        import torch
         n = len(qb.learn_set)
-        cap = max(self._range_cap, 16 * n)
-        qi, ri = propose_range(q_emb, qb.learn_lens_t, self.r_emb, self.learn_lens_t,
-                               self.thresholds, cap, qb.range_tiles(self))
-        self._range_cap = max(self._range_cap, int(qi.numel() * 1.1) + 1)
-        return qi, ri
+        stream = torch.cuda.current_stream().cuda_stream
+        tiles = qb.range_tiles(self)
+        ntiles = -(-n // QUERY_TILE)
+        per_q = max(self._range_per_query, 1.0)
+        step = max(1, min(ntiles, int(RANGE_BLOCK_PAIRS / (per_q * QUERY_TILE))))
+        out_q, out_r, out_s = [], [], []
+        seen, t0 = 0, 0
+        while t0 < ntiles:
+            t1 = min(ntiles, t0 + step)
+            q0, q1 = t0 * QUERY_TILE, min(n, t1 * QUERY_TILE)
+            pq = torch.empty(RANGE_BLOCK_PAIRS, dtype=torch.int32, device="cuda")
+            pr = torch.empty(RANGE_BLOCK_PAIRS, dtype=torch.int32, device="cuda")
+            cnt = propose_range_into(q_emb[q0:q1].data_ptr(), q1 - q0,
+                                     qb.learn_lens_t[q0:q1].data_ptr(), self.r_emb.data_ptr(),
+                                     self.n_learn, self.learn_lens_t.data_ptr(), self.thresholds,
+                                     pq.data_ptr(), pr.data_ptr(), RANGE_BLOCK_PAIRS, stream,
+                                     tiles[2 * t0:2 * t1].data_ptr())
+            if cnt > RANGE_BLOCK_PAIRS and t1 - t0 > 1:
+                step = max(1, (t1 - t0) // 2)  # too many candidates: smaller blocks
+                continue
+            if cnt > RANGE_BLOCK_PAIRS:  # one tile alone: the exact size
+                pq = torch.empty(cnt, dtype=torch.int32, device="cuda")
+                pr = torch.empty(cnt, dtype=torch.int32, device="cuda")
+                cnt = propose_range_into(q_emb[q0:q1].data_ptr(), q1 - q0,
+                                         qb.learn_lens_t[q0:q1].data_ptr(), self.r_emb.data_ptr(),
+                                         self.n_learn, self.learn_lens_t.data_ptr(),
+                                         self.thresholds, pq.data_ptr(), pr.data_ptr(), cnt,
+                                         stream, tiles[2 * t0:2 * t1].data_ptr())
+            seen += cnt
+            if cnt:
+                pq, pr = pq[:cnt], pr[:cnt]
+                pq += q0
+                sc = torch.empty(cnt, dtype=torch.int32, device="cuda")
+                pair_scores(qb.learn_set, self.learn_refs, pq.data_ptr(), pr.data_ptr(), cnt,
+                            sc.data_ptr(), stream, matrix=self.matrix, gap_open=self.gap_open,
+                            gap_extend=self.gap_extend)
+                hit = sc <= self.max_penalty
+                out_q.append(pq[hit])
+                out_r.append(pr[hit])
+                out_s.append(sc[hit])
+            del pq, pr
+            t0 = t1
+        self._range_per_query = seen / max(n, 1)
+        if not out_q:
+            z = torch.zeros(0, dtype=torch.int32, device="cuda")
+            return z, z, z
+        return torch.cat(out_q), torch.cat(out_r), torch.cat(out_s)
+
+    def _range_pairs(self, qb: QueryBatch, q_emb):
+        """The threshold form's raw proposals of the batch's learned rows (local query and
+        learned-ref indices), all at once."""
+        n = len(qb.learn_set)
+        cap = max(int(self._range_per_query * n * 1.1) + 1, 16 * n)
+        return propose_range(q_emb, qb.learn_lens_t, self.r_emb, self.learn_lens_t,
+                             self.thresholds, cap, qb.range_tiles(self))
 
     def search_strings(self, queries) -> "SparseScores":
         """The public call: thresholded hits of host query strings against the index's refs, as
@@ -1052,12 +1130,13 @@ class LearnedIndex:
         if n and self.n_learn:
             q_emb = torch.empty((n, 64), dtype=torch.bfloat16, device="cuda")
             self.encoder.embed_into(qb.learn_set, q_emb.data_ptr(), 1, stream)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
             rows, rr, _ = self._sparse(qb.learn_set, self.learn_refs)
-            e1.record()
-            e1.synchronize()
-            if n * self.n_learn >= 1e9:
+            if n * self.n_learn >= 1e9:  # a second, warm call (the first one tunes the kernel)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                rows, rr, _ = self._sparse(qb.learn_set, self.learn_refs)
+                e1.record()
+                e1.synchronize()
                 measured["exhaustive"] = e0.elapsed_time(e1) / 1e3 / (n * self.n_learn)
             dots = torch.empty(rows.numel(), dtype=torch.float32, device="cuda")
             rows32 = rows.to(torch.int32)
@@ -1116,6 +1195,7 @@ class LearnedIndex:
         self.set_thresholds(thr.astype(np.float32))
         cand = np.take_along_axis(CL, idx[:, :, None], 2)[:, :, 0]
         cand_q = float(np.where((level >= 0) & ~covered, cand, 0.0).sum() / max(n, 1))
+        self._range_per_query = 1.25 * cand_q * n / max(1, n - wq[q_fb].sum())
         te = E.sum()
         r2 = self.recall(codes, lens)
         wq1, wr1 = wq / max(wq.sum(), 1.0), wr / max(wr.sum(), 1.0)

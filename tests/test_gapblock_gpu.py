@@ -170,6 +170,13 @@ def test_bad_input_raises(st):
         _core.gapblock_matrix(["CAS"], ["CA"], "aa", m, 8, 1, [0] * 7, 3)
     with pytest.raises(ValueError, match="longer than the prior"):
         _core.gapblock_matrix(["CASSS"], ["CA"], "aa", m, 8, 1, [0] * 64, 3)
+    # queries are checked before refs, and symbols before the prior table (src/gapblock.cpp:85-102)
+    with pytest.raises(ValueError, match="symbol '#'"):
+        st.score_matrix(["CA#S"], ["CAJS"], m, 28)
+    with pytest.raises(ValueError, match="symbol 'J'"):
+        _core.gapblock_matrix(["CAS"], ["CJ"], "aa", m, 8, 1, [0] * 7, 3)
+    # a failed call leaves nothing behind for the next one
+    assert np.asarray(st.score_matrix(["CASS"], ["CASS", "CAS"], m, 28)).tolist() == [[0, 28]]
 
 
 def test_device_sets_match_host_calls(st):
