@@ -25,7 +25,8 @@ void align_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* similarity, int
                 int32_t mode, int32_t go, int32_t ge, int32_t dist, int32_t* out_d,
                 cudaStream_t stream);
 void hamming_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream_t stream);
-void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream_t stream);
+void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream_t stream,
+                      int64_t r0 = 0, int64_t r1 = -1);
 void gapblock_pairs_sets(st_seqset_s& qs, st_seqset_s& rs, const int32_t* qi_d, const int32_t* ri_d,
                          int64_t n, const int32_t* penalty, int32_t matrix_size, int32_t go,
                          int32_t ge, const int32_t* prior, int64_t prior_len, uint32_t prior_width,
@@ -125,6 +126,33 @@ void finish(Context& ctx, int32_t* out, int64_t N, int64_t K, int32_t* out_d) {
     STB_CUDA(cudaMemcpyAsync(ctx.flags_h + 8, ctx.flags_d + 8, 8 * sizeof(int64_t),
                              cudaMemcpyDeviceToHost, ctx.stream));
     STB_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+// The result copy overlapped with the computation: `launch(r0, r1)` enqueues the kernels of rows
+// [r0, r1) on the context's stream, and each block of rows is copied to `out` on a second stream
+// as soon as its kernels are done, so the copy of one block runs beside the next block's
+// kernels.  (With a pageable `out` the copies are synchronous and nothing overlaps.)
+void finish_pipelined(Context& ctx, int32_t* out, int64_t N, int64_t K, int32_t* out_d,
+                      int blocks, const std::function<void(int64_t, int64_t)>& launch) {
+    constexpr int kMaxBlocks = 8;
+    blocks = int(std::max<int64_t>(1, std::min<int64_t>({int64_t(blocks), int64_t(kMaxBlocks), N})));
+    if (!ctx.copy_stream) {
+        STB_CUDA(cudaStreamCreateWithFlags(&ctx.copy_stream, cudaStreamNonBlocking));
+        for (int b = 0; b < kMaxBlocks; ++b)
+            STB_CUDA(cudaEventCreateWithFlags(&ctx.block_ev[b], cudaEventDisableTiming));
+    }
+    for (int b = 0; b < blocks; ++b) {
+        const int64_t r0 = N * b / blocks, r1 = N * (b + 1) / blocks;
+        launch(r0, r1);
+        STB_CUDA(cudaEventRecord(ctx.block_ev[b], ctx.stream));
+        STB_CUDA(cudaStreamWaitEvent(ctx.copy_stream, ctx.block_ev[b], 0));
+        STB_CUDA(cudaMemcpyAsync(out + r0 * K, out_d + r0 * K, size_t(r1 - r0) * size_t(K) * 4,
+                                 cudaMemcpyDeviceToHost, ctx.copy_stream));
+    }
+    STB_CUDA(cudaMemcpyAsync(ctx.flags_h + 8, ctx.flags_d + 8, 8 * sizeof(int64_t),
+                             cudaMemcpyDeviceToHost, ctx.stream));
+    STB_CUDA(cudaStreamSynchronize(ctx.stream));
+    STB_CUDA(cudaStreamSynchronize(ctx.copy_stream));
 }
 
 void check_timeout(Context& ctx) {
@@ -616,14 +644,20 @@ static int32_t distance_common(const st_strings* a, const st_strings* b, bool le
             t.r.reset(make_seqset(b, -1, ctx.stream, nullptr, nullptr, ctx.tr));
         }
         int32_t* out_d = ctx.out_buf.as<int32_t>(size_t(N) * size_t(K));
-        {
-            Phase ph("plan+launch");
-            if (lev)
-                levenshtein_sets(*t.q, *t.r, out_d, ctx.stream);
-            else
-                hamming_sets(*t.q, *t.r, out_d, ctx.stream);
-        }
-        {
+        if (lev && N * K >= (int64_t(1) << 24)) {
+            // Levenshtein's kernel time is of the order of its result copy: overlap the two.
+            Phase ph("kernels+d2h (row blocks)");
+            finish_pipelined(ctx, out, N, K, out_d, 8, [&](int64_t r0, int64_t r1) {
+                levenshtein_sets(*t.q, *t.r, out_d, ctx.stream, r0, r1);
+            });
+        } else {
+            {
+                Phase ph("plan+launch");
+                if (lev)
+                    levenshtein_sets(*t.q, *t.r, out_d, ctx.stream);
+                else
+                    hamming_sets(*t.q, *t.r, out_d, ctx.stream);
+            }
             Phase ph("kernel+d2h");
             finish(ctx, out, N, K, out_d);
         }

@@ -1,4 +1,6 @@
 // Per-device context, workspace, pinned host cache and sequence-set upload/encoding.
+#include <unistd.h>
+
 #include "common.cuh"
 
 #include <nvtx3/nvToolsExt.h>
@@ -524,9 +526,23 @@ void* host_alloc(uint64_t bytes) {
     return p;
 }
 
-// Returned blocks stay pinned for reuse up to kPinCacheBytes in total; beyond that they are
-// unpinned and freed (a huge one-off result does not stay locked in host memory).
-constexpr size_t kPinCacheBytes = size_t(8) << 30;
+// Returned blocks stay pinned for reuse up to a limit in total; beyond that they are unpinned and
+// freed.  The limit is an eighth of physical memory (at least 8 GiB), or the number of GiB in
+// SEQTREE_B200_PIN_CACHE_GB: pinning and unpinning cost about a second per 10 GB, so a repeated
+// large sparse search (22 GB of rows) reuses its blocks instead of paying that on every call,
+// while a machine's memory is never mostly locked by a cache.
+size_t pin_cache_limit() {
+    static const size_t lim = [] {
+        if (const char* v = std::getenv("SEQTREE_B200_PIN_CACHE_GB")) {
+            const double gb = std::atof(v);
+            if (gb >= 0) return size_t(gb * double(size_t(1) << 30));
+        }
+        const long pages = sysconf(_SC_PHYS_PAGES), psz = sysconf(_SC_PAGE_SIZE);
+        const size_t phys = pages > 0 && psz > 0 ? size_t(pages) * size_t(psz) : size_t(64) << 30;
+        return std::max(size_t(8) << 30, phys / 8);
+    }();
+    return lim;
+}
 
 void host_free(void* p) {
     if (!p) return;
@@ -535,7 +551,7 @@ void host_free(void* p) {
     if (it == g_pin_size.end()) return;
     size_t cached = 0;
     for (const auto& kv : g_pin_free) cached += kv.first;
-    if (cached + it->second > kPinCacheBytes) {
+    if (cached + it->second > pin_cache_limit()) {
         g_pin_size.erase(it);
         cudaFreeHost(p);
         return;

@@ -78,12 +78,15 @@ struct Context {
     // host call.
     int64_t* flags_d = nullptr;
     int64_t* flags_h = nullptr;
+    // second stream and events of the host calls that overlap the result copy with the kernels
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t block_ev[8] = {};
     // named scratch, grow-only
     DevBuf out_buf, q_codes, r_codes, table_buf, prior_buf, ftab_buf, work_a, work_b, work_c;
     // sparse output: unsorted hit keys and scores, sorted keys, radix-sort scratch
     DevBuf sp_keys, sp_vals, sp_sorted, sp_temp;
     // candidate lists of the learned-proposal kernel; the threshold form's table
-    DevBuf topk_cand, prop_thr;
+    DevBuf topk_cand, prop_thr, prop_items;
     std::vector<uint8_t> prop_thr_key;
     // bf16 operands of the training GEMM, packed in the tensor-core layout
     DevBuf gemm_a, gemm_b;

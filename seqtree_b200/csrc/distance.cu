@@ -408,16 +408,22 @@ void hamming_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream_t s
     note_launch(name);
 }
 
-void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream_t stream) {
+void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream_t stream,
+                      int64_t r0, int64_t r1) {
     if (a.alphabet != -1 || b.alphabet != -1)
         fail(ST_EINVAL, "seqtree_b200: distance sets must hold raw bytes (alphabet -1)");
-    const int64_t N = a.count, K = b.count;
+    if (r1 < 0) r1 = a.count;
+    if (r0 < 0 || r0 > r1 || r1 > a.count) fail(ST_EINVAL, "seqtree_b200: bad row range");
+    const int64_t N = r1 - r0, K = b.count;
     if (N == 0 || K == 0) return;
     Context& ctx = context();
     DistCache& dc = compute_codes(a, b, stream, ctx);
     const int sigma = std::max(1, dc.sigma);
     const uint8_t* ac = static_cast<uint8_t*>(dc.ac.ptr);
     const uint8_t* bc = static_cast<uint8_t*>(dc.bc.ptr);
+    // rows [r0, r1): their offsets and their block of the result
+    const int64_t* aoff = a.d_off + r0;
+    out_d += r0 * K;
     const dim3 grid(unsigned(ceil_div(K, kLevWarps * 32)), unsigned(ceil_div(N, kLevRows)));
     // Bit-vector path: refs up to 512 symbols (1, 2, 4 or 8 words) while the Peq table fits.
     const int words = b.max_len <= 64    ? 1
@@ -433,16 +439,16 @@ void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream
                                       : reinterpret_cast<const void*>(levenshtein_kernel<8>);
         ensure_smem_limit(kern, smem);
         if (words == 1)
-            levenshtein_kernel<1><<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off,
+            levenshtein_kernel<1><<<grid, kLevWarps * 32, smem, stream>>>(ac, aoff, bc, b.d_off,
                                                                          N, K, sigma, out_d);
         else if (words == 2)
-            levenshtein_kernel<2><<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off,
+            levenshtein_kernel<2><<<grid, kLevWarps * 32, smem, stream>>>(ac, aoff, bc, b.d_off,
                                                                          N, K, sigma, out_d);
         else if (words == 4)
-            levenshtein_kernel<4><<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off,
+            levenshtein_kernel<4><<<grid, kLevWarps * 32, smem, stream>>>(ac, aoff, bc, b.d_off,
                                                                          N, K, sigma, out_d);
         else
-            levenshtein_kernel<8><<<grid, kLevWarps * 32, smem, stream>>>(ac, a.d_off, bc, b.d_off,
+            levenshtein_kernel<8><<<grid, kLevWarps * 32, smem, stream>>>(ac, aoff, bc, b.d_off,
                                                                          N, K, sigma, out_d);
         STB_CUDA(cudaGetLastError());
         note_launch("levenshtein_kernel");
@@ -457,7 +463,7 @@ void levenshtein_sets(st_seqset_s& a, st_seqset_s& b, int32_t* out_d, cudaStream
     threads = std::max<int64_t>(256, std::min<int64_t>(threads, (int64_t(1) << 29) / per));
     threads = ceil_div(threads, 256) * 256;
     int32_t* scratch = ctx.work_a.as<int32_t>(size_t(threads) * per);
-    levenshtein_dp_kernel<<<unsigned(threads / 256), 256, 0, stream>>>(ac, a.d_off, bc, b.d_off, N, K,
+    levenshtein_dp_kernel<<<unsigned(threads / 256), 256, 0, stream>>>(ac, aoff, bc, b.d_off, N, K,
                                                                        scratch, out_d);
     STB_CUDA(cudaGetLastError());
     note_launch("levenshtein_dp_kernel");

@@ -39,6 +39,8 @@
 // warp in shared memory and flushed to global memory 512 pairs at a time (one atomicAdd each).
 #include <cuda_bf16.h>
 
+#include <cub/block/block_scan.cuh>
+
 #include <cfloat>
 #include <algorithm>
 #include <cstdint>
@@ -97,6 +99,8 @@ struct ProposeArgs {
     int32_t* pair_r;           // [cap] proposed pairs: ref index
     unsigned long long cap;
     unsigned long long* count; // every proposed pair counted, the first cap written
+    const int4* items;         // threshold form: (query tile, first, last ref tile) work items
+    const int* nitems;         //   and their count (device), or null: one unit per query tile
 };
 
 // The ref tiles a query tile scans: the caller's [first, last) clamped into [0, ntr), so every
@@ -267,6 +271,21 @@ __device__ __forceinline__ void propose_body(const ProposeArgs& a) {
     auto BAR = [&](int i) { return bar0 + 8u * uint32_t(i); };
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int64_t ntq = (a.nq + kQT - 1) / kQT, ntr = (a.nr + kRT - 1) / kRT;
+    // Work units: a query tile with its range of ref tiles, or (with an item list) a query tile
+    // with one chunk of its range.  Every role walks the same units in the same order.
+    const int64_t nunits = a.items ? int64_t(*a.nitems) : ntq;
+    auto unit = [&](int64_t u, int64_t& qt, int64_t& rt0, int64_t& rt1) {
+        if (a.items) {
+            const int4 v = a.items[u];
+            qt = v.x < 0 ? 0 : (v.x >= ntq ? ntq - 1 : v.x);
+            rt0 = v.y < 0 ? 0 : (v.y > ntr ? ntr : v.y);
+            rt1 = (v.z < rt0 || v.x < 0 || v.x >= ntq) ? rt0 : (v.z > ntr ? ntr : v.z);
+        } else {
+            qt = u;
+            rt0 = tile_first(a, qt, ntr);
+            rt1 = tile_last(a, qt, ntr);
+        }
+    };
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -307,7 +326,9 @@ __device__ __forceinline__ void propose_body(const ProposeArgs& a) {
         uint32_t issued = 0, par = 0;  // per stage: issued at least once, parity of last issue
         bool a_issued = false;
         uint32_t a_par = 0;
-        for (int64_t qt = blockIdx.x; qt < ntq; qt += gridDim.x) {
+        for (int64_t u = blockIdx.x; u < nunits; u += gridDim.x) {
+            int64_t qt, rt0, rt1;
+            unit(u, qt, rt0, rt1);
             if (!bar_wait(BAR(13), aphase ^ 1u, s_abort, a.err)) break;
             const uint32_t rows = uint32_t((a.nq - qt * kQT < kQT ? a.nq - qt * kQT : kQT));
             bar_expect_tx(BAR(12), rows * kRowB);
@@ -316,7 +337,6 @@ __device__ __forceinline__ void propose_body(const ProposeArgs& a) {
             a_par = aphase;
             aphase ^= 1u;
             bool ok = true;
-            const int64_t rt0 = tile_first(a, qt, ntr), rt1 = tile_last(a, qt, ntr);
             for (int64_t rt = rt0; rt < rt1; ++rt) {
                 if (!bar_wait(BAR(kStages + stage), sphase ^ 1u, s_abort, a.err)) {
                     ok = false;
@@ -342,12 +362,13 @@ __device__ __forceinline__ void propose_body(const ProposeArgs& a) {
         // ------------------------------------------------------------- MMA issuer ---------
         const uint32_t sA = smem_u32(smem + kSmA), sB = smem_u32(smem + kSmB);
         uint32_t stage = 0, sphase = 0, aphase = 0, acc = 0, accphase = 0;
-        for (int64_t qt = blockIdx.x; qt < ntq; qt += gridDim.x) {
+        for (int64_t u = blockIdx.x; u < nunits; u += gridDim.x) {
+            int64_t qt, rt0, rt1;
+            unit(u, qt, rt0, rt1);
             if (!bar_wait(BAR(12), aphase, s_abort, a.err)) break;
             aphase ^= 1u;
             tc_fence_after();
             bool ok = true;
-            const int64_t rt0 = tile_first(a, qt, ntr), rt1 = tile_last(a, qt, ntr);
             for (int64_t rt = rt0; rt < rt1; ++rt) {
                 if (!bar_wait(BAR(16 + acc), accphase ^ 1u, s_abort, a.err) ||
                     !bar_wait(BAR(stage), sphase, s_abort, a.err)) {
@@ -415,12 +436,13 @@ __device__ __forceinline__ void propose_body(const ProposeArgs& a) {
         };
         uint32_t acc = 0, accphase = 0;
         bool ok = true;
-        for (int64_t qt = blockIdx.x; qt < ntq && ok; qt += gridDim.x) {
+        for (int64_t u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+            int64_t qt, rt0, rt1;
+            unit(u, qt, rt0, rt1);
             const int64_t q = qt * kQT + grp * 128 + row;
             const bool qvalid = q < a.nq;
             const int ql = qvalid ? min(int(a.qlens[q]), kLenSlots - 1) : 0;
             const float* trow = thr_s + ql * kLenSlots;
-            const int64_t rt0 = tile_first(a, qt, ntr), rt1 = tile_last(a, qt, ntr);
             // Survivor mask of one 32-column group.  `uni` / `t`: the group has one ref length
             // and its threshold; otherwise each column's threshold is looked up with its length
             // (`lcol`, -1 past the refs) taken by shuffle.
@@ -572,11 +594,12 @@ __device__ __forceinline__ void propose_body(const ProposeArgs& a) {
         const uint32_t tlane = tmem + (uint32_t(quarter * 32) << 16) + uint32_t(grp) * 128u;
         uint32_t acc = 0, accphase = 0;
         bool ok = true;
-        for (int64_t qt = blockIdx.x; qt < ntq && ok; qt += gridDim.x) {
+        for (int64_t u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+            int64_t qt, rt0, rt1;
+            unit(u, qt, rt0, rt1);
             const int64_t q = qt * kQT + grp * 128 + row;
             float thr = q < a.nq ? -INFINITY : INFINITY;
             int count = 0;
-            const int64_t rt0 = tile_first(a, qt, ntr), rt1 = tile_last(a, qt, ntr);
             for (int64_t rt = rt0; rt < rt1; ++rt) {
                 if (!bar_wait(BAR(14 + acc), accphase, s_abort, a.err)) {
                     ok = false;
@@ -689,6 +712,51 @@ __global__ void __launch_bounds__(kThreads, 1) propose_range_kernel(ProposeArgs 
     propose_body<true>(a);
 }
 
+// The threshold form's work list: each query tile's ref-tile range [first, last) (every ref tile
+// without ranges; clamped like tile_first / tile_last) cut into chunks of at most kItemTiles
+// tiles, query tile by query tile.  One block of 1024 threads; a tile's pairs need no state
+// across chunks, so any split gives the same pairs, and equal-sized items keep the persistent
+// CTAs balanced whatever the ranges' lengths.
+constexpr int kItemTiles = 32;
+constexpr int kItemThreads = 1024;
+
+__global__ void __launch_bounds__(kItemThreads) range_items_kernel(const int32_t* ranges,
+                                                                   int64_t ntq, int64_t ntr,
+                                                                   int4* items, int* nitems) {
+    typedef cub::BlockScan<int, kItemThreads> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ int s_base;
+    if (threadIdx.x == 0) s_base = 0;
+    __syncthreads();
+    for (int64_t t0 = 0; t0 < ntq; t0 += kItemThreads) {
+        const int64_t t = t0 + threadIdx.x;
+        int64_t f = 0, l = 0;
+        if (t < ntq) {
+            if (ranges) {
+                f = ranges[2 * t];
+                f = f < 0 ? 0 : (f > ntr ? ntr : f);
+                l = ranges[2 * t + 1];
+                l = l < f ? f : (l > ntr ? ntr : l);
+            } else {
+                l = ntr;
+            }
+        }
+        const int cnt = int((l - f + kItemTiles - 1) / kItemTiles);
+        int excl = 0, total = 0;
+        Scan(tmp).ExclusiveSum(cnt, excl, total);
+        const int base = s_base;
+        for (int c = 0; c < cnt; ++c) {
+            const int64_t c0 = f + int64_t(c) * kItemTiles;
+            items[base + excl + c] =
+                make_int4(int(t), int(c0), int(c0 + kItemTiles < l ? c0 + kItemTiles : l), 0);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_base = base + total;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *nitems = s_base;
+}
+
 // Dot products of listed (query, ref) pairs of swizzled bf16 embeddings, one thread per pair,
 // fp32 accumulation in chunk order.  An index outside its embedding set gives NaN.
 __global__ void embed_dots_kernel(const uint4* __restrict__ qemb, int64_t nq,
@@ -774,8 +842,15 @@ int64_t propose_range(const void* qemb, int64_t nq, const uint8_t* qlens, const 
     float* d_thr = ctx.prop_thr.as<float>(kLenSlots * kLenSlots);
     if (!same_as_last(ctx.prop_thr_key, thr, kThrBytes)) h2d(d_thr, thr, kThrBytes, stream);
     ensure_smem_limit(reinterpret_cast<const void*>(propose_range_kernel), kSmemBytes);
-    const int64_t ntq = (nq + kQT - 1) / kQT;
-    const int grid = int(std::min<int64_t>(ntq, ctx.num_sms));
+    const int64_t ntq = (nq + kQT - 1) / kQT, ntr = (nr + kRT - 1) / kRT;
+    const int64_t max_items = ntq * ((ntr + kItemTiles - 1) / kItemTiles);
+    if (max_items >= (int64_t(1) << 31)) fail(ST_EINVAL, "seqtree_b200: too many proposal work items");
+    int4* items = ctx.prop_items.as<int4>(size_t(max_items));
+    int* nitems = reinterpret_cast<int*>(ctx.flags_d + 12);
+    range_items_kernel<<<1, kItemThreads, 0, stream>>>(ranges, ntq, ntr, items, nitems);
+    STB_CUDA(cudaGetLastError());
+    note_launch(nullptr);
+    const int grid = int(std::min<int64_t>(max_items, ctx.num_sms));
     ProposeArgs a{};
     a.qemb = static_cast<const uint8_t*>(qemb);
     a.remb = static_cast<const uint8_t*>(remb);
@@ -790,7 +865,9 @@ int64_t propose_range(const void* qemb, int64_t nq, const uint8_t* qlens, const 
     a.pair_r = pr;
     a.cap = static_cast<unsigned long long>(cap);
     a.count = reinterpret_cast<unsigned long long*>(ctx.flags_d + 11);
-    STB_CUDA(cudaMemsetAsync(ctx.flags_d + 8, 0, 8 * sizeof(int64_t), stream));
+    a.items = items;
+    a.nitems = nitems;
+    STB_CUDA(cudaMemsetAsync(ctx.flags_d + 8, 0, 4 * sizeof(int64_t), stream));
     propose_range_kernel<<<grid, kThreads, kSmemBytes, stream>>>(a);
     STB_CUDA(cudaGetLastError());
     note_launch("propose_range_kernel");
