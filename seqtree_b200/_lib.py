@@ -313,6 +313,21 @@ def pinned_int32(rows: int, cols: int) -> np.ndarray:
     return np.frombuffer(buf, dtype=np.int32, count=n).reshape(rows, cols)
 
 
+def pinned_array(n: int, dtype) -> np.ndarray:
+    """A 1-d int32 or int64 array of n elements in page-locked host memory from the library's
+    cache (ordinary memory when no pinned block can be had)."""
+    dtype = np.dtype(dtype)
+    ctype = {4: ctypes.c_int32, 8: ctypes.c_int64}[dtype.itemsize]
+    if n == 0:
+        return np.zeros(0, dtype)
+    ptr = lib.st_host_alloc(n * dtype.itemsize)
+    if not ptr:
+        return np.empty(n, dtype)
+    buf = (ctype * n).from_address(ptr)
+    buf._owner = _PinnedOwner(ptr)
+    return np.frombuffer(buf, dtype=dtype, count=n)
+
+
 def adopt_pinned(ptr, n: int, ctype, dtype) -> np.ndarray:
     """A numpy view of n elements of a pinned block the library allocated; the view owns the
     block (it returns to the cache when the last view is gone)."""

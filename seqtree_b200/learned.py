@@ -668,12 +668,28 @@ def _subset(codes, lens, rows):
     return SeqSet(codes_to_packed(codes[rows], lens[rows]), "aa") if rows.size else None
 
 
+def _packed_subset(packed: _lib.Packed, lens: np.ndarray, rows: np.ndarray):
+    """The listed rows of a packed string set as a device set (letters gathered on the host and
+    encoded on the device, so an invalid symbol raises the alphabet's ValueError)."""
+    from .device import SeqSet
+    if not rows.size:
+        return None
+    sl = lens[rows].astype(np.int64)
+    off = np.zeros(rows.size + 1, np.int64)
+    np.cumsum(sl, out=off[1:])
+    src = np.repeat(packed.offsets[rows] - off[:-1], sl) + np.arange(off[-1], dtype=np.int64)
+    return SeqSet(_lib.Packed.from_arrays(packed.data[src], off), "aa")
+
+
 class QueryBatch:
     """Queries resident on the device for :meth:`LearnedIndex.search`, split by the index's
     query-length fallback: ``learn`` rows go through the proposals, ``fb`` rows through the
     exhaustive kernel."""
 
-    def __init__(self, index: "LearnedIndex", codes: np.ndarray, lens: np.ndarray):
+    def __init__(self, index: "LearnedIndex", codes: np.ndarray | None, lens: np.ndarray,
+                 packed: _lib.Packed | None = None):
+        """From padded codes [n, 32] and lengths, or (``codes`` None) from a packed string set
+        whose lengths are ``lens``."""
         import torch
         self.lens = np.asarray(lens, np.int32)
         self.count = int(self.lens.size)
@@ -683,8 +699,12 @@ class QueryBatch:
         # learn rows in length order, so that a 256-query tile of the proposal kernel spans few
         # lengths (its ref band is then narrow)
         self.learn_rows = learn[np.argsort(self.lens[learn], kind="stable")]
-        self.fb_set = _subset(codes, self.lens, self.fb_rows)
-        self.learn_set = _subset(codes, self.lens, self.learn_rows)
+        if codes is None:
+            self.fb_set = _packed_subset(packed, self.lens, self.fb_rows)
+            self.learn_set = _packed_subset(packed, self.lens, self.learn_rows)
+        else:
+            self.fb_set = _subset(codes, self.lens, self.fb_rows)
+            self.learn_set = _subset(codes, self.lens, self.learn_rows)
         self.fb_rows_t = torch.from_numpy(self.fb_rows).cuda()
         self.learn_rows_t = torch.from_numpy(self.learn_rows).cuda()
         self.learn_lens_t = torch.from_numpy(
@@ -982,12 +1002,28 @@ class LearnedIndex:
 
     def search_strings(self, queries) -> "SparseScores":
         """The public call: thresholded hits of host query strings against the index's refs, as
-        host CSR (``gapblock.SparseScores``, the format of ``score_sparse``)."""
+        host CSR (``gapblock.SparseScores``, the format of ``score_sparse``).  The strings are
+        packed once by the library and uploaded as they are (the device encodes them); the rows
+        come back into pinned blocks of the library's cache."""
+        import torch
+
         from .gapblock import SparseScores
-        codes, lens = pad_codes(list(queries))
-        ip, ri, sc = self.search(self.queries(codes, lens))
-        return SparseScores(ip.cpu().numpy(), ri.cpu().numpy(), sc.cpu().numpy(),
-                            (len(lens), self.nr), self.max_penalty)
+        packed = _lib.pack(list(queries))
+        lens = np.diff(packed.offsets).astype(np.int32)
+        if lens.size and (lens.min() < 1 or lens.max() > PAD):
+            raise ValueError("encoder inputs must have 1..32 residues")
+        bad = _CODE[packed.data[:int(packed.offsets[-1])]] == 255
+        if bad.any():  # the first invalid symbol over all queries, as pad_codes reports it
+            raise ValueError(f"symbol '{chr(int(packed.data[np.argmax(bad)]))}' is not in the "
+                             "alphabet")
+        ip, ri, sc = self.search(QueryBatch(self, None, lens, packed))
+        host = []
+        for t in (ip, ri, sc):
+            h = _lib.pinned_array(t.numel(), np.int64 if t.dtype == torch.int64 else np.int32)
+            if t.numel():
+                torch.from_numpy(h).copy_(t)
+            host.append(h)
+        return SparseScores(*host, (len(lens), self.nr), self.max_penalty)
 
     def exhaustive(self, qb: QueryBatch, codes: np.ndarray):
         """The exhaustive sparse kernel's CSR for the same queries (the exact answer)."""

@@ -285,3 +285,27 @@ def test_range_learned_search_is_exact_and_calibrated(cuda_ready):
     rec = idx.recall(qc, ql)
     assert rec["subset_of_exact"]
     assert rec["recall"] >= 0.9
+
+
+@pytest.mark.gpu
+def test_search_strings_matches_the_code_path(cuda_ready):
+    """search_strings (strings packed by the library, rows copied into pinned blocks) returns
+    exactly the CSR of search() on padded codes, and rejects bad input with pad_codes' errors."""
+    import seqtree_b200 as stb
+    from seqtree_b200 import learned as L
+    M = stb.SubstitutionMatrix.blosum62()
+    enc = L.Encoder(seed=5)
+    rc, rl = L.cdr3_codes(80, 5000)
+    cc, cl = L.cdr3_codes(81, 400)
+    idx = L.LearnedIndex(enc, rc, rl, matrix=M, gap_open=8, max_penalty=24, proposal="range")
+    idx.calibrate(cc, cl, bound=0.99)
+    qc, ql = L.cdr3_codes(82, 700)
+    strings = L.codes_to_strings(qc, ql)
+    got = idx.search_strings(strings)
+    ip, ri, sc = (t.cpu().numpy() for t in idx.search(idx.queries(qc, ql)))
+    assert np.array_equal(got.indptr, ip) and np.array_equal(got.ref_ids, ri)
+    assert np.array_equal(got.scores, sc) and got.shape == (700, 5000)
+    with pytest.raises(ValueError, match="symbol 'J'"):
+        idx.search_strings(["CASSLF", "CAJSF", "CAS#F"])
+    with pytest.raises(ValueError, match="1..32 residues"):
+        idx.search_strings(["CASSLF", ""])
