@@ -200,6 +200,12 @@ def check(code: int, err: st_error) -> None:
     raise RuntimeError(msg)
 
 
+try:  # the list packer (csrc/pack_py.c); without it the join-and-split path below packs lists
+    from . import _pack
+except ImportError:
+    _pack = None
+
+
 def _pack_ascii(seqs: list):
     """(bytes, offsets) of a list of ASCII strings without a per-string Python loop: the list is
     joined with a newline separator, which the library splits (``st_split_joined``).  None when
@@ -226,6 +232,12 @@ class Packed:
 
     def __init__(self, seqs):
         seqs = seqs if isinstance(seqs, list) else list(seqs)
+        packed = _pack.pack(seqs) if _pack is not None else None
+        if packed is not None:  # ASCII strings, copied in one pass by the extension
+            self.data = np.frombuffer(packed[0], dtype=np.uint8)
+            self.offsets = np.frombuffer(packed[1], dtype=np.int64)
+            self.struct = st_strings(self.data.ctypes.data, self.offsets.ctypes.data, len(seqs))
+            return
         fast = _pack_ascii(seqs)
         if fast is not None:
             self.data, self.offsets = fast

@@ -41,7 +41,22 @@ def _stale(obj: Path, src: Path, newest_header: float) -> bool:
     return src.stat().st_mtime > t or newest_header > t
 
 
+def build_pack(force: bool = False) -> Path:
+    """The CPython extension ``seqtree_b200._pack`` (``csrc/pack_py.c``), which packs the Python
+    mirror's string lists; built with the running interpreter's headers."""
+    import sysconfig
+    src = CSRC / "pack_py.c"
+    out = HERE / ("_pack" + sysconfig.get_config_var("EXT_SUFFIX"))
+    if force or not out.exists() or src.stat().st_mtime > out.stat().st_mtime:
+        cmd = ["gcc", "-O2", "-shared", "-fPIC", f"-I{sysconfig.get_paths()['include']}",
+               str(src), "-o", str(out)]
+        print("[seqtree_b200]", "gcc", src.name, flush=True)
+        subprocess.run(cmd, check=True)
+    return out
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
+    build_pack(force)
     BUILD.mkdir(exist_ok=True)
     newest = max((h.stat().st_mtime for h in _headers()), default=0.0)
     objs = []

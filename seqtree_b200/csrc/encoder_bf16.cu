@@ -23,6 +23,9 @@
 // accumulators with tcgen05.ld.  Every wait is bounded.
 #include <cuda_bf16.h>
 
+#include <cstring>
+#include <vector>
+
 #include <algorithm>
 #include <cmath>
 #include <memory>
@@ -339,8 +342,10 @@ struct LayerArgs {
     const uint8_t* h;            // tiled input
     const __nv_bfloat16* wqkv;   // tiled [384 x 128]
     const __nv_bfloat16* wo;     // tiled [128 x 128]
-    const float* bqkv;           // 384
-    const float* bo;             // 128
+    // Biases by value: the drain warps read them with warp-uniform indices, which the kernel
+    // parameter space (constant bank) serves without a global-memory round trip.
+    float bqkv[3 * 128];
+    float bo[128];
     uint8_t* out;                // tiled output
     const int32_t* lens;
     int64_t tiles;
@@ -363,7 +368,7 @@ __device__ __forceinline__ void put_unit(uint8_t* tile, int r, int u, const floa
     *reinterpret_cast<uint4*>(tile + unit_off(r, u)) = pk.v;
 }
 
-__global__ void __launch_bounds__(kGemmThreads, 1) attn_layer_kernel(LayerArgs g) {
+__global__ void __launch_bounds__(kGemmThreads, 1) attn_layer_kernel(const __grid_constant__ LayerArgs g) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((uintptr_t(smem_raw) + 1023) & ~uintptr_t(1023));
     // barriers: 0 weights, 1 h full, 2 h empty (8), 3 QKV done, 4 Q/K staged (8), 5 S done,
@@ -662,6 +667,7 @@ __global__ void pool_out_bf16_kernel(const uint8_t* __restrict__ h, const int32_
 struct Bf16State {
     int64_t version = -1;
     DevBuf w2, wqkv[2], wo[2], lens, h1, ha, hb;
+    std::vector<float> bias[2];  // per layer: bqkv (384) then bo (128), host copies
 };
 
 void launch_conv2(const GemmArgs& g, int sms, cudaStream_t st) {
@@ -700,6 +706,15 @@ void encoder_embed_bf16(const float* prm, int64_t version, std::shared_ptr<void>
             prep(B.wo[l], prm + oL0 + l * kLayer + lWo, kW, 1);
         }
         note_launch(nullptr, 5);
+        for (int l = 0; l < 2; ++l) {  // the layers' biases travel as kernel parameters
+            B.bias[l].resize(4 * kW);
+            const float* Lp = prm + oL0 + l * kLayer;
+            STB_CUDA(cudaMemcpyAsync(B.bias[l].data(), Lp + lbqkv, sizeof(float) * 3 * kW,
+                                     cudaMemcpyDeviceToHost, st));
+            STB_CUDA(cudaMemcpyAsync(B.bias[l].data() + 3 * kW, Lp + lbo, sizeof(float) * kW,
+                                     cudaMemcpyDeviceToHost, st));
+        }
+        STB_CUDA(cudaStreamSynchronize(st));
         B.version = version;
     }
     constexpr int64_t kChunk = 32768;  // sequences per pass (8,192 tiles)
@@ -729,13 +744,12 @@ void encoder_embed_bf16(const float* prm, int64_t version, std::shared_ptr<void>
         uint8_t* hin = ha;
         uint8_t* hout = hb;
         for (int l = 0; l < 2; ++l) {
-            const float* Lp = prm + oL0 + l * kLayer;
             LayerArgs la{};
             la.h = hin;
             la.wqkv = static_cast<const __nv_bfloat16*>(B.wqkv[l].ptr);
             la.wo = static_cast<const __nv_bfloat16*>(B.wo[l].ptr);
-            la.bqkv = Lp + lbqkv;
-            la.bo = Lp + lbo;
+            std::memcpy(la.bqkv, B.bias[l].data(), sizeof la.bqkv);
+            std::memcpy(la.bo, B.bias[l].data() + 3 * kW, sizeof la.bo);
             la.out = hout;
             la.lens = lens;
             la.tiles = tiles;

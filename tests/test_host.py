@@ -126,6 +126,25 @@ def test_joined_packing_matches_the_general_path(seqs):
     assert p.max_len == max(len(e) for e in enc)
 
 
+@pytest.mark.parametrize("seqs", [["CASS", "", "AB"], [""], [], ["ACDEFGHIKLMNPQRSTVWY"] * 3,
+                                  ["A\nB", "C"], ["\n"], [b"AC", "D"], ["é", "a"], [1, "A"]])
+def test_list_packer_extension_matches_the_general_path(seqs):
+    """seqtree_b200._pack (csrc/pack_py.c) packs lists of ASCII str in one pass -- newlines
+    included -- into the bytes and offsets of the per-string path, and declines (None) anything
+    else, which then takes the general path."""
+    from seqtree_b200 import _pack
+    got = _pack.pack(list(seqs))
+    if any(not isinstance(s, str) or not s.isascii() for s in seqs):
+        assert got is None
+        return
+    enc = [s.encode() for s in seqs]
+    want_off = np.concatenate([[0], np.cumsum([len(e) for e in enc])]).astype(np.int64)
+    data, off = np.frombuffer(got[0], np.uint8), np.frombuffer(got[1], np.int64)
+    assert off.tolist() == want_off.tolist() and bytes(data[:want_off[-1]]) == b"".join(enc)
+    assert data.size >= 1
+    assert _pack.pack(tuple(seqs)) is None  # lists only; other sequences are listed first
+
+
 def test_builtin_prior_cubes_are_memoised_read_only():
     cp = central_prior(7)
     a, b = prior_cube(cp, 9), prior_cube(cp, 9)
