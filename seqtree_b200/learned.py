@@ -431,10 +431,13 @@ def cdr3_like(seed: int, n: int) -> list[str]:
     return codes_to_strings(*cdr3_codes(seed, n))
 
 
-def mutate_codes(codes: np.ndarray, lens: np.ndarray, rng) -> tuple[np.ndarray, np.ndarray]:
+def mutate_codes(codes: np.ndarray, lens: np.ndarray, rng, long_share: float = 0.0,
+                 long_max: int = 16) -> tuple[np.ndarray, np.ndarray]:
     """Near neighbours: 1-3 random substitutions, then one random indel block of 1-3 residues at
     a random position (a deletion or an insertion with equal odds, whichever keeps 1..32
-    residues; a deletion near the end removes what is there)."""
+    residues; a deletion near the end removes what is there).  A ``long_share`` of the pairs
+    takes a block of 4..``long_max`` residues instead: the gap blocks through which a short
+    junction matches a longer one."""
     n = lens.size
     out = codes.copy()
     rows = np.arange(n)
@@ -445,6 +448,8 @@ def mutate_codes(codes: np.ndarray, lens: np.ndarray, rng) -> tuple[np.ndarray, 
         m = t < nsub
         out[rows[m], pos[m]] = aa[m]
     blk = rng.integers(1, 4, size=n)
+    if long_share > 0:
+        blk = np.where(rng.random(n) < long_share, rng.integers(4, long_max + 1, size=n), blk)
     pos = np.minimum((rng.random(n) * (lens + 1)).astype(np.int64), lens)
     want_del = rng.random(n) < 0.5
     dele = want_del & (lens - blk >= 1)
@@ -468,7 +473,8 @@ def mutate(seqs, rng) -> list[str]:
     return codes_to_strings(*mutate_codes(codes, lens, rng))
 
 
-def training_pairs_codes(seed: int, n_pairs: int) -> tuple[np.ndarray, np.ndarray]:
+def training_pairs_codes(seed: int, n_pairs: int, long_share: float = 0.0,
+                         long_max: int = 16) -> tuple[np.ndarray, np.ndarray]:
     """n_pairs seeded pairs as interleaved codes [2n, 32] / lengths [2n] (rows 2i and 2i+1 are
     one pair): the first half near neighbours made by :func:`mutate_codes`, the second half two
     independent CDR3-like junctions."""
@@ -476,7 +482,7 @@ def training_pairs_codes(seed: int, n_pairs: int) -> tuple[np.ndarray, np.ndarra
     a, la = cdr3_codes(seed * 2 + 1, n_pairs)
     near = n_pairs // 2
     b, lb = cdr3_codes(seed * 2 + 2, n_pairs)
-    b[:near], lb[:near] = mutate_codes(a[:near], la[:near], rng)
+    b[:near], lb[:near] = mutate_codes(a[:near], la[:near], rng, long_share, long_max)
     codes = np.empty((2 * n_pairs, PAD), np.uint8)
     lens = np.empty(2 * n_pairs, np.int32)
     codes[0::2], codes[1::2] = a, b
@@ -541,18 +547,20 @@ def mine_partners(codes: np.ndarray, lens: np.ndarray, rows: np.ndarray, *, seed
 
 def train(enc: Encoder, n_pairs: int, *, seed: int, matrix, gap_open: int, gap_extend: int = 1,
           batch_pairs: int = 2048, lr: float = 2e-3, lr_final: float = 1e-4,
-          chunk_pairs: int = 1 << 20, mine: int = 0, log=None) -> list[float]:
+          chunk_pairs: int = 1 << 20, mine: int = 0, long_share: float = 0.0,
+          long_max: int = 16, log=None) -> list[float]:
     """Trains ``enc`` for one pass over ``n_pairs`` fresh seeded pairs labelled by the exact
     kernel (Adam, cosine learning-rate decay from ``lr`` to ``lr_final``).  Half the pairs are
-    near neighbours (:func:`mutate_codes`); the other half are random pairs, each the best of
-    ``mine`` random partners when ``mine`` > 0 (:func:`mine_partners`).  Returns the mean loss
-    of every chunk."""
+    near neighbours (:func:`mutate_codes`, ``long_share`` of them with an indel block of
+    4..``long_max`` residues); the other half are random pairs, each the best of ``mine``
+    random partners when ``mine`` > 0 (:func:`mine_partners`).  Returns the mean loss of every
+    chunk."""
     steps = max(1, -(-n_pairs // batch_pairs))
     t, losses = 0, []
     for c0 in range(0, n_pairs, chunk_pairs):
         m = min(chunk_pairs, n_pairs - c0)
         cseed = seed * 7919 + c0 // chunk_pairs
-        codes, lens = training_pairs_codes(cseed, m)
+        codes, lens = training_pairs_codes(cseed, m, long_share, long_max)
         if mine:
             mine_partners(codes, lens, np.arange(m // 2, m), seed=cseed * 31 + 5, tries=mine,
                           matrix=matrix, gap_open=gap_open, gap_extend=gap_extend)

@@ -250,3 +250,18 @@ def test_recall_allocation_prefers_cheap_proposals_and_falls_back_where_they_are
     cheap = dict(costs, candidate=0.0)
     level, qf, rf, rec, _ = allocate_recall(E, FL, CL, wq, wr, cheap, 0.95)
     assert qf == [] and rf == [] and rec >= 0.95 and (level[E > 0] >= 0).all()
+
+
+def test_long_indel_share_of_near_neighbour_pairs():
+    """training_pairs_codes: the default pairs are unchanged by the long-block option, and with
+    long_share > 0 that share of the near-neighbour pairs differs in length by 4..long_max
+    residues (insertions capped at 32 residues)."""
+    from seqtree_b200 import learned as L
+    c0, l0 = L.training_pairs_codes(11, 4000)
+    c1, l1 = L.training_pairs_codes(11, 4000, 0.0)
+    assert np.array_equal(c0, c1) and np.array_equal(l0, l1)
+    c, ln = L.training_pairs_codes(11, 20000, 0.5, 12)
+    d = np.abs(ln[0::2] - ln[1::2])[:10000]  # the near-neighbour half
+    assert d.max() == 12 and 0.3 < np.mean(d >= 4) < 0.55
+    assert ln.min() >= 1 and ln.max() <= 32
+    assert ((c[np.arange(32)[None, :] >= ln[:, None]]) == 0).all()
