@@ -37,6 +37,7 @@
 #include <cstdlib>
 #include <map>
 #include <numeric>
+#include <type_traits>
 
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -307,34 +308,44 @@ __device__ __forceinline__ void run_unit(const FastArgs& a, const uint8_t* smem,
             Cb[q] = a.bias2;
             best[q] = first;
         }
-        auto step = [&](int j, uint32_t pr) {
-            const uint32_t a0 = base0 + uint32_t(j * kRowB) + rows0[j * 32];
-            const uint32_t ad = based + uint32_t(j * kRowB) + rowsd[j * 32];
+        // The sweep, in two versions: when the query is the longer one (dr == 0) both diagonals
+        // read residue j of the ref, so one byte load serves both addresses.
+        auto sweep = [&](auto same_residue) {
+            constexpr bool kSame = decltype(same_residue)::value;
+            auto step = [&](int j, uint32_t pr) {
+                const uint32_t c0 = rows0[j * 32];
+                const uint32_t a0 = base0 + uint32_t(j * kRowB) + c0;
+                const uint32_t ad = based + uint32_t(j * kRowB) + (kSame ? c0 : uint32_t(rowsd[j * 32]));
 #pragma unroll
-            for (int q = 0; q < kPairsPerSlice; ++q) {
-                const uint32_t p0v = *reinterpret_cast<const uint32_t*>(smem + a0 + q * kPairB);
-                const uint32_t pdv = *reinterpret_cast<const uint32_t*>(smem + ad + q * kPairB);
-                S[q] += pdv;
-                Cb[q] = Cb[q] + p0v - pdv;  // per-half exact: halves stay in [0, 2^15)
-                best[q] = __viaddmin_s16x2(Cb[q], pr, best[q]);
-            }
-        };
-        // The prior values of the next group of four positions are requested one group ahead,
-        // so their load latency hides behind the current group's lookups.
-        int j = 0;
-        uint4 pnext = make_uint4(0u, 0u, 0u, 0u);
-        if constexpr (PRIOR)
-            if (L >= 4) pnext = __ldg(reinterpret_cast<const uint4*>(prow + 4));
-        for (; j + 4 <= L; j += 4) {
-            const uint4 pv = pnext;
+                for (int q = 0; q < kPairsPerSlice; ++q) {
+                    const uint32_t p0v = *reinterpret_cast<const uint32_t*>(smem + a0 + q * kPairB);
+                    const uint32_t pdv = *reinterpret_cast<const uint32_t*>(smem + ad + q * kPairB);
+                    S[q] += pdv;
+                    Cb[q] = Cb[q] + p0v - pdv;  // per-half exact: halves stay in [0, 2^15)
+                    best[q] = __viaddmin_s16x2(Cb[q], pr, best[q]);
+                }
+            };
+            // The prior values of the next group of four positions are requested one group
+            // ahead, so their load latency hides behind the current group's lookups.
+            int j = 0;
+            uint4 pnext = make_uint4(0u, 0u, 0u, 0u);
             if constexpr (PRIOR)
-                if (j + 8 <= L) pnext = __ldg(reinterpret_cast<const uint4*>(prow + j + 8));
-            step(j, pv.x);
-            step(j + 1, pv.y);
-            step(j + 2, pv.z);
-            step(j + 3, pv.w);
-        }
-        for (; j < L; ++j) step(j, PRIOR ? __ldg(prow + j + 4) : 0u);
+                if (L >= 4) pnext = __ldg(reinterpret_cast<const uint4*>(prow + 4));
+            for (; j + 4 <= L; j += 4) {
+                const uint4 pv = pnext;
+                if constexpr (PRIOR)
+                    if (j + 8 <= L) pnext = __ldg(reinterpret_cast<const uint4*>(prow + j + 8));
+                step(j, pv.x);
+                step(j + 1, pv.y);
+                step(j + 2, pv.z);
+                step(j + 3, pv.w);
+            }
+            for (; j < L; ++j) step(j, PRIOR ? __ldg(prow + j + 4) : 0u);
+        };
+        if (dr == 0)
+            sweep(std::true_type{});
+        else
+            sweep(std::false_type{});
 #pragma unroll
         for (int q = 0; q < kPairsPerSlice; ++q) res[q] = S[q] + best[q] - a.bias2;
     }
