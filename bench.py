@@ -728,7 +728,11 @@ def measure(args, name, world, rank, local, int_peaks, soak_s: float = 0.0):
     }
     if soak is not None:
         line["soak"] = soak
-        if not clocks and soak.get("clocks"):  # a timed region of ~1 ms gets no 200 ms sample
+        # a timed region of ~1 ms gets at most one 200 ms sample: the soak's record (the same
+        # step replayed for over a second right after it) stands in, the timed one kept beside
+        if (not clocks or clocks.get("samples", 0) < 3) and soak.get("clocks"):
+            if clocks:
+                line["clocks_timed_region"] = clocks
             line["clocks"] = dict(soak["clocks"], source="soak: back-to-back replays of the "
                                                          "timed step, right after it")
     if w["kind"] == "sparse":
