@@ -57,7 +57,7 @@ L2_NOTE = ("GPU arm: L2 flushed between timed steps (256 MiB write); CPU referen
 # DRAM bytes (read + write) per launch of the dominant kernel on the named workload, from the ncu
 # captures summarised in profiles/ (None until captured).
 TRAFFIC: dict[str, float | None] = {
-    "gapblock": 1.91e6,     # 1.89 MB read + 0.02 MB write (the result stays in L2)
+    "gapblock": 1.92e6,     # 1.88 MB read + 0.03 MB write (the result stays in L2)
     "hamming": 1.31e9,      # 262 MB per 4,000 rows, scaled to 20,000 rows
     "levenshtein": 1.03e9,  # 102.5 MB per 2,000 rows, scaled to 20,000 rows
     "align": 1.05e6,        # one row-bucket launch of the wavefront kernel
