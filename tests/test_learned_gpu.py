@@ -216,6 +216,18 @@ def test_learned_search_is_exact_and_training_pays(cuda_ready):
           "eval recall", bev["recall"])
     assert bev["subset_of_exact"] and bev["recall"] >= 0.99
     assert cal["exhaustive_share"] < bcal["exhaustive_share"]
+    # The threshold form with the same trained encoder, calibrated to the same bound on the same
+    # batch: exact hits, the bound met on the batch, and no more pairs scored exhaustively than
+    # without the network (held-out recall is looser at this size: a cell holds few hits).
+    thr = L.LearnedIndex(enc, rc, rl, matrix=M, gap_open=8, max_penalty=24, proposal="range")
+    tcal = thr.calibrate(cc, cl, bound=0.99)
+    tev = thr.recall(ec, el)
+    print("threshold form:", tcal["query_fallback"], tcal["ref_fallback"],
+          f"share {tcal['exhaustive_share']:.3f}", "cells", tcal["cells_with_proposals"],
+          "eval recall", tev["recall"])
+    assert tcal["subset_of_exact"] and tcal["recall"] >= 0.99
+    assert tev["subset_of_exact"] and tev["recall"] >= 0.98
+    assert tcal["exhaustive_share"] <= bcal["exhaustive_share"]
 
 
 @pytest.mark.gpu
