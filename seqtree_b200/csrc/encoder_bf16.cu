@@ -465,6 +465,18 @@ __global__ void __launch_bounds__(kGemmThreads, 1) attn_layer_kernel(const __gri
             __syncwarp();
             if (lane == 0) bar_arrive(BAR(b));
         };
+        // A phase's two 32-column groups (this warp's columns half * 64 .. + 63 from `base`):
+        // both TMEM loads in flight together, then each group handed to use(y, c0).
+        auto two_groups = [&](uint32_t base, auto&& use) {
+            uint32_t y0[32], y1[32];
+            __syncwarp();
+            tmem_ld32_issue(base + uint32_t(half * 64), y0);
+            tmem_ld32_issue(base + uint32_t(half * 64 + 32), y1);
+            tmem_ld32_wait(y0);
+            use(y0, half * 64);
+            tmem_ld32_wait(y1);
+            use(y1, half * 64 + 32);
+        };
         for (int64_t tile = blockIdx.x; tile < g.tiles; tile += gridDim.x) {
             const int L = g.lens[tile * kSeqPerTile + quarter];
             const bool valid = lane < L;
@@ -474,12 +486,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) attn_layer_kernel(const __gri
 #pragma unroll 1
             for (int part = 0; part < 2; ++part) {  // 0: q -> X, 1: k -> Y
                 uint8_t* dst = part ? Y : X;
-#pragma unroll 1
-                for (int gi = 0; gi < 2; ++gi) {
-                    const int c0 = half * 64 + gi * 32;
-                    uint32_t y[32];
-                    __syncwarp();
-                    tmem_ld32(tl + uint32_t(part * 128 + c0), y);
+                two_groups(tl + uint32_t(part * 128), [&](const uint32_t (&y)[32], int c0) {
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         float v[8];
@@ -488,7 +495,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) attn_layer_kernel(const __gri
                             v[e] = __uint_as_float(y[u * 8 + e]) + g.bqkv[part * 128 + c0 + u * 8 + e];
                         put_unit(dst, r, (c0 >> 3) + u, v);
                     }
-                }
+                });
             }
             handoff(4);
             // ---- softmax rows -> P (X); v transposed -> Y
@@ -525,12 +532,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) attn_layer_kernel(const __gri
                     put_unit(X, r, col >> 3, v);
                 }
             }
-#pragma unroll 1
-            for (int gi = 0; gi < 2; ++gi) {
-                const int c0 = half * 64 + gi * 32;  // value dimensions d
-                uint32_t y[32];
-                __syncwarp();
-                tmem_ld32(tl + 256u + uint32_t(c0), y);
+            two_groups(tl + 256u, [&](const uint32_t (&y)[32], int c0) {  // value dimensions d
                 // V^T as a K-major operand: row d, column (k) = this thread's row r
                 const int kc = r >> 6, k8 = (r & 63) >> 3, ke = r & 7;
 #pragma unroll
@@ -540,17 +542,12 @@ __global__ void __launch_bounds__(kGemmThreads, 1) attn_layer_kernel(const __gri
                     *reinterpret_cast<__nv_bfloat16*>(Y + kc * 16384 + d * 128 + ((k8 ^ (d & 7)) << 4) +
                                                       ke * 2) = __float2bfloat16_rn(v);
                 }
-            }
+            });
             handoff(6);
             // ---- O -> X
             if (!bar_wait_own(BAR(7), ph, g.err)) break;
             tc_fence_after();
-#pragma unroll 1
-            for (int gi = 0; gi < 2; ++gi) {
-                const int c0 = half * 64 + gi * 32;
-                uint32_t y[32];
-                __syncwarp();
-                tmem_ld32(tl + 384u + uint32_t(c0), y);
+            two_groups(tl + 384u, [&](const uint32_t (&y)[32], int c0) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     float v[8];
@@ -558,17 +555,12 @@ __global__ void __launch_bounds__(kGemmThreads, 1) attn_layer_kernel(const __gri
                     for (int e = 0; e < 8; ++e) v[e] = __uint_as_float(y[u * 8 + e]);
                     put_unit(X, r, (c0 >> 3) + u, v);
                 }
-            }
+            });
             handoff(8);
             // ---- h' = h + O Wo + bo (masked) -> staging Y -> bulk store
             if (!bar_wait_own(BAR(9), ph, g.err)) break;
             tc_fence_after();
-#pragma unroll 1
-            for (int gi = 0; gi < 2; ++gi) {
-                const int c0 = half * 64 + gi * 32;
-                uint32_t y[32];
-                __syncwarp();
-                tmem_ld32(tl + uint32_t(c0), y);
+            two_groups(tl, [&](const uint32_t (&y)[32], int c0) {
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const int uu = (c0 >> 3) + u;
@@ -584,7 +576,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1) attn_layer_kernel(const __gri
                     }
                     put_unit(Y, r, uu, v);
                 }
-            }
+            });
             tc_fence_before();
             fence_async_smem();
             __syncwarp();
