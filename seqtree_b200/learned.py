@@ -1000,14 +1000,6 @@ class LearnedIndex:
             return z, z, z
         return torch.cat(out_q), torch.cat(out_r), torch.cat(out_s)
 
-    def _range_pairs(self, qb: QueryBatch, q_emb):
-        """The threshold form's raw proposals of the batch's learned rows (local query and
-        learned-ref indices), all at once."""
-        n = len(qb.learn_set)
-        cap = max(int(self._range_per_query * n * 1.1) + 1, 16 * n)
-        return propose_range(q_emb, qb.learn_lens_t, self.r_emb, self.learn_lens_t,
-                             self.thresholds, cap, qb.range_tiles(self))
-
     def search_strings(self, queries) -> "SparseScores":
         """The public call: thresholded hits of host query strings against the index's refs, as
         host CSR (``gapblock.SparseScores``, the format of ``score_sparse``).  The strings are
