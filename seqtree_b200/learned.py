@@ -1237,7 +1237,11 @@ class LearnedIndex:
         wq1, wr1 = wq / max(wq.sum(), 1.0), wr / max(wr.sum(), 1.0)
         share = float(wq1[q_fb].sum() + (1.0 - wq1[q_fb].sum()) * wr1[r_fb].sum())
         return {"ref_fallback": r_fb, "query_fallback": q_fb,
-                "recall_no_fallback": float(FL[:, :, LV - 1].sum() / te) if te else 1.0,
+                # share of the batch's exact hits that the chosen proposals find (the rest of
+                # the recall comes from the exhaustively scored lengths)
+                "recall_from_proposals": float(np.take_along_axis(
+                    FL, idx[:, :, None], 2)[:, :, 0][(level >= 0) & ~covered].sum() / te)
+                if te else 0.0,
                 "recall_estimate": float(est_rec),
                 "recall": r2["recall"], "found": r2["found"], "exact": r2["exact"],
                 "subset_of_exact": r2["subset_of_exact"], "exhaustive_share": share,
