@@ -676,17 +676,23 @@ def _subset(codes, lens, rows):
     return SeqSet(codes_to_packed(codes[rows], lens[rows]), "aa") if rows.size else None
 
 
-def _packed_subset(packed: _lib.Packed, lens: np.ndarray, rows: np.ndarray):
+def gather_rows(data: np.ndarray, offsets: np.ndarray, rows: np.ndarray):
+    """(bytes, offsets) of the listed rows of a packed string set, in the listed order."""
+    rows = np.asarray(rows, np.int64)
+    sl = (offsets[rows + 1] - offsets[rows]).astype(np.int64)
+    off = np.zeros(rows.size + 1, np.int64)
+    np.cumsum(sl, out=off[1:])
+    src = np.repeat(offsets[rows] - off[:-1], sl) + np.arange(off[-1], dtype=np.int64)
+    return data[src], off
+
+
+def _packed_subset(packed: _lib.Packed, rows: np.ndarray):
     """The listed rows of a packed string set as a device set (letters gathered on the host and
     encoded on the device, so an invalid symbol raises the alphabet's ValueError)."""
     from .device import SeqSet
     if not rows.size:
         return None
-    sl = lens[rows].astype(np.int64)
-    off = np.zeros(rows.size + 1, np.int64)
-    np.cumsum(sl, out=off[1:])
-    src = np.repeat(packed.offsets[rows] - off[:-1], sl) + np.arange(off[-1], dtype=np.int64)
-    return SeqSet(_lib.Packed.from_arrays(packed.data[src], off), "aa")
+    return SeqSet(_lib.Packed.from_arrays(*gather_rows(packed.data, packed.offsets, rows)), "aa")
 
 
 class QueryBatch:
@@ -708,8 +714,8 @@ class QueryBatch:
         # lengths (its ref band is then narrow)
         self.learn_rows = learn[np.argsort(self.lens[learn], kind="stable")]
         if codes is None:
-            self.fb_set = _packed_subset(packed, self.lens, self.fb_rows)
-            self.learn_set = _packed_subset(packed, self.lens, self.learn_rows)
+            self.fb_set = _packed_subset(packed, self.fb_rows)
+            self.learn_set = _packed_subset(packed, self.learn_rows)
         else:
             self.fb_set = _subset(codes, self.lens, self.fb_rows)
             self.learn_set = _subset(codes, self.lens, self.learn_rows)

@@ -265,3 +265,16 @@ def test_long_indel_share_of_near_neighbour_pairs():
     assert d.max() == 12 and 0.3 < np.mean(d >= 4) < 0.55
     assert ln.min() >= 1 and ln.max() <= 32
     assert ((c[np.arange(32)[None, :] >= ln[:, None]]) == 0).all()
+
+
+def test_gather_rows_of_a_packed_set():
+    """learned.gather_rows: the listed rows' bytes and offsets, in the listed order (empty rows and
+    repeats included), as concatenating the strings would give."""
+    from seqtree_b200.learned import gather_rows
+    seqs = ["CASSLF", "", "CAW", "CASSPGQAYEQYF", "A"]
+    p = _lib.Packed(seqs)
+    for rows in ([4, 0, 3], [1, 1, 2], [], list(range(5))[::-1]):
+        data, off = gather_rows(p.data, p.offsets, np.array(rows, np.int64))
+        want = [seqs[i] for i in rows]
+        assert off.tolist() == np.concatenate([[0], np.cumsum([len(x) for x in want])]).tolist()
+        assert bytes(data) == "".join(want).encode()
