@@ -677,8 +677,13 @@ def _subset(codes, lens, rows):
 
 
 def gather_rows(data: np.ndarray, offsets: np.ndarray, rows: np.ndarray):
-    """(bytes, offsets) of the listed rows of a packed string set, in the listed order."""
-    rows = np.asarray(rows, np.int64)
+    """(bytes, offsets) of the listed rows of a packed string set, in the listed order (one copy
+    per row in the ``_pack`` extension when it is built)."""
+    rows = np.ascontiguousarray(rows, np.int64)
+    if _lib._pack is not None:
+        d, o = _lib._pack.gather(np.ascontiguousarray(data, np.uint8),
+                                 np.ascontiguousarray(offsets, np.int64), rows)
+        return np.frombuffer(d, np.uint8), np.frombuffer(o, np.int64)
     sl = (offsets[rows + 1] - offsets[rows]).astype(np.int64)
     off = np.zeros(rows.size + 1, np.int64)
     np.cumsum(sl, out=off[1:])
@@ -712,7 +717,9 @@ class QueryBatch:
         learn = np.flatnonzero(~fb).astype(np.int64)
         # learn rows in length order, so that a 256-query tile of the proposal kernel spans few
         # lengths (its ref band is then narrow)
-        self.learn_rows = learn[np.argsort(self.lens[learn], kind="stable")]
+        # (lengths are 1..32: as uint8 the stable sort is numpy's radix sort)
+        self.learn_rows = learn[np.argsort(np.clip(self.lens[learn], 0, 255).astype(np.uint8),
+                                           kind="stable")]
         if codes is None:
             self.fb_set = _packed_subset(packed, self.fb_rows)
             self.learn_set = _packed_subset(packed, self.learn_rows)
@@ -846,7 +853,8 @@ class LearnedIndex:
         import torch
         fb = self.ref_fallback[np.clip(self.ref_lens, 0, PAD)]
         learn = np.flatnonzero(~fb).astype(np.int64)
-        learn = learn[np.argsort(self.ref_lens[learn], kind="stable")]  # by length, then id
+        learn = learn[np.argsort(np.clip(self.ref_lens[learn], 0, 255).astype(np.uint8),
+                                 kind="stable")]  # by length, then id
         fbr = np.flatnonzero(fb).astype(np.int64)
         self.learn_lens = self.ref_lens[learn]
         self.learn_lens_t = torch.from_numpy(

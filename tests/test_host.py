@@ -273,8 +273,18 @@ def test_gather_rows_of_a_packed_set():
     from seqtree_b200.learned import gather_rows
     seqs = ["CASSLF", "", "CAW", "CASSPGQAYEQYF", "A"]
     p = _lib.Packed(seqs)
-    for rows in ([4, 0, 3], [1, 1, 2], [], list(range(5))[::-1]):
-        data, off = gather_rows(p.data, p.offsets, np.array(rows, np.int64))
-        want = [seqs[i] for i in rows]
-        assert off.tolist() == np.concatenate([[0], np.cumsum([len(x) for x in want])]).tolist()
-        assert bytes(data) == "".join(want).encode()
+    from seqtree_b200 import _lib as lib
+    ext = lib._pack
+    try:
+        for use_ext in (True, False):  # the extension's copy and the numpy fallback
+            lib._pack = ext if use_ext else None
+            for rows in ([4, 0, 3], [1, 1, 2], [], list(range(5))[::-1]):
+                data, off = gather_rows(p.data, p.offsets, np.array(rows, np.int64))
+                want = [seqs[i] for i in rows]
+                assert off.tolist() == np.concatenate(
+                    [[0], np.cumsum([len(x) for x in want])]).tolist()
+                assert bytes(data[:off[-1]]) == "".join(want).encode()
+    finally:
+        lib._pack = ext
+    with pytest.raises(IndexError):
+        gather_rows(p.data, p.offsets, np.array([5], np.int64))
