@@ -134,3 +134,19 @@ def test_reference_arm_does_not_load_the_library():
                          timeout=300, cwd=str(ROOT))
     assert res.returncode == 0, res.stdout + res.stderr
     assert "clean" in res.stdout
+
+
+def test_learned_fallback_cells(bench):
+    """fallback_cells: the pairs and gap-block cells the learned search scores exhaustively --
+    fallback-length queries against every ref, the other queries against fallback-length refs."""
+    q = [8, 8, 12, 15]
+    r = [8, 10, 12]
+    pairs, cells = bench.fallback_cells(q, r, [8], [10])
+    want_pairs = want_cells = 0.0
+    for a in q:
+        for b in r:
+            if a == 8 or b == 10:
+                want_pairs += 1
+                want_cells += min(a, b) * (1 if a == b else 2)
+    assert pairs == want_pairs and cells == want_cells
+    assert bench.fallback_cells(q, r, [], []) == (0.0, 0.0)
